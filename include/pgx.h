@@ -1,0 +1,187 @@
+/*
+ * pgx.h — C ABI of the B200-native GeMSLR-FGMRES solve phase.
+ *
+ * The library takes over the SOLVE phase of the reference ParGeMSLR
+ * (Hitenze/pargemslr): FlexGmresClass::Solve driven by the GeMSLR multilevel
+ * preconditioner (GemslrClass::Solve / SolveLevel / SolveB /
+ * SolveApplyLowRankLevel and the level-0 Schur-complement inner FGMRES).
+ * The reference's SETUP phase (partitioning, ILUT, low-rank bases) produces
+ * the structures that the pgx_gemslr_* calls below import; from then on every
+ * solve runs on one GPU with hand-written sm_100a kernels.
+ *
+ * Conventions
+ *   - Every call returns an int status: 0 on success, otherwise one of the
+ *     PGX_ERROR_* codes.  The values 100-107 are the reference's own error
+ *     codes (ParGeMSLR INC/pargemslr.hpp:9-21); 200+ are GPU-side codes.
+ *     pgx_last_error() gives a message for the calling thread's last failure.
+ *   - Matrices are CSR with 32-bit row pointers and column indices
+ *     (the reference's CsrMatrixClass layout, SRC/matrices/csr_matrix.hpp:27)
+ *     and FP64 values.  Dense matrices are column-major with leading
+ *     dimension = rows (DenseMatrixClass, SRC/matrices/dense_matrix.cpp:114).
+ *   - Import calls COPY their inputs; the handle owns its device copies,
+ *     like the hypre plugin's matrix import
+ *     (TESTS/hypre/pargemslr_hypre_interface.cpp:119-129).
+ *   - Solve calls BORROW x and b (host or device pointers, see `location`),
+ *     like hypre_PargemslrParallelGEMSLRDSolve (…interface.cpp:344-369).
+ *   - A handle is used by one host thread at a time; distinct handles may be
+ *     used concurrently (each owns its own CUDA stream).
+ */
+#ifndef PGX_H
+#define PGX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PGX_SUCCESS                0
+#define PGX_ERROR_INVALID_OPTION   100 /* PARGEMSLR_ERROR_INVALED_OPTION */
+#define PGX_ERROR_INVALID_PARAM    101 /* PARGEMSLR_ERROR_INVALED_PARAM */
+#define PGX_ERROR_IO               102 /* PARGEMSLR_ERROR_IO_ERROR */
+#define PGX_ERROR_ILU_EMPTY_ROW    103 /* PARGEMSLR_ERROR_ILU_EMPTY_ROW */
+#define PGX_ERROR_DOUBLE_INIT_FREE 104 /* PARGEMSLR_ERROR_DOUBLE_INIT_FREE */
+#define PGX_ERROR_FUNCTION_CALL    106 /* PARGEMSLR_ERROR_FUNCTION_CALL_ERR */
+#define PGX_ERROR_MEMORY_LOCATION  107 /* PARGEMSLR_ERROR_MEMORY_LOCATION */
+#define PGX_ERROR_CUDA             200 /* a CUDA runtime call failed */
+#define PGX_ERROR_OOM              201 /* device memory could not be reserved */
+#define PGX_ERROR_TIMEOUT          202 /* a bounded device-side wait expired */
+#define PGX_ERROR_NOT_FINITE       203 /* NaN/Inf met in the right-hand side or iterate */
+#define PGX_ERROR_NO_DEVICE        204 /* no usable CUDA device */
+
+/* ---- precision of the preconditioner apply -------------------------------
+ * PGX_PRECISION_FP64: everything in FP64 (the reference's arithmetic).
+ * PGX_PRECISION_MIXED: factors, coupling blocks, low-rank bases and the
+ *   whole preconditioner apply (including the level-0 inner FGMRES) stored
+ *   and accumulated in FP32; the outer FGMRES (residual SpMV, Arnoldi
+ *   orthogonalisation, Givens rotations, least squares, true residual)
+ *   stays FP64. */
+#define PGX_PRECISION_FP64  0
+#define PGX_PRECISION_MIXED 1
+
+/* ---- memory location of borrowed vectors (reference kMemoryHost/Device) */
+#define PGX_LOCATION_HOST   0
+#define PGX_LOCATION_DEVICE 1
+
+typedef struct pgx_gemslr_s *pgx_handle;
+
+/* A CSR matrix view: rows x cols, nnz entries.  rowptr has rows+1 entries
+ * (rowptr[0] == 0); colidx/values have nnz entries.  An absent matrix is
+ * {0, 0, 0, NULL, NULL, NULL}. */
+typedef struct {
+   int32_t rows;
+   int32_t cols;
+   int64_t nnz;
+   const int32_t *rowptr;
+   const int32_t *colidx;
+   const double *values;
+} pgx_csr;
+
+/* One level l of the GeMSLR hierarchy after setup, in the permuted ordering
+ * (rows lev_ptr[l] .. lev_ptr[l+1]-1 of P A P^T form the block-diagonal B_l).
+ *   ncomp, dom_ptr: subdomains of the level, dom_ptr[0..ncomp] relative to
+ *       the level start (GemslrClass::_dom_ptr_v2, gemslr.hpp:1630).
+ *   L, U, dinv: the level's ILU factors with all subdomains concatenated
+ *       block-diagonally, column indices relative to the level start.
+ *       L strictly lower (unit diagonal implied), U strictly upper, dinv the
+ *       INVERSE diagonal (IluClass::_L/_U/_D, ilu.cpp:3677-3790).
+ *   B:  the unfactored block-diagonal B_l (GemslrLevelClass::_B_mat_v), used
+ *       by the Schur-complement operator of the level-0 inner solve.
+ *   E, F: coupling blocks, E is m_l x n_l, F is n_l x m_l with
+ *       m_l = n - lev_ptr[l+1] (GemslrLevelClass::_E_mat/_F_mat).  Absent on
+ *       the last level.
+ *   rank, W, WH: low-rank correction, W and WH are m_l x rank column-major,
+ *       WH = W ((I - H)^-1 - I) (GemslrLevelClass::_Wk/_WHk, applied by
+ *       SolveApplyLowRankLevel, gemslr.cpp:3681-3722).  rank 0: none. */
+typedef struct {
+   int32_t ncomp;
+   const int32_t *dom_ptr;
+   pgx_csr L;
+   pgx_csr U;
+   const double *dinv;
+   pgx_csr B;
+   pgx_csr E;
+   pgx_csr F;
+   int32_t rank;
+   const double *W;
+   const double *WH;
+} pgx_level;
+
+/* Per-solve outcome. */
+typedef struct {
+   int32_t status;        /* PGX_SUCCESS or an error code */
+   int32_t iters;         /* FlexGmresClass::GetNumberIterations */
+   double rel_res;        /* FlexGmresClass::GetFinalRelativeResidual: the
+                             Givens estimate |rs|/||b|| (fgmres.hpp:542) */
+   double true_rel_res;   /* ||b - A x||_2 / ||b||_2 computed in FP64 on the GPU */
+   double solve_ms;       /* device time of the solve (CUDA events) */
+} pgx_result;
+
+/* ---- library ----------------------------------------------------------- */
+
+/* Select the CUDA device for handles created afterwards by this thread
+ * (replaces the device part of PargemslrInit, SRC/utils/parallel.cpp:304). */
+int pgx_init(int device);
+/* Release library-wide state (PargemslrFinalize, parallel.cpp:554). */
+int pgx_finalize(void);
+/* Message describing the calling thread's most recent error. */
+const char *pgx_last_error(void);
+/* Library version as major*10000 + minor*100 + patch. */
+int pgx_version(void);
+
+/* ---- GeMSLR solve handle (replaces GemslrClass + FlexGmresClass solve) ---
+ *
+ * Import sequence, mirroring what GemslrClass::Setup leaves behind
+ * (gemslr.cpp:1602-1711):
+ *   pgx_gemslr_create      n, precision
+ *   pgx_gemslr_set_matrix  A (the unpermuted system matrix, FlexGmres's A)
+ *   pgx_gemslr_set_perm    pperm (and qperm for unsymmetric reorderings)
+ *   pgx_gemslr_set_levels  nlev, lev_ptr[nlev+1]
+ *   pgx_gemslr_set_level   once per level
+ *   pgx_gemslr_set_inner   the level-0 Schur FGMRES settings
+ *   pgx_gemslr_commit      build schedules, upload, allocate work space
+ */
+int pgx_gemslr_create(pgx_handle *handle, int32_t n, int32_t precision);
+int pgx_gemslr_set_matrix(pgx_handle handle, const pgx_csr *A);
+int pgx_gemslr_set_perm(pgx_handle handle, const int32_t *pperm, const int32_t *qperm);
+int pgx_gemslr_set_levels(pgx_handle handle, int32_t nlev, const int32_t *lev_ptr);
+int pgx_gemslr_set_level(pgx_handle handle, int32_t level, const pgx_level *desc);
+int pgx_gemslr_set_inner(pgx_handle handle, int32_t enable, int32_t maxits, double tol);
+int pgx_gemslr_commit(pgx_handle handle);
+int pgx_gemslr_destroy(pgx_handle handle);
+
+/* Bytes of device memory the committed handle holds (factors, matrices,
+ * Krylov basis for kdim, work vectors); used for admission control. */
+int pgx_gemslr_device_bytes(pgx_handle handle, int32_t kdim, int64_t *bytes);
+
+/* FGMRES(kdim) solve of A x = b right-preconditioned by GeMSLR
+ * (FlexGmresClass::Solve, fgmres.hpp:263-558).  params is the reference's
+ * double[180] parameter array (PARGEMSLR_IO_*, utils.hpp:77-297) from which
+ * SOLVER_KDIM (11), SOLVER_MAXITS (12), SOLVER_TOL (13) and SOLVER_ATOL (14)
+ * are read; NULL keeps kdim 50, maxits 100, tol 1e-6 relative.  x holds the
+ * initial guess on entry and the solution on return. */
+int pgx_gemslr_solve(pgx_handle handle, double *x, const double *b, int32_t location,
+                     const double *params, pgx_result *result);
+
+/* Apply the preconditioner once, z = M^-1 v (GemslrClass::Solve,
+ * gemslr.cpp:3431-3472), on host or device vectors. */
+int pgx_gemslr_precond_apply(pgx_handle handle, double *z, const double *v, int32_t location);
+
+/* ---- building blocks (each is also used inside the solve) ---------------
+ * The level-set schedule of a unit-lower (uplo 'L') or upper (uplo 'U')
+ * triangular CSR factor, by the rule of IluClass::BuildLevels
+ * (ilu.cpp:832-1062): level(i) = 1 + max level over the row's dependencies,
+ * rows ordered by level then by index.  level_ptr needs n+1 entries,
+ * order n entries; *nlevels receives the number of levels. */
+int pgx_build_levels(char uplo, int32_t n, const int32_t *rowptr, const int32_t *colidx,
+                     int32_t *nlevels, int32_t *level_ptr, int32_t *order);
+
+/* y = alpha * A x + beta * y on device pointers (CSR SpMV kernel). */
+int pgx_csr_spmv_device(const pgx_csr *A_device, double alpha, const double *x, double beta, double *y);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PGX_H */

@@ -1,0 +1,140 @@
+"""ctypes binding of the C ABI declared in ``include/pgx.h``.
+
+The library is the in-tree ``pargemslr_b200/_lib/libpgx.so``.  There is no
+fallback: if the library cannot be loaded, :func:`lib` raises, so a missing or
+broken CUDA build fails loudly instead of silently computing elsewhere.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libpgx.so")
+
+SUCCESS = 0
+ERROR_INVALID_OPTION = 100
+ERROR_INVALID_PARAM = 101
+ERROR_IO = 102
+ERROR_FUNCTION_CALL = 106
+ERROR_MEMORY_LOCATION = 107
+ERROR_CUDA = 200
+ERROR_OOM = 201
+ERROR_TIMEOUT = 202
+ERROR_NOT_FINITE = 203
+ERROR_NO_DEVICE = 204
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+LOCATION_HOST = 0
+LOCATION_DEVICE = 1
+
+# every symbol include/pgx.h declares
+EXPORTS = (
+    "pgx_init", "pgx_finalize", "pgx_last_error", "pgx_version",
+    "pgx_gemslr_create", "pgx_gemslr_set_matrix", "pgx_gemslr_set_perm",
+    "pgx_gemslr_set_levels", "pgx_gemslr_set_level", "pgx_gemslr_set_inner",
+    "pgx_gemslr_commit", "pgx_gemslr_destroy", "pgx_gemslr_device_bytes",
+    "pgx_gemslr_solve", "pgx_gemslr_precond_apply", "pgx_build_levels",
+    "pgx_csr_spmv_device",
+)
+
+
+class PgxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"pgx error {code}: {msg}")
+        self.code = code
+
+
+class Csr(C.Structure):
+    _fields_ = [
+        ("rows", C.c_int32), ("cols", C.c_int32), ("nnz", C.c_int64),
+        ("rowptr", C.c_void_p), ("colidx", C.c_void_p), ("values", C.c_void_p),
+    ]
+
+
+class Level(C.Structure):
+    _fields_ = [
+        ("ncomp", C.c_int32), ("dom_ptr", C.c_void_p),
+        ("L", Csr), ("U", Csr), ("dinv", C.c_void_p), ("B", Csr), ("E", Csr), ("F", Csr),
+        ("rank", C.c_int32), ("W", C.c_void_p), ("WH", C.c_void_p),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32), ("iters", C.c_int32), ("rel_res", C.c_double),
+        ("true_rel_res", C.c_double), ("solve_ms", C.c_double),
+    ]
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Load libpgx.so (once).  Raises if it is missing: no CPU fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m pargemslr_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    L.pgx_init.argtypes = [C.c_int]
+    L.pgx_last_error.restype = C.c_char_p
+    L.pgx_gemslr_create.argtypes = [C.POINTER(vp), i32, i32]
+    L.pgx_gemslr_set_matrix.argtypes = [vp, C.POINTER(Csr)]
+    L.pgx_gemslr_set_perm.argtypes = [vp, vp, vp]
+    L.pgx_gemslr_set_levels.argtypes = [vp, i32, vp]
+    L.pgx_gemslr_set_level.argtypes = [vp, i32, C.POINTER(Level)]
+    L.pgx_gemslr_set_inner.argtypes = [vp, i32, i32, dbl]
+    L.pgx_gemslr_commit.argtypes = [vp]
+    L.pgx_gemslr_destroy.argtypes = [vp]
+    L.pgx_gemslr_device_bytes.argtypes = [vp, i32, C.POINTER(i64)]
+    L.pgx_gemslr_solve.argtypes = [vp, vp, vp, i32, vp, C.POINTER(Result)]
+    L.pgx_gemslr_precond_apply.argtypes = [vp, vp, vp, i32]
+    L.pgx_build_levels.argtypes = [C.c_char, i32, vp, vp, C.POINTER(i32), vp, vp]
+    L.pgx_csr_spmv_device.argtypes = [C.POINTER(Csr), dbl, vp, dbl, vp]
+    for name in EXPORTS:
+        if name != "pgx_last_error":
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != SUCCESS:
+        msg = lib().pgx_last_error()
+        raise PgxError(rc, msg.decode() if msg else "")
+
+
+def ptr(a: Optional[np.ndarray]) -> Optional[int]:
+    return None if a is None else a.ctypes.data
+
+
+def csr_struct(rp: Optional[np.ndarray], cj: Optional[np.ndarray], va: Optional[np.ndarray], rows: int,
+               cols: int, keep: list) -> Csr:
+    """A pgx_csr view over numpy arrays (kept alive through `keep`)."""
+    if rp is None or rows == 0:
+        return Csr(0, 0, 0, None, None, None)
+    rp = np.ascontiguousarray(rp, dtype=np.int32)
+    cj = np.ascontiguousarray(cj, dtype=np.int32)
+    va = np.ascontiguousarray(va, dtype=np.float64)
+    keep.extend([rp, cj, va])
+    return Csr(rows, cols, int(cj.size), ptr(rp), ptr(cj) if cj.size else None, ptr(va) if va.size else None)
+
+
+def build_levels(uplo: str, rp: np.ndarray, cj: np.ndarray):
+    """Level-set schedule of a triangular factor (pgx_build_levels)."""
+    n = rp.size - 1
+    rp = np.ascontiguousarray(rp, dtype=np.int32)
+    cj = np.ascontiguousarray(cj, dtype=np.int32)
+    nlev = C.c_int32(0)
+    lptr = np.zeros(n + 1, dtype=np.int32)
+    order = np.zeros(max(n, 1), dtype=np.int32)
+    check(lib().pgx_build_levels(uplo.encode(), n, ptr(rp), ptr(cj) if cj.size else None, C.byref(nlev),
+                                 ptr(lptr), ptr(order)))
+    return lptr[: nlev.value + 1].copy(), order[:n].copy()

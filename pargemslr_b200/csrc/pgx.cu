@@ -1,0 +1,1106 @@
+// pgx — B200-native solve phase of ParGeMSLR's GeMSLR-preconditioned FGMRES.
+//
+// Host side: import and validation of the post-setup GeMSLR structures,
+// level-set schedules, device layout, and the enqueue logic that mirrors the
+// reference's solve-phase call tree:
+//
+//   FlexGmresClass::Solve                 (ParGeMSLR SRC/solvers/fgmres.hpp:263-558)
+//     GemslrClass::Solve                  (SRC/preconditioners/gemslr.cpp:3431-3472)
+//       GemslrClass::SolveLevel           (gemslr.cpp:3474-3630)
+//         SolveB -> IluClass::SolveHost   (gemslr.cpp:3632-3678, ilu.cpp:3677-3790)
+//         E/F MatVec                      (gemslr.cpp:3551-3555, 3595-3599)
+//         SolveApplyLowRankLevel          (gemslr.cpp:3681-3722)
+//         level-0 inner FlexGmres over GemslrSchurMatrixClass
+//                                         (gemslr.cpp:282-330, 3566-3572, 3799-3960)
+//
+// All of it runs on one GPU; the host only enqueues kernels and reads the
+// FGMRES state word once per restart cycle.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstddef>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/pgx.h"
+#include "pgx_device.cuh"
+
+namespace pgx {
+
+// ------------------------------------------------------------ error state
+static thread_local std::string g_last_error;
+static thread_local int g_device = 0;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define PGX_CUDA(call)                                                                       \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? PGX_ERROR_OOM : PGX_ERROR_CUDA, "%s: %s", \
+                  #call, cudaGetErrorString(e_));                                            \
+  } while (0)
+
+#define PGX_TRY(expr)              \
+  do {                             \
+    int rc_ = (expr);              \
+    if (rc_ != PGX_SUCCESS) return rc_; \
+  } while (0)
+
+// ---------------------------------------------------------- host structures
+struct HostCsr {
+  int rows = 0, cols = 0;
+  std::vector<int> rp, cj;
+  std::vector<double> va;
+  long long nnz() const { return (long long)cj.size(); }
+  bool empty() const { return rows == 0; }
+};
+
+static int copy_csr(const pgx_csr* in, HostCsr& out, const char* what) {
+  out = HostCsr();
+  if (!in || in->rows == 0) return PGX_SUCCESS;
+  if (in->rows < 0 || in->cols < 0 || in->nnz < 0 || !in->rowptr)
+    return fail(PGX_ERROR_INVALID_PARAM, "%s: bad CSR header", what);
+  if (in->nnz > 0 && (!in->colidx || !in->values))
+    return fail(PGX_ERROR_INVALID_PARAM, "%s: missing CSR arrays", what);
+  if (in->nnz > INT32_MAX) return fail(PGX_ERROR_INVALID_PARAM, "%s: nnz exceeds 32-bit indices", what);
+  out.rows = in->rows;
+  out.cols = in->cols;
+  out.rp.assign(in->rowptr, in->rowptr + in->rows + 1);
+  out.cj.assign(in->colidx, in->colidx + in->nnz);
+  out.va.assign(in->values, in->values + in->nnz);
+  if (out.rp[0] != 0 || out.rp[in->rows] != in->nnz)
+    return fail(PGX_ERROR_INVALID_PARAM, "%s: row pointer does not span nnz", what);
+  for (int r = 0; r < out.rows; r++)
+    if (out.rp[r + 1] < out.rp[r]) return fail(PGX_ERROR_INVALID_PARAM, "%s: row pointer decreases", what);
+  for (long long k = 0; k < in->nnz; k++)
+    if (out.cj[k] < 0 || out.cj[k] >= out.cols)
+      return fail(PGX_ERROR_INVALID_PARAM, "%s: column index %d out of range", what, out.cj[k]);
+  return PGX_SUCCESS;
+}
+
+struct HostLevel {
+  bool set = false;
+  int ncomp = 0;
+  std::vector<int> dom_ptr;
+  HostCsr L, U, B, E, F;
+  std::vector<double> dinv, W, WH;
+  int rank = 0;
+};
+
+// ------------------------------------------- level sets (BuildLevels rule)
+// level(i) = 1 + max level of the entries row i depends on (0 if none);
+// rows ordered by level, then by index (IluClass::BuildLevels,
+// ParGeMSLR SRC/preconditioners/ilu.cpp:832-1062).  Lower factors are swept
+// from the first row, upper factors from the last.
+static int build_levels(bool upper, int n, const int* rp, const int* cj, std::vector<int>& level_ptr,
+                        std::vector<int>& order) {
+  std::vector<int> lev(n, -1);
+  int max_level = 0;
+  for (int t = 0; t < n; t++) {
+    int i = upper ? n - 1 - t : t;
+    int l = -1;
+    for (int k = rp[i]; k < rp[i + 1]; k++) {
+      int j = cj[k];
+      if (upper ? (j <= i) : (j >= i))
+        return fail(PGX_ERROR_INVALID_PARAM, "%s factor is not strictly %s triangular (row %d, col %d)",
+                    upper ? "U" : "L", upper ? "upper" : "lower", i, j);
+      l = std::max(l, lev[j]);
+    }
+    lev[i] = l + 1;
+    max_level = std::max(max_level, lev[i]);
+  }
+  int nlev = n > 0 ? max_level + 1 : 0;
+  level_ptr.assign(nlev + 1, 0);
+  for (int i = 0; i < n; i++) level_ptr[lev[i] + 1]++;
+  for (int l = 0; l < nlev; l++) level_ptr[l + 1] += level_ptr[l];
+  order.assign(n, 0);
+  std::vector<int> pos(level_ptr.begin(), level_ptr.end() - (nlev > 0 ? 1 : 0));
+  for (int i = 0; i < n; i++) order[pos[lev[i]]++] = i;
+  return PGX_SUCCESS;
+}
+
+static int pick_lanes(long long nnz, long long rows) {
+  double avg = rows > 0 ? (double)nnz / (double)rows : 0.0;
+  if (avg > 16) return 32;
+  if (avg > 8) return 16;
+  if (avg > 4) return 8;
+  if (avg > 2) return 4;
+  return 2;
+}
+
+// -------------------------------------------------------- device memory
+struct Arena {
+  std::vector<void*> ptrs;
+  size_t bytes = 0;
+  ~Arena() { release(); }
+  void release() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+    bytes = 0;
+  }
+  template <typename T>
+  int alloc(T** out, size_t count) {
+    *out = nullptr;
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? PGX_ERROR_OOM : PGX_ERROR_CUDA, "cudaMalloc(%zu): %s",
+                  count * sizeof(T), cudaGetErrorString(e));
+    ptrs.push_back(p);
+    bytes += count * sizeof(T);
+    *out = (T*)p;
+    return PGX_SUCCESS;
+  }
+  template <typename T, typename U>
+  int upload(T** out, const U* src, size_t count, cudaStream_t s) {
+    PGX_TRY(alloc(out, count));
+    if (count == 0) return PGX_SUCCESS;
+    std::vector<T> tmp(src, src + count);
+    PGX_CUDA(cudaMemcpyAsync(*out, tmp.data(), count * sizeof(T), cudaMemcpyHostToDevice, s));
+    PGX_CUDA(cudaStreamSynchronize(s));
+    return PGX_SUCCESS;
+  }
+  template <typename T>
+  int zeros(T** out, size_t count, cudaStream_t s) {
+    PGX_TRY(alloc(out, count));
+    PGX_CUDA(cudaMemsetAsync(*out, 0, std::max<size_t>(count, 1) * sizeof(T), s));
+    return PGX_SUCCESS;
+  }
+};
+
+template <typename T>
+struct DCsr {
+  int rows = 0, cols = 0, S = 8;
+  long long nnz = 0;
+  int *rp = nullptr, *cj = nullptr;
+  T* va = nullptr;
+};
+
+template <typename T>
+static int upload_csr(Arena& ar, const HostCsr& h, DCsr<T>& d, cudaStream_t s) {
+  d.rows = h.rows;
+  d.cols = h.cols;
+  d.nnz = h.nnz();
+  d.S = pick_lanes(d.nnz, d.rows);
+  if (h.rows == 0) return PGX_SUCCESS;
+  PGX_TRY(ar.upload(&d.rp, h.rp.data(), h.rp.size(), s));
+  PGX_TRY(ar.upload(&d.cj, h.cj.data(), h.cj.size(), s));
+  PGX_TRY(ar.upload(&d.va, h.va.data(), h.va.size(), s));
+  return PGX_SUCCESS;
+}
+
+// A triangular factor stored in padded level-set order.
+template <typename T>
+struct DTri {
+  int n = 0, S = 32, ngroups = 0, nlevels = 0, nblocks = 1;
+  int *ord = nullptr, *rp = nullptr, *cj = nullptr;
+  T* va = nullptr;
+  unsigned long long* ticket = nullptr;
+};
+
+// persistent grid of the triangular solve: a few warps per group of an
+// average level keeps the frontier busy without flooding L2 with pollers
+static int tri_blocks(int ngroups, int nlevels) {
+  const int wpb = 256 / kWarp;
+  double avg = nlevels > 0 ? (double)ngroups / nlevels : (double)ngroups;
+  long long warps = (long long)std::ceil(8.0 * avg);
+  warps = std::max<long long>(warps, 64);
+  warps = std::min<long long>(warps, 148LL * 32);
+  warps = std::min<long long>(warps, ((long long)ngroups + wpb - 1) / wpb * wpb);
+  return (int)std::max<long long>(1, (warps + wpb - 1) / wpb);
+}
+
+template <typename T>
+static int upload_tri(Arena& ar, const HostCsr& h, bool upper, DTri<T>& d, cudaStream_t s) {
+  d.n = h.rows;
+  if (d.n == 0) return PGX_SUCCESS;
+  std::vector<int> lptr, order;
+  PGX_TRY(build_levels(upper, h.rows, h.rp.data(), h.cj.data(), lptr, order));
+  d.nlevels = (int)lptr.size() - 1;
+  d.S = pick_lanes(h.nnz(), h.rows);
+  const int G = kWarp / d.S;
+  // padded schedule: each level starts on a group boundary
+  std::vector<int> ord, rp(1, 0), cj;
+  std::vector<double> va;
+  ord.reserve(h.rows + (size_t)d.nlevels * G);
+  cj.reserve(h.nnz());
+  va.reserve(h.nnz());
+  for (int l = 0; l < d.nlevels; l++) {
+    for (int p = lptr[l]; p < lptr[l + 1]; p++) {
+      int r = order[p];
+      ord.push_back(r);
+      for (int k = h.rp[r]; k < h.rp[r + 1]; k++) {
+        cj.push_back(h.cj[k]);
+        va.push_back(h.va[k]);
+      }
+      rp.push_back((int)cj.size());
+    }
+    while (ord.size() % G) {
+      ord.push_back(-1);
+      rp.push_back((int)cj.size());
+    }
+  }
+  d.ngroups = (int)(ord.size() / G);
+  d.nblocks = tri_blocks(d.ngroups, d.nlevels);
+  PGX_TRY(ar.upload(&d.ord, ord.data(), ord.size(), s));
+  PGX_TRY(ar.upload(&d.rp, rp.data(), rp.size(), s));
+  PGX_TRY(ar.upload(&d.cj, cj.data(), cj.size(), s));
+  PGX_TRY(ar.upload(&d.va, va.data(), va.size(), s));
+  PGX_TRY(ar.zeros(&d.ticket, 1, s));
+  return PGX_SUCCESS;
+}
+
+template <typename P>
+struct DLevel {
+  int start = 0, nl = 0, m = 0, rank = 0;
+  DTri<P> L, U;
+  P* dinv = nullptr;
+  P* y = nullptr;  // lower-pass result, holds the sentinel between solves
+  DCsr<P> E, F;
+  P *W = nullptr, *WH = nullptr;
+  P *z = nullptr, *xlr = nullptr;
+  double* lrt = nullptr;
+};
+
+static inline Skip mk_skip(const int* a = nullptr, const int* b = nullptr, const int* c = nullptr) {
+  Skip s;
+  s.f0 = a;
+  s.f1 = b;
+  s.f2 = c;
+  return s;
+}
+
+static inline int grid_for(long long work, int per_block, int cap) {
+  long long g = (work + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+// ---------------------------------------------------------------- engine
+struct EngineBase {
+  virtual ~EngineBase() {}
+  virtual int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+                    pgx_result* res) = 0;
+  virtual int apply(double* z, const double* v, int location) = 0;
+  virtual int64_t device_bytes(int kdim) const = 0;
+};
+
+struct Import {
+  int n = 0, precision = 0, nlev = 0;
+  HostCsr A;
+  std::vector<int> pperm, qperm, lev_ptr;
+  std::vector<HostLevel> levels;
+  int inner_enable = 0, inner_maxits = 5;
+  double inner_tol = 1e-2;
+};
+
+template <typename P>
+struct Engine : EngineBase {
+  int n = 0, nlev = 0;
+  std::vector<int> lev_ptr;
+  cudaStream_t stream = nullptr;
+  Arena ar, krylov;
+  int kdim_alloc = 0;
+  DCsr<double> A;
+  int *pperm = nullptr, *qperm = nullptr;
+  std::vector<DLevel<P>> lv;
+  // level-0 Schur-complement operator C0 x - E0 B0^-1 F0 x and its work space
+  DCsr<P> C0;
+  P *s_zu = nullptr, *s_wu = nullptr;
+  // inner FGMRES on level 0
+  int inner = 0, inner_maxits = 5;
+  double inner_tol = 1e-2;
+  P *Vin = nullptr, *Zin = nullptr;
+  FgmresDev* st_in = nullptr;
+  // outer FGMRES
+  double* V = nullptr;
+  P* Z = nullptr;
+  FgmresDev* st = nullptr;
+  double *bdev = nullptr, *xdev = nullptr, *rdev = nullptr, *scal = nullptr;
+  P *rt = nullptr, *xt = nullptr;
+  double* partial = nullptr;
+  unsigned int* counter = nullptr;
+  int* err = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // one FGMRES restart cycle captured as a CUDA graph, keyed by its arguments
+  cudaGraphExec_t cycle_exec = nullptr;
+  int g_kdim = -1;
+  const void *g_x = nullptr, *g_b = nullptr;
+
+  void drop_graph() {
+    if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
+    cycle_exec = nullptr;
+    g_kdim = -1;
+  }
+
+  ~Engine() override {
+    if (stream) cudaStreamSynchronize(stream);
+    drop_graph();
+    ar.release();
+    krylov.release();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  int64_t device_bytes(int kdim) const override {
+    int64_t b = (int64_t)ar.bytes;
+    b += (int64_t)n * (kdim + 1) * (sizeof(double) + sizeof(P));
+    return b;
+  }
+
+  // ------------------------------------------------------------ commit
+  int commit(Import& im) {
+    n = im.n;
+    nlev = im.nlev;
+    lev_ptr = im.lev_ptr;
+    PGX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    PGX_CUDA(cudaEventCreate(&ev0));
+    PGX_CUDA(cudaEventCreate(&ev1));
+    PGX_TRY(upload_csr(ar, im.A, A, stream));
+    PGX_TRY(ar.upload(&pperm, im.pperm.data(), im.pperm.size(), stream));
+    if (!im.qperm.empty()) PGX_TRY(ar.upload(&qperm, im.qperm.data(), im.qperm.size(), stream));
+    lv.resize(nlev);
+    for (int l = 0; l < nlev; l++) {
+      HostLevel& h = im.levels[l];
+      DLevel<P>& d = lv[l];
+      d.start = lev_ptr[l];
+      d.nl = lev_ptr[l + 1] - lev_ptr[l];
+      d.m = n - lev_ptr[l + 1];
+      PGX_TRY(upload_tri(ar, h.L, false, d.L, stream));
+      PGX_TRY(upload_tri(ar, h.U, true, d.U, stream));
+      PGX_TRY(ar.upload(&d.dinv, h.dinv.data(), h.dinv.size(), stream));
+      PGX_TRY(ar.alloc(&d.y, (size_t)d.nl));
+      sentinel_fill_kernel<P><<<grid_for(d.nl, 256, 148 * 8), 256, 0, stream>>>(d.nl, d.y);
+      PGX_CUDA(cudaGetLastError());
+      if (l < nlev - 1) {
+        PGX_TRY(upload_csr(ar, h.E, d.E, stream));
+        PGX_TRY(upload_csr(ar, h.F, d.F, stream));
+        d.rank = h.rank;
+        if (d.rank > 0) {
+          PGX_TRY(ar.upload(&d.W, h.W.data(), h.W.size(), stream));
+          PGX_TRY(ar.upload(&d.WH, h.WH.data(), h.WH.size(), stream));
+        }
+        PGX_TRY(ar.zeros(&d.xlr, (size_t)d.m, stream));
+        PGX_TRY(ar.zeros(&d.lrt, (size_t)KMAX + 1, stream));
+      }
+      PGX_TRY(ar.zeros(&d.z, (size_t)(n - d.start), stream));
+    }
+    inner = (im.inner_enable && nlev >= 2) ? 1 : 0;
+    inner_maxits = im.inner_maxits;
+    inner_tol = im.inner_tol;
+    if (inner) {
+      PGX_TRY(assemble_c0(im));
+      const int m0 = lv[0].m;
+      PGX_TRY(ar.zeros(&s_zu, (size_t)lv[0].nl, stream));
+      PGX_TRY(ar.zeros(&s_wu, (size_t)lv[0].nl, stream));
+      PGX_TRY(ar.zeros(&Vin, (size_t)m0 * (inner_maxits + 1), stream));
+      PGX_TRY(ar.zeros(&Zin, (size_t)m0 * (inner_maxits + 1), stream));
+      PGX_TRY(ar.zeros(&st_in, 1, stream));
+      FgmresDev h;
+      memset(&h, 0, sizeof(h));
+      h.kdim = inner_maxits;
+      h.maxits = inner_maxits;
+      h.tol = inner_tol;
+      h.eps = std::is_same<P, float>::value ? (double)FLT_EPSILON : DBL_EPSILON;
+      PGX_CUDA(cudaMemcpyAsync(st_in, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+    }
+    PGX_TRY(ar.zeros(&st, 1, stream));
+    PGX_TRY(ar.zeros(&bdev, (size_t)n, stream));
+    PGX_TRY(ar.zeros(&xdev, (size_t)n, stream));
+    PGX_TRY(ar.zeros(&rdev, (size_t)n, stream));
+    PGX_TRY(ar.zeros(&scal, 8, stream));
+    PGX_TRY(ar.zeros(&rt, (size_t)n, stream));
+    PGX_TRY(ar.zeros(&xt, (size_t)n, stream));
+    PGX_TRY(ar.zeros(&partial, (size_t)(KMAX + 1) * kTsMaxBlocks, stream));
+    PGX_TRY(ar.zeros(&counter, 1, stream));
+    PGX_TRY(ar.zeros(&err, 1, stream));
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    return PGX_SUCCESS;
+  }
+
+  // C0 = the matrix of GemslrClass::CMatVec(0) (gemslr.cpp:3962-4080): the
+  // unfactored B_j blocks of levels j >= 1 on the diagonal, E_j / F_j of the
+  // non-last levels j >= 1 off the diagonal, in the local numbering of the
+  // trailing m_0 unknowns.
+  int assemble_c0(Import& im) {
+    const int base = lev_ptr[1];
+    const int m0 = n - base;
+    std::vector<std::vector<std::pair<int, double>>> rows(m0);
+    auto add = [&](const HostCsr& M, int roff, int coff) {
+      for (int r = 0; r < M.rows; r++)
+        for (int k = M.rp[r]; k < M.rp[r + 1]; k++) rows[roff + r].push_back({coff + M.cj[k], M.va[k]});
+    };
+    for (int j = 1; j < nlev; j++) {
+      const HostLevel& h = im.levels[j];
+      const int o = lev_ptr[j] - base, o1 = lev_ptr[j + 1] - base;
+      add(h.B, o, o);
+      if (j < nlev - 1) {
+        add(h.F, o, o1);
+        add(h.E, o1, o);
+      }
+    }
+    HostCsr c;
+    c.rows = c.cols = m0;
+    c.rp.assign(m0 + 1, 0);
+    for (int r = 0; r < m0; r++) {
+      std::sort(rows[r].begin(), rows[r].end());
+      for (auto& e : rows[r]) {
+        c.cj.push_back(e.first);
+        c.va.push_back(e.second);
+      }
+      c.rp[r + 1] = (int)c.cj.size();
+    }
+    return upload_csr(ar, c, C0, stream);
+  }
+
+  int ensure_krylov(int kdim) {
+    if (kdim <= kdim_alloc) return PGX_SUCCESS;
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    drop_graph();
+    krylov.release();
+    PGX_TRY(krylov.zeros(&V, (size_t)n * (kdim + 1), stream));
+    PGX_TRY(krylov.zeros(&Z, (size_t)n * (kdim + 1), stream));
+    kdim_alloc = kdim;
+    return PGX_SUCCESS;
+  }
+
+  // ---------------------------------------------------------- enqueues
+  template <typename TA, typename TX, typename TY, typename TC>
+  void spmv(const DCsr<TA>& M, const TX* x, TC alpha, const DCsr<TA>* M2, const TX* x2, TC alpha2,
+            const TY* b, TC beta, TY* y, const double* xscale, Skip sk) {
+    if (M.rows == 0) return;
+    const int S = M.S;
+    const int gpb = 256 / S;
+    const int grid = grid_for(M.rows, gpb, 148 * 16);
+    const int *rp2 = M2 ? M2->rp : nullptr, *cj2 = M2 ? M2->cj : nullptr;
+    const TA* va2 = M2 ? M2->va : nullptr;
+#define PGX_SPMV(SS)                                                                                  \
+  spmv_kernel<TA, TX, TY, TC, SS><<<grid, 256, 0, stream>>>(M.rows, M.rp, M.cj, M.va, x, alpha, rp2, cj2, \
+                                                            va2, x2, alpha2, b, beta, y, xscale, sk)
+    switch (S) {
+      case 2: PGX_SPMV(2); break;
+      case 4: PGX_SPMV(4); break;
+      case 8: PGX_SPMV(8); break;
+      case 16: PGX_SPMV(16); break;
+      default: PGX_SPMV(32); break;
+    }
+#undef PGX_SPMV
+  }
+
+  // one triangular pass; lower: y = L^-1 rhs (x set to the sentinel),
+  // upper: x = D U^-1 y (y set back to the sentinel)
+  void trsv(const DTri<P>& T, bool upper, const P* dinv, const P* rhs, const double* rhs_scale, P* y, P* x,
+            Skip sk) {
+    if (T.n == 0) return;
+#define PGX_TRSV(SS)                                                                                   \
+  if (upper)                                                                                           \
+    trsv_kernel<P, SS, true><<<T.nblocks, 256, 0, stream>>>(T.n, T.ngroups, T.ord, T.rp, T.cj, T.va,    \
+                                                            dinv, rhs, rhs_scale, y, x, T.ticket, err, sk); \
+  else                                                                                                 \
+    trsv_kernel<P, SS, false><<<T.nblocks, 256, 0, stream>>>(T.n, T.ngroups, T.ord, T.rp, T.cj, T.va,   \
+                                                             dinv, rhs, rhs_scale, y, x, T.ticket, err, sk)
+    switch (T.S) {
+      case 2: PGX_TRSV(2); break;
+      case 4: PGX_TRSV(4); break;
+      case 8: PGX_TRSV(8); break;
+      case 16: PGX_TRSV(16); break;
+      default: PGX_TRSV(32); break;
+    }
+#undef PGX_TRSV
+  }
+
+  template <typename TV, typename TM, typename TW, int MODE>
+  void ts(TsArgs<TV, TM, TW> a) {
+    a.partial = partial;
+    a.counter = counter;
+    const int grid = grid_for(a.n, kTsThreads, kTsMaxBlocks);
+    ts_kernel<TV, TM, TW, MODE><<<grid, kTsThreads, 0, stream>>>(a);
+  }
+
+  template <typename TV, typename TM, typename TW>
+  static TsArgs<TV, TM, TW> ts_args(int nrows, Skip sk) {
+    TsArgs<TV, TM, TW> a;
+    memset(&a, 0, sizeof(a));
+    a.n = nrows;
+    a.sign = 1.0;
+    a.skip = sk;
+    return a;
+  }
+
+  // B-solve of level l: x = U^-1 L^-1 rhs  (GemslrClass::SolveB)
+  void solve_b(int l, const P* rhs, const double* rhs_scale, P* x, Skip sk) {
+    DLevel<P>& d = lv[l];
+    trsv(d.L, false, nullptr, rhs, rhs_scale, d.y, x, sk);
+    trsv(d.U, true, d.dinv, nullptr, nullptr, d.y, x, sk);
+  }
+
+  // x += WH (W^T x) in place  (SolveApplyLowRankLevel + Axpy, gemslr.cpp:3585-3590)
+  void lowrank_inplace(int l, P* x, Skip sk) {
+    DLevel<P>& d = lv[l];
+    auto a = ts_args<P, P, P>(d.m, sk);
+    a.ncols = d.rank;
+    a.V = d.W;
+    a.ldv = d.m;
+    a.in = x;
+    a.epi = EPI_STORE;
+    a.dst = d.lrt;
+    ts<P, P, P, TS_DOT>(a);
+    auto u = ts_args<P, P, P>(d.m, sk);
+    u.ncols = d.rank;
+    u.M = d.WH;
+    u.ldm = d.m;
+    u.coef = d.lrt;
+    u.in = x;
+    u.out = x;
+    ts<P, P, P, TS_UPDATE>(u);
+  }
+
+  // GemslrClass::SolveLevel (gemslr.cpp:3474-3630); x and rhs hold the
+  // trailing n - lev_ptr[l] unknowns.  rhs may carry a lazy scale (level 0).
+  void solve_level(int l, P* x, const P* rhs, Skip sk) {
+    DLevel<P>& d = lv[l];
+    if (l == nlev - 1) {
+      solve_b(l, rhs, nullptr, x, sk);
+      return;
+    }
+    P* zu = d.z;
+    P* zl = d.z + d.nl;
+    P* xl = x + d.nl;
+    solve_b(l, rhs, nullptr, zu, sk);                                              // 1. zu = B^-1 rhs_u
+    spmv<P, P, P, P>(d.E, zu, (P)-1, nullptr, nullptr, (P)0, rhs + d.nl, (P)1, zl, nullptr, sk);  // 2-3.
+    if (l == 0 && inner) {
+      inner_solve(xl, zl, sk);                                                     // 4. inner FGMRES
+    } else {
+      if (d.rank > 0) lowrank_inplace(l, zl, sk);                                  // 4. low rank
+      solve_level(l + 1, xl, zl, sk);                                              //    recursion
+    }
+    spmv<P, P, P, P>(d.F, xl, (P)-1, nullptr, nullptr, (P)0, rhs, (P)1, zu, nullptr, sk);  // 5-6.
+    solve_b(l, zu, nullptr, x, sk);                                                // 7. xu = B^-1 zu
+  }
+
+  // Level-0 inner flexible GMRES on the Schur complement S0 = C0 - E0 B0^-1 F0,
+  // from x0 = 0, one cycle of inner_maxits steps (gemslr.cpp:1660-1674, 3566-3572).
+  void inner_solve(P* xl, const P* zl, Skip outer) {
+    DLevel<P>& d0 = lv[0];
+    const int m0 = d0.m;
+    const long long ld = m0;
+    Skip it = mk_skip(outer.f0, outer.f1, &st_in->cycle_done);
+    {
+      auto a = ts_args<P, P, P>(m0, outer);
+      a.in = zl;
+      a.out = Vin;
+      a.epi = EPI_INIT_INNER;
+      a.st = st_in;
+      ts<P, P, P, TS_NORM_COPY>(a);
+    }
+    for (int j = 0; j < inner_maxits; j++) {
+      P* vj = Vin + (long long)j * ld;
+      P* zj = Zin + (long long)j * ld;
+      P* wj = Vin + (long long)(j + 1) * ld;
+      // Schur preconditioner (GemslrSchurMatrixClass::Solve, gemslr.cpp:294-330):
+      // xlr = v + WH W^T v, then the level-1 recursion
+      if (d0.rank > 0) {
+        auto a = ts_args<P, P, P>(m0, it);
+        a.ncols = d0.rank;
+        a.V = d0.W;
+        a.ldv = m0;
+        a.in = vj;
+        a.in_scale = &st_in->sc[j];
+        a.epi = EPI_STORE;
+        a.dst = d0.lrt;
+        ts<P, P, P, TS_DOT>(a);
+      }
+      {
+        auto u = ts_args<P, P, P>(m0, it);
+        u.ncols = d0.rank;
+        u.M = d0.WH;
+        u.ldm = m0;
+        u.coef = d0.lrt;
+        u.in = vj;
+        u.in_scale = &st_in->sc[j];
+        u.out = d0.xlr;
+        ts<P, P, P, TS_UPDATE>(u);
+      }
+      solve_level(1, zj, d0.xlr, it);
+      // w = S0 z  (GemslrClass::SchurMatVec, gemslr.cpp:3799-3960)
+      spmv<P, P, P, P>(d0.F, zj, (P)1, nullptr, nullptr, (P)0, (const P*)nullptr, (P)0, s_zu, nullptr, it);
+      solve_b(0, s_zu, nullptr, s_wu, it);
+      spmv<P, P, P, P>(C0, zj, (P)1, &d0.E, s_wu, (P)-1, (const P*)nullptr, (P)0, wj, nullptr, it);
+      arnoldi_step<P, P>(Vin, ld, j, st_in, m0, it);
+    }
+    {
+      auto u = ts_args<P, P, P>(m0, outer);
+      u.ncols_dev = &st_in->i;
+      u.M = Zin;
+      u.ldm = ld;
+      u.coef = st_in->rs;
+      u.in = nullptr;
+      u.out = xl;
+      ts<P, P, P, TS_UPDATE>(u);
+    }
+  }
+
+  // Orthogonalise column j+1 of the basis against columns 0..j by classical
+  // Gram-Schmidt with one re-orthogonalisation (CGS2, matrixops.cpp:10588-10708),
+  // then finish the Hessenberg column with Givens rotations (fgmres.hpp:430-458).
+  template <typename TV, typename TW>
+  void arnoldi_step(TV* Vb, long long ld, int j, FgmresDev* s, int nrows, Skip sk) {
+    TW* w = (TW*)(Vb + (long long)(j + 1) * ld);
+    auto a = ts_args<TV, TV, TW>(nrows, sk);
+    a.ncols = j + 1;
+    a.V = Vb;
+    a.ldv = ld;
+    a.vsc = s->sc;
+    a.in = w;
+    a.epi = EPI_CGS_FIRST;
+    a.st = s;
+    ts<TV, TV, TW, TS_DOT>(a);
+    auto b = a;
+    b.M = Vb;
+    b.ldm = ld;
+    b.msc = s->sc;
+    b.coef = s->coefA;
+    b.sign = -1.0;
+    b.out = w;
+    b.epi = EPI_CGS_SECOND;
+    ts<TV, TV, TW, TS_UPDATE_DOT>(b);
+    auto c = b;
+    c.coef = s->coefB;
+    c.epi = EPI_GIVENS;
+    c.j = j;
+    ts<TV, TV, TW, TS_UPDATE_NORM>(c);
+  }
+
+  // GemslrClass::Solve (gemslr.cpp:3431-3472): gather by pperm, SolveLevel(0),
+  // scatter by qperm (or pperm for symmetric reorderings).
+  template <typename TO>
+  void precond(const double* v, const double* v_scale, TO* z, Skip sk) {
+    const int grid = grid_for(n, 256, 148 * 16);
+    gather_kernel<double, P><<<grid, 256, 0, stream>>>(n, pperm, v, v_scale, rt, sk);
+    solve_level(0, xt, rt, sk);
+    scatter_kernel<P, TO><<<grid, 256, 0, stream>>>(n, qperm ? qperm : pperm, xt, z, sk);
+  }
+
+  int check_err() {
+    int h = 0;
+    PGX_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    if (h & kErrIndex) return fail(PGX_ERROR_INVALID_PARAM, "device index check failed");
+    if (h & kErrTimeout) return fail(PGX_ERROR_TIMEOUT, "triangular-solve dependency wait timed out");
+    return PGX_SUCCESS;
+  }
+
+  int apply(double* z, const double* v, int location) override {
+    const double* vin = v;
+    double* zout = z;
+    if (location == PGX_LOCATION_HOST) {
+      PGX_CUDA(cudaMemcpyAsync(bdev, v, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      vin = bdev;
+      zout = xdev;
+    }
+    PGX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
+    precond<double>(vin, nullptr, zout, mk_skip());
+    PGX_CUDA(cudaGetLastError());
+    if (location == PGX_LOCATION_HOST)
+      PGX_CUDA(cudaMemcpyAsync(z, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+    return check_err();
+  }
+
+  // One restart cycle of FlexGmresClass::Solve (fgmres.hpp:379-514): kdim
+  // Arnoldi steps, the solution update, the restart residual and the cycle
+  // reset.  Steps after convergence see the cycle flag and return at once.
+  void enqueue_cycle(int kdim, double* xd, const double* bd) {
+    const long long ld = n;
+    Skip sk = mk_skip(&st->done, &st->cycle_done);
+    for (int j = 0; j < kdim; j++) {
+      double* vj = V + (long long)j * ld;
+      P* zj = Z + (long long)j * ld;
+      precond<P>(vj, &st->sc[j], zj, sk);                                            // z = M^-1 v
+      spmv<double, P, double, double>(A, zj, 1.0, nullptr, nullptr, 0.0, (const double*)nullptr, 0.0,
+                                      V + (long long)(j + 1) * ld, nullptr, sk);   // w = A z
+      arnoldi_step<double, double>(V, ld, j, st, n, sk);
+    }
+    {
+      auto u = ts_args<P, P, double>(n, mk_skip());
+      u.ncols_dev = &st->i;
+      u.M = Z;
+      u.ldm = ld;
+      u.coef = st->rs;
+      u.in = xd;
+      u.out = xd;
+      ts<P, P, double, TS_UPDATE>(u);                                                // x += Z y
+    }
+    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
+                                         mk_skip(&st->done));                        // restart residual
+    fgmres_cycle_reset_kernel<<<1, 1, 0, stream>>>(st, mk_skip());
+  }
+
+  // FlexGmresClass::Solve (fgmres.hpp:263-558) with the basis, Hessenberg and
+  // rotations on the device; the host reads the state once per restart cycle.
+  int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+            pgx_result* res) override {
+    if (kdim < 1 || kdim > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", kdim, KMAX);
+    if (maxits < 0) return fail(PGX_ERROR_INVALID_PARAM, "maxits %d < 0", maxits);
+    PGX_TRY(ensure_krylov(kdim));
+    double* xd = x;
+    const double* bd = b;
+    if (location == PGX_LOCATION_HOST) {
+      PGX_CUDA(cudaMemcpyAsync(bdev, b, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaMemcpyAsync(xdev, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      xd = xdev;
+      bd = bdev;
+    }
+    FgmresDev h;
+    memset(&h, 0, sizeof(h));
+    h.kdim = kdim;
+    h.maxits = maxits;
+    h.tol = tol;
+    h.absolute = atol;
+    h.eps = DBL_EPSILON;
+    h.cycle_done = 1;
+    const size_t head = offsetof(FgmresDev, sc);
+    PGX_CUDA(cudaMemcpyAsync(st, &h, head, cudaMemcpyHostToDevice, stream));
+    PGX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
+    PGX_CUDA(cudaEventRecord(ev0, stream));
+    // ||b||, v = b - A x, ||v||  (fgmres.hpp:319-360)
+    {
+      auto a = ts_args<double, double, double>(n, mk_skip());
+      a.in = bd;
+      a.epi = EPI_NORMB;
+      a.st = st;
+      ts<double, double, double, TS_NORM_COPY>(a);
+    }
+    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
+                                         mk_skip(&st->done));
+    {
+      auto a = ts_args<double, double, double>(n, mk_skip());
+      a.in = V;
+      a.epi = EPI_INIT;
+      a.st = st;
+      ts<double, double, double, TS_NORM_COPY>(a);
+    }
+    const int max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
+    if (max_cycles > 0 && (!cycle_exec || g_kdim != kdim || g_x != xd || g_b != bd)) {
+      drop_graph();
+      cudaGraph_t g = nullptr;
+      PGX_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_cycle(kdim, xd, bd);
+      cudaError_t ce = cudaStreamEndCapture(stream, &g);
+      if (ce != cudaSuccess) return fail(PGX_ERROR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&cycle_exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) {
+        cycle_exec = nullptr;
+        return fail(PGX_ERROR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      }
+      g_kdim = kdim;
+      g_x = xd;
+      g_b = bd;
+    }
+    for (int cyc = 0; cyc < max_cycles; cyc++) {
+      PGX_CUDA(cudaGraphLaunch(cycle_exec, stream));
+      FgmresDev hs;
+      PGX_CUDA(cudaMemcpyAsync(&hs, st, head, cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaStreamSynchronize(stream));
+      if (hs.done || hs.iter >= maxits) break;
+    }
+    // FP64 true residual ||b - A x|| / ||b||
+    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, rdev, nullptr, mk_skip());
+    {
+      auto a = ts_args<double, double, double>(n, mk_skip());
+      a.in = rdev;
+      a.epi = EPI_STORE;
+      a.dst = scal;
+      ts<double, double, double, TS_NORM_COPY>(a);
+    }
+    PGX_CUDA(cudaEventRecord(ev1, stream));
+    FgmresDev hs;
+    double r2 = 0.0;
+    PGX_CUDA(cudaMemcpyAsync(&hs, st, head, cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaMemcpyAsync(&r2, scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    int rc = check_err();
+    float ms = 0.f;
+    PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+    if (hs.normb < DBL_EPSILON) {
+      // zero right-hand side: x = 0 (fgmres.hpp:321-329)
+      PGX_CUDA(cudaMemsetAsync(xd, 0, sizeof(double) * n, stream));
+    }
+    if (location == PGX_LOCATION_HOST)
+      PGX_CUDA(cudaMemcpyAsync(x, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    if (res) {
+      res->status = rc;
+      res->iters = hs.iter;
+      res->rel_res = hs.normb > 0 ? hs.normr / hs.normb : 0.0;
+      res->true_rel_res = hs.normb > 0 ? sqrt(r2) / hs.normb : 0.0;
+      res->solve_ms = ms;
+    }
+    if (rc == PGX_SUCCESS && !(std::isfinite(hs.normr)))
+      return fail(PGX_ERROR_NOT_FINITE, "FGMRES residual is not finite");
+    return rc;
+  }
+};
+
+}  // namespace pgx
+
+// ===================================================================== C ABI
+using namespace pgx;
+
+struct pgx_gemslr_s {
+  Import im;
+  std::unique_ptr<EngineBase> eng;
+  int device = 0;
+};
+
+extern "C" {
+
+int pgx_init(int device) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return fail(PGX_ERROR_NO_DEVICE, "no CUDA device available");
+  if (device < 0 || device >= count) return fail(PGX_ERROR_INVALID_PARAM, "device %d not in [0, %d)", device, count);
+  PGX_CUDA(cudaSetDevice(device));
+  g_device = device;
+  return PGX_SUCCESS;
+}
+
+int pgx_finalize(void) { return PGX_SUCCESS; }
+
+const char* pgx_last_error(void) { return g_last_error.c_str(); }
+
+int pgx_version(void) { return 100; }
+
+int pgx_gemslr_create(pgx_handle* handle, int32_t n, int32_t precision) {
+  if (!handle) return fail(PGX_ERROR_INVALID_PARAM, "null handle pointer");
+  *handle = nullptr;
+  if (n <= 0) return fail(PGX_ERROR_INVALID_PARAM, "n must be positive");
+  if (precision != PGX_PRECISION_FP64 && precision != PGX_PRECISION_MIXED)
+    return fail(PGX_ERROR_INVALID_OPTION, "unknown precision %d", precision);
+  pgx_gemslr_s* h = new pgx_gemslr_s();
+  h->im.n = n;
+  h->im.precision = precision;
+  h->device = g_device;
+  *handle = h;
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_set_matrix(pgx_handle h, const pgx_csr* A) {
+  if (!h || !A) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (A->rows != h->im.n || A->cols != h->im.n) return fail(PGX_ERROR_INVALID_PARAM, "A must be n x n");
+  return copy_csr(A, h->im.A, "A");
+}
+
+static int check_perm(const int32_t* p, int n, const char* what) {
+  std::vector<char> seen(n, 0);
+  for (int i = 0; i < n; i++) {
+    if (p[i] < 0 || p[i] >= n || seen[p[i]]) return fail(PGX_ERROR_INVALID_PARAM, "%s is not a permutation", what);
+    seen[p[i]] = 1;
+  }
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_set_perm(pgx_handle h, const int32_t* pperm, const int32_t* qperm) {
+  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+  const int n = h->im.n;
+  if (pperm) {
+    PGX_TRY(check_perm(pperm, n, "pperm"));
+    h->im.pperm.assign(pperm, pperm + n);
+  } else {
+    h->im.pperm.resize(n);
+    for (int i = 0; i < n; i++) h->im.pperm[i] = i;
+  }
+  h->im.qperm.clear();
+  if (qperm) {
+    PGX_TRY(check_perm(qperm, n, "qperm"));
+    h->im.qperm.assign(qperm, qperm + n);
+  }
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_set_levels(pgx_handle h, int32_t nlev, const int32_t* lev_ptr) {
+  if (!h || !lev_ptr) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (nlev < 1) return fail(PGX_ERROR_INVALID_PARAM, "nlev must be >= 1");
+  if (lev_ptr[0] != 0 || lev_ptr[nlev] != h->im.n) return fail(PGX_ERROR_INVALID_PARAM, "lev_ptr must span [0, n]");
+  for (int l = 0; l < nlev; l++)
+    if (lev_ptr[l + 1] <= lev_ptr[l]) return fail(PGX_ERROR_INVALID_PARAM, "level %d is empty", l);
+  h->im.nlev = nlev;
+  h->im.lev_ptr.assign(lev_ptr, lev_ptr + nlev + 1);
+  h->im.levels.assign(nlev, HostLevel());
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_set_level(pgx_handle h, int32_t level, const pgx_level* d) {
+  if (!h || !d) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  Import& im = h->im;
+  if (level < 0 || level >= im.nlev) return fail(PGX_ERROR_INVALID_PARAM, "level %d out of range", level);
+  const int nl = im.lev_ptr[level + 1] - im.lev_ptr[level];
+  const int m = im.n - im.lev_ptr[level + 1];
+  const bool last = level == im.nlev - 1;
+  HostLevel hl;
+  hl.ncomp = d->ncomp;
+  if (d->dom_ptr && d->ncomp > 0) hl.dom_ptr.assign(d->dom_ptr, d->dom_ptr + d->ncomp + 1);
+  PGX_TRY(copy_csr(&d->L, hl.L, "L"));
+  PGX_TRY(copy_csr(&d->U, hl.U, "U"));
+  PGX_TRY(copy_csr(&d->B, hl.B, "B"));
+  if (hl.L.rows != nl || hl.L.cols != nl || hl.U.rows != nl || hl.U.cols != nl)
+    return fail(PGX_ERROR_INVALID_PARAM, "level %d: L/U must be %d x %d", level, nl, nl);
+  if (!d->dinv) return fail(PGX_ERROR_INVALID_PARAM, "level %d: missing dinv", level);
+  hl.dinv.assign(d->dinv, d->dinv + nl);
+  if (!hl.B.empty() && (hl.B.rows != nl || hl.B.cols != nl))
+    return fail(PGX_ERROR_INVALID_PARAM, "level %d: B must be %d x %d", level, nl, nl);
+  if (!last) {
+    PGX_TRY(copy_csr(&d->E, hl.E, "E"));
+    PGX_TRY(copy_csr(&d->F, hl.F, "F"));
+    if (hl.E.rows != m || hl.E.cols != nl) return fail(PGX_ERROR_INVALID_PARAM, "level %d: E must be %d x %d", level, m, nl);
+    if (hl.F.rows != nl || hl.F.cols != m) return fail(PGX_ERROR_INVALID_PARAM, "level %d: F must be %d x %d", level, nl, m);
+    if (d->rank < 0 || d->rank > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "level %d: rank %d outside [0, %d]", level, d->rank, KMAX);
+    hl.rank = d->rank;
+    if (hl.rank > 0) {
+      if (!d->W || !d->WH) return fail(PGX_ERROR_INVALID_PARAM, "level %d: missing W/WH", level);
+      hl.W.assign(d->W, d->W + (size_t)m * hl.rank);
+      hl.WH.assign(d->WH, d->WH + (size_t)m * hl.rank);
+    }
+  }
+  hl.set = true;
+  im.levels[level] = std::move(hl);
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_set_inner(pgx_handle h, int32_t enable, int32_t maxits, double tol) {
+  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+  if (enable && (maxits < 1 || maxits > KMAX)) return fail(PGX_ERROR_INVALID_PARAM, "inner maxits outside [1, %d]", KMAX);
+  h->im.inner_enable = enable ? 1 : 0;
+  h->im.inner_maxits = maxits;
+  h->im.inner_tol = tol;
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_commit(pgx_handle h) {
+  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+  Import& im = h->im;
+  if (im.A.rows != im.n) return fail(PGX_ERROR_FUNCTION_CALL, "commit before set_matrix");
+  if (im.nlev < 1) return fail(PGX_ERROR_FUNCTION_CALL, "commit before set_levels");
+  if (im.pperm.empty()) PGX_TRY(pgx_gemslr_set_perm(h, nullptr, nullptr));
+  for (int l = 0; l < im.nlev; l++)
+    if (!im.levels[l].set) return fail(PGX_ERROR_FUNCTION_CALL, "level %d not set", l);
+  if (im.inner_enable && im.nlev >= 2)
+    for (int l = 1; l < im.nlev; l++)
+      if (im.levels[l].B.empty()) return fail(PGX_ERROR_INVALID_PARAM, "inner iteration needs B of level %d", l);
+  PGX_CUDA(cudaSetDevice(h->device));
+  h->eng.reset();
+  if (im.precision == PGX_PRECISION_MIXED) {
+    auto* e = new Engine<float>();
+    h->eng.reset(e);
+    PGX_TRY(e->commit(im));
+  } else {
+    auto* e = new Engine<double>();
+    h->eng.reset(e);
+    PGX_TRY(e->commit(im));
+  }
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_destroy(pgx_handle h) {
+  if (!h) return PGX_SUCCESS;
+  cudaSetDevice(h->device);
+  delete h;
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_device_bytes(pgx_handle h, int32_t kdim, int64_t* bytes) {
+  if (!h || !bytes) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+  *bytes = h->eng->device_bytes(kdim);
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_solve(pgx_handle h, double* x, const double* b, int32_t location, const double* params,
+                     pgx_result* result) {
+  if (!h || !x || !b) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "solve before commit");
+  if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
+    return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+  int kdim = 50, maxits = 100, atol = 0;
+  double tol = 1e-6;
+  if (params) {
+    kdim = (int)params[11];
+    maxits = (int)params[12];
+    tol = params[13];
+    atol = params[14] != 0.0;
+  }
+  if (location == PGX_LOCATION_HOST) {
+    for (int i = 0; i < h->im.n; i++)
+      if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%d] is not finite", i);
+  }
+  PGX_CUDA(cudaSetDevice(h->device));
+  return h->eng->solve(x, b, location, kdim, maxits, tol, atol, result);
+}
+
+int pgx_gemslr_precond_apply(pgx_handle h, double* z, const double* v, int32_t location) {
+  if (!h || !z || !v) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "apply before commit");
+  PGX_CUDA(cudaSetDevice(h->device));
+  return h->eng->apply(z, v, location);
+}
+
+int pgx_build_levels(char uplo, int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_t* nlevels,
+                     int32_t* level_ptr, int32_t* order) {
+  if (n < 0 || (n > 0 && (!rowptr || !nlevels || !level_ptr || !order)))
+    return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (uplo != 'L' && uplo != 'U') return fail(PGX_ERROR_INVALID_OPTION, "uplo must be 'L' or 'U'");
+  for (int i = 0; i < n; i++)
+    for (int k = rowptr[i]; k < rowptr[i + 1]; k++)
+      if (colidx[k] < 0 || colidx[k] >= n) return fail(PGX_ERROR_INVALID_PARAM, "column index out of range");
+  std::vector<int> lptr, ord;
+  PGX_TRY(build_levels(uplo == 'U', n, rowptr, colidx, lptr, ord));
+  *nlevels = (int)lptr.size() - 1;
+  std::copy(lptr.begin(), lptr.end(), level_ptr);
+  std::copy(ord.begin(), ord.end(), order);
+  return PGX_SUCCESS;
+}
+
+int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double beta, double* y) {
+  if (!Ad || !x || !y) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (Ad->rows == 0) return PGX_SUCCESS;
+  const int S = pick_lanes(Ad->nnz, Ad->rows);
+  const int grid = grid_for(Ad->rows, 256 / S, 148 * 16);
+  Skip sk = mk_skip();
+#define PGX_SPMV1(SS)                                                                                        \
+  spmv_kernel<double, double, double, double, SS><<<grid, 256>>>(Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, \
+                                                                 x, alpha, nullptr, nullptr, nullptr, nullptr, \
+                                                                 0.0, beta != 0.0 ? y : nullptr, beta, y,      \
+                                                                 nullptr, sk)
+  switch (S) {
+    case 2: PGX_SPMV1(2); break;
+    case 4: PGX_SPMV1(4); break;
+    case 8: PGX_SPMV1(8); break;
+    case 16: PGX_SPMV1(16); break;
+    default: PGX_SPMV1(32); break;
+  }
+#undef PGX_SPMV1
+  PGX_CUDA(cudaGetLastError());
+  PGX_CUDA(cudaDeviceSynchronize());
+  return PGX_SUCCESS;
+}
+
+}  // extern "C"

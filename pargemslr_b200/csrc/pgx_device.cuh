@@ -1,0 +1,558 @@
+// Device-side building blocks of the GeMSLR-FGMRES solve phase (sm_100a).
+//
+// Every kernel takes a Skip descriptor: up to three device flags (the
+// "cycle finished" / "solve finished" words of the enclosing FGMRES solves).
+// A kernel whose flags are set returns at once, so a whole restart cycle can
+// be enqueued (or captured in a CUDA graph) ahead of time and the iterations
+// after convergence cost one launch each and no memory traffic.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pgx {
+
+constexpr int kWarp = 32;
+constexpr int KMAX = 128;          // largest Krylov dimension a handle accepts
+constexpr int kTsThreads = 512;    // block size of the tall-skinny kernels
+constexpr int kTsMaxBlocks = 296;  // 2 blocks per SM on a 148-SM B200
+constexpr int kSpinLimit = 1 << 21;  // bounded waits in the sync-free triangular solve
+
+// status bits written by kernels into the handle's error word
+constexpr int kErrTimeout = 1;
+constexpr int kErrIndex = 2;
+
+struct Skip {
+  const int* f0;
+  const int* f1;
+  const int* f2;
+  __device__ __forceinline__ bool on() const {
+    return (f0 && *(const volatile int*)f0) || (f1 && *(const volatile int*)f1) ||
+           (f2 && *(const volatile int*)f2);
+  }
+};
+
+// ---------------------------------------------------------------- FGMRES
+// Device-resident state of one flexible GMRES solve (FlexGmresClass::Solve,
+// ParGeMSLR SRC/solvers/fgmres.hpp:263-558).  H is column-major (KMAX+1) x KMAX.
+struct FgmresDev {
+  int done;        // solve finished (converged, max iterations or breakdown)
+  int cycle_done;  // current restart cycle finished
+  int breakdown;   // Givens breakdown: the reference skips the x update
+  int converged;
+  int iter;        // iterations so far (FlexGmresClass::_iter)
+  int i;           // columns built in the current cycle
+  int kdim;
+  int maxits;
+  double tolr;     // absolute threshold on the Givens residual estimate
+  double tol;
+  double normb;
+  double normr;    // Givens residual estimate (reference: normr)
+  double eps;      // numeric_limits<RealDataType>::epsilon() of the solver
+  int absolute;
+  int pad;
+  double sc[KMAX + 1];     // V(:,c) = Vstored(:,c) * sc[c] (lazy normalisation)
+  double hcol[KMAX + 1];   // column of H being built
+  double coefA[KMAX + 1];  // first Gram-Schmidt coefficients
+  double coefB[KMAX + 1];  // re-orthogonalisation coefficients
+  double c[KMAX], s[KMAX], rs[KMAX + 1], y[KMAX];
+  double H[(KMAX + 1) * KMAX];
+};
+
+template <typename T>
+__device__ __forceinline__ T ldcg(const T* p) { return __ldcg(p); }
+
+template <typename T>
+__device__ __forceinline__ T group_reduce(T v, int S, int lane) {
+  // sum over this lane's aligned group of S lanes; only that group's lanes
+  // take part, so other groups of the warp may be elsewhere (spinning)
+  const unsigned mask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane & ~(S - 1)));
+  for (int off = S >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(mask, v, off);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_reduce(T v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// ------------------------------------------------------------ CSR SpMV
+// y = alpha * (A1 x1) + alpha2 * (A2 x2) + beta * b, S lanes per row.
+// A2 may be absent (rp2 == nullptr); b may be absent or alias y.
+// Follows CsrMatrixPMatVecHostTemplate (ParGeMSLR SRC/matrices/matrixops.cpp:5139)
+// for one matrix; the two-matrix form fuses the Schur operator
+// C x - E (B^-1 F x) of GemslrClass::SchurMatVec (gemslr.cpp:3799-3960).
+template <typename TA, typename TX, typename TY, typename TC, int S>
+__global__ void __launch_bounds__(256) spmv_kernel(
+    int nrows, const int* __restrict__ rp1, const int* __restrict__ cj1, const TA* __restrict__ va1,
+    const TX* __restrict__ x1, TC alpha, const int* __restrict__ rp2, const int* __restrict__ cj2,
+    const TA* __restrict__ va2, const TX* __restrict__ x2, TC alpha2, const TY* b, TC beta, TY* y,
+    const double* __restrict__ xscale, Skip skip) {
+  if (skip.on()) return;
+  const int lane = threadIdx.x & (S - 1);
+  const int wlane = threadIdx.x & 31;
+  const int groups_per_block = blockDim.x / S;
+  const TC xs = xscale ? (TC)(*xscale) : (TC)1;
+  for (int row = blockIdx.x * groups_per_block + threadIdx.x / S; row < nrows;
+       row += gridDim.x * groups_per_block) {
+    TC acc = 0;
+    const int k1 = rp1[row], k2 = rp1[row + 1];
+    for (int k = k1 + lane; k < k2; k += S) acc += (TC)va1[k] * (TC)x1[cj1[k]];
+    acc = group_reduce(acc, S, wlane);
+    TC acc2 = 0;
+    if (rp2) {
+      const int q1 = rp2[row], q2 = rp2[row + 1];
+      for (int k = q1 + lane; k < q2; k += S) acc2 += (TC)va2[k] * (TC)x2[cj2[k]];
+      acc2 = group_reduce(acc2, S, wlane);
+    }
+    if (lane == 0) {
+      TC v = alpha * (acc * xs);
+      if (rp2) v += alpha2 * acc2;
+      if (b) v += beta * (TC)b[row];
+      y[row] = (TY)v;
+    }
+  }
+}
+
+// ----------------------------------------------- sync-free triangular solve
+// One pass of the ILU solve of IluClass::SolveHost (ParGeMSLR
+// SRC/preconditioners/ilu.cpp:3677-3790) over a whole level (all subdomains
+// of the level concatenated block-diagonally):
+//   lower:  y_r = rhs_r - sum_j L_rj y_j               (unit diagonal)
+//   upper:  x_r = (y_r - sum_j U_rj x_j) * dinv_r     (dinv = inverse diagonal)
+// Rows are stored in level-set order (IluClass::BuildLevels rule,
+// ilu.cpp:832-1062), each level padded to whole groups of G = 32/S rows, so a
+// group never holds two rows of which one depends on the other.
+//
+// Readiness is carried by the value itself: entries not yet computed hold a
+// signalling-NaN sentinel that arithmetic never produces.  A row publishes
+// its result with one relaxed store; a consumer polls the entry with relaxed
+// loads until the sentinel is gone - one L2 round trip per dependency and no
+// fences.  The lower pass writes y and sets x to the sentinel; the upper pass
+// consumes y, writes x and puts the sentinel back into y, so each pass leaves
+// the buffers ready for the next one.
+//
+// The grid is persistent and sized to the level width (few pollers, little
+// L2 pressure).  Warps claim groups from a monotone 64-bit ticket counter in
+// schedule order; a row only waits on rows of earlier levels, whose groups
+// were claimed earlier by warps that are running, so the waits always end.
+// Each warp stops at its first ticket past the last group, so every launch
+// consumes exactly ngroups + nwarps tickets and ticket % (ngroups + nwarps)
+// is the group index without any reset between launches.  Waits are bounded;
+// on expiry the kernel records kErrTimeout and finishes.
+template <typename T>
+struct Sentinel;
+template <>
+struct Sentinel<double> {
+  static __device__ __forceinline__ double value() { return __longlong_as_double(0xFFF4DEADBEEF0001LL); }
+  static __device__ __forceinline__ bool is(double v) { return __double_as_longlong(v) == 0xFFF4DEADBEEF0001LL; }
+  static __device__ __forceinline__ double load(const double* p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+  }
+  static __device__ __forceinline__ void store(double* p, double v) {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+  }
+};
+template <>
+struct Sentinel<float> {
+  static __device__ __forceinline__ float value() { return __int_as_float((int)0xFFA0BEEFu); }
+  static __device__ __forceinline__ bool is(float v) { return __float_as_int(v) == (int)0xFFA0BEEFu; }
+  static __device__ __forceinline__ float load(const float* p) {
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+  }
+  static __device__ __forceinline__ void store(float* p, float v) {
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+  }
+};
+
+template <typename T>
+__global__ void sentinel_fill_kernel(int n, T* p) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = Sentinel<T>::value();
+}
+
+template <typename T, int S, bool UPPER>
+__global__ void __launch_bounds__(256) trsv_kernel(
+    int n, int ngroups, const int* __restrict__ ord, const int* __restrict__ rp, const int* __restrict__ cj,
+    const T* __restrict__ va, const T* __restrict__ dinv, const T* __restrict__ rhs,
+    const double* __restrict__ rhs_scale, T* y, T* x, unsigned long long* ticket, int* err, Skip skip) {
+  constexpr int G = kWarp / S;  // rows per warp
+  if (skip.on()) return;
+  const unsigned long long period = (unsigned long long)ngroups + (unsigned long long)(gridDim.x * (blockDim.x / kWarp));
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int sl = lane & (S - 1);
+  const double rs = rhs_scale ? *rhs_scale : 1.0;
+  T* dep = UPPER ? x : y;  // the vector this pass polls
+  while (true) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(ticket, 1ULL);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    const unsigned long long g = t % period;
+    if (g >= (unsigned long long)ngroups) break;
+    const int pos = (int)g * G + lane / S;
+    const int r = ord[pos];  // -1 marks padding; uniform over the S-lane group
+    if (r >= 0) {
+      T acc = 0;
+      const int k1 = rp[pos], k2 = rp[pos + 1];
+      for (int k = k1 + sl; k < k2; k += S) {
+        const int j = cj[k];
+        if ((unsigned)j >= (unsigned)n) {
+          atomicOr(err, kErrIndex);
+          continue;
+        }
+        T v = Sentinel<T>::load(&dep[j]);
+        if (Sentinel<T>::is(v)) {
+          int spins = 0;
+          do {
+            if (++spins > kSpinLimit || (*(volatile int*)err & kErrTimeout)) {
+              atomicOr(err, kErrTimeout);
+              v = 0;
+              break;
+            }
+            __nanosleep(20);
+            v = Sentinel<T>::load(&dep[j]);
+          } while (Sentinel<T>::is(v));
+        }
+        acc += va[k] * v;
+      }
+      acc = group_reduce(acc, S, lane);
+      if (sl == 0) {
+        if (UPPER) {
+          const T yr = y[r];
+          y[r] = Sentinel<T>::value();
+          Sentinel<T>::store(&x[r], (yr - acc) * dinv[r]);
+        } else {
+          T b = rhs[r];
+          if (rhs_scale) b = (T)((double)b * rs);
+          x[r] = Sentinel<T>::value();
+          Sentinel<T>::store(&y[r], b - acc);
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------- tall-skinny kernels
+// One kernel family covers every operation on a block of dense columns:
+// the Gram-Schmidt passes of the Arnoldi step (PargemslrMgs / PargemslrCgs2,
+// ParGeMSLR SRC/matrices/matrixops.cpp:10588-10806), the Woodbury low-rank
+// correction W^T x then WH y (GemslrClass::SolveApplyLowRankLevel,
+// gemslr.cpp:3681-3722) and the solution update x += Z y (fgmres.hpp:483-490).
+//
+//   TS_DOT          sums[c] = V(:,c) . w,            w = in * in_scale
+//   TS_UPDATE       out = in * in_scale + sign * M coef'
+//   TS_UPDATE_DOT   out = w' = (update above); sums[c] = V(:,c) . w'
+//   TS_UPDATE_NORM  out = w' = (update above); sums[0] = w' . w'
+//   TS_NORM_COPY    sums[0] = w . w; out = w (if out)
+// with coef'[c] = coef[c] * msc[c] and msc the lazy column scales of M.
+// Columns are column-major with leading dimension ld.  Each block walks
+// 512-row tiles; per tile, thread t updates row t, then warp w reduces the
+// columns c = w mod 16 over the tile (the tile is re-read from L1/L2, so DRAM
+// sees each column once).  Block partials are combined by the last block to
+// finish, in a fixed order, so results do not depend on block scheduling;
+// that block then runs the epilogue (storing coefficients, or the Givens
+// update of the Hessenberg column).
+enum TsMode { TS_DOT = 0, TS_UPDATE = 1, TS_UPDATE_DOT = 2, TS_UPDATE_NORM = 3, TS_NORM_COPY = 4 };
+enum EpiKind {
+  EPI_NONE = 0,
+  EPI_STORE = 1,       // dst[c] = sums[c] * vsc[c]
+  EPI_CGS_FIRST = 2,   // hcol = coefA = sums * vsc
+  EPI_CGS_SECOND = 3,  // coefB = sums * vsc; hcol += coefB
+  EPI_GIVENS = 4,      // finish column j: norm, rotations, convergence, back-solve
+  EPI_NORMB = 5,       // st->normb = sqrt(sums[0])
+  EPI_INIT = 6,        // outer start of solve: normr, tolr, rs[0], sc[0]
+  EPI_INIT_INNER = 7,  // inner solve from x0 = 0: normb = normr = ||rhs||
+};
+
+template <typename TV, typename TM, typename TW>
+struct TsArgs {
+  int n;
+  int ncols;
+  const int* ncols_dev;  // if set, the column count is read here (<= KMAX)
+  const TV* V;
+  long long ldv;
+  const double* vsc;
+  const TM* M;
+  long long ldm;
+  const double* msc;
+  const double* coef;
+  double sign;
+  const TW* in;          // null: zero input
+  const double* in_scale;
+  TW* out;
+  double* partial;       // [KMAX+1][gridDim.x]
+  unsigned int* counter; // zero between launches
+  int epi;
+  FgmresDev* st;
+  double* dst;
+  int j;
+  Skip skip;
+};
+
+__device__ inline void fgmres_givens(FgmresDev* st, int j, double t) {
+  // H(:, j) from the Gram-Schmidt coefficients and ||w||
+  // (PargemslrMgs sets H(0..k, k) and H(k+1, k), matrixops.cpp:10728-10806)
+  const int ldh = KMAX + 1;
+  double* H = st->H + (size_t)j * ldh;
+  for (int c = 0; c <= j; c++) H[c] = st->hcol[c];
+  H[j + 1] = t;
+  st->sc[j + 1] = 1.0 / t;
+  st->iter += 1;
+  st->i = j + 1;
+  // apply the previous rotations, then form the new one (fgmres.hpp:430-458)
+  for (int k = 1; k <= j; k++) {
+    double hii = H[k - 1];
+    H[k - 1] = st->c[k - 1] * hii + st->s[k - 1] * H[k];
+    H[k] = -st->s[k - 1] * hii + st->c[k - 1] * H[k];
+  }
+  double hii = H[j], hii1 = H[j + 1];
+  double gam = sqrt(fabs(hii) * fabs(hii) + fabs(hii1) * fabs(hii1));
+  if (fabs(gam) < st->eps) {
+    // breakdown: the reference jumps past the solution update (fgmres.hpp:440-443)
+    st->breakdown = 1;
+    st->i = 0;
+    st->cycle_done = 1;
+    st->done = 1;
+    return;
+  }
+  st->c[j] = hii / gam;
+  st->s[j] = hii1 / gam;
+  st->rs[j + 1] = -st->s[j] * st->rs[j];
+  st->rs[j] = st->c[j] * st->rs[j];
+  H[j] = st->c[j] * hii + st->s[j] * hii1;
+  st->normr = fabs(st->rs[j + 1]);
+  const bool conv = st->normr <= st->tolr;
+  if (conv) st->converged = 1;
+  if (conv || st->i >= st->kdim || st->iter >= st->maxits) {
+    st->cycle_done = 1;
+    if (conv || st->iter >= st->maxits) st->done = 1;
+    // back substitution H y = rs, in place in rs (fgmres.hpp:471-480)
+    const int i = st->i;
+    double* rs = st->rs;
+    rs[i - 1] /= st->H[(size_t)(i - 1) * ldh + (i - 1)];
+    for (int k = i - 2; k >= 0; k--) {
+      for (int jj = k + 1; jj < i; jj++) rs[k] -= st->H[(size_t)jj * ldh + k] * rs[jj];
+      rs[k] /= st->H[(size_t)k * ldh + k];
+    }
+  }
+}
+
+template <typename TV, typename TM, typename TW>
+__device__ inline void ts_epilogue(const TsArgs<TV, TM, TW>& a, const double* sums, int ncols) {
+  FgmresDev* st = a.st;
+  switch (a.epi) {
+    case EPI_STORE:
+      for (int c = 0; c < ncols; c++) a.dst[c] = sums[c] * (a.vsc ? a.vsc[c] : 1.0);
+      break;
+    case EPI_CGS_FIRST:
+      for (int c = 0; c < ncols; c++) {
+        double h = sums[c] * (a.vsc ? a.vsc[c] : 1.0);
+        st->hcol[c] = h;
+        st->coefA[c] = h;
+      }
+      break;
+    case EPI_CGS_SECOND:
+      for (int c = 0; c < ncols; c++) {
+        double h = sums[c] * (a.vsc ? a.vsc[c] : 1.0);
+        st->hcol[c] += h;
+        st->coefB[c] = h;
+      }
+      break;
+    case EPI_GIVENS:
+      fgmres_givens(st, a.j, sqrt(sums[0]));
+      break;
+    case EPI_NORMB:
+      st->normb = sqrt(sums[0]);
+      if (st->normb < st->eps) {
+        st->done = 1;
+        st->cycle_done = 1;
+        st->normr = 0.0;
+        st->i = 0;
+      }
+      break;
+    case EPI_INIT: {
+      st->i = 0;
+      st->iter = 0;
+      st->converged = 0;
+      st->breakdown = 0;
+      if (st->done) break;  // zero right-hand side
+      const double normr = sqrt(sums[0]);
+      st->normr = normr;
+      if (normr < st->eps) {
+        st->done = 1;
+        st->cycle_done = 1;
+        st->converged = 1;
+        break;
+      }
+      st->tolr = st->absolute ? st->tol : st->tol * st->normb;
+      st->rs[0] = normr;
+      st->sc[0] = 1.0 / normr;
+      st->cycle_done = 0;
+      break;
+    }
+    case EPI_INIT_INNER: {
+      const double normb = sqrt(sums[0]);
+      st->normb = normb;
+      st->normr = normb;
+      st->i = 0;
+      st->iter = 0;
+      st->converged = 0;
+      st->breakdown = 0;
+      st->done = 0;
+      st->cycle_done = 0;
+      if (normb < st->eps) {
+        st->done = 1;
+        st->cycle_done = 1;
+        break;
+      }
+      st->tolr = st->absolute ? st->tol : st->tol * normb;
+      st->rs[0] = normb;
+      st->sc[0] = 1.0 / normb;
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+template <typename TV, typename TM, typename TW, int MODE>
+__global__ void __launch_bounds__(kTsThreads) ts_kernel(TsArgs<TV, TM, TW> a) {
+  if (a.skip.on()) return;
+  __shared__ double scoef[KMAX + 1];
+  __shared__ double sacc[KMAX + 1];
+  __shared__ double swarp[kTsThreads / 32];
+  __shared__ int s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = kTsThreads / 32;
+  const int ncols = a.ncols_dev ? min(*(const volatile int*)a.ncols_dev, KMAX + 1) : a.ncols;
+  const bool update = MODE == TS_UPDATE || MODE == TS_UPDATE_DOT || MODE == TS_UPDATE_NORM;
+  const bool reduce = MODE != TS_UPDATE;
+  const int nred = (MODE == TS_DOT || MODE == TS_UPDATE_DOT) ? ncols : 1;
+  if (MODE == TS_UPDATE && ncols == 0 && a.in == a.out) return;  // nothing to add
+  const double in_s = a.in_scale ? *a.in_scale : 1.0;
+  for (int c = tid; c <= KMAX; c += kTsThreads) {
+    scoef[c] = (update && c < ncols) ? a.sign * a.coef[c] * (a.msc ? a.msc[c] : 1.0) : 0.0;
+    sacc[c] = 0.0;
+  }
+  if (tid < NW) swarp[tid] = 0.0;
+  __syncthreads();
+  const int ntiles = (a.n + kTsThreads - 1) / kTsThreads;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r0 = tile * kTsThreads;
+    const int row = r0 + tid;
+    double wv = 0.0;
+    if (row < a.n) {
+      wv = a.in ? (double)a.in[row] * in_s : 0.0;
+      if (update) {
+        double acc = 0.0;
+        const TM* m = a.M + row;
+        for (int c = 0; c < ncols; c++) acc += (double)m[(long long)c * a.ldm] * scoef[c];
+        wv += acc;
+      }
+      if (MODE != TS_DOT && a.out) a.out[row] = (TW)wv;
+    }
+    if (MODE == TS_UPDATE_NORM || MODE == TS_NORM_COPY) {
+      double sq = (row < a.n) ? wv * wv : 0.0;
+      if (MODE == TS_UPDATE_NORM) {
+        // the norm of the stored (rounded) vector, as Norm2 of the reference
+        TW stored = (TW)wv;
+        sq = (row < a.n) ? (double)stored * (double)stored : 0.0;
+      }
+      sq = warp_reduce(sq);
+      if (lane == 0) swarp[warp] += sq;  // one writer per slot: deterministic
+    }
+    if (MODE == TS_DOT || MODE == TS_UPDATE_DOT) {
+      __syncthreads();  // out[] of this tile written by the whole block
+      const int nrows_tile = min(kTsThreads, a.n - r0);
+      for (int c = warp; c < ncols; c += NW) {
+        const TV* v = a.V + (long long)c * a.ldv + r0;
+        double acc = 0.0;
+        for (int k = lane; k < nrows_tile; k += 32) {
+          double w = (MODE == TS_DOT) ? (a.in ? (double)a.in[r0 + k] * in_s : 0.0)
+                                      : (double)a.out[r0 + k];
+          acc += (double)v[k] * w;
+        }
+        acc = warp_reduce(acc);
+        if (lane == 0) sacc[c] += acc;
+      }
+      __syncthreads();
+    }
+  }
+  if (!reduce) return;
+  __syncthreads();
+  if ((MODE == TS_UPDATE_NORM || MODE == TS_NORM_COPY) && tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < NW; w++) t += swarp[w];
+    sacc[0] = t;
+  }
+  __syncthreads();
+  // block partials -> global, column-major by block
+  for (int c = tid; c < nred; c += kTsThreads) a.partial[(long long)c * gridDim.x + blockIdx.x] = sacc[c];
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) {
+    unsigned int prev = atomicAdd(a.counter, 1u);
+    s_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int c = warp; c < nred; c += NW) {
+    double acc = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) acc += __ldcg(&a.partial[(long long)c * gridDim.x + b]);
+    acc = warp_reduce(acc);
+    if (lane == 0) sacc[c] = acc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    ts_epilogue(a, sacc, nred);
+    *a.counter = 0u;
+    __threadfence();
+  }
+}
+
+__global__ void fgmres_cycle_reset_kernel(FgmresDev* st, Skip skip) {
+  if (skip.on()) return;
+  st->i = 0;
+  if (st->done) return;
+  st->cycle_done = 0;
+  st->rs[0] = st->normr;
+  st->sc[0] = 1.0 / st->normr;
+}
+
+// --------------------------------------------------- permutation + convert
+// out[i] = (TO)(in[perm[i]] * scale)  (IntVectorClass::GatherPerm, int_vector.cpp:668)
+template <typename TI, typename TO>
+__global__ void gather_kernel(int n, const int* __restrict__ perm, const TI* __restrict__ in,
+                              const double* __restrict__ scale, TO* __restrict__ out, Skip skip) {
+  if (skip.on()) return;
+  const double s = scale ? *scale : 1.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int p = perm ? perm[i] : i;
+    out[i] = scale ? (TO)((double)in[p] * s) : (TO)in[p];
+  }
+}
+
+// out[perm[i]] = in[i]  (IntVectorClass::ScatterRperm, int_vector.cpp:629)
+template <typename TI, typename TO>
+__global__ void scatter_kernel(int n, const int* __restrict__ perm, const TI* __restrict__ in,
+                               TO* __restrict__ out, Skip skip) {
+  if (skip.on()) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int p = perm ? perm[i] : i;
+    out[p] = (TO)in[i];
+  }
+}
+
+template <typename T>
+__global__ void fill_kernel(int n, T v, T* out, Skip skip) {
+  if (skip.on()) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = v;
+}
+
+}  // namespace pgx

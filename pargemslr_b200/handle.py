@@ -1,0 +1,120 @@
+"""Device solve handle: the Python face of the pgx_gemslr_* C ABI."""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from .structures import GemslrStructures
+
+_initialized_device: Optional[int] = None
+
+
+def init(device: int = 0) -> None:
+    global _initialized_device
+    if _initialized_device != device:
+        _abi.check(_abi.lib().pgx_init(device))
+        _initialized_device = device
+
+
+class GemslrHandle:
+    """GeMSLR-preconditioned FGMRES on one GPU, built from post-setup structures.
+
+    precision: ``"fp64"`` (the reference's arithmetic) or ``"mixed"`` (FP32
+    preconditioner apply inside FP64 FGMRES).
+    """
+
+    def __init__(self, st: GemslrStructures, precision: str = "fp64", device: int = 0):
+        init(device)
+        self.n = st.n
+        self.precision = precision
+        prec = {"fp64": _abi.PRECISION_FP64, "mixed": _abi.PRECISION_MIXED}[precision]
+        L = _abi.lib()
+        h = C.c_void_p()
+        _abi.check(L.pgx_gemslr_create(C.byref(h), st.n, prec))
+        self._h = h
+        keep: list = []
+        try:
+            A = _abi.csr_struct(*st.A, keep=keep)
+            _abi.check(L.pgx_gemslr_set_matrix(h, C.byref(A)))
+            pp = np.ascontiguousarray(st.pperm, np.int32)
+            qp = None if st.qperm is None else np.ascontiguousarray(st.qperm, np.int32)
+            keep.extend([pp, qp])
+            _abi.check(L.pgx_gemslr_set_perm(h, _abi.ptr(pp), _abi.ptr(qp)))
+            lp = np.ascontiguousarray(st.lev_ptr, np.int32)
+            keep.append(lp)
+            _abi.check(L.pgx_gemslr_set_levels(h, st.nlev, _abi.ptr(lp)))
+            for l, lv in enumerate(st.levels):
+                desc = _abi.Level()
+                dom = np.ascontiguousarray(lv.dom_ptr, np.int32)
+                dinv = np.ascontiguousarray(lv.dinv, np.float64)
+                keep.extend([dom, dinv])
+                desc.ncomp = lv.ncomp
+                desc.dom_ptr = _abi.ptr(dom)
+                desc.L = _abi.csr_struct(*lv.L, keep=keep)
+                desc.U = _abi.csr_struct(*lv.U, keep=keep)
+                desc.dinv = _abi.ptr(dinv)
+                desc.B = _abi.csr_struct(*lv.B, keep=keep)
+                if lv.E is not None:
+                    desc.E = _abi.csr_struct(*lv.E, keep=keep)
+                    desc.F = _abi.csr_struct(*lv.F, keep=keep)
+                desc.rank = lv.rank
+                if lv.rank > 0:
+                    W = np.ascontiguousarray(lv.W, np.float64)
+                    WH = np.ascontiguousarray(lv.WH, np.float64)
+                    keep.extend([W, WH])
+                    desc.W = _abi.ptr(W)
+                    desc.WH = _abi.ptr(WH)
+                _abi.check(L.pgx_gemslr_set_level(h, l, C.byref(desc)))
+            _abi.check(L.pgx_gemslr_set_inner(h, st.inner_enable, st.inner_maxits, st.inner_tol))
+            _abi.check(L.pgx_gemslr_commit(h))
+        except Exception:
+            L.pgx_gemslr_destroy(h)
+            self._h = None
+            raise
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _abi.lib().pgx_gemslr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_bytes(self, kdim: int) -> int:
+        b = C.c_int64(0)
+        _abi.check(_abi.lib().pgx_gemslr_device_bytes(self._h, kdim, C.byref(b)))
+        return int(b.value)
+
+    def solve(self, b: np.ndarray, x0: Optional[np.ndarray] = None, params: Optional[np.ndarray] = None):
+        """Host-array solve; returns (x, result dict)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        p = None if params is None else np.ascontiguousarray(params, np.float64)
+        res = _abi.Result()
+        rc = _abi.lib().pgx_gemslr_solve(self._h, _abi.ptr(x), _abi.ptr(b), _abi.LOCATION_HOST, _abi.ptr(p),
+                                         C.byref(res))
+        _abi.check(rc)
+        return x, {"iters": res.iters, "rel_res": res.rel_res, "true_rel_res": res.true_rel_res,
+                   "solve_ms": res.solve_ms, "status": res.status}
+
+    def solve_device(self, x_ptr: int, b_ptr: int, params: Optional[np.ndarray] = None):
+        """Solve on device pointers (e.g. torch tensors' data_ptr())."""
+        p = None if params is None else np.ascontiguousarray(params, np.float64)
+        res = _abi.Result()
+        _abi.check(_abi.lib().pgx_gemslr_solve(self._h, x_ptr, b_ptr, _abi.LOCATION_DEVICE, _abi.ptr(p),
+                                               C.byref(res)))
+        return {"iters": res.iters, "rel_res": res.rel_res, "true_rel_res": res.true_rel_res,
+                "solve_ms": res.solve_ms, "status": res.status}
+
+    def apply(self, v: np.ndarray) -> np.ndarray:
+        """z = M^-1 v (one preconditioner application) on host arrays."""
+        v = np.ascontiguousarray(v, np.float64)
+        z = np.zeros(self.n)
+        _abi.check(_abi.lib().pgx_gemslr_precond_apply(self._h, _abi.ptr(z), _abi.ptr(v), _abi.LOCATION_HOST))
+        return z

@@ -1,0 +1,125 @@
+"""Post-setup GeMSLR structures, as the solve phase consumes them.
+
+``GemslrStructures`` holds exactly what GemslrClass::Setup leaves behind for
+the solve (ParGeMSLR SRC/preconditioners/gemslr.cpp:1602-1711): the symmetric
+permutation ``pperm`` (and ``qperm`` when unsymmetric), the level pointers
+``lev_ptr``, per level the subdomain pointers and ILU factors of the block-
+diagonal B_l (L strictly lower, U strictly upper, ``dinv`` the inverse
+diagonal), the unfactored B_l, the coupling blocks E_l / F_l, the low-rank
+bases W_l / WH_l, and the settings of the level-0 inner FGMRES.
+
+Per-subdomain factors are concatenated block-diagonally per level here, which
+is the layout the device solve uses (one level = one triangular system).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from . import pgxd
+
+CsrT = Tuple[np.ndarray, np.ndarray, np.ndarray, int, int]  # rowptr, colidx, values, rows, cols
+
+
+def empty_csr(rows: int, cols: int) -> CsrT:
+    return (np.zeros(rows + 1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float64), rows, cols)
+
+
+def block_diag(blocks: List[CsrT], offsets: List[int], n: int) -> CsrT:
+    """Concatenate square CSR blocks on the diagonal at the given offsets."""
+    rp = np.zeros(n + 1, np.int64)
+    cjs, vas = [], []
+    for (brp, bcj, bva, br, _), off in zip(blocks, offsets):
+        rp[off + 1: off + br + 1] = np.diff(brp)
+        cjs.append(bcj.astype(np.int64) + off)
+        vas.append(bva)
+    rp = np.cumsum(rp)
+    cj = np.concatenate(cjs) if cjs else np.zeros(0, np.int64)
+    va = np.concatenate(vas) if vas else np.zeros(0)
+    # blocks are visited in offset order, so rows come out contiguous
+    return (rp.astype(np.int32), cj.astype(np.int32), va.astype(np.float64), n, n)
+
+
+@dataclass
+class LevelStructures:
+    ncomp: int
+    dom_ptr: np.ndarray           # relative to the level start, ncomp + 1 entries
+    L: CsrT
+    U: CsrT
+    dinv: np.ndarray
+    B: CsrT
+    E: Optional[CsrT] = None
+    F: Optional[CsrT] = None
+    rank: int = 0
+    W: Optional[np.ndarray] = None   # m x rank, column-major (flattened)
+    WH: Optional[np.ndarray] = None
+
+
+@dataclass
+class GemslrStructures:
+    n: int
+    A: CsrT
+    pperm: np.ndarray
+    qperm: Optional[np.ndarray]
+    lev_ptr: np.ndarray
+    levels: List[LevelStructures] = field(default_factory=list)
+    inner_enable: int = 1
+    inner_maxits: int = 5
+    inner_tol: float = 1e-2
+
+    @property
+    def nlev(self) -> int:
+        return len(self.levels)
+
+    def nnz_factors(self) -> int:
+        return int(sum(lv.L[1].size + lv.U[1].size for lv in self.levels))
+
+
+def _csr(d: Dict[str, np.ndarray], name: str) -> CsrT:
+    shape = d[name + ".shape"]
+    return (d[name + ".i"].astype(np.int32), d[name + ".j"].astype(np.int32), d[name + ".a"].astype(np.float64),
+            int(shape[0]), int(shape[1]))
+
+
+def from_dump(path: str) -> GemslrStructures:
+    """Load the structures a reference GemslrClass exported (PGXD container)."""
+    d = pgxd.read(path)
+    n = int(d["n"][0])
+    nlev = int(d["nlev"][0])
+    lev_ptr = d["lev_ptr"].astype(np.int32)
+    qperm = d["qperm"].astype(np.int32) if d["qperm"].size else None
+    st = GemslrStructures(n=n, A=_csr(d, "A"), pperm=d["pperm"].astype(np.int32), qperm=qperm, lev_ptr=lev_ptr,
+                          inner_enable=int(d["inner.enable"][0]), inner_maxits=int(d["inner.maxits"][0]),
+                          inner_tol=float(d["inner.tol"][0]))
+    if int(d["solve_option"][0]) != 0:
+        raise ValueError("only the LU global solve option (the reference default) is supported")
+    for l in range(nlev):
+        pre = f"L{l}."
+        ncomp = int(d[pre + "ncomp"][0])
+        start, end = int(lev_ptr[l]), int(lev_ptr[l + 1])
+        nl = end - start
+        dom = d[pre + "dom_ptr"].astype(np.int64) - start
+        offs = [int(dom[c]) for c in range(ncomp)]
+        Ls, Us, Bs, Ds = [], [], [], []
+        for c in range(ncomp):
+            pc = f"{pre}B{c}."
+            if d[pc + "rperm"].size or d[pc + "cperm"].size:
+                raise ValueError("ILU factors with an internal permutation are not supported")
+            Ls.append(_csr(d, pc + "L"))
+            Us.append(_csr(d, pc + "U"))
+            Bs.append(_csr(d, pc + "A"))
+            Ds.append(d[pc + "D"])
+        lv = LevelStructures(ncomp=ncomp, dom_ptr=dom.astype(np.int32), L=block_diag(Ls, offs, nl),
+                             U=block_diag(Us, offs, nl), dinv=np.concatenate(Ds).astype(np.float64),
+                             B=block_diag(Bs, offs, nl))
+        if l < nlev - 1:
+            lv.E = _csr(d, pre + "E")
+            lv.F = _csr(d, pre + "F")
+            lv.rank = int(d[pre + "lrc"][0])
+            if lv.rank > 0:
+                lv.W = d[pre + "W"].astype(np.float64)
+                lv.WH = d[pre + "WH"].astype(np.float64)
+        st.levels.append(lv)
+    return st

@@ -1,0 +1,106 @@
+"""GPU parity of the GeMSLR-FGMRES solve against the reference CPU solver.
+
+The reference (oracle) runs GemslrClass::Setup and FlexGmresClass::Solve on
+the CPU; its post-setup structures are imported through the C ABI and the
+same right-hand side is solved on the GPU.  Bars (north-star parity):
+  FP64 path:  iterations within +-1 of the reference, FP64 true relative
+              residual <= 1e-8, ||x - x_ref|| / ||x_ref|| <= 1e-6;
+  mixed path: iterations at most 15% above the reference (plus one), FP64
+              true relative residual <= 1e-8.
+"""
+import numpy as np
+import pytest
+
+from pargemslr_b200 import params as P
+from pargemslr_b200 import pgxd
+from pargemslr_b200.structures import from_dump
+from tests import oracle_runs
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    # name: (stencil grid nx ny nz shift ax ay az, workload parameters)
+    "lap2d_64": ((64, 64, 1, 0.0, 0.0, 0.0, 0.0), "lap2d_256"),
+    "lap2d_256": ((256, 256, 1, 0.0, 0.0, 0.0, 0.0), "lap2d_256"),
+    "lap3d_32": ((32, 32, 32, 0.0, 0.0, 0.0, 0.0), "lap3d_128"),
+    "convdiff2d_96": ((96, 96, 1, 0.0, 0.3, -0.2, 0.0), "lap2d_256"),
+}
+
+
+def _run(name, apply_k=0):
+    if not oracle_runs.available():
+        pytest.fail("oracle/_ref/pgx_ref_driver is missing (build it with make -C oracle)")
+    lap, wl = CASES[name]
+    p = P.workload_params(wl)
+    n = lap[0] * lap[1] * lap[2]
+    ref = oracle_runs.run(lap=lap, params=p, xtrue=oracle_runs.x_true(n, seed=7), apply_k=apply_k)
+    return ref, p
+
+
+@pytest.fixture(scope="module")
+def handles():
+    from pargemslr_b200.handle import GemslrHandle
+    cache = {}
+
+    def get(name, precision):
+        key = (name, precision)
+        if key not in cache:
+            ref, p = _run(name, apply_k=2)
+            cache[key] = (GemslrHandle(from_dump(ref["setup"]), precision=precision), ref, p)
+        return cache[key]
+    yield get
+    for h, _, _ in cache.values():
+        h.close()
+
+
+@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32"])
+def test_precond_apply_fp64_matches_reference(handles, name):
+    h, ref, _ = handles(name, "fp64")
+    ap = ref["apply"]
+    n = h.n
+    for k in range(int(ap["k"][0])):
+        v = ap["in"][k * n:(k + 1) * n]
+        z_ref = ap["out"][k * n:(k + 1) * n]
+        z = h.apply(v)
+        err = np.linalg.norm(z - z_ref) / np.linalg.norm(z_ref)
+        assert err <= 1e-9, f"apply {k}: relative difference {err:.3e}"
+
+
+@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32", "convdiff2d_96"])
+def test_solve_fp64_matches_reference(handles, name):
+    h, ref, p = handles(name, "fp64")
+    b = pgxd.read(ref["problem"])["b"]
+    x_ref = ref["solution"]["x"]
+    x, r = h.solve(b, params=p)
+    assert r["status"] == 0
+    assert abs(r["iters"] - ref["iters"]) <= 1, (r["iters"], ref["iters"])
+    assert r["true_rel_res"] <= 1e-8
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32", "convdiff2d_96"])
+def test_solve_mixed_within_budget(handles, name):
+    h, ref, p = handles(name, "mixed")
+    b = pgxd.read(ref["problem"])["b"]
+    x, r = h.solve(b, params=p)
+    assert r["status"] == 0
+    assert r["iters"] <= int(np.floor(1.15 * ref["iters"])) + 1, (r["iters"], ref["iters"])
+    assert r["true_rel_res"] <= 1e-8
+    x_ref = ref["solution"]["x"]
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) <= 1e-6
+
+
+def test_solve_twice_is_identical(handles):
+    h, ref, p = handles("lap2d_64", "fp64")
+    b = pgxd.read(ref["problem"])["b"]
+    x1, r1 = h.solve(b, params=p)
+    x2, r2 = h.solve(b, params=p)
+    assert r1["iters"] == r2["iters"]
+    assert np.array_equal(x1, x2)
+
+
+def test_zero_rhs_returns_zero(handles):
+    h, ref, p = handles("lap2d_64", "fp64")
+    x, r = h.solve(np.zeros(h.n), x0=np.ones(h.n), params=p)
+    assert r["iters"] == 0
+    assert not np.any(x)
