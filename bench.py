@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Benchmark: solves/s of GeMSLR-preconditioned FGMRES on one B200 per rank.
+
+Workload (the headline configuration): 3D 7-point Laplacian on a 128^3 grid
+(2,097,152 unknowns, 14.6M nonzeros, the reference's stencil), b = A x_true
+with x_true = 2u - 1 seeded; 4 GeMSLR levels, ILUT drop 1e-3 / 200 per row,
+rank 16 per level, inner Schur FGMRES on level 0 (tol 1e-2, 5 steps),
+FGMRES(50) to relative residual 1e-8.  The preconditioner is built once by
+this library's host setup (pgx_gemslr_setup, untimed).  A "step" is one
+complete solve from x0 = 0.
+
+  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp64]
+  python bench.py --impl reference ...   (the reference CPU solver, oracle/_ref)
+
+Under torchrun (N > 1) every rank solves its own replica on its own GPU; the
+solve does not shard, so there is no collective in the data path; the
+device time is reduced with MAX over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from pargemslr_b200 import params as P  # noqa: E402
+from pargemslr_b200 import pgxd, problems  # noqa: E402
+
+GRID = (128, 128, 128)
+WORKLOAD = "lap3d_128"
+SEED = 7
+# FGMRES iterations of the reference solver on this workload (measured with
+# oracle/_ref on the same parameters: 39 iterations, 72.9 s single-thread);
+# the CPU sample times the first iterations and scales by this count
+REF_ITERS = 39
+
+
+def metric_name() -> str:
+    return "solves/s (GeMSLR-FGMRES(50), rel-res 1e-8, 3D Laplacian 128^3)"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(prefix="pgx_clocks_", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [t.strip() for t in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.out.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def build_problem():
+    A = problems.laplacian(*GRID)
+    n = A[0].size - 1
+    xt = problems.x_true(n, SEED)
+    b = problems.spmv(A, xt)
+    return A, n, b, xt
+
+
+def cpu_sample(n_threads: int, iters: int, steps: int = 1):
+    """Time the reference CPU solver (oracle/_ref) on the same workload."""
+    driver = os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver")
+    if not os.path.exists(driver):
+        return None, "oracle/_ref/pgx_ref_driver not built"
+    p = P.workload_params(WORKLOAD)
+    out = tempfile.mkdtemp(prefix="pgx_ref_")
+    A, n, b, xt = build_problem()
+    pgxd.write(os.path.join(out, "xtrue.bin"), {"x_true": xt})
+    cmd = [driver, "--out", out, "--lap", *[str(g) for g in GRID], "0", "0", "0", "0", "--xtrue",
+           os.path.join(out, "xtrue.bin"), "--threads", str(n_threads), "--solve", "--max-iters-timed", str(iters),
+           "--repeat", str(steps)]
+    for i, v in enumerate(p):
+        cmd += ["--param", f"{i}={float(v)!r}"]
+    env = dict(os.environ, OMP_NUM_THREADS=str(n_threads), OPENBLAS_NUM_THREADS="1")
+    t0 = time.time()
+    subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
+    wall = time.time() - t0
+    res = {}
+    with open(os.path.join(out, "result.txt")) as f:
+        for line in f:
+            k, v = line.strip().split("=", 1)
+            res[k] = v
+    times = [float(t) for t in res["solve_times"].split(",")]
+    its = int(res["iters"])
+    return {"times": times, "iters": its, "setup_s": float(res["setup_s"]), "wall_s": wall}, None
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    steps = args.warmup + args.steps
+    r, why = cpu_sample(threads, args.ref_iters, steps)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    per_iter = [t / max(r["iters"], 1) for t in r["times"][args.warmup:]]
+    t_solve = statistics.mean(per_iter) * REF_ITERS
+    value = 1.0 / t_solve
+    sample = (f"reference FGMRES+GemslrClass (oracle/_ref), first {r['iters']} iterations of the 128^3 solve per "
+              f"step on {threads} threads, scaled to the full {REF_ITERS}-iteration solve")
+    line = {
+        "impl": "reference", "metric": metric_name(), "value": value, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_solve * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "3D 7-point Laplacian 128^3, 4 levels, ILUT 1e-3/200, rank 16, FGMRES(50), 1e-8",
+                   "setup_s": r["setup_s"]},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_pgx(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from pargemslr_b200.handle import GemslrHandle
+
+    torch.cuda.set_device(local)
+    p = P.workload_params(WORKLOAD)
+    A, n, b, xt = build_problem()
+    t0 = time.time()
+    h = GemslrHandle.from_matrix(A, p, precision=args.precision, device=local)
+    setup_s = time.time() - t0
+    dev = torch.device("cuda", local)
+    b_dev = torch.from_numpy(b).to(dev)
+    x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def device_solve():
+        x_dev.zero_()
+        torch.cuda.synchronize()
+        return h.solve_device(x_dev.data_ptr(), b_dev.data_ptr(), params=p)
+
+    for _ in range(args.warmup):
+        r = device_solve()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    wall0 = time.perf_counter()
+    ms, iters, rel, launches = [], [], [], []
+    for _ in range(args.steps):
+        r = device_solve()
+        ms.append(r["solve_ms"])
+        iters.append(r["iters"])
+        rel.append(r["true_rel_res"])
+        launches.append(r["launches"])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    total_ms = float(sum(ms))
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = world * args.steps / (total_ms / 1e3)
+    x_err = float(np.linalg.norm(x_dev.cpu().numpy() - xt) / np.linalg.norm(xt))
+
+    # end to end through the host-buffer C ABI call, pinned host memory
+    b_host = torch.from_numpy(b).pin_memory()
+    x_host = torch.zeros(n, dtype=torch.float64).pin_memory()
+    e2e_wall = []
+    for _ in range(args.steps):
+        x_host.zero_()
+        t1 = time.perf_counter()
+        h.solve_host_ptr(x_host.data_ptr(), b_host.data_ptr(), params=p)
+        e2e_wall.append(time.perf_counter() - t1)
+    e2e_total = sum(e2e_wall)
+    if world > 1:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    # roofline of the dominant kernel: the level-0 triangular passes
+    lo_ms, lo_bytes = h.kernel_stats(0, 0, reps=5)
+    up_ms, up_bytes = h.kernel_stats(1, 0, reps=5)
+    spmv_ms, spmv_bytes = h.kernel_stats(2, 0, reps=5)
+    peak, peak_kind = measured_peak_hbm()
+    tri_bytes = (lo_bytes + up_bytes) / 2.0
+    tri_ms = (lo_ms + up_ms) / 2.0
+    achieved = tri_bytes / (tri_ms * 1e-3) / 1e9
+    traffic = ncu_traffic()
+    line = {
+        "metric": metric_name(), "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 preconditioner / f64 FGMRES" if args.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": "3D 7-point Laplacian 128^3 (n=2,097,152), 4 levels, ILUT 1e-3/200, rank 16, "
+                               "inner Schur FGMRES(5) tol 1e-2, FGMRES(50) to 1e-8, x0 = 0",
+                   "precision": args.precision, "setup": "pgx_gemslr_setup (this library), untimed",
+                   "setup_s": round(setup_s, 2), "iters": iters[-1], "true_rel_res": rel[-1], "x_err": x_err,
+                   "l2": "inputs larger than L2 (preconditioner %.2f GB)" % (h.device_bytes(50) / 1e9),
+                   "host_wall_s": wall},
+        "e2e": {"value": world * args.steps / e2e_total, "unit": "solves/s", "h2d_bytes_per_step": 16 * n,
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": int(sum(launches)),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "kernel": "trsv_seg_kernel (level-0 ILU L and U passes, mean)",
+                     "bytes_per_launch": tri_bytes, "ms_per_launch": tri_ms,
+                     "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                     "spmv": {"achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "ms": spmv_ms}},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, why = cpu_sample(os.cpu_count() or 1, args.ref_iters, 1)
+        if cpu is None:
+            line["cpu_baseline"] = None
+        else:
+            t_solve = cpu["times"][-1] / max(cpu["iters"], 1) * REF_ITERS
+            line["cpu_baseline"] = {
+                "value": 1.0 / t_solve, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "reference",
+                "sample": f"reference CPU solver (oracle/_ref), first {cpu['iters']} FGMRES iterations of the same "
+                          f"128^3 solve, scaled to its full {REF_ITERS}-iteration solve; reference setup "
+                          f"{cpu['setup_s']:.1f} s untimed"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    h.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["pgx", "reference"], default="pgx")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--ref-iters", type=int, default=3, help="FGMRES iterations in one reference CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_pgx(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -116,6 +116,7 @@ typedef struct {
                              Givens estimate |rs|/||b|| (fgmres.hpp:542) */
    double true_rel_res;   /* ||b - A x||_2 / ||b||_2 computed in FP64 on the GPU */
    double solve_ms;       /* device time of the solve (CUDA events) */
+   int32_t launches;      /* kernels this library launched for the solve */
 } pgx_result;
 
 /* ---- library ----------------------------------------------------------- */
@@ -151,6 +152,20 @@ int pgx_gemslr_set_inner(pgx_handle handle, int32_t enable, int32_t maxits, doub
 int pgx_gemslr_commit(pgx_handle handle);
 int pgx_gemslr_destroy(pgx_handle handle);
 
+/* Build a committed handle from A alone: the host-side GeMSLR setup of this
+ * library (nested-dissection levels, RCM inside subdomains, dual-threshold
+ * ILUT per subdomain, coupling blocks) followed by the low-rank corrections
+ * computed on the GPU by subspace iteration (the reference's option
+ * kGemslrLowrankSubspaceIteration, gemslr.cpp:2592-2656).  params is the
+ * reference's double[180] array; the slots read are NLEV_GLOBAL (20),
+ * ILU_DROPTOL_B/C_GLOBAL (40, 44), ILU_ROWNNZ_B/C_GLOBAL (48, 50),
+ * ILU_PERM_OPTION_GLOBAL (58, 0 = none, otherwise RCM), LR_RANK1/2_GLOBAL
+ * (74, 75), LR_RANK_FACTOR1/2_GLOBAL (78, 79), LR_MAXITS1_GLOBAL (90) and
+ * SCHUR_ENABLE / SCHUR_ITER_TOL / SCHUR_MAXITS (130-132).  Replaces
+ * GemslrClass::Setup (gemslr.cpp:1602-1711) when no reference library is
+ * linked; partitions come from this library's own bisection, not METIS. */
+int pgx_gemslr_setup(pgx_handle *handle, const pgx_csr *A, const double *params, int32_t precision);
+
 /* Bytes of device memory the committed handle holds (factors, matrices,
  * Krylov basis for kdim, work vectors); used for admission control. */
 int pgx_gemslr_device_bytes(pgx_handle handle, int32_t kdim, int64_t *bytes);
@@ -167,6 +182,15 @@ int pgx_gemslr_solve(pgx_handle handle, double *x, const double *b, int32_t loca
 /* Apply the preconditioner once, z = M^-1 v (GemslrClass::Solve,
  * gemslr.cpp:3431-3472), on host or device vectors. */
 int pgx_gemslr_precond_apply(pgx_handle handle, double *z, const double *v, int32_t location);
+
+/* Measurement: average device time (CUDA events on the handle's stream,
+ * over `reps` launches) and algorithmic bytes per launch of one building
+ * block of the solve: which 0 = lower triangular pass of `level`, 1 = upper
+ * triangular pass of `level`, 2 = outer CSR SpMV.  Algorithmic bytes count
+ * every operand once: nnz*(value+index) + row pointers + schedule + vectors
+ * in and out. */
+int pgx_gemslr_kernel_stats(pgx_handle handle, int32_t which, int32_t level, int32_t reps, double *avg_ms,
+                            double *bytes);
 
 /* ---- building blocks (each is also used inside the solve) ---------------
  * The level-set schedule of a unit-lower (uplo 'L') or upper (uplo 'U')

@@ -156,6 +156,7 @@ static void put_csr(Writer &w, const std::string &name, Csr &A)
       return;
    }
    /* CSC -> CSR */
+   w.scalar(name + ".was_csc", 1);
    const int *cp = A.GetI(), *ri = A.GetJ();
    const double *va = A.GetData();
    std::vector<int> ip(nr + 1, 0), jp(nnz);
@@ -270,7 +271,7 @@ static void usage()
 int main(int argc, char **argv)
 {
    std::string out, csr_file, xtrue_file, rhs_file;
-   bool lap = false, do_dump = false, do_solve = false, verbose = false;
+   bool lap = false, do_dump = false, do_solve = false, verbose = false, probe = false;
    int nx = 0, ny = 0, nz = 0, apply_k = 0, repeat = 1, threads = 1, timed_maxits = 0;
    double shift = 0, ax = 0, ay = 0, az = 0;
    std::vector<std::pair<int, double>> overrides;
@@ -300,6 +301,7 @@ int main(int argc, char **argv)
       }
       else if (a == "--dump") do_dump = true;
       else if (a == "--verbose") verbose = true;
+      else if (a == "--probe") probe = true;
       else if (a == "--solve") do_solve = true;
       else if (a == "--apply") { need(1); apply_k = std::atoi(argv[++i]); }
       else if (a == "--repeat") { need(1); repeat = std::max(1, std::atoi(argv[++i])); }
@@ -417,10 +419,36 @@ int main(int argc, char **argv)
       std::fprintf(res, "apply_s=%.9g\n", t_apply);
    }
 
+   if (probe && precond._nlev_used >= 2)
+   {
+      /* pieces of the level-0 inner solve on seeded vectors: the Schur
+       * operator, its preconditioner and the level-1 recursion */
+      std::mt19937_64 gen(777ULL);
+      std::uniform_real_distribution<double> U(-1.0, 1.0);
+      int m0 = n - precond._lev_ptr_v[1];
+      Vec xv, yv;
+      xv.Setup(m0, kMemoryHost, false);
+      yv.Setup(m0, kMemoryHost, false);
+      for (int i = 0; i < m0; i++) xv[i] = U(gen);
+      std::vector<double> xin(xv.GetData(), xv.GetData() + m0);
+      precond.SchurMatVec(0, 'N', 1.0, xv, 0.0, yv);
+      std::vector<double> schur(yv.GetData(), yv.GetData() + m0);
+      precond._inner_iters_matrix.Solve(yv, xv);
+      std::vector<double> ssolve(yv.GetData(), yv.GetData() + m0);
+      precond.SolveLevel(yv, xv, 1);
+      std::vector<double> lev1(yv.GetData(), yv.GetData() + m0);
+      Writer w(out + "/probe.bin");
+      w.f64("x", xin.data(), m0);
+      w.f64("schur", schur.data(), m0);
+      w.f64("schur_solve", ssolve.data(), m0);
+      w.f64("level1", lev1.data(), m0);
+   }
+
    if (do_solve)
    {
       if (timed_maxits > 0) solver.SetMaxNumberIterations(timed_maxits);
       double best = 1e300, total = 0.0;
+      std::string times;
       for (int r = 0; r < repeat; r++)
       {
          x.Fill(0.0);
@@ -429,7 +457,11 @@ int main(int argc, char **argv)
          double dt = now_s() - ts;
          best = std::min(best, dt);
          total += dt;
+         char buf[64];
+         std::snprintf(buf, sizeof(buf), "%s%.9g", r ? "," : "", dt);
+         times += buf;
       }
+      std::fprintf(res, "solve_times=%s\n", times.c_str());
       /* true relative residual in FP64 */
       Vec r;
       r.Setup(n, kMemoryHost, false);

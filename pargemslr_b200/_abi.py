@@ -39,7 +39,7 @@ EXPORTS = (
     "pgx_gemslr_set_levels", "pgx_gemslr_set_level", "pgx_gemslr_set_inner",
     "pgx_gemslr_commit", "pgx_gemslr_destroy", "pgx_gemslr_device_bytes",
     "pgx_gemslr_solve", "pgx_gemslr_precond_apply", "pgx_build_levels",
-    "pgx_csr_spmv_device",
+    "pgx_csr_spmv_device", "pgx_gemslr_setup", "pgx_gemslr_kernel_stats",
 )
 
 
@@ -67,7 +67,7 @@ class Level(C.Structure):
 class Result(C.Structure):
     _fields_ = [
         ("status", C.c_int32), ("iters", C.c_int32), ("rel_res", C.c_double),
-        ("true_rel_res", C.c_double), ("solve_ms", C.c_double),
+        ("true_rel_res", C.c_double), ("solve_ms", C.c_double), ("launches", C.c_int32),
     ]
 
 
@@ -98,6 +98,8 @@ def lib() -> C.CDLL:
     L.pgx_gemslr_precond_apply.argtypes = [vp, vp, vp, i32]
     L.pgx_build_levels.argtypes = [C.c_char, i32, vp, vp, C.POINTER(i32), vp, vp]
     L.pgx_csr_spmv_device.argtypes = [C.POINTER(Csr), dbl, vp, dbl, vp]
+    L.pgx_gemslr_setup.argtypes = [C.POINTER(vp), C.POINTER(Csr), vp, i32]
+    L.pgx_gemslr_kernel_stats.argtypes = [vp, i32, i32, i32, C.POINTER(dbl), C.POINTER(dbl)]
     for name in EXPORTS:
         if name != "pgx_last_error":
             getattr(L, name).restype = C.c_int

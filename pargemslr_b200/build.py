@@ -17,14 +17,14 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libpgx.so")
-SOURCES = [os.path.join(CSRC, "pgx.cu")]
-HEADERS = [os.path.join(CSRC, "pgx_device.cuh"), os.path.join(ROOT, "include", "pgx.h")]
+SOURCES = [os.path.join(CSRC, "pgx.cu"), os.path.join(CSRC, "setup.cpp")]
+HEADERS = [os.path.join(CSRC, "pgx_device.cuh"), os.path.join(CSRC, "pgx_setup.h"), os.path.join(ROOT, "include", "pgx.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
-    "-shared",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-fopenmp",
+    "-shared", "-lgomp",
 ]
 
 

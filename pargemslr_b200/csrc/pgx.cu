@@ -31,6 +31,7 @@
 
 #include "../../include/pgx.h"
 #include "pgx_device.cuh"
+#include "pgx_setup.h"
 
 namespace pgx {
 
@@ -109,7 +110,7 @@ struct HostLevel {
 // ParGeMSLR SRC/preconditioners/ilu.cpp:832-1062).  Lower factors are swept
 // from the first row, upper factors from the last.
 static int build_levels(bool upper, int n, const int* rp, const int* cj, std::vector<int>& level_ptr,
-                        std::vector<int>& order) {
+                        std::vector<int>& order, std::vector<int>* lev_out = nullptr) {
   std::vector<int> lev(n, -1);
   int max_level = 0;
   for (int t = 0; t < n; t++) {
@@ -132,6 +133,7 @@ static int build_levels(bool upper, int n, const int* rp, const int* cj, std::ve
   order.assign(n, 0);
   std::vector<int> pos(level_ptr.begin(), level_ptr.end() - (nlev > 0 ? 1 : 0));
   for (int i = 0; i < n; i++) order[pos[lev[i]]++] = i;
+  if (lev_out) lev_out->swap(lev);
   return PGX_SUCCESS;
 }
 
@@ -213,6 +215,12 @@ struct DTri {
   int *ord = nullptr, *rp = nullptr, *cj = nullptr;
   T* va = nullptr;
   unsigned long long* ticket = nullptr;
+  // segmented schedule (trsv_seg_kernel); seg == false uses trsv_kernel
+  bool seg = false;
+  int nseg = 0;
+  long long nnz_total = 0;  // nonzeros of the factor (without padding)
+  int *seg_row0 = nullptr, *seg_rp0 = nullptr, *seg_nnz0 = nullptr, *seg_lv0 = nullptr, *seg_nlvb = nullptr,
+      *lvb = nullptr;
 };
 
 // persistent grid of the triangular solve: a few warps per group of an
@@ -230,6 +238,7 @@ static int tri_blocks(int ngroups, int nlevels) {
 template <typename T>
 static int upload_tri(Arena& ar, const HostCsr& h, bool upper, DTri<T>& d, cudaStream_t s) {
   d.n = h.rows;
+  d.nnz_total = h.nnz();
   if (d.n == 0) return PGX_SUCCESS;
   std::vector<int> lptr, order;
   PGX_TRY(build_levels(upper, h.rows, h.rp.data(), h.cj.data(), lptr, order));
@@ -267,6 +276,140 @@ static int upload_tri(Arena& ar, const HostCsr& h, bool upper, DTri<T>& d, cudaS
   return PGX_SUCCESS;
 }
 
+// Segmented schedule for trsv_seg_kernel.  Rows of each subdomain, in
+// level-set order, are cut into segments that fit the kernel's shared-memory
+// staging; segments are ordered by (first level, subdomain, position), so a
+// segment depends only on segments before it.  Each per-segment block of the
+// flat arrays starts 16-byte aligned and has a 16-byte multiple length.
+template <typename T>
+static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::vector<int>& dom, DTri<T>& d,
+                          cudaStream_t s) {
+  const int n = h.rows;
+  d.n = n;
+  d.seg = true;
+  d.nnz_total = h.nnz();
+  std::vector<int> lptr, order, lev;
+  PGX_TRY(build_levels(upper, n, h.rp.data(), h.cj.data(), lptr, order, &lev));
+  d.nlevels = (int)lptr.size() - 1;
+  d.S = pick_lanes(h.nnz(), n);
+  const int NNZCAP = SegCfg<T>::nnz - 4, ROWCAP = kSegRows - 4;
+  std::vector<int> cuts = dom;
+  bool cuts_ok = cuts.size() >= 2 && cuts.front() == 0 && cuts.back() == n;
+  for (size_t c = 0; cuts_ok && c + 1 < cuts.size(); c++) cuts_ok = cuts[c] <= cuts[c + 1];
+  if (!cuts_ok) cuts = {0, n};
+  {
+    // the factor must be block diagonal over the subdomains: a segment may only
+    // wait on earlier segments of its own subdomain
+    std::vector<int> comp_of(n);
+    for (size_t c = 0; c + 1 < cuts.size(); c++)
+      for (int r = cuts[c]; r < cuts[c + 1]; r++) comp_of[r] = (int)c;
+    for (int r = 0; r < n; r++)
+      for (int k = h.rp[r]; k < h.rp[r + 1]; k++)
+        if (comp_of[h.cj[k]] != comp_of[r]) {
+          cuts = {0, n};
+          r = n;
+          break;
+        }
+  }
+  struct Seg {
+    int first_level, comp, idx;
+    std::vector<int> rows;
+  };
+  std::vector<Seg> segs;
+  for (size_t c = 0; c + 1 < cuts.size(); c++) {
+    // rows of the subdomain ordered by (level, index): filter the global order
+    Seg cur{-1, (int)c, 0, {}};
+    long long nnz = 0;
+    int idx = 0;
+    for (int p = 0; p < n; p++) {
+      const int r = order[p];
+      if (r < cuts[c] || r >= cuts[c + 1]) continue;
+      const int rn = h.rp[r + 1] - h.rp[r];
+      if (rn > NNZCAP) return fail(PGX_ERROR_INVALID_PARAM, "row %d of a factor has %d entries (> %d)", r, rn, NNZCAP);
+      if ((int)cur.rows.size() == ROWCAP || nnz + rn > NNZCAP) {
+        segs.push_back(std::move(cur));
+        cur = Seg{-1, (int)c, ++idx, {}};
+        nnz = 0;
+      }
+      if (cur.rows.empty()) cur.first_level = lev[r];
+      cur.rows.push_back(r);
+      nnz += rn;
+    }
+    if (!cur.rows.empty()) segs.push_back(std::move(cur));
+  }
+  std::stable_sort(segs.begin(), segs.end(), [](const Seg& a, const Seg& b) {
+    if (a.first_level != b.first_level) return a.first_level < b.first_level;
+    if (a.comp != b.comp) return a.comp < b.comp;
+    return a.idx < b.idx;
+  });
+  d.nseg = (int)segs.size();
+  std::vector<int> seg_of(n, -1), slot_of(n, -1);
+  for (int q = 0; q < d.nseg; q++)
+    for (size_t i = 0; i < segs[q].rows.size(); i++) {
+      seg_of[segs[q].rows[i]] = q;
+      slot_of[segs[q].rows[i]] = (int)i;
+    }
+  auto pad4 = [](std::vector<int>& v, int fill) {
+    while (v.size() % 4) v.push_back(fill);
+  };
+  std::vector<int> ord, rp, cj, lvb, row0(1, 0), rp0(1, 0), nnz0(1, 0), lv0(1, 0), nlvb;
+  std::vector<double> va;
+  for (int q = 0; q < d.nseg; q++) {
+    const Seg& g = segs[q];
+    for (int r : g.rows) ord.push_back(r);
+    pad4(ord, -1);
+    row0.push_back((int)ord.size());
+    int acc = 0;
+    rp.push_back(0);
+    for (int r : g.rows) {
+      for (int k = h.rp[r]; k < h.rp[r + 1]; k++) {
+        const int j = h.cj[k];
+        cj.push_back(seg_of[j] == q ? -(slot_of[j] + 1) : j);
+        va.push_back(h.va[k]);
+      }
+      acc += h.rp[r + 1] - h.rp[r];
+      rp.push_back(acc);
+    }
+    pad4(rp, acc);
+    rp0.push_back((int)rp.size());
+    while (cj.size() % 4) {
+      cj.push_back(0);
+      va.push_back(0.0);
+    }
+    nnz0.push_back((int)cj.size());
+    const int base = (int)lvb.size();
+    lvb.push_back(0);
+    for (size_t i = 1; i < g.rows.size(); i++)
+      if (lev[g.rows[i]] != lev[g.rows[i - 1]]) lvb.push_back((int)i);
+    lvb.push_back((int)g.rows.size());
+    nlvb.push_back((int)lvb.size() - base);
+    pad4(lvb, (int)g.rows.size());
+    lv0.push_back((int)lvb.size());
+  }
+  d.nblocks = std::max(1, std::min(d.nseg, 148));
+  PGX_TRY(ar.upload(&d.ord, ord.data(), ord.size(), s));
+  PGX_TRY(ar.upload(&d.rp, rp.data(), rp.size(), s));
+  PGX_TRY(ar.upload(&d.cj, cj.data(), cj.size(), s));
+  PGX_TRY(ar.upload(&d.va, va.data(), va.size(), s));
+  PGX_TRY(ar.upload(&d.lvb, lvb.data(), lvb.size(), s));
+  PGX_TRY(ar.upload(&d.seg_row0, row0.data(), row0.size(), s));
+  PGX_TRY(ar.upload(&d.seg_rp0, rp0.data(), rp0.size(), s));
+  PGX_TRY(ar.upload(&d.seg_nnz0, nnz0.data(), nnz0.size(), s));
+  PGX_TRY(ar.upload(&d.seg_lv0, lv0.data(), lv0.size(), s));
+  PGX_TRY(ar.upload(&d.seg_nlvb, nlvb.data(), nlvb.size(), s));
+  PGX_TRY(ar.zeros(&d.ticket, 1, s));
+  return PGX_SUCCESS;
+}
+
+// the segmented schedule pays off when segments hold many rows
+static bool want_segments(const HostCsr& h, int nnz_cap) {
+  if (h.rows == 0) return false;
+  int maxlen = 0;
+  for (int r = 0; r < h.rows; r++) maxlen = std::max(maxlen, h.rp[r + 1] - h.rp[r]);
+  const double avg = (double)h.nnz() / h.rows;
+  return maxlen <= nnz_cap - 4 && avg * 32.0 <= (double)nnz_cap;
+}
+
 template <typename P>
 struct DLevel {
   int start = 0, nl = 0, m = 0, rank = 0;
@@ -295,14 +438,6 @@ static inline int grid_for(long long work, int per_block, int cap) {
 }
 
 // ---------------------------------------------------------------- engine
-struct EngineBase {
-  virtual ~EngineBase() {}
-  virtual int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
-                    pgx_result* res) = 0;
-  virtual int apply(double* z, const double* v, int location) = 0;
-  virtual int64_t device_bytes(int kdim) const = 0;
-};
-
 struct Import {
   int n = 0, precision = 0, nlev = 0;
   HostCsr A;
@@ -311,6 +446,17 @@ struct Import {
   int inner_enable = 0, inner_maxits = 5;
   double inner_tol = 1e-2;
 };
+
+struct EngineBase {
+  virtual ~EngineBase() {}
+  virtual int kernel_stats(int which, int level, int reps, double* avg_ms, double* bytes, int* launches) = 0;
+  virtual int build_lowrank_level(Import& im, int l, int k, int its, unsigned long long seed) = 0;
+  virtual int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+                    pgx_result* res) = 0;
+  virtual int apply(double* z, const double* v, int location) = 0;
+  virtual int64_t device_bytes(int kdim) const = 0;
+};
+
 
 template <typename P>
 struct Engine : EngineBase {
@@ -342,6 +488,7 @@ struct Engine : EngineBase {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // one FGMRES restart cycle captured as a CUDA graph, keyed by its arguments
   cudaGraphExec_t cycle_exec = nullptr;
+  int cycle_nodes = 0;  // kernels in one captured cycle
   int g_kdim = -1;
   const void *g_x = nullptr, *g_b = nullptr;
 
@@ -361,6 +508,22 @@ struct Engine : EngineBase {
     if (stream) cudaStreamDestroy(stream);
   }
 
+  bool use_seg = true;
+
+  int set_seg_smem() {
+    const int bytes = (int)SegCfg<P>::bytes;
+#define PGX_SEGATTR(SS)                                                                                     \
+  PGX_CUDA(cudaFuncSetAttribute(trsv_seg_kernel<P, SS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); \
+  PGX_CUDA(cudaFuncSetAttribute(trsv_seg_kernel<P, SS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))
+    PGX_SEGATTR(2);
+    PGX_SEGATTR(4);
+    PGX_SEGATTR(8);
+    PGX_SEGATTR(16);
+    PGX_SEGATTR(32);
+#undef PGX_SEGATTR
+    return PGX_SUCCESS;
+  }
+
   int64_t device_bytes(int kdim) const override {
     int64_t b = (int64_t)ar.bytes;
     b += (int64_t)n * (kdim + 1) * (sizeof(double) + sizeof(P));
@@ -369,6 +532,7 @@ struct Engine : EngineBase {
 
   // ------------------------------------------------------------ commit
   int commit(Import& im) {
+    PGX_TRY(set_seg_smem());
     n = im.n;
     nlev = im.nlev;
     lev_ptr = im.lev_ptr;
@@ -385,8 +549,13 @@ struct Engine : EngineBase {
       d.start = lev_ptr[l];
       d.nl = lev_ptr[l + 1] - lev_ptr[l];
       d.m = n - lev_ptr[l + 1];
-      PGX_TRY(upload_tri(ar, h.L, false, d.L, stream));
-      PGX_TRY(upload_tri(ar, h.U, true, d.U, stream));
+      if (use_seg && want_segments(h.L, SegCfg<P>::nnz) && want_segments(h.U, SegCfg<P>::nnz)) {
+        PGX_TRY(upload_tri_seg(ar, h.L, false, h.dom_ptr, d.L, stream));
+        PGX_TRY(upload_tri_seg(ar, h.U, true, h.dom_ptr, d.U, stream));
+      } else {
+        PGX_TRY(upload_tri(ar, h.L, false, d.L, stream));
+        PGX_TRY(upload_tri(ar, h.U, true, d.U, stream));
+      }
       PGX_TRY(ar.upload(&d.dinv, h.dinv.data(), h.dinv.size(), stream));
       PGX_TRY(ar.alloc(&d.y, (size_t)d.nl));
       sentinel_fill_kernel<P><<<grid_for(d.nl, 256, 148 * 8), 256, 0, stream>>>(d.nl, d.y);
@@ -437,19 +606,19 @@ struct Engine : EngineBase {
     return PGX_SUCCESS;
   }
 
-  // C0 = the matrix of GemslrClass::CMatVec(0) (gemslr.cpp:3962-4080): the
-  // unfactored B_j blocks of levels j >= 1 on the diagonal, E_j / F_j of the
-  // non-last levels j >= 1 off the diagonal, in the local numbering of the
-  // trailing m_0 unknowns.
-  int assemble_c0(Import& im) {
-    const int base = lev_ptr[1];
-    const int m0 = n - base;
-    std::vector<std::vector<std::pair<int, double>>> rows(m0);
+  // C_l = the matrix of GemslrClass::CMatVec(l) (gemslr.cpp:3962-4080): the
+  // unfactored B_j blocks of levels j > l on the diagonal, E_j / F_j of the
+  // non-last levels j > l off the diagonal, in the local numbering of the
+  // trailing m_l unknowns.
+  int assemble_c(Import& im, int l, DCsr<P>& out) {
+    const int base = lev_ptr[l + 1];
+    const int m = n - base;
+    std::vector<std::vector<std::pair<int, double>>> rows(m);
     auto add = [&](const HostCsr& M, int roff, int coff) {
       for (int r = 0; r < M.rows; r++)
         for (int k = M.rp[r]; k < M.rp[r + 1]; k++) rows[roff + r].push_back({coff + M.cj[k], M.va[k]});
     };
-    for (int j = 1; j < nlev; j++) {
+    for (int j = l + 1; j < nlev; j++) {
       const HostLevel& h = im.levels[j];
       const int o = lev_ptr[j] - base, o1 = lev_ptr[j + 1] - base;
       add(h.B, o, o);
@@ -459,9 +628,9 @@ struct Engine : EngineBase {
       }
     }
     HostCsr c;
-    c.rows = c.cols = m0;
-    c.rp.assign(m0 + 1, 0);
-    for (int r = 0; r < m0; r++) {
+    c.rows = c.cols = m;
+    c.rp.assign(m + 1, 0);
+    for (int r = 0; r < m; r++) {
       std::sort(rows[r].begin(), rows[r].end());
       for (auto& e : rows[r]) {
         c.cj.push_back(e.first);
@@ -469,7 +638,149 @@ struct Engine : EngineBase {
       }
       c.rp[r + 1] = (int)c.cj.size();
     }
-    return upload_csr(ar, c, C0, stream);
+    return upload_csr(ar, c, out, stream);
+  }
+  int assemble_c0(Import& im) { return assemble_c(im, 0, C0); }
+
+  // replace the low-rank correction of level l
+  int set_lowrank(int l, const std::vector<double>& W, const std::vector<double>& WH, int rank) {
+    DLevel<P>& d = lv[l];
+    d.rank = rank;
+    if (rank > 0) {
+      PGX_TRY(ar.upload(&d.W, W.data(), W.size(), stream));
+      PGX_TRY(ar.upload(&d.WH, WH.data(), WH.size(), stream));
+    }
+    return PGX_SUCCESS;
+  }
+
+  // y = (I - C_l C~_l^-1) x + E_l B_l^-1 F_l C~_l^-1 x, the operator whose
+  // dominant invariant subspace gives the level's low-rank correction
+  // (GemslrClass::EBFCMatVec, gemslr.cpp:3737-3797).  C~_l^-1 is the
+  // preconditioner of the lower levels, SolveLevel(l+1).
+  void apply_ebfc(int l, const DCsr<P>& Cl, const P* x, P* y, P* tm, P* tu, P* tw) {
+    DLevel<P>& d = lv[l];
+    Skip sk = mk_skip();
+    solve_level(l + 1, tm, x, sk);
+    spmv<P, P, P, P>(Cl, tm, (P)-1, nullptr, nullptr, (P)0, x, (P)1, y, nullptr, sk);
+    spmv<P, P, P, P>(d.F, tm, (P)1, nullptr, nullptr, (P)0, (const P*)nullptr, (P)0, tu, nullptr, sk);
+    solve_b(l, tu, nullptr, tw, sk);
+    spmv<P, P, P, P>(d.E, tw, (P)1, nullptr, nullptr, (P)0, y, (P)1, y, nullptr, sk);
+  }
+
+  // Low-rank correction of level l by subspace iteration
+  // (PargemslrSubSpaceIteration, matrixops.cpp:8999-9180, kept-all branch of
+  // SetupLowRankBuildLowRank, gemslr.cpp:3059-3150): Q = orth(B); B = G Q,
+  // its times; then H = Q^T G Q, W = Q, WH = Q ((I - H)^-1 - I).
+  int build_lowrank(Import& im, int l, int k, int its, unsigned long long seed, std::vector<double>& W,
+                    std::vector<double>& WH, int& rank) {
+    DLevel<P>& d = lv[l];
+    const int m = d.m;
+    rank = 0;
+    k = std::min(k, m);
+    if (k <= 0) return PGX_SUCCESS;
+    DCsr<P> Cl;
+    Arena tmp;
+    P *Qd = nullptr, *Bd = nullptr, *tm = nullptr, *tu = nullptr, *tw = nullptr;
+    {
+      // C_l lives in the handle arena only for the duration of the build
+      PGX_TRY(assemble_c(im, l, Cl));
+    }
+    PGX_TRY(tmp.alloc(&Qd, (size_t)m * k));
+    PGX_TRY(tmp.alloc(&Bd, (size_t)m * k));
+    PGX_TRY(tmp.alloc(&tm, (size_t)m));
+    PGX_TRY(tmp.alloc(&tu, (size_t)d.nl));
+    PGX_TRY(tmp.alloc(&tw, (size_t)d.nl));
+    std::vector<double> B((size_t)m * k), Q((size_t)m * k);
+    unsigned long long st = seed ? seed : 0x9E3779B97F4A7C15ULL;
+    for (auto& v : B) {  // uniform [0, 1) from a 64-bit xorshift*
+      st ^= st >> 12;
+      st ^= st << 25;
+      st ^= st >> 27;
+      v = (double)((st * 0x2545F4914F6CDD1DULL) >> 11) * (1.0 / 9007199254740992.0);
+    }
+    std::vector<P> buf((size_t)m * k);
+    int kk = k;
+    for (int it = 0; it < std::max(its, 1); it++) {
+      // Q = orth(B) by classical Gram-Schmidt with re-orthogonalisation
+      Q = B;
+      kk = k;
+      for (int c = 0; c < kk; c++) {
+        double* q = &Q[(size_t)c * m];
+        for (int pass = 0; pass < 2; pass++)
+          for (int p = 0; p < c; p++) {
+            const double* qp = &Q[(size_t)p * m];
+            double h = 0.0;
+            for (int i = 0; i < m; i++) h += qp[i] * q[i];
+            for (int i = 0; i < m; i++) q[i] -= h * qp[i];
+          }
+        double nr = 0.0;
+        for (int i = 0; i < m; i++) nr += q[i] * q[i];
+        nr = std::sqrt(nr);
+        if (!(nr > 1e-13)) {  // numerically dependent: stop at this rank
+          kk = c;
+          break;
+        }
+        for (int i = 0; i < m; i++) q[i] /= nr;
+      }
+      if (kk == 0) return PGX_SUCCESS;
+      for (size_t i = 0; i < (size_t)m * kk; i++) buf[i] = (P)Q[i];
+      PGX_CUDA(cudaMemcpyAsync(Qd, buf.data(), sizeof(P) * (size_t)m * kk, cudaMemcpyHostToDevice, stream));
+      for (int c = 0; c < kk; c++) apply_ebfc(l, Cl, Qd + (size_t)c * m, Bd + (size_t)c * m, tm, tu, tw);
+      PGX_CUDA(cudaGetLastError());
+      PGX_CUDA(cudaMemcpyAsync(buf.data(), Bd, sizeof(P) * (size_t)m * kk, cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaStreamSynchronize(stream));
+      for (size_t i = 0; i < (size_t)m * kk; i++) B[i] = (double)buf[i];
+      PGX_TRY(check_err());
+    }
+    // H = Q^T B; R = (I - H)^-1 - I via LU with partial pivoting
+    std::vector<double> H((size_t)kk * kk), Rm((size_t)kk * kk), inv((size_t)kk * kk, 0.0);
+    for (int a = 0; a < kk; a++)
+      for (int b = 0; b < kk; b++) {
+        double h = 0.0;
+        for (int i = 0; i < m; i++) h += Q[(size_t)a * m + i] * B[(size_t)b * m + i];
+        H[(size_t)b * kk + a] = h;  // column-major
+      }
+    for (int a = 0; a < kk; a++)
+      for (int b = 0; b < kk; b++) Rm[(size_t)b * kk + a] = (a == b ? 1.0 : 0.0) - H[(size_t)b * kk + a];
+    for (int a = 0; a < kk; a++) inv[(size_t)a * kk + a] = 1.0;
+    for (int c = 0; c < kk; c++) {
+      int piv = c;
+      for (int r = c + 1; r < kk; r++)
+        if (std::fabs(Rm[(size_t)c * kk + r]) > std::fabs(Rm[(size_t)c * kk + piv])) piv = r;
+      if (Rm[(size_t)c * kk + piv] == 0.0) return fail(PGX_ERROR_FUNCTION_CALL, "low-rank: I - H is singular");
+      if (piv != c)
+        for (int b = 0; b < kk; b++) {
+          std::swap(Rm[(size_t)b * kk + c], Rm[(size_t)b * kk + piv]);
+          std::swap(inv[(size_t)b * kk + c], inv[(size_t)b * kk + piv]);
+        }
+      const double dv = Rm[(size_t)c * kk + c];
+      for (int b = 0; b < kk; b++) {
+        Rm[(size_t)b * kk + c] /= dv;
+        inv[(size_t)b * kk + c] /= dv;
+      }
+      for (int r = 0; r < kk; r++) {
+        if (r == c) continue;
+        const double f = Rm[(size_t)c * kk + r];
+        if (f == 0.0) continue;
+        for (int b = 0; b < kk; b++) {
+          Rm[(size_t)b * kk + r] -= f * Rm[(size_t)b * kk + c];
+          inv[(size_t)b * kk + r] -= f * inv[(size_t)b * kk + c];
+        }
+      }
+    }
+    for (int a = 0; a < kk; a++) inv[(size_t)a * kk + a] -= 1.0;
+    W.assign(Q.begin(), Q.begin() + (size_t)m * kk);
+    WH.assign((size_t)m * kk, 0.0);
+    for (int b = 0; b < kk; b++)
+      for (int a = 0; a < kk; a++) {
+        const double r = inv[(size_t)b * kk + a];
+        if (r == 0.0) continue;
+        const double* q = &Q[(size_t)a * m];
+        double* w = &WH[(size_t)b * m];
+        for (int i = 0; i < m; i++) w[i] += q[i] * r;
+      }
+    rank = kk;
+    return PGX_SUCCESS;
   }
 
   int ensure_krylov(int kdim) {
@@ -511,6 +822,27 @@ struct Engine : EngineBase {
   void trsv(const DTri<P>& T, bool upper, const P* dinv, const P* rhs, const double* rhs_scale, P* y, P* x,
             Skip sk) {
     if (T.n == 0) return;
+    if (T.seg) {
+      const size_t bytes = SegCfg<P>::bytes;
+#define PGX_TRSVSEG(SS)                                                                                       \
+  if (upper)                                                                                                  \
+    trsv_seg_kernel<P, SS, true><<<T.nblocks, kSegThreads, bytes, stream>>>(                                  \
+        T.n, T.nseg, T.seg_row0, T.seg_rp0, T.seg_nnz0, T.seg_lv0, T.seg_nlvb, T.ord, T.rp, T.cj, T.va, T.lvb,  \
+        dinv, rhs, rhs_scale, y, x, T.ticket, err, sk);                                                       \
+  else                                                                                                        \
+    trsv_seg_kernel<P, SS, false><<<T.nblocks, kSegThreads, bytes, stream>>>(                                 \
+        T.n, T.nseg, T.seg_row0, T.seg_rp0, T.seg_nnz0, T.seg_lv0, T.seg_nlvb, T.ord, T.rp, T.cj, T.va, T.lvb,  \
+        dinv, rhs, rhs_scale, y, x, T.ticket, err, sk)
+      switch (T.S) {
+        case 2: PGX_TRSVSEG(2); break;
+        case 4: PGX_TRSVSEG(4); break;
+        case 8: PGX_TRSVSEG(8); break;
+        case 16: PGX_TRSVSEG(16); break;
+        default: PGX_TRSVSEG(32); break;
+      }
+#undef PGX_TRSVSEG
+      return;
+    }
 #define PGX_TRSV(SS)                                                                                   \
   if (upper)                                                                                           \
     trsv_kernel<P, SS, true><<<T.nblocks, 256, 0, stream>>>(T.n, T.ngroups, T.ord, T.rp, T.cj, T.va,    \
@@ -709,6 +1041,70 @@ struct Engine : EngineBase {
     return PGX_SUCCESS;
   }
 
+  // Device time of one building block, measured with CUDA events on the
+  // handle's stream over `reps` launches, and its algorithmic bytes per
+  // launch (every operand read or written once):
+  //   which 0: lower triangular pass of level `level`
+  //   which 1: upper triangular pass of level `level`
+  //   which 2: outer SpMV w = A z
+  int kernel_stats(int which, int level, int reps, double* avg_ms, double* bytes, int* launches) override {
+    if (reps < 1) reps = 1;
+    if (which < 0 || which > 2) return fail(PGX_ERROR_INVALID_OPTION, "unknown kernel %d", which);
+    if ((which <= 1) && (level < 0 || level >= nlev)) return fail(PGX_ERROR_INVALID_PARAM, "level out of range");
+    PGX_TRY(ensure_krylov(1));
+    Skip sk = mk_skip();
+    const double vb = sizeof(P);
+    float total = 0.f;
+    if (which <= 1) {
+      DLevel<P>& d = lv[level];
+      const DTri<P>& T = which == 0 ? d.L : d.U;
+      const double nnz = (double)(which == 0 ? d.L.nnz_total : d.U.nnz_total);
+      *bytes = nnz * (vb + 4.0) + 4.0 * (d.nl + 1) + 4.0 * d.nl + 2.0 * vb * d.nl + (which == 1 ? vb * d.nl : 0.0);
+      *launches = T.n > 0 ? 1 : 0;
+      // lower and upper passes alternate so the sentinel protocol stays valid;
+      // the events bracket only the pass being measured
+      for (int r = 0; r < reps; r++) {
+        if (which == 0) PGX_CUDA(cudaEventRecord(ev0, stream));
+        trsv(d.L, false, nullptr, rt, nullptr, d.y, xt, sk);
+        if (which == 0) PGX_CUDA(cudaEventRecord(ev1, stream));
+        if (which == 1) PGX_CUDA(cudaEventRecord(ev0, stream));
+        trsv(d.U, true, d.dinv, nullptr, nullptr, d.y, xt, sk);
+        if (which == 1) PGX_CUDA(cudaEventRecord(ev1, stream));
+        PGX_CUDA(cudaStreamSynchronize(stream));
+        float ms = 0.f;
+        PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        total += ms;
+      }
+    } else {
+      *bytes = (double)A.nnz * (sizeof(double) + 4.0) + 4.0 * (n + 1) + (double)n * (sizeof(P) + sizeof(double));
+      *launches = 1;
+      for (int r = 0; r < reps; r++) {
+        PGX_CUDA(cudaEventRecord(ev0, stream));
+        spmv<double, P, double, double>(A, Z, 1.0, nullptr, nullptr, 0.0, (const double*)nullptr, 0.0, V,
+                                        nullptr, sk);
+        PGX_CUDA(cudaEventRecord(ev1, stream));
+        PGX_CUDA(cudaStreamSynchronize(stream));
+        float ms = 0.f;
+        PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        total += ms;
+      }
+    }
+    PGX_TRY(check_err());
+    *avg_ms = total / reps;
+    return PGX_SUCCESS;
+  }
+
+  int build_lowrank_level(Import& im, int l, int k, int its, unsigned long long seed) override {
+    std::vector<double> W, WH;
+    int rank = 0;
+    PGX_TRY(build_lowrank(im, l, k, its, seed, W, WH, rank));
+    PGX_TRY(set_lowrank(l, W, WH, rank));
+    im.levels[l].rank = rank;
+    im.levels[l].W.swap(W);
+    im.levels[l].WH.swap(WH);
+    return PGX_SUCCESS;
+  }
+
   int apply(double* z, const double* v, int location) override {
     const double* vin = v;
     double* zout = z;
@@ -806,6 +1202,9 @@ struct Engine : EngineBase {
       enqueue_cycle(kdim, xd, bd);
       cudaError_t ce = cudaStreamEndCapture(stream, &g);
       if (ce != cudaSuccess) return fail(PGX_ERROR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      size_t nodes = 0;
+      cudaGraphGetNodes(g, nullptr, &nodes);
+      cycle_nodes = (int)nodes;
       ce = cudaGraphInstantiate(&cycle_exec, g, 0);
       cudaGraphDestroy(g);
       if (ce != cudaSuccess) {
@@ -816,8 +1215,10 @@ struct Engine : EngineBase {
       g_x = xd;
       g_b = bd;
     }
+    int launches = 5;  // ||b||, residual, ||r0||, final residual and its norm
     for (int cyc = 0; cyc < max_cycles; cyc++) {
       PGX_CUDA(cudaGraphLaunch(cycle_exec, stream));
+      launches += cycle_nodes;
       FgmresDev hs;
       PGX_CUDA(cudaMemcpyAsync(&hs, st, head, cudaMemcpyDeviceToHost, stream));
       PGX_CUDA(cudaStreamSynchronize(stream));
@@ -854,6 +1255,7 @@ struct Engine : EngineBase {
       res->rel_res = hs.normb > 0 ? hs.normr / hs.normb : 0.0;
       res->true_rel_res = hs.normb > 0 ? sqrt(r2) / hs.normb : 0.0;
       res->solve_ms = ms;
+      res->launches = launches;
     }
     if (rc == PGX_SUCCESS && !(std::isfinite(hs.normr)))
       return fail(PGX_ERROR_NOT_FINITE, "FGMRES residual is not finite");
@@ -1020,6 +1422,122 @@ int pgx_gemslr_commit(pgx_handle h) {
   return PGX_SUCCESS;
 }
 
+// ------------------------------------------------------------ host setup
+static void append_block(HostCsr& dst, const setup::Csr& b, int off) {
+  for (int r = 0; r < b.rows; r++) {
+    for (int k = b.rp[r]; k < b.rp[r + 1]; k++) {
+      dst.cj.push_back(b.cj[k] + off);
+      dst.va.push_back(b.va[k]);
+    }
+    dst.rp.push_back((int)dst.cj.size());
+  }
+}
+
+static HostCsr to_host(const setup::Csr& b) {
+  HostCsr h;
+  h.rows = b.rows;
+  h.cols = b.cols;
+  h.rp = b.rp;
+  h.cj = b.cj;
+  h.va = b.va;
+  return h;
+}
+
+int pgx_gemslr_setup(pgx_handle* handle, const pgx_csr* A, const double* params, int32_t precision) {
+  if (!handle || !A || !params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  *handle = nullptr;
+  if (A->rows != A->cols) return fail(PGX_ERROR_INVALID_PARAM, "A must be square");
+  pgx_handle h = nullptr;
+  PGX_TRY(pgx_gemslr_create(&h, A->rows, precision));
+  std::unique_ptr<pgx_gemslr_s> guard(h);
+  Import& im = h->im;
+  PGX_TRY(copy_csr(A, im.A, "A"));
+  const int n = im.n;
+  // parameters (PARGEMSLR_IO_* slots, SRC/utils/utils.hpp:77-297)
+  const int nlev_req = std::max(1, (int)params[20]);
+  const int perm_opt = (int)params[58];
+  const double tolB = params[40], tolC = params[44];
+  const int lfilB = std::max(1, (int)params[48]), lfilC = std::max(1, (int)params[50]);
+  const int rank1 = std::max(0, (int)params[74]), rank2 = std::max(0, (int)params[75]);
+  const double rfac1 = params[78] > 0 ? params[78] : 1.0, rfac2 = params[79] > 0 ? params[79] : 1.0;
+  const int lr_its = std::max(1, (int)params[90]);
+  im.inner_enable = params[130] != 0.0;
+  im.inner_tol = params[131];
+  im.inner_maxits = std::max(1, (int)params[132]);
+  if (im.inner_maxits > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "inner maxits above %d", KMAX);
+  // 1. levels and ordering
+  setup::Graph g = setup::symmetric_graph(n, im.A.rp.data(), im.A.cj.data());
+  setup::Ordering ord = setup::gemslr_ordering(g, nlev_req, 10, perm_opt != 0);
+  const int nlev = (int)ord.lev_ptr.size() - 1;
+  std::vector<int> iperm(n);
+  for (int i = 0; i < n; i++) iperm[ord.perm[i]] = i;
+  im.pperm = ord.perm;
+  im.qperm.clear();
+  PGX_TRY(pgx_gemslr_set_levels(h, nlev, ord.lev_ptr.data()));
+  // 2. blocks and ILUT factors per level (subdomains in parallel)
+  for (int l = 0; l < nlev; l++) {
+    HostLevel& hl = im.levels[l];
+    const int start = ord.lev_ptr[l], end = ord.lev_ptr[l + 1], nl = end - start;
+    const std::vector<int>& dom = ord.dom_ptr[l];
+    const int ncomp = (int)dom.size() - 1;
+    const bool last = l == nlev - 1;
+    std::vector<setup::Csr> B(ncomp);
+    std::vector<setup::Factor> F(ncomp);
+    std::vector<int> rc(ncomp, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < ncomp; c++) {
+      const int r0 = start + dom[c], r1 = start + dom[c + 1];
+      B[c] = setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm, r0, r1, r0, r1);
+      rc[c] = setup::ilut(B[c].rows, B[c].rp.data(), B[c].cj.data(), B[c].va.data(), last ? tolC : tolB,
+                          last ? lfilC : lfilB, F[c]);
+    }
+    for (int c = 0; c < ncomp; c++)
+      if (rc[c]) return fail(PGX_ERROR_ILU_EMPTY_ROW, "ILUT met an empty row (level %d, subdomain %d)", l, c);
+    hl.ncomp = ncomp;
+    hl.dom_ptr = dom;
+    hl.L = HostCsr();
+    hl.U = HostCsr();
+    hl.B = HostCsr();
+    for (HostCsr* M : {&hl.L, &hl.U, &hl.B}) {
+      M->rows = M->cols = nl;
+      M->rp.assign(1, 0);
+    }
+    hl.dinv.clear();
+    for (int c = 0; c < ncomp; c++) {
+      append_block(hl.L, F[c].L, dom[c]);
+      append_block(hl.U, F[c].U, dom[c]);
+      append_block(hl.B, B[c], dom[c]);
+      hl.dinv.insert(hl.dinv.end(), F[c].dinv.begin(), F[c].dinv.end());
+    }
+    if (!last) {
+      hl.E = to_host(setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm, end,
+                                           n, start, end));
+      hl.F = to_host(setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm,
+                                           start, end, end, n));
+    }
+    hl.rank = 0;
+    hl.set = true;
+  }
+  // 3. low-rank corrections, bottom-up, on the GPU in FP64
+  PGX_CUDA(cudaSetDevice(h->device));
+  if (nlev >= 2 && (rank1 > 0 || rank2 > 0)) {
+    const int inner = im.inner_enable;
+    im.inner_enable = 0;
+    auto* e = new Engine<double>();
+    std::unique_ptr<EngineBase> eng(e);
+    PGX_TRY(e->commit(im));
+    for (int l = nlev - 2; l >= 0; l--) {
+      const int k = (int)((l == 0 ? rank1 : rank2) * (l == 0 ? rfac1 : rfac2));
+      PGX_TRY(e->build_lowrank_level(im, l, k, lr_its, 0x5EEDULL + (unsigned long long)l));
+    }
+    im.inner_enable = inner;
+  }
+  // 4. the solve engine in the requested precision
+  PGX_TRY(pgx_gemslr_commit(h));
+  *handle = guard.release();
+  return PGX_SUCCESS;
+}
+
 int pgx_gemslr_destroy(pgx_handle h) {
   if (!h) return PGX_SUCCESS;
   cudaSetDevice(h->device);
@@ -1061,6 +1579,15 @@ int pgx_gemslr_precond_apply(pgx_handle h, double* z, const double* v, int32_t l
   if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "apply before commit");
   PGX_CUDA(cudaSetDevice(h->device));
   return h->eng->apply(z, v, location);
+}
+
+int pgx_gemslr_kernel_stats(pgx_handle h, int32_t which, int32_t level, int32_t reps, double* avg_ms,
+                            double* bytes) {
+  if (!h || !avg_ms || !bytes) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+  PGX_CUDA(cudaSetDevice(h->device));
+  int launches = 0;
+  return h->eng->kernel_stats(which, level, reps, avg_ms, bytes, &launches);
 }
 
 int pgx_build_levels(char uplo, int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_t* nlevels,

@@ -237,6 +237,181 @@ __global__ void __launch_bounds__(256) trsv_kernel(
   }
 }
 
+// ------------------------------------- segmented (CTA-local) triangular solve
+// Same arithmetic as trsv_kernel, different schedule.  Each subdomain's rows,
+// in level-set order, are cut into segments of at most kSegRows rows and
+// kSegNnz nonzeros.  A CTA claims a segment (ticket order: by first level,
+// then subdomain, so a segment only depends on segments claimed earlier),
+// stages the segment's row list, row pointers, column indices and values into
+// shared memory with cp.async, then sweeps the segment's levels with one
+// __syncthreads per level.  Dependencies inside the segment are read from the
+// shared-memory copy of the results (column index encoded as -(slot+1));
+// dependencies on earlier segments are polled in global memory through the
+// sentinel protocol of trsv_kernel.  Every result is also published to global
+// memory for later segments and the next kernel.
+constexpr int kSegThreads = 1024;
+constexpr int kSegRows = 1024;
+constexpr int kSegNnzF64 = 8192;    // staged cj + va + gathered operands: 160 KB (FP64)
+constexpr int kSegNnzF32 = 12288;   // 144 KB (FP32)
+
+template <typename T>
+struct SegCfg {
+  static constexpr int nnz = sizeof(T) == 8 ? kSegNnzF64 : kSegNnzF32;
+  // smem layout: xs[kSegRows] T | sb[kSegRows] T | sd[kSegRows] T | va[nnz] T | ext[nnz] T |
+  // cj[nnz] int | ord[kSegRows] int | rp[kSegRows+4] int | lvb[kSegRows+4] int; the host keeps
+  // segments within kSegRows-4 rows and nnz-4 nonzeros
+  static constexpr size_t bytes =
+      sizeof(T) * (size_t)(3 * kSegRows + 2 * nnz) + sizeof(int) * (size_t)(nnz + kSegRows + 2 * (kSegRows + 4));
+};
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// copy `bytes` (multiple of 16, both addresses 16-byte aligned) with cp.async
+__device__ __forceinline__ void stage16(void* dst, const void* src, int bytes) {
+  for (int o = threadIdx.x * 16; o < bytes; o += blockDim.x * 16) cp_async16((char*)dst + o, (const char*)src + o);
+}
+
+template <typename T, int S, bool UPPER>
+__global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
+    int n, int nseg, const int* __restrict__ seg_row0,  // nseg+1: first slot in ord
+    const int* __restrict__ seg_rp0,                     // nseg+1: first slot in rp (segment-relative values)
+    const int* __restrict__ seg_nnz0,                    // nseg+1: first slot in cj / va
+    const int* __restrict__ seg_lv0,                     // nseg+1: first slot in lvb
+    const int* __restrict__ seg_nlvb,                    // nseg: number of level boundaries
+    const int* __restrict__ ord, const int* __restrict__ rp,  // rp: segment-relative row pointers
+    const int* __restrict__ cj, const T* __restrict__ va, const int* __restrict__ lvb,  // lvb: segment-relative
+    const T* __restrict__ dinv, const T* __restrict__ rhs, const double* __restrict__ rhs_scale, T* y, T* x,
+    unsigned long long* ticket, int* err, Skip skip) {
+  if (skip.on()) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NNZ = SegCfg<T>::nnz;
+  T* xs = (T*)smem_raw;
+  T* sb = xs + kSegRows;  // rhs (lower) or y (upper) of the segment's rows
+  T* sd = sb + kSegRows;  // dinv of the segment's rows (upper)
+  T* sva = sd + kSegRows;
+  T* sext = sva + NNZ;  // operands from earlier segments, gathered at staging
+  int* scj = (int*)(sext + NNZ);
+  int* sord = scj + NNZ;
+  int* srp = sord + kSegRows;
+  int* slvb = srp + kSegRows + 4;
+  __shared__ unsigned long long s_t;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int sl = lane & (S - 1);
+  const int group = tid / S, ngroups = kSegThreads / S;
+  const unsigned long long period = (unsigned long long)nseg + gridDim.x;
+  const double rs = rhs_scale ? *rhs_scale : 1.0;
+  T* dep = UPPER ? x : y;
+  while (true) {
+    if (tid == 0) s_t = atomicAdd(ticket, 1ULL);
+    __syncthreads();
+    const unsigned long long g = s_t % period;
+    if (g >= (unsigned long long)nseg) break;
+    const int sgi = (int)g;
+    // every per-segment block starts 16-byte aligned and has a 16-byte
+    // multiple length (padded on the host)
+    const int r0 = seg_row0[sgi], r1 = seg_row0[sgi + 1];
+    const int p0 = seg_rp0[sgi], p1 = seg_rp0[sgi + 1];
+    const int z0 = seg_nnz0[sgi], z1 = seg_nnz0[sgi + 1];
+    const int v0 = seg_lv0[sgi];
+    const int nlvb = seg_nlvb[sgi];
+    stage16(sva, va + z0, (z1 - z0) * (int)sizeof(T));
+    stage16(scj, cj + z0, (z1 - z0) * 4);
+    stage16(sord, ord + r0, (r1 - r0) * 4);
+    stage16(srp, rp + p0, (p1 - p0) * 4);
+    stage16(slvb, lvb + v0, (seg_lv0[sgi + 1] - v0) * 4);
+    // gather the per-row operands while the copies are in flight (plain
+    // loads: independent, so they overlap)
+    for (int i = tid; i < r1 - r0; i += blockDim.x) {
+      const int r = __ldg(&ord[r0 + i]);
+      if (r < 0) continue;
+      if (UPPER) {
+        sb[i] = __ldcg(&y[r]);
+        sd[i] = __ldg(&dinv[r]);
+      } else {
+        T bb = __ldg(&rhs[r]);
+        if (rhs_scale) bb = (T)((double)bb * rs);
+        sb[i] = bb;
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // gather every operand owned by an earlier segment in one parallel sweep
+    // through L2; most are final already, the rest still read the sentinel
+    // and are polled in the sweep below.  Entries are written with single
+    // 4/8-byte stores, so a load sees either the sentinel or the final value.
+    for (int k = tid; k < z1 - z0; k += blockDim.x) {
+      const int c = scj[k];
+      if (c >= 0 && c < n) sext[k] = __ldcg(&dep[c]);
+    }
+    // this segment's rows: hand the buffers to the next pass
+    for (int i = tid; i < r1 - r0; i += blockDim.x) {
+      const int r = sord[i];
+      if (r < 0) continue;
+      if (UPPER)
+        y[r] = Sentinel<T>::value();
+      else
+        x[r] = Sentinel<T>::value();
+    }
+    __syncthreads();
+    for (int lv = 0; lv + 1 < nlvb; lv++) {
+      const int a = slvb[lv], b = slvb[lv + 1];
+      for (int i = a + group; i < b; i += ngroups) {
+        const int r = sord[i];
+        if (r < 0) continue;  // padding slot
+        T acc = 0;
+        const int k1 = srp[i], k2 = srp[i + 1];
+        for (int k = k1 + sl; k < k2; k += S) {
+          const int c = scj[k];
+          T v;
+          if (c < 0) {
+            v = xs[-c - 1];
+          } else {
+            if ((unsigned)c >= (unsigned)n) {
+              atomicOr(err, kErrIndex);
+              continue;
+            }
+            v = sext[k];
+            if (Sentinel<T>::is(v)) {
+              v = Sentinel<T>::load(&dep[c]);
+            }
+            if (Sentinel<T>::is(v)) {
+              int spins = 0;
+              do {
+                if (++spins > kSpinLimit || (*(volatile int*)err & kErrTimeout)) {
+                  atomicOr(err, kErrTimeout);
+                  v = 0;
+                  break;
+                }
+                __nanosleep(20);
+                v = Sentinel<T>::load(&dep[c]);
+              } while (Sentinel<T>::is(v));
+            }
+          }
+          acc += sva[k] * v;
+        }
+        acc = group_reduce(acc, S, lane);
+        if (sl == 0) {
+          T out;
+          if (UPPER) {
+            out = (sb[i] - acc) * sd[i];
+            Sentinel<T>::store(&x[r], out);
+          } else {
+            out = sb[i] - acc;
+            Sentinel<T>::store(&y[r], out);
+          }
+          xs[i] = out;
+        }
+      }
+      __syncthreads();
+    }
+    __syncthreads();  // s_t and the staged arrays are reused by the next claim
+  }
+}
+
 // ------------------------------------------------- tall-skinny kernels
 // One kernel family covers every operation on a block of dense columns:
 // the Gram-Schmidt passes of the Arnoldi step (PargemslrMgs / PargemslrCgs2,

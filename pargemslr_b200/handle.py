@@ -12,6 +12,11 @@ from .structures import GemslrStructures
 _initialized_device: Optional[int] = None
 
 
+def _result(res) -> dict:
+    return {"iters": res.iters, "rel_res": res.rel_res, "true_rel_res": res.true_rel_res,
+            "solve_ms": res.solve_ms, "status": res.status, "launches": res.launches}
+
+
 def init(device: int = 0) -> None:
     global _initialized_device
     if _initialized_device != device:
@@ -75,6 +80,31 @@ class GemslrHandle:
             self._h = None
             raise
 
+    @classmethod
+    def from_matrix(cls, A, params: np.ndarray, precision: str = "fp64", device: int = 0) -> "GemslrHandle":
+        """Set up GeMSLR for A with this library's host setup (pgx_gemslr_setup).
+
+        A is (rowptr, colidx, values) or a scipy-style CSR object; params is
+        the reference's double[180] parameter array.
+        """
+        init(device)
+        if hasattr(A, "indptr"):
+            rp, cj, va, n = A.indptr, A.indices, A.data, A.shape[0]
+        else:
+            rp, cj, va = A
+            n = len(rp) - 1
+        keep: list = []
+        Ac = _abi.csr_struct(rp, cj, va, n, n, keep=keep)
+        p = np.ascontiguousarray(params, np.float64)
+        prec = {"fp64": _abi.PRECISION_FP64, "mixed": _abi.PRECISION_MIXED}[precision]
+        h = C.c_void_p()
+        _abi.check(_abi.lib().pgx_gemslr_setup(C.byref(h), C.byref(Ac), _abi.ptr(p), prec))
+        self = cls.__new__(cls)
+        self.n = n
+        self.precision = precision
+        self._h = h
+        return self
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             _abi.lib().pgx_gemslr_destroy(self._h)
@@ -100,8 +130,7 @@ class GemslrHandle:
         rc = _abi.lib().pgx_gemslr_solve(self._h, _abi.ptr(x), _abi.ptr(b), _abi.LOCATION_HOST, _abi.ptr(p),
                                          C.byref(res))
         _abi.check(rc)
-        return x, {"iters": res.iters, "rel_res": res.rel_res, "true_rel_res": res.true_rel_res,
-                   "solve_ms": res.solve_ms, "status": res.status}
+        return x, _result(res)
 
     def solve_device(self, x_ptr: int, b_ptr: int, params: Optional[np.ndarray] = None):
         """Solve on device pointers (e.g. torch tensors' data_ptr())."""
@@ -109,8 +138,22 @@ class GemslrHandle:
         res = _abi.Result()
         _abi.check(_abi.lib().pgx_gemslr_solve(self._h, x_ptr, b_ptr, _abi.LOCATION_DEVICE, _abi.ptr(p),
                                                C.byref(res)))
-        return {"iters": res.iters, "rel_res": res.rel_res, "true_rel_res": res.true_rel_res,
-                "solve_ms": res.solve_ms, "status": res.status}
+        return _result(res)
+
+    def solve_host_ptr(self, x_ptr: int, b_ptr: int, params: Optional[np.ndarray] = None):
+        """Solve on host pointers (e.g. pinned torch tensors): the copies are part of the call."""
+        p = None if params is None else np.ascontiguousarray(params, np.float64)
+        res = _abi.Result()
+        _abi.check(_abi.lib().pgx_gemslr_solve(self._h, x_ptr, b_ptr, _abi.LOCATION_HOST, _abi.ptr(p),
+                                               C.byref(res)))
+        return _result(res)
+
+    def kernel_stats(self, which: int, level: int = 0, reps: int = 5):
+        """(average ms, algorithmic bytes) of one building block (pgx_gemslr_kernel_stats)."""
+        ms = C.c_double(0)
+        b = C.c_double(0)
+        _abi.check(_abi.lib().pgx_gemslr_kernel_stats(self._h, which, level, reps, C.byref(ms), C.byref(b)))
+        return ms.value, b.value
 
     def apply(self, v: np.ndarray) -> np.ndarray:
         """z = M^-1 v (one preconditioner application) on host arrays."""

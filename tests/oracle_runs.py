@@ -66,7 +66,10 @@ def run(lap=None, csr_file: Optional[str] = None, params: Optional[np.ndarray] =
     with open(done) as f:
         for line in f:
             k, v = line.strip().split("=", 1)
-            res[k] = float(v) if any(c in v for c in ".e") else int(v)
+            if "," in v:
+                res[k] = [float(t) for t in v.split(",")]
+            else:
+                res[k] = float(v) if any(c in v for c in ".e") else int(v)
     res["setup"] = os.path.join(out, "setup.bin")
     res["problem"] = os.path.join(out, "problem.bin")
     if solve:
