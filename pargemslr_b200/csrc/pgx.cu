@@ -217,7 +217,12 @@ struct DTri {
   unsigned long long* ticket = nullptr;
   // segmented schedule (trsv_seg_kernel); seg == false uses trsv_kernel
   bool seg = false;
-  int nseg = 0;
+  bool comp = false;  // one CTA per subdomain (trsv_comp_kernel)
+  int nseg = 0, ncomp = 1;
+  int *comp_ch0 = nullptr, *ch_pos0 = nullptr, *far_ptr = nullptr, *far_k = nullptr;
+  T* dslot = nullptr;   // upper pass: inverse diagonal in slot order
+  int* uslot = nullptr; // lower pass: upper-pass slot of each row, in slot order
+  int nslots = 0;       // length of the slot arrays (padded row list)
   long long nnz_total = 0;  // nonzeros of the factor (without padding)
   int *seg_row0 = nullptr, *seg_rp0 = nullptr, *seg_nnz0 = nullptr, *seg_lv0 = nullptr, *seg_nlvb = nullptr,
       *lvb = nullptr;
@@ -272,15 +277,15 @@ static int upload_tri(Arena& ar, const HostCsr& h, bool upper, DTri<T>& d, cudaS
   PGX_TRY(ar.upload(&d.rp, rp.data(), rp.size(), s));
   PGX_TRY(ar.upload(&d.cj, cj.data(), cj.size(), s));
   PGX_TRY(ar.upload(&d.va, va.data(), va.size(), s));
-  PGX_TRY(ar.zeros(&d.ticket, 1, s));
+  PGX_TRY(ar.zeros(&d.ticket, 2, s));
   return PGX_SUCCESS;
 }
 
 // Segmented schedule for trsv_seg_kernel.  Rows of each subdomain, in
 // level-set order, are cut into segments that fit the kernel's shared-memory
-// staging; segments are ordered by (first level, subdomain, position), so a
-// segment depends only on segments before it.  Each per-segment block of the
-// flat arrays starts 16-byte aligned and has a 16-byte multiple length.
+// staging; segments are ordered by (position in the subdomain, subdomain), so
+// a segment depends only on segments before it.  Each per-segment block of
+// the flat arrays starts 16-byte aligned and has a 16-byte multiple length.
 template <typename T>
 static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::vector<int>& dom, DTri<T>& d,
                           cudaStream_t s) {
@@ -337,10 +342,13 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
     }
     if (!cur.rows.empty()) segs.push_back(std::move(cur));
   }
+  // claim order: round robin over the subdomains by segment index, so every
+  // subdomain's chain of segments advances at the same rate (ordering by
+  // level would starve subdomains whose segments span many thin levels);
+  // within a subdomain the order is the schedule order
   std::stable_sort(segs.begin(), segs.end(), [](const Seg& a, const Seg& b) {
-    if (a.first_level != b.first_level) return a.first_level < b.first_level;
-    if (a.comp != b.comp) return a.comp < b.comp;
-    return a.idx < b.idx;
+    if (a.idx != b.idx) return a.idx < b.idx;
+    return a.comp < b.comp;
   });
   d.nseg = (int)segs.size();
   std::vector<int> seg_of(n, -1), slot_of(n, -1);
@@ -386,6 +394,7 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
     pad4(lvb, (int)g.rows.size());
     lv0.push_back((int)lvb.size());
   }
+  d.ncomp = (int)cuts.size() - 1;
   d.nblocks = std::max(1, std::min(d.nseg, 148));
   PGX_TRY(ar.upload(&d.ord, ord.data(), ord.size(), s));
   PGX_TRY(ar.upload(&d.rp, rp.data(), rp.size(), s));
@@ -397,7 +406,168 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
   PGX_TRY(ar.upload(&d.seg_nnz0, nnz0.data(), nnz0.size(), s));
   PGX_TRY(ar.upload(&d.seg_lv0, lv0.data(), lv0.size(), s));
   PGX_TRY(ar.upload(&d.seg_nlvb, nlvb.data(), nlvb.size(), s));
-  PGX_TRY(ar.zeros(&d.ticket, 1, s));
+  PGX_TRY(ar.zeros(&d.ticket, 2, s));
+  return PGX_SUCCESS;
+}
+
+// Chunked per-subdomain schedule for trsv_comp_kernel: each subdomain's
+// rows in level-set order, cut into chunks that fit the kernel's staging
+// buffers, subdomain after subdomain.  A dependency is encoded as the
+// negative ring slot -(q % ring + 1) when its schedule position q is close
+// enough that no row of the consumer's level can have overwritten the slot
+// (end of the consumer's level - q < ring); otherwise as the row index, read
+// back from global memory.  Returns PGX_ERROR_INVALID_PARAM (and builds
+// nothing) when the factor couples two subdomains.
+template <typename T>
+static int upload_tri_comp(Arena& ar, const HostCsr& h, bool upper, const std::vector<int>& dom, DTri<T>& d,
+                           cudaStream_t s, const std::vector<double>* dinv, std::vector<int>* slot_of_row,
+                           const std::vector<int>* upper_slot_of_row) {
+  using CC = CompCfg<T>;
+  const int n = h.rows;
+  std::vector<int> lptr, order, lev;
+  PGX_TRY(build_levels(upper, n, h.rp.data(), h.cj.data(), lptr, order, &lev));
+  std::vector<int> cuts = dom;
+  bool ok = cuts.size() >= 2 && cuts.front() == 0 && cuts.back() == n;
+  for (size_t c = 0; ok && c + 1 < cuts.size(); c++) ok = cuts[c] <= cuts[c + 1];
+  if (!ok) cuts = {0, n};
+  const int ncomp = (int)cuts.size() - 1;
+  std::vector<int> comp_of(n);
+  for (int c = 0; c < ncomp; c++)
+    for (int r = cuts[c]; r < cuts[c + 1]; r++) comp_of[r] = c;
+  for (int r = 0; r < n; r++)
+    for (int k = h.rp[r]; k < h.rp[r + 1]; k++)
+      if (comp_of[h.cj[k]] != comp_of[r]) return PGX_ERROR_INVALID_PARAM;
+  for (int r = 0; r < n; r++)
+    if (h.rp[r + 1] - h.rp[r] > CC::nnz - 4) return PGX_ERROR_INVALID_PARAM;
+  // positions inside each subdomain, in level order
+  std::vector<std::vector<int>> sched(ncomp);
+  for (int p = 0; p < n; p++) sched[comp_of[order[p]]].push_back(order[p]);
+  std::vector<int> posc(n), lvl_end(n);
+  for (int c = 0; c < ncomp; c++) {
+    auto& sc = sched[c];
+    for (size_t p = 0; p < sc.size(); p++) posc[sc[p]] = (int)p;
+    // end position (exclusive) of each row's level
+    size_t a = 0;
+    while (a < sc.size()) {
+      size_t e = a;
+      while (e < sc.size() && lev[sc[e]] == lev[sc[a]]) e++;
+      for (size_t p = a; p < e; p++) lvl_end[sc[p]] = (int)e;
+      a = e;
+    }
+  }
+  auto pad4 = [](std::vector<int>& v, int fill) {
+    while (v.size() % 4) v.push_back(fill);
+  };
+  std::vector<int> ord, rp, cj, lvb, row0(1, 0), rp0(1, 0), nnz0(1, 0), lv0(1, 0), nlvb, pos0, comp_ch0(1, 0);
+  std::vector<int> far_ptr(1, 0), far_k;
+  std::vector<double> va;
+  const int ROWCAP = CC::rows - 4, NNZCAP = CC::nnz - 4;
+  for (int c = 0; c < ncomp; c++) {
+    const auto& sc = sched[c];
+    size_t p = 0;
+    int prev_start = 0;
+    while (p < sc.size()) {
+      // one chunk: consecutive positions within the row and nonzero caps
+      size_t e = p;
+      long long nz = 0;
+      while (e < sc.size() && (int)(e - p) < ROWCAP) {
+        const int rn = h.rp[sc[e] + 1] - h.rp[sc[e]];
+        if (nz + rn > NNZCAP) break;
+        nz += rn;
+        e++;
+      }
+      pos0.push_back((int)p);
+      rp.push_back(0);
+      int acc = 0;
+      const size_t chunk_nnz0 = cj.size();
+      for (size_t q = p; q < e; q++) {
+        const int r = sc[q];
+        ord.push_back(r);
+        for (int k = h.rp[r]; k < h.rp[r + 1]; k++) {
+          const int j = h.cj[k];
+          const int qj = posc[j];
+          const bool near = lvl_end[r] - qj < CC::ring;
+          if (!near) {
+            // far: the producer folds it in while the previous chunk is being
+            // solved, so it must lie before that chunk (ring >> chunk size)
+            if (qj >= prev_start) return PGX_ERROR_INVALID_PARAM;
+            far_k.push_back((int)(cj.size() - chunk_nnz0));
+          }
+          cj.push_back(near ? -((qj & (CC::ring - 1)) + 1) : j);
+          va.push_back(h.va[k]);
+        }
+        acc += h.rp[r + 1] - h.rp[r];
+        rp.push_back(acc);
+      }
+      pad4(ord, -1);
+      row0.push_back((int)ord.size());
+      pad4(rp, acc);
+      rp0.push_back((int)rp.size());
+      while (cj.size() % 4) {
+        cj.push_back(0);
+        va.push_back(0.0);
+      }
+      nnz0.push_back((int)cj.size());
+      const int base = (int)lvb.size();
+      lvb.push_back(0);
+      for (size_t q = p + 1; q < e; q++)
+        if (lev[sc[q]] != lev[sc[q - 1]]) lvb.push_back((int)(q - p));
+      lvb.push_back((int)(e - p));
+      nlvb.push_back((int)lvb.size() - base);
+      pad4(lvb, (int)(e - p));
+      lv0.push_back((int)lvb.size());
+      far_ptr.push_back((int)far_k.size());
+      prev_start = (int)p;
+      p = e;
+    }
+    comp_ch0.push_back((int)pos0.size());
+  }
+  // slot of every row in the flat row list; the upper pass's slots index its
+  // dinv and the y the lower pass leaves behind
+  std::vector<int> slot(n, -1);
+  for (size_t i = 0; i < ord.size(); i++)
+    if (ord[i] >= 0) slot[ord[i]] = (int)i;
+  std::vector<double> dsl;
+  std::vector<int> usl;
+  if (upper) {
+    dsl.assign(ord.size(), 0.0);
+    for (size_t i = 0; i < ord.size(); i++)
+      if (ord[i] >= 0) dsl[i] = (*dinv)[ord[i]];
+  } else {
+    usl.assign(ord.size(), 0);
+    for (size_t i = 0; i < ord.size(); i++)
+      if (ord[i] >= 0) usl[i] = (*upper_slot_of_row)[ord[i]];
+  }
+  if (slot_of_row) *slot_of_row = slot;
+  d.n = n;
+  d.comp = true;
+  d.seg = false;
+  d.ncomp = ncomp;
+  d.nslots = (int)ord.size();
+  d.nlevels = (int)lptr.size() - 1;
+  d.nseg = (int)pos0.size();
+  d.nnz_total = h.nnz();
+  // lanes per row: one level of an average chunk in one sweep of the workers
+  d.S = std::min(pick_lanes(h.nnz(), n), 16);
+  d.nblocks = ncomp;
+  PGX_TRY(ar.upload(&d.ord, ord.data(), ord.size(), s));
+  PGX_TRY(ar.upload(&d.rp, rp.data(), rp.size(), s));
+  PGX_TRY(ar.upload(&d.cj, cj.data(), cj.size(), s));
+  PGX_TRY(ar.upload(&d.va, va.data(), va.size(), s));
+  PGX_TRY(ar.upload(&d.lvb, lvb.data(), lvb.size(), s));
+  PGX_TRY(ar.upload(&d.seg_row0, row0.data(), row0.size(), s));
+  PGX_TRY(ar.upload(&d.seg_rp0, rp0.data(), rp0.size(), s));
+  PGX_TRY(ar.upload(&d.seg_nnz0, nnz0.data(), nnz0.size(), s));
+  PGX_TRY(ar.upload(&d.seg_lv0, lv0.data(), lv0.size(), s));
+  PGX_TRY(ar.upload(&d.seg_nlvb, nlvb.data(), nlvb.size(), s));
+  PGX_TRY(ar.upload(&d.ch_pos0, pos0.data(), pos0.size(), s));
+  PGX_TRY(ar.upload(&d.comp_ch0, comp_ch0.data(), comp_ch0.size(), s));
+  PGX_TRY(ar.upload(&d.far_ptr, far_ptr.data(), far_ptr.size(), s));
+  PGX_TRY(ar.upload(&d.far_k, far_k.data(), far_k.size(), s));
+  if (upper)
+    PGX_TRY(ar.upload(&d.dslot, dsl.data(), dsl.size(), s));
+  else
+    PGX_TRY(ar.upload(&d.uslot, usl.data(), usl.size(), s));
   return PGX_SUCCESS;
 }
 
@@ -416,6 +586,7 @@ struct DLevel {
   DTri<P> L, U;
   P* dinv = nullptr;
   P* y = nullptr;  // lower-pass result, holds the sentinel between solves
+  P* yslot = nullptr;  // lower-pass result in the upper pass's slot order (per-subdomain kernels)
   DCsr<P> E, F;
   P *W = nullptr, *WH = nullptr;
   P *z = nullptr, *xlr = nullptr;
@@ -521,6 +692,16 @@ struct Engine : EngineBase {
     PGX_SEGATTR(16);
     PGX_SEGATTR(32);
 #undef PGX_SEGATTR
+    const int cbytes = (int)CompCfg<P>::bytes;
+#define PGX_COMPATTR(SS)                                                                                         \
+  PGX_CUDA(cudaFuncSetAttribute(trsv_comp_kernel<P, SS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, cbytes)); \
+  PGX_CUDA(cudaFuncSetAttribute(trsv_comp_kernel<P, SS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, cbytes))
+    PGX_COMPATTR(2);
+    PGX_COMPATTR(4);
+    PGX_COMPATTR(8);
+    PGX_COMPATTR(16);
+    PGX_COMPATTR(32);
+#undef PGX_COMPATTR
     return PGX_SUCCESS;
   }
 
@@ -549,10 +730,24 @@ struct Engine : EngineBase {
       d.start = lev_ptr[l];
       d.nl = lev_ptr[l + 1] - lev_ptr[l];
       d.m = n - lev_ptr[l + 1];
-      if (use_seg && want_segments(h.L, SegCfg<P>::nnz) && want_segments(h.U, SegCfg<P>::nnz)) {
+      int rcL = PGX_ERROR_INVALID_PARAM, rcU = PGX_ERROR_INVALID_PARAM;
+      if (h.L.rows > 0) {
+        std::vector<int> uslot_of_row;
+        rcU = upload_tri_comp(ar, h.U, true, h.dom_ptr, d.U, stream, &h.dinv, &uslot_of_row, nullptr);
+        if (rcU == PGX_SUCCESS)
+          rcL = upload_tri_comp(ar, h.L, false, h.dom_ptr, d.L, stream, nullptr, nullptr, &uslot_of_row);
+      }
+      if (rcL == PGX_SUCCESS && rcU == PGX_SUCCESS) {
+        // one CTA per subdomain; y travels from the lower to the upper pass in slot order
+        PGX_TRY(ar.zeros(&d.yslot, (size_t)d.U.nslots, stream));
+      } else if (use_seg && want_segments(h.L, SegCfg<P>::nnz) && want_segments(h.U, SegCfg<P>::nnz)) {
+        d.L = DTri<P>();
+        d.U = DTri<P>();
         PGX_TRY(upload_tri_seg(ar, h.L, false, h.dom_ptr, d.L, stream));
         PGX_TRY(upload_tri_seg(ar, h.U, true, h.dom_ptr, d.U, stream));
       } else {
+        d.L = DTri<P>();
+        d.U = DTri<P>();
         PGX_TRY(upload_tri(ar, h.L, false, d.L, stream));
         PGX_TRY(upload_tri(ar, h.U, true, d.U, stream));
       }
@@ -603,7 +798,62 @@ struct Engine : EngineBase {
     PGX_TRY(ar.zeros(&counter, 1, stream));
     PGX_TRY(ar.zeros(&err, 1, stream));
     PGX_CUDA(cudaStreamSynchronize(stream));
+    PGX_TRY(autotune());
     return PGX_SUCCESS;
+  }
+
+  // Autotuner: the persistent grid of each large segmented factor is picked
+  // by timing the lower/upper pass pair at a few sizes (the number of
+  // segments kept in flight per subdomain trades staging overlap against
+  // idle CTAs holding shared memory).
+  int autotune() {
+    Skip sk = mk_skip();
+    for (int l = 0; l < nlev; l++) {
+      DLevel<P>& d = lv[l];
+      if (!d.L.seg || !d.U.seg || d.nl < 32768) continue;  // one-CTA-per-subdomain kernels have no grid choice
+      const int comps = std::max(d.L.ncomp, 1);
+      std::vector<int> cand;
+      for (int f : {2, 4, 8, 16}) cand.push_back(std::min(148, comps * f));
+      cand.push_back(148);
+      std::sort(cand.begin(), cand.end());
+      cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+      int bestL = d.L.nblocks, bestU = d.U.nblocks;
+      float tL = 1e30f, tU = 1e30f;
+      for (int g : cand) {
+        d.L.nblocks = std::min(g, d.L.nseg);
+        d.U.nblocks = std::min(g, d.U.nseg);
+        float mL = 0.f, mU = 0.f;
+        for (int rep = 0; rep < 3; rep++) {
+          PGX_CUDA(cudaEventRecord(ev0, stream));
+          trsv(d.L, false, nullptr, rt + d.start, nullptr, d.y, xt + d.start, sk, d.yslot);
+          PGX_CUDA(cudaEventRecord(ev1, stream));
+          PGX_CUDA(cudaStreamSynchronize(stream));
+          float a = 0.f;
+          PGX_CUDA(cudaEventElapsedTime(&a, ev0, ev1));
+          PGX_CUDA(cudaEventRecord(ev0, stream));
+          trsv(d.U, true, d.dinv, nullptr, nullptr, d.y, xt + d.start, sk, d.yslot);
+          PGX_CUDA(cudaEventRecord(ev1, stream));
+          PGX_CUDA(cudaStreamSynchronize(stream));
+          float b = 0.f;
+          PGX_CUDA(cudaEventElapsedTime(&b, ev0, ev1));
+          if (rep > 0) {
+            mL += a;
+            mU += b;
+          }
+        }
+        if (mL < tL) {
+          tL = mL;
+          bestL = d.L.nblocks;
+        }
+        if (mU < tU) {
+          tU = mU;
+          bestU = d.U.nblocks;
+        }
+      }
+      d.L.nblocks = bestL;
+      d.U.nblocks = bestU;
+    }
+    return check_err();
   }
 
   // C_l = the matrix of GemslrClass::CMatVec(l) (gemslr.cpp:3962-4080): the
@@ -820,8 +1070,41 @@ struct Engine : EngineBase {
   // one triangular pass; lower: y = L^-1 rhs (x set to the sentinel),
   // upper: x = D U^-1 y (y set back to the sentinel)
   void trsv(const DTri<P>& T, bool upper, const P* dinv, const P* rhs, const double* rhs_scale, P* y, P* x,
-            Skip sk) {
+            Skip sk, P* yslot = nullptr) {
     if (T.n == 0) return;
+    if (T.comp) {
+      const size_t bytes = CompCfg<P>::bytes;
+      CompArrays ca;
+      ca.ch_row0 = T.seg_row0;
+      ca.ch_rp0 = T.seg_rp0;
+      ca.ch_nnz0 = T.seg_nnz0;
+      ca.ch_lv0 = T.seg_lv0;
+      ca.ord = T.ord;
+      ca.rp = T.rp;
+      ca.cj = T.cj;
+      ca.lvb = T.lvb;
+      ca.uslot = T.uslot;
+      ca.far_ptr = T.far_ptr;
+      ca.far_k = T.far_k;
+#define PGX_TRSVCOMP(SS)                                                                                        \
+  if (upper)                                                                                                    \
+    trsv_comp_kernel<P, SS, true><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, T.ch_pos0, ca, T.va, \
+                                                                            T.dslot, yslot, rhs, rhs_scale, y, x, \
+                                                                            err, sk);                             \
+  else                                                                                                          \
+    trsv_comp_kernel<P, SS, false><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, T.ch_pos0, ca, T.va, \
+                                                                             T.dslot, yslot, rhs, rhs_scale, y,    \
+                                                                             x, err, sk)
+      switch (T.S) {
+        case 2: PGX_TRSVCOMP(2); break;
+        case 4: PGX_TRSVCOMP(4); break;
+        case 8: PGX_TRSVCOMP(8); break;
+        case 16: PGX_TRSVCOMP(16); break;
+        default: PGX_TRSVCOMP(32); break;
+      }
+#undef PGX_TRSVCOMP
+      return;
+    }
     if (T.seg) {
       const size_t bytes = SegCfg<P>::bytes;
 #define PGX_TRSVSEG(SS)                                                                                       \
@@ -881,8 +1164,8 @@ struct Engine : EngineBase {
   // B-solve of level l: x = U^-1 L^-1 rhs  (GemslrClass::SolveB)
   void solve_b(int l, const P* rhs, const double* rhs_scale, P* x, Skip sk) {
     DLevel<P>& d = lv[l];
-    trsv(d.L, false, nullptr, rhs, rhs_scale, d.y, x, sk);
-    trsv(d.U, true, d.dinv, nullptr, nullptr, d.y, x, sk);
+    trsv(d.L, false, nullptr, rhs, rhs_scale, d.y, x, sk, d.yslot);
+    trsv(d.U, true, d.dinv, nullptr, nullptr, d.y, x, sk, d.yslot);
   }
 
   // x += WH (W^T x) in place  (SolveApplyLowRankLevel + Axpy, gemslr.cpp:3585-3590)
@@ -1065,10 +1348,10 @@ struct Engine : EngineBase {
       // the events bracket only the pass being measured
       for (int r = 0; r < reps; r++) {
         if (which == 0) PGX_CUDA(cudaEventRecord(ev0, stream));
-        trsv(d.L, false, nullptr, rt, nullptr, d.y, xt, sk);
+        trsv(d.L, false, nullptr, rt, nullptr, d.y, xt, sk, d.yslot);
         if (which == 0) PGX_CUDA(cudaEventRecord(ev1, stream));
         if (which == 1) PGX_CUDA(cudaEventRecord(ev0, stream));
-        trsv(d.U, true, d.dinv, nullptr, nullptr, d.y, xt, sk);
+        trsv(d.U, true, d.dinv, nullptr, nullptr, d.y, xt, sk, d.yslot);
         if (which == 1) PGX_CUDA(cudaEventRecord(ev1, stream));
         PGX_CUDA(cudaStreamSynchronize(stream));
         float ms = 0.f;

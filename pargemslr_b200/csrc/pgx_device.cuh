@@ -7,6 +7,7 @@
 // after convergence cost one launch each and no memory traffic.
 #pragma once
 
+#include <climits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -135,13 +136,12 @@ __global__ void __launch_bounds__(256) spmv_kernel(
 // the buffers ready for the next one.
 //
 // The grid is persistent and sized to the level width (few pollers, little
-// L2 pressure).  Warps claim groups from a monotone 64-bit ticket counter in
-// schedule order; a row only waits on rows of earlier levels, whose groups
-// were claimed earlier by warps that are running, so the waits always end.
-// Each warp stops at its first ticket past the last group, so every launch
-// consumes exactly ngroups + nwarps tickets and ticket % (ngroups + nwarps)
-// is the group index without any reset between launches.  Waits are bounded;
-// on expiry the kernel records kErrTimeout and finishes.
+// L2 pressure).  Warps claim groups from a 64-bit ticket counter in schedule
+// order; a row only waits on rows of earlier levels, whose groups were
+// claimed earlier by warps that are running, so the waits always end.  The
+// last warp to leave resets the counter (ticket[0]) and the exit count
+// (ticket[1]) for the next launch, whatever the grid size.  Waits are
+// bounded; on expiry the kernel records kErrTimeout and finishes.
 template <typename T>
 struct Sentinel;
 template <>
@@ -183,16 +183,15 @@ __global__ void __launch_bounds__(256) trsv_kernel(
     const double* __restrict__ rhs_scale, T* y, T* x, unsigned long long* ticket, int* err, Skip skip) {
   constexpr int G = kWarp / S;  // rows per warp
   if (skip.on()) return;
-  const unsigned long long period = (unsigned long long)ngroups + (unsigned long long)(gridDim.x * (blockDim.x / kWarp));
   const int lane = threadIdx.x & (kWarp - 1);
   const int sl = lane & (S - 1);
   const double rs = rhs_scale ? *rhs_scale : 1.0;
   T* dep = UPPER ? x : y;  // the vector this pass polls
   while (true) {
     unsigned long long t = 0;
-    if (lane == 0) t = atomicAdd(ticket, 1ULL);
+    if (lane == 0) t = atomicAdd(&ticket[0], 1ULL);
     t = __shfl_sync(0xffffffffu, t, 0);
-    const unsigned long long g = t % period;
+    const unsigned long long g = t;
     if (g >= (unsigned long long)ngroups) break;
     const int pos = (int)g * G + lane / S;
     const int r = ord[pos];  // -1 marks padding; uniform over the S-lane group
@@ -233,6 +232,16 @@ __global__ void __launch_bounds__(256) trsv_kernel(
           Sentinel<T>::store(&y[r], b - acc);
         }
       }
+    }
+  }
+  // the last warp to leave rewinds the counters for the next launch
+  if (lane == 0) {
+    __threadfence();
+    const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x / kWarp);
+    if (atomicAdd(&ticket[1], 1ULL) == nw - 1) {
+      ticket[0] = 0ULL;
+      ticket[1] = 0ULL;
+      __threadfence();
     }
   }
 }
@@ -302,13 +311,12 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
   const int tid = threadIdx.x, lane = tid & 31;
   const int sl = lane & (S - 1);
   const int group = tid / S, ngroups = kSegThreads / S;
-  const unsigned long long period = (unsigned long long)nseg + gridDim.x;
   const double rs = rhs_scale ? *rhs_scale : 1.0;
   T* dep = UPPER ? x : y;
   while (true) {
-    if (tid == 0) s_t = atomicAdd(ticket, 1ULL);
+    if (tid == 0) s_t = atomicAdd(&ticket[0], 1ULL);
     __syncthreads();
-    const unsigned long long g = s_t % period;
+    const unsigned long long g = s_t;
     if (g >= (unsigned long long)nseg) break;
     const int sgi = (int)g;
     // every per-segment block starts 16-byte aligned and has a 16-byte
@@ -409,6 +417,224 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
       __syncthreads();
     }
     __syncthreads();  // s_t and the staged arrays are reused by the next claim
+  }
+  // the last CTA to leave rewinds the counters for the next launch
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(&ticket[1], 1ULL) == (unsigned long long)gridDim.x - 1) {
+      ticket[0] = 0ULL;
+      ticket[1] = 0ULL;
+      __threadfence();
+    }
+  }
+}
+
+// ----------------------------- one-CTA-per-subdomain triangular solve
+// Same arithmetic as trsv_kernel.  In level-set order the dependencies of an
+// ILU factor are short-range: for the RCM-ordered subdomains of a 3D problem
+// the median distance between a row and the rows it needs is ~10^3
+// positions and almost all are within 10^4.  So one CTA walks a whole
+// subdomain in level order and keeps the most recent results in a shared-
+// memory ring indexed by schedule position; a dependency within the ring is a
+// shared-memory read.  An older one was computed by this CTA at least `ring`
+// positions earlier, before the current chunk was staged, so it is read back
+// from global memory once per chunk and folded into the staged value
+// (column index marked kFarDone).  The host encodes each column index as
+// -(ring slot + 1) or as the row index of a far dependency.
+//
+// The subdomain's schedule is cut into chunks that fit a staging buffer;
+// there are two buffers.  While the CTA sweeps the levels of chunk k (one
+// barrier per level), every thread has already issued its cp.async copies of
+// chunk k+1 (row list, row pointers, columns, values, level boundaries and,
+// for the upper pass, the inverse diagonal and y in slot order).  At the
+// chunk boundary the lower pass gathers the right-hand side of chunk k+1
+// through its staged row list and both passes fold in far dependencies.  No
+// CTA waits on another: no deadlock, no tickets, one CTA per subdomain.
+constexpr int kCompThreads = 1024;
+constexpr int kFarDone = INT_MIN;
+template <typename T>
+struct CompCfg {
+  static constexpr int ring = 8192;                           // 32 KB (f32) / 64 KB (f64)
+  static constexpr int nnz = sizeof(T) == 8 ? 4096 : 8192;    // per chunk buffer
+  static constexpr int rows = sizeof(T) == 8 ? 768 : 1024;    // per chunk buffer (incl. padding)
+  // per buffer: va[nnz] T | sb[rows] T | sd[rows] T | cj[nnz] int | ord[rows] int | rp[rows+4] int | lvb[rows+4] int
+  static constexpr size_t buf_bytes =
+      sizeof(T) * (size_t)(nnz + 2 * rows) + sizeof(int) * (size_t)(nnz + rows + 2 * (rows + 4));
+  static constexpr size_t bytes = sizeof(T) * (size_t)ring + 2 * buf_bytes;
+};
+
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* dst, const T* src) {
+  if (sizeof(T) == 8)
+    cp_async8(dst, src);
+  else
+    cp_async4(dst, src);
+}
+
+template <typename T>
+struct CompBuf {
+  T *va, *sb, *sd;
+  int *cj, *ord, *rp, *lvb;
+};
+
+template <typename T>
+__device__ __forceinline__ CompBuf<T> comp_buf(unsigned char* base, int which) {
+  using C = CompCfg<T>;
+  unsigned char* b = base + sizeof(T) * (size_t)C::ring + (size_t)which * C::buf_bytes;
+  CompBuf<T> o;
+  o.va = (T*)b;
+  o.sb = o.va + C::nnz;
+  o.sd = o.sb + C::rows;
+  o.cj = (int*)(o.sd + C::rows);
+  o.ord = o.cj + C::nnz;
+  o.rp = o.ord + C::rows;
+  o.lvb = o.rp + C::rows + 4;
+  return o;
+}
+
+struct CompArrays {
+  const int *ch_row0, *ch_rp0, *ch_nnz0, *ch_lv0, *ord, *rp, *cj, *lvb, *uslot, *far_ptr, *far_k;
+};
+
+// all threads: issue the bulk copies of chunk ch into buffer b
+template <typename T, bool UPPER>
+__device__ __forceinline__ void comp_stage_bulk(const CompBuf<T>& b, int ch, const CompArrays& g,
+                                                const T* __restrict__ va, const T* __restrict__ dslot,
+                                                const T* yslot) {
+  const int r0 = g.ch_row0[ch], r1 = g.ch_row0[ch + 1];
+  const int p0 = g.ch_rp0[ch], p1 = g.ch_rp0[ch + 1];
+  const int z0 = g.ch_nnz0[ch], z1 = g.ch_nnz0[ch + 1];
+  const int v0 = g.ch_lv0[ch], v1 = g.ch_lv0[ch + 1];
+  stage16(b.va, va + z0, (z1 - z0) * (int)sizeof(T));
+  stage16(b.cj, g.cj + z0, (z1 - z0) * 4);
+  stage16(b.ord, g.ord + r0, (r1 - r0) * 4);
+  stage16(b.rp, g.rp + p0, (p1 - p0) * 4);
+  stage16(b.lvb, g.lvb + v0, (v1 - v0) * 4);
+  if (UPPER) {
+    stage16(b.sd, dslot + r0, (r1 - r0) * (int)sizeof(T));
+    stage16(b.sb, yslot + r0, (r1 - r0) * (int)sizeof(T));
+  } else {
+    stage16(b.sd, g.uslot + r0, (r1 - r0) * 4);  // upper-pass slot of each row (ints in sd)
+  }
+}
+
+// all threads, after the bulk copies of chunk ch have landed: gather the
+// lower pass's right-hand side and fold in far dependencies
+template <typename T, bool UPPER>
+__device__ __forceinline__ void comp_stage_gather(const CompBuf<T>& b, int ch, const CompArrays& g, const T* rhs,
+                                                  const T* out, int n, int* err) {
+  const int r0 = g.ch_row0[ch], r1 = g.ch_row0[ch + 1];
+  if (!UPPER) {
+    for (int i = threadIdx.x; i < r1 - r0; i += blockDim.x) {
+      const int r = b.ord[i];
+      if (r >= 0) cp_async_elem(&b.sb[i], &rhs[r]);
+    }
+  }
+  const int f0 = g.far_ptr[ch], f1 = g.far_ptr[ch + 1];
+  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
+    const int k = __ldg(&g.far_k[f]);
+    const int c = b.cj[k];
+    if ((unsigned)c < (unsigned)n) {
+      b.va[k] = b.va[k] * __ldcg(&out[c]);
+    } else {
+      atomicOr(err, kErrIndex);
+      b.va[k] = 0;
+    }
+    b.cj[k] = kFarDone;
+  }
+}
+
+template <typename T, int S, bool UPPER>
+__global__ void __launch_bounds__(kCompThreads) trsv_comp_kernel(
+    int n, const int* __restrict__ comp_ch0,  // ncomp+1: chunk range of each subdomain
+    const int* __restrict__ ch_pos0,          // first schedule position of each chunk
+    CompArrays g, const T* __restrict__ va, const T* __restrict__ dslot, T* yslot, const T* rhs,
+    const double* __restrict__ rhs_scale, T* y, T* x, int* err, Skip skip) {
+  if (skip.on()) return;
+  using C = CompCfg<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = (T*)smem_raw;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int c0 = comp_ch0[blockIdx.x], c1 = comp_ch0[blockIdx.x + 1];
+  T* out = UPPER ? x : y;  // this pass's result, also the far-dependency store
+  const double rs = rhs_scale ? *rhs_scale : 1.0;
+  if (c0 >= c1) return;
+  comp_stage_bulk<T, UPPER>(comp_buf<T>(smem_raw, 0), c0, g, va, dslot, yslot);
+  cp_async_wait_all();
+  __syncthreads();
+  comp_stage_gather<T, UPPER>(comp_buf<T>(smem_raw, 0), c0, g, rhs, out, n, err);
+  cp_async_wait_all();
+  __syncthreads();
+  const int sl = tid & (S - 1), group = tid / S, ngroups = kCompThreads / S;
+  for (int ch = c0; ch < c1; ch++) {
+    const int bi = (ch - c0) & 1;
+    if (ch + 1 < c1) comp_stage_bulk<T, UPPER>(comp_buf<T>(smem_raw, bi ^ 1), ch + 1, g, va, dslot, yslot);
+    const CompBuf<T> b = comp_buf<T>(smem_raw, bi);
+    const int pos0 = ch_pos0[ch];
+    const int r0 = g.ch_row0[ch];
+    const int nl = g.ch_lv0[ch + 1] - g.ch_lv0[ch];
+    for (int lv = 0; lv + 1 < nl; lv++) {
+      const int a = b.lvb[lv], e = b.lvb[lv + 1];
+      if (a >= e) break;  // padding after the last boundary
+      for (int i = a + group; i < e; i += ngroups) {
+        T acc = 0;
+        const int k1 = b.rp[i], k2 = b.rp[i + 1];
+        for (int k = k1 + sl; k < k2; k += S) {
+          const int c = b.cj[k];
+          if (c == kFarDone) {
+            acc += b.va[k];  // dependency already folded into the value
+          } else if (c < 0) {
+            acc += b.va[k] * ring[-c - 1];
+          } else if ((unsigned)c < (unsigned)n) {
+            acc += b.va[k] * __ldcg(&out[c]);
+          } else {
+            atomicOr(err, kErrIndex);
+          }
+        }
+        acc = group_reduce(acc, S, lane);
+        if (sl == 0) {
+          T o;
+          if (UPPER) {
+            o = (b.sb[i] - acc) * b.sd[i];
+          } else {
+            T bb = b.sb[i];
+            if (rhs_scale) bb = (T)((double)bb * rs);
+            o = bb - acc;
+          }
+          ring[(pos0 + i) & (C::ring - 1)] = o;
+        }
+      }
+      __syncthreads();
+    }
+    // publish the chunk's results from the ring: natural order (far
+    // dependencies and the consumer) and, for the lower pass, the upper
+    // pass's slot order
+    (void)r0;
+    {
+      const int nrows_ch = g.ch_row0[ch + 1] - g.ch_row0[ch];
+      for (int i = tid; i < nrows_ch; i += blockDim.x) {
+        const int r = b.ord[i];
+        if (r < 0) continue;
+        const T o = ring[(pos0 + i) & (C::ring - 1)];
+        out[r] = o;
+        if (!UPPER) yslot[((const int*)b.sd)[i]] = o;
+      }
+    }
+    if (ch + 1 < c1) {
+      cp_async_wait_all();
+      __syncthreads();
+      comp_stage_gather<T, UPPER>(comp_buf<T>(smem_raw, bi ^ 1), ch + 1, g, rhs, out, n, err);
+      cp_async_wait_all();
+      __syncthreads();
+    }
   }
 }
 
