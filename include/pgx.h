@@ -179,6 +179,44 @@ int pgx_gemslr_device_bytes(pgx_handle handle, int32_t kdim, int64_t *bytes);
 int pgx_gemslr_solve(pgx_handle handle, double *x, const double *b, int32_t location,
                      const double *params, pgx_result *result);
 
+/* ---- concurrent solves and serving --------------------------------------
+ * A committed handle holds the preconditioner (factors, coupling blocks,
+ * low-rank bases) once; each solve slot adds its own work space (CUDA
+ * stream, work vectors, Krylov basis, FGMRES state, captured restart cycle).
+ * Solves in different slots run concurrently on the GPU and read the factors
+ * in common.  A result does not depend on the slot that computed it or on
+ * what ran beside it: every reduction has a fixed order.  The reference
+ * solves one right-hand side at a time per process; slots have no
+ * counterpart there. */
+typedef struct pgx_server_s *pgx_server;
+
+/* Number of solve slots (1..256; slot 0 is the handle itself).  Refused while
+ * a server created on the handle is live. */
+int pgx_gemslr_set_slots(pgx_handle handle, int32_t nslots);
+/* Device bytes one additional slot needs for FGMRES(kdim). */
+int pgx_gemslr_slot_bytes(pgx_handle handle, int32_t kdim, int64_t *bytes);
+
+/* Solve nrhs systems A X(:,r) = B(:,r) (columns with leading dimensions ldx
+ * and ldb, x0 = the incoming X), spreading them over the slots; results[r]
+ * receives each outcome.  Returns the first error met, PGX_SUCCESS
+ * otherwise. */
+int pgx_gemslr_solve_batch(pgx_handle handle, int32_t nrhs, double *X, int64_t ldx, const double *B,
+                           int64_t ldb, int32_t location, const double *params, pgx_result *results);
+
+/* Serving loop over one resident preconditioned matrix.  Requests queue in
+ * submission order; pgx_server_step admits the oldest waiting request into
+ * every free slot and advances each in-flight solve by at most one restart
+ * cycle, without blocking; pgx_server_collect hands back finished requests
+ * with their ids (request_id >= 0).  x and b stay borrowed until their
+ * request is collected.  While a server is live, the handle's slots belong
+ * to it: set_slots, solve, solve_batch, commit and destroy are refused.
+ * pgx_server_destroy finishes the in-flight solves first. */
+int pgx_server_create(pgx_handle handle, const double *params, pgx_server *server);
+int pgx_server_submit(pgx_server server, double *x, const double *b, int32_t location, int64_t request_id);
+int pgx_server_step(pgx_server server, int32_t *n_active, int32_t *n_queued);
+int pgx_server_collect(pgx_server server, int32_t max, int64_t *ids, pgx_result *results, int32_t *n);
+int pgx_server_destroy(pgx_server server);
+
 /* Apply the preconditioner once, z = M^-1 v (GemslrClass::Solve,
  * gemslr.cpp:3431-3472), on host or device vectors. */
 int pgx_gemslr_precond_apply(pgx_handle handle, double *z, const double *v, int32_t location);

@@ -40,6 +40,8 @@ EXPORTS = (
     "pgx_gemslr_commit", "pgx_gemslr_destroy", "pgx_gemslr_device_bytes",
     "pgx_gemslr_solve", "pgx_gemslr_precond_apply", "pgx_build_levels",
     "pgx_csr_spmv_device", "pgx_gemslr_setup", "pgx_gemslr_kernel_stats",
+    "pgx_gemslr_set_slots", "pgx_gemslr_slot_bytes", "pgx_gemslr_solve_batch",
+    "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
 )
 
 
@@ -100,6 +102,14 @@ def lib() -> C.CDLL:
     L.pgx_csr_spmv_device.argtypes = [C.POINTER(Csr), dbl, vp, dbl, vp]
     L.pgx_gemslr_setup.argtypes = [C.POINTER(vp), C.POINTER(Csr), vp, i32]
     L.pgx_gemslr_kernel_stats.argtypes = [vp, i32, i32, i32, C.POINTER(dbl), C.POINTER(dbl)]
+    L.pgx_gemslr_set_slots.argtypes = [vp, i32]
+    L.pgx_gemslr_slot_bytes.argtypes = [vp, i32, C.POINTER(i64)]
+    L.pgx_gemslr_solve_batch.argtypes = [vp, i32, vp, i64, vp, i64, i32, vp, vp]
+    L.pgx_server_create.argtypes = [vp, vp, C.POINTER(vp)]
+    L.pgx_server_submit.argtypes = [vp, vp, vp, i32, i64]
+    L.pgx_server_step.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.pgx_server_collect.argtypes = [vp, i32, vp, vp, C.POINTER(i32)]
+    L.pgx_server_destroy.argtypes = [vp]
     for name in EXPORTS:
         if name != "pgx_last_error":
             getattr(L, name).restype = C.c_int

@@ -24,8 +24,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <memory>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -626,6 +628,12 @@ struct EngineBase {
                     pgx_result* res) = 0;
   virtual int apply(double* z, const double* v, int location) = 0;
   virtual int64_t device_bytes(int kdim) const = 0;
+  // a solve slot: begin() enqueues the start of a solve and its first
+  // restart cycle, poll() advances it by at most one cycle
+  virtual int64_t slot_bytes(int kdim) const = 0;
+  virtual int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol) = 0;
+  virtual int poll(bool block, bool* finished, pgx_result* res) = 0;
+  virtual int make_clone(std::unique_ptr<EngineBase>& out) = 0;
 };
 
 
@@ -634,7 +642,10 @@ struct Engine : EngineBase {
   int n = 0, nlev = 0;
   std::vector<int> lev_ptr;
   cudaStream_t stream = nullptr;
-  Arena ar, krylov;
+  // ar: factors and operators, uploaded once by the owning slot and read by
+  // every clone; wk: this slot's work vectors; krylov: this slot's basis
+  Arena ar, wk, krylov;
+  bool owner = true;
   int kdim_alloc = 0;
   DCsr<double> A;
   int *pperm = nullptr, *qperm = nullptr;
@@ -656,7 +667,9 @@ struct Engine : EngineBase {
   double* partial = nullptr;
   unsigned int* counter = nullptr;
   int* err = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_poll = nullptr;
+  FgmresDev* hs_pin = nullptr;  // pinned copy of the FGMRES state header
+  double* r2_pin = nullptr;     // pinned copy of the final residual norm
   // one FGMRES restart cycle captured as a CUDA graph, keyed by its arguments
   cudaGraphExec_t cycle_exec = nullptr;
   int cycle_nodes = 0;  // kernels in one captured cycle
@@ -673,9 +686,13 @@ struct Engine : EngineBase {
     if (stream) cudaStreamSynchronize(stream);
     drop_graph();
     ar.release();
+    wk.release();
     krylov.release();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_poll) cudaEventDestroy(ev_poll);
+    if (hs_pin) cudaFreeHost(hs_pin);
+    if (r2_pin) cudaFreeHost(r2_pin);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -705,21 +722,41 @@ struct Engine : EngineBase {
     return PGX_SUCCESS;
   }
 
-  int64_t device_bytes(int kdim) const override {
-    int64_t b = (int64_t)ar.bytes;
-    b += (int64_t)n * (kdim + 1) * (sizeof(double) + sizeof(P));
-    return b;
+  int64_t device_bytes(int kdim) const override { return (int64_t)ar.bytes + slot_bytes(kdim); }
+
+  int64_t slot_bytes(int kdim) const override {
+    return (int64_t)wk.bytes + (int64_t)n * (kdim + 1) * (sizeof(double) + sizeof(P));
   }
 
   // ------------------------------------------------------------ commit
+  // The factors and operators are uploaded once; every solve slot (this
+  // engine and its clones) adds its own stream and work space.
   int commit(Import& im) {
     PGX_TRY(set_seg_smem());
-    n = im.n;
-    nlev = im.nlev;
-    lev_ptr = im.lev_ptr;
+    PGX_TRY(init_stream());
+    PGX_TRY(upload_factors(im));
+    PGX_TRY(alloc_work());
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    PGX_TRY(autotune());
+    return PGX_SUCCESS;
+  }
+
+  int init_stream() {
     PGX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     PGX_CUDA(cudaEventCreate(&ev0));
     PGX_CUDA(cudaEventCreate(&ev1));
+    PGX_CUDA(cudaEventCreateWithFlags(&ev_poll, cudaEventDisableTiming));
+    PGX_CUDA(cudaMallocHost((void**)&hs_pin, sizeof(FgmresDev)));
+    PGX_CUDA(cudaMallocHost((void**)&r2_pin, sizeof(double)));
+    memset(hs_pin, 0, sizeof(FgmresDev));
+    *r2_pin = 0.0;
+    return PGX_SUCCESS;
+  }
+
+  int upload_factors(Import& im) {
+    n = im.n;
+    nlev = im.nlev;
+    lev_ptr = im.lev_ptr;
     PGX_TRY(upload_csr(ar, im.A, A, stream));
     PGX_TRY(ar.upload(&pperm, im.pperm.data(), im.pperm.size(), stream));
     if (!im.qperm.empty()) PGX_TRY(ar.upload(&qperm, im.qperm.data(), im.qperm.size(), stream));
@@ -739,7 +776,6 @@ struct Engine : EngineBase {
       }
       if (rcL == PGX_SUCCESS && rcU == PGX_SUCCESS) {
         // one CTA per subdomain; y travels from the lower to the upper pass in slot order
-        PGX_TRY(ar.zeros(&d.yslot, (size_t)d.U.nslots, stream));
       } else if (use_seg && want_segments(h.L, SegCfg<P>::nnz) && want_segments(h.U, SegCfg<P>::nnz)) {
         d.L = DTri<P>();
         d.U = DTri<P>();
@@ -752,9 +788,6 @@ struct Engine : EngineBase {
         PGX_TRY(upload_tri(ar, h.U, true, d.U, stream));
       }
       PGX_TRY(ar.upload(&d.dinv, h.dinv.data(), h.dinv.size(), stream));
-      PGX_TRY(ar.alloc(&d.y, (size_t)d.nl));
-      sentinel_fill_kernel<P><<<grid_for(d.nl, 256, 148 * 8), 256, 0, stream>>>(d.nl, d.y);
-      PGX_CUDA(cudaGetLastError());
       if (l < nlev - 1) {
         PGX_TRY(upload_csr(ar, h.E, d.E, stream));
         PGX_TRY(upload_csr(ar, h.F, d.F, stream));
@@ -763,42 +796,82 @@ struct Engine : EngineBase {
           PGX_TRY(ar.upload(&d.W, h.W.data(), h.W.size(), stream));
           PGX_TRY(ar.upload(&d.WH, h.WH.data(), h.WH.size(), stream));
         }
-        PGX_TRY(ar.zeros(&d.xlr, (size_t)d.m, stream));
-        PGX_TRY(ar.zeros(&d.lrt, (size_t)KMAX + 1, stream));
       }
-      PGX_TRY(ar.zeros(&d.z, (size_t)(n - d.start), stream));
     }
     inner = (im.inner_enable && nlev >= 2) ? 1 : 0;
     inner_maxits = im.inner_maxits;
     inner_tol = im.inner_tol;
+    if (inner) PGX_TRY(assemble_c0(im));
+    return PGX_SUCCESS;
+  }
+
+  // the work space of one solve slot
+  int alloc_work() {
+    for (int l = 0; l < nlev; l++) {
+      DLevel<P>& d = lv[l];
+      if (d.L.comp) PGX_TRY(wk.zeros(&d.yslot, (size_t)d.U.nslots, stream));
+      if (!owner) {
+        // the level-set and segmented kernels count their CTAs per slot
+        if (d.L.ticket) PGX_TRY(wk.zeros(&d.L.ticket, 2, stream));
+        if (d.U.ticket) PGX_TRY(wk.zeros(&d.U.ticket, 2, stream));
+      }
+      PGX_TRY(wk.alloc(&d.y, (size_t)d.nl));
+      sentinel_fill_kernel<P><<<grid_for(d.nl, 256, 148 * 8), 256, 0, stream>>>(d.nl, d.y);
+      PGX_CUDA(cudaGetLastError());
+      if (l < nlev - 1) {
+        PGX_TRY(wk.zeros(&d.xlr, (size_t)d.m, stream));
+        PGX_TRY(wk.zeros(&d.lrt, (size_t)KMAX + 1, stream));
+      }
+      PGX_TRY(wk.zeros(&d.z, (size_t)(n - d.start), stream));
+    }
     if (inner) {
-      PGX_TRY(assemble_c0(im));
       const int m0 = lv[0].m;
-      PGX_TRY(ar.zeros(&s_zu, (size_t)lv[0].nl, stream));
-      PGX_TRY(ar.zeros(&s_wu, (size_t)lv[0].nl, stream));
-      PGX_TRY(ar.zeros(&Vin, (size_t)m0 * (inner_maxits + 1), stream));
-      PGX_TRY(ar.zeros(&Zin, (size_t)m0 * (inner_maxits + 1), stream));
-      PGX_TRY(ar.zeros(&st_in, 1, stream));
+      PGX_TRY(wk.zeros(&s_zu, (size_t)lv[0].nl, stream));
+      PGX_TRY(wk.zeros(&s_wu, (size_t)lv[0].nl, stream));
+      PGX_TRY(wk.zeros(&Vin, (size_t)m0 * (inner_maxits + 1), stream));
+      PGX_TRY(wk.zeros(&Zin, (size_t)m0 * (inner_maxits + 1), stream));
+      PGX_TRY(wk.zeros(&st_in, 1, stream));
       FgmresDev h;
       memset(&h, 0, sizeof(h));
       h.kdim = inner_maxits;
       h.maxits = inner_maxits;
       h.tol = inner_tol;
       h.eps = std::is_same<P, float>::value ? (double)FLT_EPSILON : DBL_EPSILON;
-      PGX_CUDA(cudaMemcpyAsync(st_in, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+      *hs_pin = h;
+      PGX_CUDA(cudaMemcpyAsync(st_in, hs_pin, sizeof(h), cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaStreamSynchronize(stream));
     }
-    PGX_TRY(ar.zeros(&st, 1, stream));
-    PGX_TRY(ar.zeros(&bdev, (size_t)n, stream));
-    PGX_TRY(ar.zeros(&xdev, (size_t)n, stream));
-    PGX_TRY(ar.zeros(&rdev, (size_t)n, stream));
-    PGX_TRY(ar.zeros(&scal, 8, stream));
-    PGX_TRY(ar.zeros(&rt, (size_t)n, stream));
-    PGX_TRY(ar.zeros(&xt, (size_t)n, stream));
-    PGX_TRY(ar.zeros(&partial, (size_t)(KMAX + 1) * kTsMaxBlocks, stream));
-    PGX_TRY(ar.zeros(&counter, 1, stream));
-    PGX_TRY(ar.zeros(&err, 1, stream));
+    PGX_TRY(wk.zeros(&st, 1, stream));
+    PGX_TRY(wk.zeros(&bdev, (size_t)n, stream));
+    PGX_TRY(wk.zeros(&xdev, (size_t)n, stream));
+    PGX_TRY(wk.zeros(&rdev, (size_t)n, stream));
+    PGX_TRY(wk.zeros(&scal, 8, stream));
+    PGX_TRY(wk.zeros(&rt, (size_t)n, stream));
+    PGX_TRY(wk.zeros(&xt, (size_t)n, stream));
+    PGX_TRY(wk.zeros(&partial, (size_t)(KMAX + 1) * kTsMaxBlocks, stream));
+    PGX_TRY(wk.zeros(&counter, 1, stream));
+    PGX_TRY(wk.zeros(&err, 1, stream));
+    return PGX_SUCCESS;
+  }
+
+  // another solve slot over the same factors (the owner must outlive it)
+  int clone_from(const Engine& s) {
+    owner = false;
+    n = s.n;
+    nlev = s.nlev;
+    lev_ptr = s.lev_ptr;
+    A = s.A;
+    pperm = s.pperm;
+    qperm = s.qperm;
+    lv = s.lv;  // factor pointers are shared, work pointers are replaced by alloc_work
+    C0 = s.C0;
+    inner = s.inner;
+    inner_maxits = s.inner_maxits;
+    inner_tol = s.inner_tol;
+    use_seg = s.use_seg;
+    PGX_TRY(init_stream());
+    PGX_TRY(alloc_work());
     PGX_CUDA(cudaStreamSynchronize(stream));
-    PGX_TRY(autotune());
     return PGX_SUCCESS;
   }
 
@@ -1434,11 +1507,26 @@ struct Engine : EngineBase {
   }
 
   // FlexGmresClass::Solve (fgmres.hpp:263-558) with the basis, Hessenberg and
-  // rotations on the device; the host reads the state once per restart cycle.
-  int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
-            pgx_result* res) override {
+  // rotations on the device.  The solve is a small state machine so that one
+  // host thread can drive many slots at once: begin() enqueues the start of
+  // the solve and the first restart cycle, poll() looks at the state header
+  // copied back after each cycle and enqueues either the next cycle or the
+  // final residual check.
+  enum { IDLE = 0, RUNNING = 1, FINISHING = 2 };
+  int phase = IDLE;
+  int s_cyc = 0, s_max_cycles = 0, s_maxits = 0, s_launches = 0, s_location = 0;
+  double* s_xd = nullptr;
+  const double* s_bd = nullptr;
+  double* s_xuser = nullptr;
+
+  int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol) override {
+    if (phase != IDLE) return fail(PGX_ERROR_FUNCTION_CALL, "slot busy");
     if (kdim < 1 || kdim > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", kdim, KMAX);
     if (maxits < 0) return fail(PGX_ERROR_INVALID_PARAM, "maxits %d < 0", maxits);
+    if (location == PGX_LOCATION_HOST) {
+      for (int i = 0; i < n; i++)
+        if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%d] is not finite", i);
+    }
     PGX_TRY(ensure_krylov(kdim));
     double* xd = x;
     const double* bd = b;
@@ -1457,7 +1545,8 @@ struct Engine : EngineBase {
     h.eps = DBL_EPSILON;
     h.cycle_done = 1;
     const size_t head = offsetof(FgmresDev, sc);
-    PGX_CUDA(cudaMemcpyAsync(st, &h, head, cudaMemcpyHostToDevice, stream));
+    *hs_pin = h;
+    PGX_CUDA(cudaMemcpyAsync(st, hs_pin, head, cudaMemcpyHostToDevice, stream));
     PGX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
     PGX_CUDA(cudaEventRecord(ev0, stream));
     // ||b||, v = b - A x, ||v||  (fgmres.hpp:319-360)
@@ -1477,8 +1566,8 @@ struct Engine : EngineBase {
       a.st = st;
       ts<double, double, double, TS_NORM_COPY>(a);
     }
-    const int max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
-    if (max_cycles > 0 && (!cycle_exec || g_kdim != kdim || g_x != xd || g_b != bd)) {
+    s_max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
+    if (s_max_cycles > 0 && (!cycle_exec || g_kdim != kdim || g_x != xd || g_b != bd)) {
       drop_graph();
       cudaGraph_t g = nullptr;
       PGX_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -1498,17 +1587,31 @@ struct Engine : EngineBase {
       g_x = xd;
       g_b = bd;
     }
-    int launches = 5;  // ||b||, residual, ||r0||, final residual and its norm
-    for (int cyc = 0; cyc < max_cycles; cyc++) {
+    s_cyc = 0;
+    s_maxits = maxits;
+    s_launches = 5;  // ||b||, residual, ||r0||, final residual and its norm
+    s_location = location;
+    s_xd = xd;
+    s_bd = bd;
+    s_xuser = x;
+    phase = RUNNING;
+    const int rc = launch_cycle_or_finish(false);
+    if (rc != PGX_SUCCESS) phase = IDLE;
+    return rc;
+  }
+
+  // after a cycle: either the next cycle or the final FP64 residual check
+  int launch_cycle_or_finish(bool last_done) {
+    if (!last_done && s_cyc < s_max_cycles) {
       PGX_CUDA(cudaGraphLaunch(cycle_exec, stream));
-      launches += cycle_nodes;
-      FgmresDev hs;
-      PGX_CUDA(cudaMemcpyAsync(&hs, st, head, cudaMemcpyDeviceToHost, stream));
-      PGX_CUDA(cudaStreamSynchronize(stream));
-      if (hs.done || hs.iter >= maxits) break;
+      s_launches += cycle_nodes;
+      s_cyc++;
+      PGX_CUDA(cudaMemcpyAsync(hs_pin, st, offsetof(FgmresDev, sc), cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaEventRecord(ev_poll, stream));
+      return PGX_SUCCESS;
     }
     // FP64 true residual ||b - A x|| / ||b||
-    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, rdev, nullptr, mk_skip());
+    spmv<double, double, double, double>(A, s_xd, -1.0, nullptr, nullptr, 0.0, s_bd, 1.0, rdev, nullptr, mk_skip());
     {
       auto a = ts_args<double, double, double>(n, mk_skip());
       a.in = rdev;
@@ -1517,20 +1620,59 @@ struct Engine : EngineBase {
       ts<double, double, double, TS_NORM_COPY>(a);
     }
     PGX_CUDA(cudaEventRecord(ev1, stream));
-    FgmresDev hs;
-    double r2 = 0.0;
-    PGX_CUDA(cudaMemcpyAsync(&hs, st, head, cudaMemcpyDeviceToHost, stream));
-    PGX_CUDA(cudaMemcpyAsync(&r2, scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
-    PGX_CUDA(cudaStreamSynchronize(stream));
-    int rc = check_err();
+    PGX_CUDA(cudaMemcpyAsync(hs_pin, st, offsetof(FgmresDev, sc), cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaMemcpyAsync(r2_pin, scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaEventRecord(ev_poll, stream));
+    phase = FINISHING;
+    return PGX_SUCCESS;
+  }
+
+  int poll(bool block, bool* finished, pgx_result* res) override {
+    *finished = false;
+    if (phase == IDLE) {
+      *finished = true;
+      return PGX_SUCCESS;
+    }
+    if (block) {
+      cudaError_t q = cudaEventSynchronize(ev_poll);
+      if (q != cudaSuccess) {
+        phase = IDLE;
+        *finished = true;
+        return fail(PGX_ERROR_CUDA, "cudaEventSynchronize: %s", cudaGetErrorString(q));
+      }
+    } else {
+      cudaError_t q = cudaEventQuery(ev_poll);
+      if (q == cudaErrorNotReady) return PGX_SUCCESS;
+      if (q != cudaSuccess) {
+        phase = IDLE;
+        *finished = true;
+        return fail(PGX_ERROR_CUDA, "cudaEventQuery: %s", cudaGetErrorString(q));
+      }
+    }
+    if (phase == RUNNING) {
+      const FgmresDev& hs = *hs_pin;
+      const bool over = hs.done || hs.iter >= s_maxits;
+      const int rc = launch_cycle_or_finish(over);
+      if (rc != PGX_SUCCESS) {
+        phase = IDLE;
+        *finished = true;
+      }
+      return rc;
+    }
+    // FINISHING: the state header and the residual norm are on the host
+    phase = IDLE;
+    *finished = true;
+    const FgmresDev hs = *hs_pin;
+    const double r2 = *r2_pin;
+    const int rc = check_err();
     float ms = 0.f;
     PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
     if (hs.normb < DBL_EPSILON) {
       // zero right-hand side: x = 0 (fgmres.hpp:321-329)
-      PGX_CUDA(cudaMemsetAsync(xd, 0, sizeof(double) * n, stream));
+      PGX_CUDA(cudaMemsetAsync(s_xd, 0, sizeof(double) * n, stream));
     }
-    if (location == PGX_LOCATION_HOST)
-      PGX_CUDA(cudaMemcpyAsync(x, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+    if (s_location == PGX_LOCATION_HOST)
+      PGX_CUDA(cudaMemcpyAsync(s_xuser, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
     PGX_CUDA(cudaStreamSynchronize(stream));
     if (res) {
       res->status = rc;
@@ -1538,11 +1680,25 @@ struct Engine : EngineBase {
       res->rel_res = hs.normb > 0 ? hs.normr / hs.normb : 0.0;
       res->true_rel_res = hs.normb > 0 ? sqrt(r2) / hs.normb : 0.0;
       res->solve_ms = ms;
-      res->launches = launches;
+      res->launches = s_launches;
     }
     if (rc == PGX_SUCCESS && !(std::isfinite(hs.normr)))
       return fail(PGX_ERROR_NOT_FINITE, "FGMRES residual is not finite");
     return rc;
+  }
+
+  int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+            pgx_result* res) override {
+    PGX_TRY(begin(x, b, location, kdim, maxits, tol, atol));
+    bool finished = false;
+    while (!finished) PGX_TRY(poll(true, &finished, res));
+    return PGX_SUCCESS;
+  }
+
+  int make_clone(std::unique_ptr<EngineBase>& out) override {
+    auto* e = new Engine<P>();
+    out.reset(e);
+    return e->clone_from(*this);
   }
 };
 
@@ -1553,8 +1709,33 @@ using namespace pgx;
 
 struct pgx_gemslr_s {
   Import im;
-  std::unique_ptr<EngineBase> eng;
+  std::unique_ptr<EngineBase> eng;                 // slot 0: owns the factors
+  std::vector<std::unique_ptr<EngineBase>> extra;  // slots 1..: borrow them
   int device = 0;
+  int servers = 0;  // live pgx_server objects driving the slots
+  int nslots() const { return eng ? 1 + (int)extra.size() : 0; }
+  EngineBase* slot(int i) { return i == 0 ? eng.get() : extra[i - 1].get(); }
+  ~pgx_gemslr_s() {
+    extra.clear();  // clones first: they read the owner's factors
+    eng.reset();
+  }
+};
+
+// The serving loop of one handle: a FIFO of requests and the request each
+// slot is working on.
+struct pgx_server_s {
+  pgx_handle h = nullptr;
+  bool has_params = false;
+  double params[180];
+  struct Req {
+    double* x;
+    const double* b;
+    int location;
+    int64_t id;
+  };
+  std::deque<Req> queue;
+  std::vector<int64_t> slot_id;  // request in each slot, -1 if the slot is free
+  std::deque<std::pair<int64_t, pgx_result>> done;
 };
 
 extern "C" {
@@ -1691,7 +1872,9 @@ int pgx_gemslr_commit(pgx_handle h) {
   if (im.inner_enable && im.nlev >= 2)
     for (int l = 1; l < im.nlev; l++)
       if (im.levels[l].B.empty()) return fail(PGX_ERROR_INVALID_PARAM, "inner iteration needs B of level %d", l);
+  if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "commit while a server is live");
   PGX_CUDA(cudaSetDevice(h->device));
+  h->extra.clear();
   h->eng.reset();
   if (im.precision == PGX_PRECISION_MIXED) {
     auto* e = new Engine<float>();
@@ -1823,6 +2006,7 @@ int pgx_gemslr_setup(pgx_handle* handle, const pgx_csr* A, const double* params,
 
 int pgx_gemslr_destroy(pgx_handle h) {
   if (!h) return PGX_SUCCESS;
+  if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "destroy the handle's servers first");
   cudaSetDevice(h->device);
   delete h;
   return PGX_SUCCESS;
@@ -1835,24 +2019,30 @@ int pgx_gemslr_device_bytes(pgx_handle h, int32_t kdim, int64_t* bytes) {
   return PGX_SUCCESS;
 }
 
-int pgx_gemslr_solve(pgx_handle h, double* x, const double* b, int32_t location, const double* params,
-                     pgx_result* result) {
-  if (!h || !x || !b) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "solve before commit");
-  if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
-    return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
-  int kdim = 50, maxits = 100, atol = 0;
-  double tol = 1e-6;
+// FlexGmres options of the reference's parameter array (PARGEMSLR_IO_SOLVER_*)
+static void read_solver_params(const double* params, int& kdim, int& maxits, double& tol, int& atol) {
+  kdim = 50;
+  maxits = 100;
+  tol = 1e-6;
+  atol = 0;
   if (params) {
     kdim = (int)params[11];
     maxits = (int)params[12];
     tol = params[13];
     atol = params[14] != 0.0;
   }
-  if (location == PGX_LOCATION_HOST) {
-    for (int i = 0; i < h->im.n; i++)
-      if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%d] is not finite", i);
-  }
+}
+
+int pgx_gemslr_solve(pgx_handle h, double* x, const double* b, int32_t location, const double* params,
+                     pgx_result* result) {
+  if (!h || !x || !b) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "solve before commit");
+  if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
+    return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+  if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "solve while a server drives the slots");
+  int kdim, maxits, atol;
+  double tol;
+  read_solver_params(params, kdim, maxits, tol, atol);
   PGX_CUDA(cudaSetDevice(h->device));
   return h->eng->solve(x, b, location, kdim, maxits, tol, atol, result);
 }
@@ -1862,6 +2052,182 @@ int pgx_gemslr_precond_apply(pgx_handle h, double* z, const double* v, int32_t l
   if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "apply before commit");
   PGX_CUDA(cudaSetDevice(h->device));
   return h->eng->apply(z, v, location);
+}
+
+int pgx_gemslr_set_slots(pgx_handle h, int32_t nslots) {
+  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+  if (nslots < 1 || nslots > 256) return fail(PGX_ERROR_INVALID_PARAM, "nslots %d outside [1, 256]", nslots);
+  if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "slots cannot change while a server is live");
+  PGX_CUDA(cudaSetDevice(h->device));
+  while ((int)h->extra.size() > nslots - 1) h->extra.pop_back();
+  while ((int)h->extra.size() < nslots - 1) {
+    std::unique_ptr<EngineBase> e;
+    const int rc = h->eng->make_clone(e);
+    if (rc != PGX_SUCCESS) return rc;
+    h->extra.push_back(std::move(e));
+  }
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_slot_bytes(pgx_handle h, int32_t kdim, int64_t* bytes) {
+  if (!h || !bytes) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+  *bytes = h->eng->slot_bytes(kdim);
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, const double* B, int64_t ldb,
+                           int32_t location, const double* params, pgx_result* results) {
+  if (!h || (nrhs > 0 && (!X || !B))) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "solve before commit");
+  if (nrhs < 0 || ldx < h->im.n || ldb < h->im.n) return fail(PGX_ERROR_INVALID_PARAM, "bad batch shape");
+  if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
+    return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+  if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "batch solve while a server drives the slots");
+  int kdim, maxits, atol;
+  double tol;
+  read_solver_params(params, kdim, maxits, tol, atol);
+  PGX_CUDA(cudaSetDevice(h->device));
+  if (results) memset(results, 0, sizeof(pgx_result) * (size_t)nrhs);
+  const int ns = h->nslots();
+  std::vector<int> busy(ns, -1);
+  int next = 0, remaining = nrhs, first_err = PGX_SUCCESS;
+  std::string first_msg;
+  auto note = [&](int rc) {
+    if (rc != PGX_SUCCESS && first_err == PGX_SUCCESS) {
+      first_err = rc;
+      first_msg = g_last_error;
+    }
+  };
+  while (remaining > 0) {
+    bool progressed = false;
+    for (int sidx = 0; sidx < ns; sidx++) {
+      EngineBase* e = h->slot(sidx);
+      if (busy[sidx] < 0 && next < nrhs) {
+        const int r = next++;
+        const int rc = e->begin(X + (size_t)r * ldx, B + (size_t)r * ldb, location, kdim, maxits, tol, atol);
+        progressed = true;
+        if (rc != PGX_SUCCESS) {
+          if (results) results[r].status = rc;
+          note(rc);
+          remaining--;
+          continue;
+        }
+        busy[sidx] = r;
+      }
+      if (busy[sidx] >= 0) {
+        bool fin = false;
+        pgx_result res;
+        memset(&res, 0, sizeof(res));
+        const int rc = e->poll(false, &fin, &res);
+        if (rc != PGX_SUCCESS || fin) {
+          if (rc != PGX_SUCCESS) res.status = rc;
+          if (results) results[busy[sidx]] = res;
+          note(res.status);
+          busy[sidx] = -1;
+          remaining--;
+          progressed = true;
+        }
+      }
+    }
+    if (!progressed) std::this_thread::yield();
+  }
+  if (first_err != PGX_SUCCESS) g_last_error = first_msg;
+  return first_err;
+}
+
+int pgx_server_create(pgx_handle h, const double* params, pgx_server* out) {
+  if (!h || !out) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+  pgx_server_s* srv = new pgx_server_s();
+  srv->h = h;
+  srv->has_params = params != nullptr;
+  if (params) memcpy(srv->params, params, sizeof(srv->params));
+  srv->slot_id.assign(h->nslots(), -1);
+  h->servers++;
+  *out = srv;
+  return PGX_SUCCESS;
+}
+
+int pgx_server_submit(pgx_server srv, double* x, const double* b, int32_t location, int64_t request_id) {
+  if (!srv || !x || !b) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (request_id < 0) return fail(PGX_ERROR_INVALID_PARAM, "request id %lld < 0", (long long)request_id);
+  if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
+    return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+  srv->queue.push_back({x, b, location, request_id});
+  return PGX_SUCCESS;
+}
+
+int pgx_server_step(pgx_server srv, int32_t* n_active, int32_t* n_queued) {
+  if (!srv) return fail(PGX_ERROR_INVALID_PARAM, "null server");
+  pgx_handle h = srv->h;
+  PGX_CUDA(cudaSetDevice(h->device));
+  int kdim, maxits, atol;
+  double tol;
+  read_solver_params(srv->has_params ? srv->params : nullptr, kdim, maxits, tol, atol);
+  int active = 0;
+  for (int sidx = 0; sidx < h->nslots(); sidx++) {
+    EngineBase* e = h->slot(sidx);
+    if (srv->slot_id[sidx] < 0 && !srv->queue.empty()) {
+      // the oldest waiting request goes to the free slot
+      const pgx_server_s::Req r = srv->queue.front();
+      srv->queue.pop_front();
+      const int rc = e->begin(r.x, r.b, r.location, kdim, maxits, tol, atol);
+      if (rc != PGX_SUCCESS) {
+        pgx_result res;
+        memset(&res, 0, sizeof(res));
+        res.status = rc;
+        srv->done.push_back({r.id, res});
+        continue;
+      }
+      srv->slot_id[sidx] = r.id;
+    }
+    if (srv->slot_id[sidx] >= 0) {
+      bool fin = false;
+      pgx_result res;
+      memset(&res, 0, sizeof(res));
+      const int rc = e->poll(false, &fin, &res);
+      if (rc != PGX_SUCCESS || fin) {
+        if (rc != PGX_SUCCESS) res.status = rc;
+        srv->done.push_back({srv->slot_id[sidx], res});
+        srv->slot_id[sidx] = -1;
+      } else {
+        active++;
+      }
+    }
+  }
+  if (n_active) *n_active = active;
+  if (n_queued) *n_queued = (int32_t)srv->queue.size();
+  return PGX_SUCCESS;
+}
+
+int pgx_server_collect(pgx_server srv, int32_t max, int64_t* ids, pgx_result* results, int32_t* n) {
+  if (!srv || !n) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  int k = 0;
+  while (k < max && !srv->done.empty()) {
+    if (ids) ids[k] = srv->done.front().first;
+    if (results) results[k] = srv->done.front().second;
+    srv->done.pop_front();
+    k++;
+  }
+  *n = k;
+  return PGX_SUCCESS;
+}
+
+int pgx_server_destroy(pgx_server srv) {
+  if (!srv) return PGX_SUCCESS;
+  cudaSetDevice(srv->h->device);
+  // finish the in-flight solves so that no slot is left in the middle of a cycle
+  for (int sidx = 0; sidx < srv->h->nslots(); sidx++) {
+    if (srv->slot_id[sidx] < 0) continue;
+    bool fin = false;
+    while (!fin)
+      if (srv->h->slot(sidx)->poll(true, &fin, nullptr) != PGX_SUCCESS) break;
+  }
+  srv->h->servers--;
+  delete srv;
+  return PGX_SUCCESS;
 }
 
 int pgx_gemslr_kernel_stats(pgx_handle h, int32_t which, int32_t level, int32_t reps, double* avg_ms,

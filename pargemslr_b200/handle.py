@@ -148,6 +148,38 @@ class GemslrHandle:
                                                C.byref(res)))
         return _result(res)
 
+    def set_slots(self, nslots: int) -> None:
+        """Solve slots for concurrent solves (pgx_gemslr_set_slots); slot 0 is the handle."""
+        _abi.check(_abi.lib().pgx_gemslr_set_slots(self._h, nslots))
+
+    def slot_bytes(self, kdim: int) -> int:
+        """Device bytes of one additional slot for FGMRES(kdim)."""
+        b = C.c_int64(0)
+        _abi.check(_abi.lib().pgx_gemslr_slot_bytes(self._h, kdim, C.byref(b)))
+        return int(b.value)
+
+    def solve_batch_ptr(self, nrhs: int, x_ptr: int, ldx: int, b_ptr: int, ldb: int, location: int,
+                        params: Optional[np.ndarray] = None):
+        """Solve nrhs column systems spread over the slots; returns one result dict per column."""
+        p = None if params is None else np.ascontiguousarray(params, np.float64)
+        res = (_abi.Result * max(nrhs, 1))()
+        rc = _abi.lib().pgx_gemslr_solve_batch(self._h, nrhs, x_ptr, ldx, b_ptr, ldb, location, _abi.ptr(p),
+                                               C.cast(res, C.c_void_p))
+        _abi.check(rc)
+        return [_result(res[i]) for i in range(nrhs)]
+
+    def solve_batch(self, B: np.ndarray, X0: Optional[np.ndarray] = None, params: Optional[np.ndarray] = None):
+        """Host-array batch solve: B is (nrhs, n), one right-hand side per row; returns (X, results)."""
+        B = np.ascontiguousarray(B, np.float64)
+        X = np.zeros_like(B) if X0 is None else np.array(X0, dtype=np.float64, copy=True, order="C")
+        res = self.solve_batch_ptr(B.shape[0], _abi.ptr(X), self.n, _abi.ptr(B), self.n, _abi.LOCATION_HOST,
+                                   params)
+        return X, res
+
+    def server(self, params: Optional[np.ndarray] = None) -> "Server":
+        """A serving loop over this handle's slots (pgx_server_*)."""
+        return Server(self, params)
+
     def kernel_stats(self, which: int, level: int = 0, reps: int = 5):
         """(average ms, algorithmic bytes) of one building block (pgx_gemslr_kernel_stats)."""
         ms = C.c_double(0)
@@ -161,3 +193,76 @@ class GemslrHandle:
         z = np.zeros(self.n)
         _abi.check(_abi.lib().pgx_gemslr_precond_apply(self._h, _abi.ptr(z), _abi.ptr(v), _abi.LOCATION_HOST))
         return z
+
+
+class Server:
+    """Serving loop over one resident preconditioned matrix (pgx_server_*).
+
+    Requests queue in submission order; step() admits waiting requests into
+    free slots and advances the in-flight solves without blocking; collect()
+    returns finished (request id, result) pairs.  The arrays given to submit()
+    are kept alive here until their request is collected.
+    """
+
+    def __init__(self, handle: GemslrHandle, params: Optional[np.ndarray] = None):
+        self.handle = handle
+        self._params = None if params is None else np.ascontiguousarray(params, np.float64)
+        self._keep: dict = {}
+        s = C.c_void_p()
+        _abi.check(_abi.lib().pgx_server_create(handle._h, _abi.ptr(self._params), C.byref(s)))
+        self._s = s
+
+    def submit(self, x: np.ndarray, b: np.ndarray, request_id: int) -> None:
+        """Queue a host-array solve; x (contiguous float64, the initial guess) receives the solution."""
+        if x.dtype != np.float64 or not x.flags.c_contiguous or x.size != self.handle.n:
+            raise ValueError("x must be a contiguous float64 array of length n")
+        b = np.ascontiguousarray(b, np.float64)
+        _abi.check(_abi.lib().pgx_server_submit(self._s, _abi.ptr(x), _abi.ptr(b), _abi.LOCATION_HOST,
+                                                request_id))
+        self._keep[request_id] = (x, b)
+
+    def submit_ptr(self, x_ptr: int, b_ptr: int, location: int, request_id: int) -> None:
+        """Queue a solve on raw pointers (host or device, per location)."""
+        _abi.check(_abi.lib().pgx_server_submit(self._s, x_ptr, b_ptr, location, request_id))
+
+    def step(self):
+        """Advance every slot once without blocking; returns (active, queued)."""
+        a = C.c_int32(0)
+        q = C.c_int32(0)
+        _abi.check(_abi.lib().pgx_server_step(self._s, C.byref(a), C.byref(q)))
+        return a.value, q.value
+
+    def collect(self, max_n: int = 256):
+        ids = (C.c_int64 * max_n)()
+        res = (_abi.Result * max_n)()
+        n = C.c_int32(0)
+        _abi.check(_abi.lib().pgx_server_collect(self._s, max_n, C.cast(ids, C.c_void_p),
+                                                 C.cast(res, C.c_void_p), C.byref(n)))
+        out = []
+        for i in range(n.value):
+            self._keep.pop(int(ids[i]), None)
+            out.append((int(ids[i]), _result(res[i])))
+        return out
+
+    def run(self):
+        """Step until the queue and the slots are empty; returns every collected (id, result)."""
+        done = []
+        while True:
+            a, q = self.step()
+            done.extend(self.collect())
+            if a == 0 and q == 0:
+                break
+        done.extend(self.collect())
+        return done
+
+    def close(self) -> None:
+        if getattr(self, "_s", None):
+            _abi.lib().pgx_server_destroy(self._s)
+            self._s = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,88 @@
+"""Concurrent solve slots, batch solves and the serving loop.
+
+Every reduction on the solve path has a fixed order, so a right-hand side
+gives the same bits whether it is solved alone, in a batch spread over
+several slots, or among other requests in the serving queue.
+"""
+import numpy as np
+import pytest
+
+from pargemslr_b200 import params as P
+from pargemslr_b200 import problems
+from pargemslr_b200._abi import PgxError
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(grid=(24, 24, 24), nrhs=6, seed=5):
+    A = problems.laplacian(*grid)
+    n = A[0].size - 1
+    rng = np.random.default_rng(seed)
+    return A, n, rng.standard_normal((nrhs, n))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_equals_single_solves(precision):
+    from pargemslr_b200.handle import GemslrHandle
+    p = P.workload_params("lap3d_128")
+    A, n, B = _system()
+    h = GemslrHandle.from_matrix(A, p, precision=precision)
+    singles = [h.solve(b, params=p) for b in B]
+    h.set_slots(4)
+    assert h.slot_bytes(int(p[P.SOLVER_KDIM])) > 0
+    X, res = h.solve_batch(B, params=p)
+    for r, (x1, r1) in enumerate(singles):
+        assert res[r]["status"] == 0
+        assert res[r]["iters"] == r1["iters"]
+        assert res[r]["true_rel_res"] <= 1e-8
+        np.testing.assert_array_equal(X[r], x1)
+    # shrinking and growing the slot count keeps the shared factors intact
+    h.set_slots(2)
+    X2, _ = h.solve_batch(B[:3], params=p)
+    np.testing.assert_array_equal(X2, X[:3])
+    h.set_slots(1)
+    x0, _ = h.solve(B[0], params=p)
+    np.testing.assert_array_equal(x0, X[0])
+    h.close()
+
+
+def test_server_matches_single_solves_in_any_order():
+    from pargemslr_b200.handle import GemslrHandle
+    p = P.workload_params("lap3d_128")
+    A, n, B = _system(nrhs=7, seed=9)
+    h = GemslrHandle.from_matrix(A, p, precision="mixed")
+    singles = [h.solve(b, params=p)[0] for b in B]
+    h.set_slots(3)
+    srv = h.server(p)
+    xs = {}
+    for rid in (4, 0, 6, 2, 1, 5, 3):
+        xs[rid] = np.zeros(n)
+        srv.submit(xs[rid], B[rid], rid)
+    done = srv.run()
+    assert sorted(i for i, _ in done) == list(range(7))
+    for rid, res in done:
+        assert res["status"] == 0 and res["true_rel_res"] <= 1e-8
+        np.testing.assert_array_equal(xs[rid], singles[rid])
+    # a live server owns the slots
+    with pytest.raises(PgxError):
+        h.set_slots(5)
+    with pytest.raises(PgxError):
+        h.solve(B[0], params=p)
+    srv.close()
+    h.set_slots(5)
+    h.close()
+
+
+def test_batch_reports_a_bad_column():
+    from pargemslr_b200.handle import GemslrHandle
+    p = P.workload_params("lap3d_128")
+    A, n, B = _system(grid=(12, 12, 12), nrhs=3)
+    h = GemslrHandle.from_matrix(A, p, precision="fp64")
+    h.set_slots(2)
+    B[1, 7] = np.nan
+    with pytest.raises(PgxError):
+        h.solve_batch(B, params=p)
+    B[1, 7] = 0.0
+    X, res = h.solve_batch(B, params=p)
+    assert all(r["status"] == 0 for r in res)
+    h.close()
