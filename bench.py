@@ -7,7 +7,9 @@ with x_true = 2u - 1 seeded; 4 GeMSLR levels, ILUT drop 1e-3 / 200 per row,
 rank 16 per level, inner Schur FGMRES on level 0 (tol 1e-2, 5 steps),
 FGMRES(50) to relative residual 1e-8.  The preconditioner is built once by
 this library's host setup (pgx_gemslr_setup, untimed).  A "step" is one
-complete solve from x0 = 0.
+batch of --slots right-hand sides (b_r = A x_r, x_r seeded), each solved
+completely from x0 = 0, concurrently in that many solve slots over the one
+resident preconditioner (pgx_gemslr_solve_batch); value = solves/s.
 
   python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp64]
   python bench.py --impl reference ...   (the reference CPU solver, oracle/_ref)
@@ -35,6 +37,7 @@ sys.path.insert(0, ROOT)
 
 from pargemslr_b200 import params as P  # noqa: E402
 from pargemslr_b200 import pgxd, problems  # noqa: E402
+from pargemslr_b200._abi import LOCATION_DEVICE, LOCATION_HOST  # noqa: E402
 
 GRID = (128, 128, 128)
 WORKLOAD = "lap3d_128"
@@ -46,7 +49,7 @@ REF_ITERS = 39
 
 
 def metric_name() -> str:
-    return "solves/s (GeMSLR-FGMRES(50), rel-res 1e-8, 3D Laplacian 128^3)"
+    return "solves/s (GeMSLR-FGMRES(50), rel-res 1e-8, 3D Laplacian %d^3)" % GRID[0]
 
 
 class ClockSampler:
@@ -118,6 +121,17 @@ def ncu_traffic():
             return json.load(f)
     except (OSError, ValueError):
         return None
+
+
+def max_over_ranks(value: float, device) -> float:
+    """The largest value over all ranks (a one-element all-reduce; identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def build_problem():
@@ -198,60 +212,90 @@ def run_pgx(args):
 
     torch.cuda.set_device(local)
     p = P.workload_params(WORKLOAD)
-    A, n, b, xt = build_problem()
+    A, n, _, _ = build_problem()
+    R = args.slots
+    # one step = R right-hand sides b_r = A x_r (x_r seeded), solved concurrently in R slots
+    xts = np.stack([problems.x_true(n, SEED + r) for r in range(R)])
+    B = np.stack([problems.spmv(A, xts[r]) for r in range(R)])
     t0 = time.time()
     h = GemslrHandle.from_matrix(A, p, precision=args.precision, device=local)
     setup_s = time.time() - t0
+    h.set_slots(R)
     dev = torch.device("cuda", local)
-    b_dev = torch.from_numpy(b).to(dev)
-    x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+    B_dev = torch.from_numpy(B).to(dev)
+    X_dev = torch.zeros_like(B_dev)
+    ev_a = torch.cuda.Event(enable_timing=True)
+    ev_b = torch.cuda.Event(enable_timing=True)
 
-    def device_solve():
-        x_dev.zero_()
+    def device_step():
+        X_dev.zero_()
         torch.cuda.synchronize()
-        return h.solve_device(x_dev.data_ptr(), b_dev.data_ptr(), params=p)
+        ev_a.record()
+        res = h.solve_batch_ptr(R, X_dev.data_ptr(), n, B_dev.data_ptr(), n, LOCATION_DEVICE, p)
+        ev_b.record()
+        ev_b.synchronize()
+        return res, ev_a.elapsed_time(ev_b)
 
     for _ in range(args.warmup):
-        r = device_solve()
+        device_step()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
     wall0 = time.perf_counter()
-    ms, iters, rel, launches = [], [], [], []
+    ms, iters, rel, launches, lat = [], [], [], [], []
     for _ in range(args.steps):
-        r = device_solve()
-        ms.append(r["solve_ms"])
-        iters.append(r["iters"])
-        rel.append(r["true_rel_res"])
-        launches.append(r["launches"])
+        res, t_ms = device_step()
+        ms.append(t_ms)
+        lat.extend(r["solve_ms"] for r in res)
+        iters.extend(r["iters"] for r in res)
+        rel.extend(r["true_rel_res"] for r in res)
+        launches.append(sum(r["launches"] for r in res))
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     clk = clocks.stop()
-    total_ms = float(sum(ms))
+    total_ms = max_over_ranks(sum(ms), dev)
     if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
-    value = world * args.steps / (total_ms / 1e3)
-    x_err = float(np.linalg.norm(x_dev.cpu().numpy() - xt) / np.linalg.norm(xt))
+    value = world * args.steps * R / (total_ms / 1e3)
+    X = X_dev.cpu().numpy()
+    x_err = max(float(np.linalg.norm(X[r] - xts[r]) / np.linalg.norm(xts[r])) for r in range(R))
 
-    # end to end through the host-buffer C ABI call, pinned host memory
-    b_host = torch.from_numpy(b).pin_memory()
-    x_host = torch.zeros(n, dtype=torch.float64).pin_memory()
-    e2e_wall = []
+    # end to end through the host-buffer C ABI call: pinned host B and X, the
+    # copies in and out are inside every timed call
+    B_host = torch.from_numpy(B).pin_memory()
+    X_host = torch.zeros((R, n), dtype=torch.float64).pin_memory()
+    e2e_ms = []
     for _ in range(args.steps):
-        x_host.zero_()
-        t1 = time.perf_counter()
-        h.solve_host_ptr(x_host.data_ptr(), b_host.data_ptr(), params=p)
-        e2e_wall.append(time.perf_counter() - t1)
-    e2e_total = sum(e2e_wall)
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+        X_host.zero_()
+        torch.cuda.synchronize()
+        ev_a.record()
+        h.solve_batch_ptr(R, X_host.data_ptr(), n, B_host.data_ptr(), n, LOCATION_HOST, p)
+        ev_b.record()
+        ev_b.synchronize()
+        e2e_ms.append(ev_a.elapsed_time(ev_b))
+    e2e_total = max_over_ranks(sum(e2e_ms) / 1e3, dev)
+    h.set_slots(1)
+
+    # the plain FP64 path for comparison: FP64 preconditioner, one solve at a time
+    plain = None
+    if world == 1 and not args.no_fp64_plain:
+        h64 = GemslrHandle.from_matrix(A, p, precision="fp64", device=local)
+        pm, pit = [], []
+        for k in range(3):
+            x1 = torch.zeros(n, dtype=torch.float64, device=dev)
+            torch.cuda.synchronize()
+            ev_a.record()
+            r1 = h64.solve_device(x1.data_ptr(), B_dev[k % R].data_ptr(), params=p)
+            ev_b.record()
+            ev_b.synchronize()
+            if k > 0:  # the first solve is warm-up
+                pm.append(ev_a.elapsed_time(ev_b))
+                pit.append(r1["iters"])
+        h64.close()
+        plain = {"solves_per_s": len(pm) / (sum(pm) / 1e3), "ms_per_solve": sum(pm) / len(pm), "iters": pit,
+                 "what": "FP64 preconditioner, one solve at a time (pgx_gemslr_solve), same setup and RHS"}
 
     # roofline of the dominant kernel: the level-0 triangular passes
     lo_ms, lo_bytes = h.kernel_stats(0, 0, reps=5)
@@ -267,23 +311,27 @@ def run_pgx(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 preconditioner / f64 FGMRES" if args.precision == "mixed" else "f64",
         "data": "synthetic",
-        "config": {"workload": "3D 7-point Laplacian 128^3 (n=2,097,152), 4 levels, ILUT 1e-3/200, rank 16, "
-                               "inner Schur FGMRES(5) tol 1e-2, FGMRES(50) to 1e-8, x0 = 0",
+        "config": {"workload": "3D 7-point Laplacian %d^3 (n=%d), 4 levels, ILUT 1e-3/200, rank 16, "
+                               "inner Schur FGMRES(5) tol 1e-2, FGMRES(50) to 1e-8, x0 = 0" % (GRID[0], n),
                    "precision": args.precision, "setup": "pgx_gemslr_setup (this library), untimed",
-                   "setup_s": round(setup_s, 2), "iters": iters[-1], "true_rel_res": rel[-1], "x_err": x_err,
+                   "solves_per_step": R, "slots": R, "setup_s": round(setup_s, 2),
+                   "iters": [min(iters), max(iters)], "true_rel_res_max": max(rel), "x_err_max": x_err,
+                   "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                                  "what": "device time of each solve inside the batch (its slot's events)"},
+                   "fp64_plain": plain,
                    "l2": "inputs larger than L2 (preconditioner %.2f GB)" % (h.device_bytes(50) / 1e9),
                    "host_wall_s": wall},
-        "e2e": {"value": world * args.steps / e2e_total, "unit": "solves/s", "h2d_bytes_per_step": 16 * n,
-                "d2h_bytes_per_step": 8 * n},
+        "e2e": {"value": world * args.steps * R / e2e_total, "unit": "solves/s", "h2d_bytes_per_step": 16 * n * R,
+                "d2h_bytes_per_step": 8 * n * R},
         "gpu_launches": int(sum(launches)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "kernel": "trsv_seg_kernel (level-0 ILU L and U passes, mean)",
+                     "peak_kind": peak_kind, "kernel": "trsv_comp_kernel (level-0 ILU L and U passes, mean; one CTA per subdomain)",
                      "bytes_per_launch": tri_bytes, "ms_per_launch": tri_ms,
                      "traffic": traffic.get("bytes_per_launch") if traffic else None,
                      "spmv": {"achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "ms": spmv_ms}},
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and GRID == (128, 128, 128):
         cpu, why = cpu_sample(os.cpu_count() or 1, args.ref_iters, 1)
         if cpu is None:
             line["cpu_baseline"] = None
@@ -308,9 +356,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["pgx", "reference"], default="pgx")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--slots", type=int, default=32, help="right-hand sides solved concurrently per step")
+    ap.add_argument("--no-fp64-plain", action="store_true", help="skip the plain FP64 comparison solves")
     ap.add_argument("--ref-iters", type=int, default=3, help="FGMRES iterations in one reference CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=128,
+                    help="cube edge of the Laplacian (128 is the headline workload; smaller grids for profiling)")
     args = ap.parse_args()
+    global GRID
+    GRID = (args.grid,) * 3
     if args.impl == "reference":
         run_reference(args)
     else:
