@@ -221,7 +221,7 @@ struct DTri {
   bool seg = false;
   bool comp = false;  // one CTA per subdomain (trsv_comp_kernel)
   int nseg = 0, ncomp = 1;
-  int *comp_ch0 = nullptr, *ch_pos0 = nullptr, *far_ptr = nullptr, *far_k = nullptr;
+  int *comp_ch0 = nullptr, *cmeta = nullptr, *far_col = nullptr;  // one-CTA-per-subdomain schedule
   T* dslot = nullptr;   // upper pass: inverse diagonal in slot order
   int* uslot = nullptr; // lower pass: upper-pass slot of each row, in slot order
   int nslots = 0;       // length of the slot arrays (padded row list)
@@ -460,70 +460,80 @@ static int upload_tri_comp(Arena& ar, const HostCsr& h, bool upper, const std::v
   auto pad4 = [](std::vector<int>& v, int fill) {
     while (v.size() % 4) v.push_back(fill);
   };
-  std::vector<int> ord, rp, cj, lvb, row0(1, 0), rp0(1, 0), nnz0(1, 0), lv0(1, 0), nlvb, pos0, comp_ch0(1, 0);
-  std::vector<int> far_ptr(1, 0), far_k;
+  // far operands of each row: producers at least `ring` positions before the
+  // end of the row's level
+  std::vector<int> nfar(n, 0);
+  for (int r = 0; r < n; r++)
+    for (int k = h.rp[r]; k < h.rp[r + 1]; k++)
+      if (lvl_end[r] - posc[h.cj[k]] >= CC::ring) nfar[r]++;
+  for (int r = 0; r < n; r++)
+    if (nfar[r] > CC::far) return PGX_ERROR_INVALID_PARAM;
+  std::vector<int> ord, rp, cj, lvb, meta, comp_ch0(1, 0), far_col;
   std::vector<double> va;
   const int ROWCAP = CC::rows - 4, NNZCAP = CC::nnz - 4;
+  auto push_meta = [&](int pos0) {
+    meta.insert(meta.end(), {(int)ord.size(), (int)rp.size(), (int)cj.size(), (int)lvb.size(), pos0,
+                             (int)far_col.size(), 0, 0});
+  };
   for (int c = 0; c < ncomp; c++) {
     const auto& sc = sched[c];
     size_t p = 0;
-    int prev_start = 0;
+    int prev_start = 0, chunk_in_comp = 0;
     while (p < sc.size()) {
-      // one chunk: consecutive positions within the row and nonzero caps
+      // one chunk: consecutive positions within the row, nonzero and far caps
       size_t e = p;
       long long nz = 0;
+      int nf = 0;
       while (e < sc.size() && (int)(e - p) < ROWCAP) {
         const int rn = h.rp[sc[e] + 1] - h.rp[sc[e]];
-        if (nz + rn > NNZCAP) break;
+        if (nz + rn > NNZCAP || nf + nfar[sc[e]] > CC::far) break;
         nz += rn;
+        nf += nfar[sc[e]];
         e++;
       }
-      pos0.push_back((int)p);
+      push_meta((int)p);
+      const int far_base = CC::ring + (chunk_in_comp & 1) * CC::far;
+      const int far0 = (int)far_col.size();
       rp.push_back(0);
       int acc = 0;
-      const size_t chunk_nnz0 = cj.size();
       for (size_t q = p; q < e; q++) {
         const int r = sc[q];
         ord.push_back(r);
         for (int k = h.rp[r]; k < h.rp[r + 1]; k++) {
           const int j = h.cj[k];
           const int qj = posc[j];
-          const bool near = lvl_end[r] - qj < CC::ring;
-          if (!near) {
-            // far: the producer folds it in while the previous chunk is being
-            // solved, so it must lie before that chunk (ring >> chunk size)
+          if (lvl_end[r] - qj < CC::ring) {
+            cj.push_back(-((qj & (CC::ring - 1)) + 1));
+          } else {
+            // far: gathered while the previous chunk is solved, so it must
+            // have been published before that chunk began
             if (qj >= prev_start) return PGX_ERROR_INVALID_PARAM;
-            far_k.push_back((int)(cj.size() - chunk_nnz0));
+            cj.push_back(-(far_base + ((int)far_col.size() - far0) + 1));
+            far_col.push_back(j);
           }
-          cj.push_back(near ? -((qj & (CC::ring - 1)) + 1) : j);
           va.push_back(h.va[k]);
         }
         acc += h.rp[r + 1] - h.rp[r];
         rp.push_back(acc);
       }
       pad4(ord, -1);
-      row0.push_back((int)ord.size());
       pad4(rp, acc);
-      rp0.push_back((int)rp.size());
       while (cj.size() % 4) {
         cj.push_back(0);
         va.push_back(0.0);
       }
-      nnz0.push_back((int)cj.size());
-      const int base = (int)lvb.size();
       lvb.push_back(0);
       for (size_t q = p + 1; q < e; q++)
         if (lev[sc[q]] != lev[sc[q - 1]]) lvb.push_back((int)(q - p));
       lvb.push_back((int)(e - p));
-      nlvb.push_back((int)lvb.size() - base);
       pad4(lvb, (int)(e - p));
-      lv0.push_back((int)lvb.size());
-      far_ptr.push_back((int)far_k.size());
       prev_start = (int)p;
+      chunk_in_comp++;
       p = e;
     }
-    comp_ch0.push_back((int)pos0.size());
+    comp_ch0.push_back((int)meta.size() / 8);
   }
+  push_meta(0);  // closes the last chunk
   // slot of every row in the flat row list; the upper pass's slots index its
   // dinv and the y the lower pass leaves behind
   std::vector<int> slot(n, -1);
@@ -547,7 +557,7 @@ static int upload_tri_comp(Arena& ar, const HostCsr& h, bool upper, const std::v
   d.ncomp = ncomp;
   d.nslots = (int)ord.size();
   d.nlevels = (int)lptr.size() - 1;
-  d.nseg = (int)pos0.size();
+  d.nseg = (int)meta.size() / 8 - 1;
   d.nnz_total = h.nnz();
   // lanes per row: one level of an average chunk in one sweep of the workers
   d.S = std::min(pick_lanes(h.nnz(), n), 16);
@@ -557,15 +567,9 @@ static int upload_tri_comp(Arena& ar, const HostCsr& h, bool upper, const std::v
   PGX_TRY(ar.upload(&d.cj, cj.data(), cj.size(), s));
   PGX_TRY(ar.upload(&d.va, va.data(), va.size(), s));
   PGX_TRY(ar.upload(&d.lvb, lvb.data(), lvb.size(), s));
-  PGX_TRY(ar.upload(&d.seg_row0, row0.data(), row0.size(), s));
-  PGX_TRY(ar.upload(&d.seg_rp0, rp0.data(), rp0.size(), s));
-  PGX_TRY(ar.upload(&d.seg_nnz0, nnz0.data(), nnz0.size(), s));
-  PGX_TRY(ar.upload(&d.seg_lv0, lv0.data(), lv0.size(), s));
-  PGX_TRY(ar.upload(&d.seg_nlvb, nlvb.data(), nlvb.size(), s));
-  PGX_TRY(ar.upload(&d.ch_pos0, pos0.data(), pos0.size(), s));
+  PGX_TRY(ar.upload(&d.cmeta, meta.data(), meta.size(), s));
   PGX_TRY(ar.upload(&d.comp_ch0, comp_ch0.data(), comp_ch0.size(), s));
-  PGX_TRY(ar.upload(&d.far_ptr, far_ptr.data(), far_ptr.size(), s));
-  PGX_TRY(ar.upload(&d.far_k, far_k.data(), far_k.size(), s));
+  PGX_TRY(ar.upload(&d.far_col, far_col.data(), far_col.size(), s));
   if (upper)
     PGX_TRY(ar.upload(&d.dslot, dsl.data(), dsl.size(), s));
   else
@@ -1148,24 +1152,20 @@ struct Engine : EngineBase {
     if (T.comp) {
       const size_t bytes = CompCfg<P>::bytes;
       CompArrays ca;
-      ca.ch_row0 = T.seg_row0;
-      ca.ch_rp0 = T.seg_rp0;
-      ca.ch_nnz0 = T.seg_nnz0;
-      ca.ch_lv0 = T.seg_lv0;
+      ca.meta = (const int4*)T.cmeta;
       ca.ord = T.ord;
       ca.rp = T.rp;
       ca.cj = T.cj;
       ca.lvb = T.lvb;
       ca.uslot = T.uslot;
-      ca.far_ptr = T.far_ptr;
-      ca.far_k = T.far_k;
+      ca.far_col = T.far_col;
 #define PGX_TRSVCOMP(SS)                                                                                        \
   if (upper)                                                                                                    \
-    trsv_comp_kernel<P, SS, true><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, T.ch_pos0, ca, T.va, \
+    trsv_comp_kernel<P, SS, true><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, ca, T.va, \
                                                                             T.dslot, yslot, rhs, rhs_scale, y, x, \
                                                                             err, sk);                             \
   else                                                                                                          \
-    trsv_comp_kernel<P, SS, false><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, T.ch_pos0, ca, T.va, \
+    trsv_comp_kernel<P, SS, false><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, ca, T.va, \
                                                                              T.dslot, yslot, rhs, rhs_scale, y,    \
                                                                              x, err, sk)
       switch (T.S) {
@@ -1700,6 +1700,7 @@ struct Engine : EngineBase {
     out.reset(e);
     return e->clone_from(*this);
   }
+
 };
 
 }  // namespace pgx

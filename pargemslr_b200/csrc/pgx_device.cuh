@@ -434,34 +434,42 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
 // ILU factor are short-range: for the RCM-ordered subdomains of a 3D problem
 // the median distance between a row and the rows it needs is ~10^3
 // positions and almost all are within 10^4.  So one CTA walks a whole
-// subdomain in level order and keeps the most recent results in a shared-
-// memory ring indexed by schedule position; a dependency within the ring is a
-// shared-memory read.  An older one was computed by this CTA at least `ring`
-// positions earlier, before the current chunk was staged, so it is read back
-// from global memory once per chunk and folded into the staged value
-// (column index marked kFarDone).  The host encodes each column index as
-// -(ring slot + 1) or as the row index of a far dependency.
-//
-// The subdomain's schedule is cut into chunks that fit a staging buffer;
-// there are two buffers.  While the CTA sweeps the levels of chunk k (one
-// barrier per level), every thread has already issued its cp.async copies of
-// chunk k+1 (row list, row pointers, columns, values, level boundaries and,
-// for the upper pass, the inverse diagonal and y in slot order).  At the
-// chunk boundary the lower pass gathers the right-hand side of chunk k+1
-// through its staged row list and both passes fold in far dependencies.  No
-// CTA waits on another: no deadlock, no tickets, one CTA per subdomain.
+// subdomain (trsv_comp_kernel below).
 constexpr int kCompThreads = 1024;
-constexpr int kFarDone = INT_MIN;
 template <typename T>
 struct CompCfg {
   static constexpr int ring = 8192;                           // 32 KB (f32) / 64 KB (f64)
+  static constexpr int far = 1024;                            // far operands per chunk (per buffer)
   static constexpr int nnz = sizeof(T) == 8 ? 4096 : 8192;    // per chunk buffer
   static constexpr int rows = sizeof(T) == 8 ? 768 : 1024;    // per chunk buffer (incl. padding)
   // per buffer: va[nnz] T | sb[rows] T | sd[rows] T | cj[nnz] int | ord[rows] int | rp[rows+4] int | lvb[rows+4] int
   static constexpr size_t buf_bytes =
       sizeof(T) * (size_t)(nnz + 2 * rows) + sizeof(int) * (size_t)(nnz + rows + 2 * (rows + 4));
-  static constexpr size_t bytes = sizeof(T) * (size_t)ring + 2 * buf_bytes;
+  // ring and the two far-operand buffers are one array: operand index -(c+1)
+  static constexpr size_t bytes = sizeof(T) * (size_t)(ring + 2 * far) + 2 * buf_bytes;
+  static_assert(bytes <= 227 * 1024, "per-subdomain solve exceeds the shared memory of one CTA");
+  static_assert(far <= 1024 && rows <= 1024, "one gather per thread of a 1024-thread CTA");
 };
+
+// Per-chunk metadata, two int4 per chunk: {row0, rp0, nnz0, lv0} and
+// {pos0, far0, 0, 0}: first slot of the chunk in the row list, the row
+// pointers, the nonzeros and the level boundaries; its first schedule
+// position; its first far operand.  One record past the last chunk closes the
+// ranges.
+struct ChunkMeta {
+  int row0, rp0, nnz0, lv0, pos0, far0;
+};
+__device__ __forceinline__ ChunkMeta load_meta(const int4* __restrict__ meta, int ch) {
+  const int4 a = __ldg(&meta[2 * ch]), b = __ldg(&meta[2 * ch + 1]);
+  ChunkMeta m;
+  m.row0 = a.x;
+  m.rp0 = a.y;
+  m.nnz0 = a.z;
+  m.lv0 = a.w;
+  m.pos0 = b.x;
+  m.far0 = b.y;
+  return m;
+}
 
 __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -488,7 +496,7 @@ struct CompBuf {
 template <typename T>
 __device__ __forceinline__ CompBuf<T> comp_buf(unsigned char* base, int which) {
   using C = CompCfg<T>;
-  unsigned char* b = base + sizeof(T) * (size_t)C::ring + (size_t)which * C::buf_bytes;
+  unsigned char* b = base + sizeof(T) * (size_t)(C::ring + 2 * C::far) + (size_t)which * C::buf_bytes;
   CompBuf<T> o;
   o.va = (T*)b;
   o.sb = o.va + C::nnz;
@@ -501,86 +509,90 @@ __device__ __forceinline__ CompBuf<T> comp_buf(unsigned char* base, int which) {
 }
 
 struct CompArrays {
-  const int *ch_row0, *ch_rp0, *ch_nnz0, *ch_lv0, *ord, *rp, *cj, *lvb, *uslot, *far_ptr, *far_k;
+  const int4* meta;
+  const int *ord, *rp, *cj, *lvb, *uslot, *far_col;
 };
 
-// all threads: issue the bulk copies of chunk ch into buffer b
+// all threads: issue the bulk copies of the chunk [m, me) into buffer b
 template <typename T, bool UPPER>
-__device__ __forceinline__ void comp_stage_bulk(const CompBuf<T>& b, int ch, const CompArrays& g,
-                                                const T* __restrict__ va, const T* __restrict__ dslot,
-                                                const T* yslot) {
-  const int r0 = g.ch_row0[ch], r1 = g.ch_row0[ch + 1];
-  const int p0 = g.ch_rp0[ch], p1 = g.ch_rp0[ch + 1];
-  const int z0 = g.ch_nnz0[ch], z1 = g.ch_nnz0[ch + 1];
-  const int v0 = g.ch_lv0[ch], v1 = g.ch_lv0[ch + 1];
-  stage16(b.va, va + z0, (z1 - z0) * (int)sizeof(T));
-  stage16(b.cj, g.cj + z0, (z1 - z0) * 4);
-  stage16(b.ord, g.ord + r0, (r1 - r0) * 4);
-  stage16(b.rp, g.rp + p0, (p1 - p0) * 4);
-  stage16(b.lvb, g.lvb + v0, (v1 - v0) * 4);
+__device__ __forceinline__ void comp_stage_bulk(const CompBuf<T>& b, const ChunkMeta& m, const ChunkMeta& me,
+                                                const CompArrays& g, const T* __restrict__ va,
+                                                const T* __restrict__ dslot, const T* yslot) {
+  stage16(b.va, va + m.nnz0, (me.nnz0 - m.nnz0) * (int)sizeof(T));
+  stage16(b.cj, g.cj + m.nnz0, (me.nnz0 - m.nnz0) * 4);
+  stage16(b.ord, g.ord + m.row0, (me.row0 - m.row0) * 4);
+  stage16(b.rp, g.rp + m.rp0, (me.rp0 - m.rp0) * 4);
+  stage16(b.lvb, g.lvb + m.lv0, (me.lv0 - m.lv0) * 4);
   if (UPPER) {
-    stage16(b.sd, dslot + r0, (r1 - r0) * (int)sizeof(T));
-    stage16(b.sb, yslot + r0, (r1 - r0) * (int)sizeof(T));
+    stage16(b.sd, dslot + m.row0, (me.row0 - m.row0) * (int)sizeof(T));
+    stage16(b.sb, yslot + m.row0, (me.row0 - m.row0) * (int)sizeof(T));
   } else {
-    stage16(b.sd, g.uslot + r0, (r1 - r0) * 4);  // upper-pass slot of each row (ints in sd)
+    stage16(b.sd, g.uslot + m.row0, (me.row0 - m.row0) * 4);  // upper-pass slot of each row (ints in sd)
   }
 }
 
-// all threads, after the bulk copies of chunk ch have landed: gather the
-// lower pass's right-hand side and fold in far dependencies
-template <typename T, bool UPPER>
-__device__ __forceinline__ void comp_stage_gather(const CompBuf<T>& b, int ch, const CompArrays& g, const T* rhs,
-                                                  const T* out, int n, int* err) {
-  const int r0 = g.ch_row0[ch], r1 = g.ch_row0[ch + 1];
-  if (!UPPER) {
-    for (int i = threadIdx.x; i < r1 - r0; i += blockDim.x) {
-      const int r = b.ord[i];
-      if (r >= 0) cp_async_elem(&b.sb[i], &rhs[r]);
-    }
-  }
-  const int f0 = g.far_ptr[ch], f1 = g.far_ptr[ch + 1];
-  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
-    const int k = __ldg(&g.far_k[f]);
-    const int c = b.cj[k];
-    if ((unsigned)c < (unsigned)n) {
-      b.va[k] = b.va[k] * __ldcg(&out[c]);
-    } else {
-      atomicOr(err, kErrIndex);
-      b.va[k] = 0;
-    }
-    b.cj[k] = kFarDone;
-  }
-}
-
+// One CTA per subdomain solves its rows level by level (the schedule of
+// IluClass::BuildLevels, ilu.cpp:832-1062, restricted to the subdomain): a
+// lower pass y = L^-1 rhs or an upper pass x = D U^-1 y.  Results live in a
+// shared-memory ring indexed by schedule position, so a dependency on the
+// last `ring` positions is a shared-memory read.  An older ("far") operand
+// lies, by construction on the host, before the start of the previous chunk:
+// it was published to global memory before that chunk began, so it is
+// gathered into the far buffer while the previous chunk is being solved and
+// is read from there.  Column indices are encoded as -(index + 1) into the
+// ring-plus-far array.
+//
+// The subdomain's schedule is cut into chunks that fit a staging buffer;
+// there are two buffers.  While the CTA sweeps the levels of chunk k (one
+// barrier per level), the copies of chunk k+1 are in flight: the bulk
+// arrays at once, and, after the first level, the far operands and (lower
+// pass) the right-hand side gathered through the row list.  The chunk
+// metadata is loaded three chunks ahead.  At a chunk boundary the CTA only
+// publishes the chunk's results and waits for its copies.  No CTA waits on
+// another: no tickets, no deadlock.
 template <typename T, int S, bool UPPER>
 __global__ void __launch_bounds__(kCompThreads) trsv_comp_kernel(
     int n, const int* __restrict__ comp_ch0,  // ncomp+1: chunk range of each subdomain
-    const int* __restrict__ ch_pos0,          // first schedule position of each chunk
     CompArrays g, const T* __restrict__ va, const T* __restrict__ dslot, T* yslot, const T* rhs,
     const double* __restrict__ rhs_scale, T* y, T* x, int* err, Skip skip) {
   if (skip.on()) return;
   using C = CompCfg<T>;
+  constexpr int RF = C::ring + 2 * C::far;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* ring = (T*)smem_raw;
+  T* ring = (T*)smem_raw;  // ring, then far buffer 0, then far buffer 1
   const int tid = threadIdx.x, lane = tid & 31;
   const int c0 = comp_ch0[blockIdx.x], c1 = comp_ch0[blockIdx.x + 1];
-  T* out = UPPER ? x : y;  // this pass's result, also the far-dependency store
+  T* out = UPPER ? x : y;  // this pass's result, also the store of far operands
   const double rs = rhs_scale ? *rhs_scale : 1.0;
   if (c0 >= c1) return;
-  comp_stage_bulk<T, UPPER>(comp_buf<T>(smem_raw, 0), c0, g, va, dslot, yslot);
-  cp_async_wait_all();
-  __syncthreads();
-  comp_stage_gather<T, UPPER>(comp_buf<T>(smem_raw, 0), c0, g, rhs, out, n, err);
-  cp_async_wait_all();
-  __syncthreads();
+  ChunkMeta m0 = load_meta(g.meta, c0), m1 = load_meta(g.meta, c0 + 1);
+  ChunkMeta m2 = c0 + 2 <= c1 ? load_meta(g.meta, c0 + 2) : m1;
+  {
+    // the first chunk of a subdomain has no far operands
+    const CompBuf<T> b = comp_buf<T>(smem_raw, 0);
+    comp_stage_bulk<T, UPPER>(b, m0, m1, g, va, dslot, yslot);
+    if (!UPPER && tid < m1.row0 - m0.row0) {
+      const int r = __ldg(&g.ord[m0.row0 + tid]);
+      if (r >= 0) cp_async_elem(&b.sb[tid], &rhs[r]);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
   const int sl = tid & (S - 1), group = tid / S, ngroups = kCompThreads / S;
   for (int ch = c0; ch < c1; ch++) {
     const int bi = (ch - c0) & 1;
-    if (ch + 1 < c1) comp_stage_bulk<T, UPPER>(comp_buf<T>(smem_raw, bi ^ 1), ch + 1, g, va, dslot, yslot);
+    const CompBuf<T> nb = comp_buf<T>(smem_raw, bi ^ 1);
+    int rhs_row = -1, far_col = -1;
+    if (ch + 1 < c1) {
+      comp_stage_bulk<T, UPPER>(nb, m1, m2, g, va, dslot, yslot);
+      if (!UPPER && tid < m2.row0 - m1.row0) rhs_row = __ldg(&g.ord[m1.row0 + tid]);
+      if (tid < m2.far0 - m1.far0) far_col = __ldg(&g.far_col[m1.far0 + tid]);
+    }
+    const ChunkMeta m3 = ch + 3 <= c1 ? load_meta(g.meta, ch + 3) : m2;
     const CompBuf<T> b = comp_buf<T>(smem_raw, bi);
-    const int pos0 = ch_pos0[ch];
-    const int r0 = g.ch_row0[ch];
-    const int nl = g.ch_lv0[ch + 1] - g.ch_lv0[ch];
+    const int pos0 = m0.pos0;
+    const int nl = m1.lv0 - m0.lv0;
+    bool gathered = false;
     for (int lv = 0; lv + 1 < nl; lv++) {
       const int a = b.lvb[lv], e = b.lvb[lv + 1];
       if (a >= e) break;  // padding after the last boundary
@@ -588,16 +600,11 @@ __global__ void __launch_bounds__(kCompThreads) trsv_comp_kernel(
         T acc = 0;
         const int k1 = b.rp[i], k2 = b.rp[i + 1];
         for (int k = k1 + sl; k < k2; k += S) {
-          const int c = b.cj[k];
-          if (c == kFarDone) {
-            acc += b.va[k];  // dependency already folded into the value
-          } else if (c < 0) {
-            acc += b.va[k] * ring[-c - 1];
-          } else if ((unsigned)c < (unsigned)n) {
-            acc += b.va[k] * __ldcg(&out[c]);
-          } else {
+          const int q = -b.cj[k] - 1;
+          if ((unsigned)q < (unsigned)RF)
+            acc += b.va[k] * ring[q];
+          else
             atomicOr(err, kErrIndex);
-          }
         }
         acc = group_reduce(acc, S, lane);
         if (sl == 0) {
@@ -613,28 +620,39 @@ __global__ void __launch_bounds__(kCompThreads) trsv_comp_kernel(
         }
       }
       __syncthreads();
-    }
-    // publish the chunk's results from the ring: natural order (far
-    // dependencies and the consumer) and, for the lower pass, the upper
-    // pass's slot order
-    (void)r0;
-    {
-      const int nrows_ch = g.ch_row0[ch + 1] - g.ch_row0[ch];
-      for (int i = tid; i < nrows_ch; i += blockDim.x) {
-        const int r = b.ord[i];
-        if (r < 0) continue;
-        const T o = ring[(pos0 + i) & (C::ring - 1)];
-        out[r] = o;
-        if (!UPPER) yslot[((const int*)b.sd)[i]] = o;
+      if (!gathered) {
+        // the next chunk's gathers, once the loads of their indices had a level to land
+        gathered = true;
+        if (rhs_row >= 0) cp_async_elem(&nb.sb[tid], &rhs[rhs_row]);
+        if (far_col >= 0) {
+          if ((unsigned)far_col < (unsigned)n)
+            cp_async_elem(&ring[C::ring + (bi ^ 1) * C::far + tid], &out[far_col]);
+          else
+            atomicOr(err, kErrIndex);
+        }
       }
+    }
+    if (!gathered) {
+      if (rhs_row >= 0) cp_async_elem(&nb.sb[tid], &rhs[rhs_row]);
+      if (far_col >= 0 && (unsigned)far_col < (unsigned)n)
+        cp_async_elem(&ring[C::ring + (bi ^ 1) * C::far + tid], &out[far_col]);
+    }
+    // publish the chunk's results from the ring: natural order (far operands
+    // and the consumer) and, for the lower pass, the upper pass's slot order
+    for (int i = tid; i < m1.row0 - m0.row0; i += blockDim.x) {
+      const int r = b.ord[i];
+      if (r < 0) continue;
+      const T o = ring[(pos0 + i) & (C::ring - 1)];
+      out[r] = o;
+      if (!UPPER) yslot[((const int*)b.sd)[i]] = o;
     }
     if (ch + 1 < c1) {
       cp_async_wait_all();
       __syncthreads();
-      comp_stage_gather<T, UPPER>(comp_buf<T>(smem_raw, bi ^ 1), ch + 1, g, rhs, out, n, err);
-      cp_async_wait_all();
-      __syncthreads();
     }
+    m0 = m1;
+    m1 = m2;
+    m2 = m3;
   }
 }
 
