@@ -179,6 +179,42 @@ int pgx_gemslr_device_bytes(pgx_handle handle, int32_t kdim, int64_t *bytes);
 int pgx_gemslr_solve(pgx_handle handle, double *x, const double *b, int32_t location,
                      const double *params, pgx_result *result);
 
+/* ---- solve without device allocation -------------------------------------
+ * No counterpart in the reference: it exists for callers of this library
+ * that must not allocate device memory at solve time.  pgx_gemslr_solve
+ * allocates a slot's Krylov basis on its first solve (and again when kdim
+ * grows) and instantiates a CUDA graph of the restart cycle.  Some callers
+ * cannot let that happen: an application whose device memory is owned by
+ * its own pool (a framework's caching allocator or a fixed arena sized at
+ * start-up) can see cudaMalloc fail although the pool has room; a
+ * latency-bound loop cannot take the device-wide synchronisation that
+ * cudaMalloc and cudaFree may cause; a service with a fixed memory budget
+ * must not grow after start-up.
+ *
+ * pgx_gemslr_solve_static is pgx_gemslr_solve (same arguments, results and
+ * errors) with the Krylov basis taken from a fixed pool of
+ * PGX_STATIC_BASIS_BYTES in the library's static device memory, and with the
+ * restart cycles enqueued kernel by kernel; it calls no cudaMalloc, cudaFree
+ * or allocating library routine.  The pool must hold the basis:
+ * 8*n*(kdim+1) bytes (rounded up to 256) plus n*(kdim+1) entries of the
+ * preconditioner precision (8 bytes FP64, 4 bytes mixed); e.g. kdim = 50
+ * allows n up to 41,120 in FP64 and 54,827 in the mixed precision.  Larger
+ * problems are refused with PGX_ERROR_INVALID_PARAM and a message giving
+ * both sizes.  The handle's own work space (allocated by commit) is used
+ * as by pgx_gemslr_solve.
+ *
+ * Every GPU on which the library is loaded holds the pool until the process
+ * exits.  The first call on a device looks up the pool's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture
+ * begins.  All calls on one device share the pool and each clears the part
+ * it uses before the solve, but calls that overlap on the GPU (from several
+ * host threads, on one or several handles of the same device) race on it:
+ * the caller must serialise them.  result->launches is 0: the kernels are
+ * not counted by this variant. */
+#define PGX_STATIC_BASIS_BYTES (32u << 20)
+int pgx_gemslr_solve_static(pgx_handle handle, double *x, const double *b, int32_t location,
+                            const double *params, pgx_result *result);
+
 /* ---- concurrent solves and serving --------------------------------------
  * A committed handle holds the preconditioner (factors, coupling blocks,
  * low-rank bases) once; each solve slot adds its own work space (CUDA

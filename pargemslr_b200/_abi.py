@@ -42,6 +42,7 @@ EXPORTS = (
     "pgx_csr_spmv_device", "pgx_gemslr_setup", "pgx_gemslr_kernel_stats",
     "pgx_gemslr_set_slots", "pgx_gemslr_slot_bytes", "pgx_gemslr_solve_batch",
     "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
+    "pgx_gemslr_solve_static",
 )
 
 
@@ -110,6 +111,7 @@ def lib() -> C.CDLL:
     L.pgx_server_step.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
     L.pgx_server_collect.argtypes = [vp, i32, vp, vp, C.POINTER(i32)]
     L.pgx_server_destroy.argtypes = [vp]
+    L.pgx_gemslr_solve_static.argtypes = [vp, vp, vp, i32, vp, vp]
     for name in EXPORTS:
         if name != "pgx_last_error":
             getattr(L, name).restype = C.c_int

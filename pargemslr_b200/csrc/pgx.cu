@@ -26,6 +26,7 @@
 #include <cstring>
 #include <deque>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <type_traits>
@@ -638,6 +639,8 @@ struct EngineBase {
   virtual int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol) = 0;
   virtual int poll(bool block, bool* finished, pgx_result* res) = 0;
   virtual int make_clone(std::unique_ptr<EngineBase>& out) = 0;
+  virtual int solve_fixed_basis(double* x, const double* b, int location, int kdim, int maxits, double tol,
+                                int atol, void* pool, size_t pool_bytes, pgx_result* res) = 0;
 };
 
 
@@ -1701,12 +1704,148 @@ struct Engine : EngineBase {
     return e->clone_from(*this);
   }
 
+  // FGMRES with the Krylov basis in memory handed in by the caller (the
+  // static pool of pgx_gemslr_solve_static) and every restart cycle enqueued
+  // directly on the stream instead of through a captured graph: nothing is
+  // allocated and no graph is instantiated.  The arithmetic and its order are
+  // those of begin()/poll().
+  int solve_fixed_basis(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+                        void* pool, size_t pool_bytes, pgx_result* res) override {
+    if (phase != IDLE) return fail(PGX_ERROR_FUNCTION_CALL, "slot busy");
+    if (kdim < 1 || kdim > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", kdim, KMAX);
+    if (maxits < 0) return fail(PGX_ERROR_INVALID_PARAM, "maxits %d < 0", maxits);
+    const size_t cols = (size_t)kdim + 1;
+    const size_t vbytes = (sizeof(double) * (size_t)n * cols + 255) & ~(size_t)255;
+    const size_t zbytes = sizeof(P) * (size_t)n * cols;
+    if (vbytes + zbytes > pool_bytes)
+      return fail(PGX_ERROR_INVALID_PARAM,
+                  "n = %d with kdim = %d needs %zu bytes of Krylov basis; the static pool holds %zu", n, kdim,
+                  vbytes + zbytes, pool_bytes);
+    if (location == PGX_LOCATION_HOST) {
+      for (int i = 0; i < n; i++)
+        if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%d] is not finite", i);
+    }
+    double* own_V = V;
+    P* own_Z = Z;
+    V = (double*)pool;
+    Z = (P*)((char*)pool + vbytes);
+    const int rc = run_fixed_basis(x, b, location, kdim, maxits, tol, atol, vbytes, zbytes, res);
+    V = own_V;
+    Z = own_Z;
+    return rc;
+  }
+
+  int run_fixed_basis(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+                      size_t vbytes, size_t zbytes, pgx_result* res) {
+    double* xd = x;
+    const double* bd = b;
+    if (location == PGX_LOCATION_HOST) {
+      PGX_CUDA(cudaMemcpyAsync(bdev, b, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaMemcpyAsync(xdev, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      xd = xdev;
+      bd = bdev;
+    }
+    // the pool keeps whatever the previous call left in it
+    PGX_CUDA(cudaMemsetAsync(V, 0, vbytes, stream));
+    PGX_CUDA(cudaMemsetAsync(Z, 0, zbytes, stream));
+    FgmresDev h;
+    memset(&h, 0, sizeof(h));
+    h.kdim = kdim;
+    h.maxits = maxits;
+    h.tol = tol;
+    h.absolute = atol;
+    h.eps = DBL_EPSILON;
+    h.cycle_done = 1;
+    const size_t head = offsetof(FgmresDev, sc);
+    *hs_pin = h;
+    PGX_CUDA(cudaMemcpyAsync(st, hs_pin, head, cudaMemcpyHostToDevice, stream));
+    PGX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
+    PGX_CUDA(cudaEventRecord(ev0, stream));
+    {
+      auto a = ts_args<double, double, double>(n, mk_skip());
+      a.in = bd;
+      a.epi = EPI_NORMB;
+      a.st = st;
+      ts<double, double, double, TS_NORM_COPY>(a);
+    }
+    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
+                                         mk_skip(&st->done));
+    {
+      auto a = ts_args<double, double, double>(n, mk_skip());
+      a.in = V;
+      a.epi = EPI_INIT;
+      a.st = st;
+      ts<double, double, double, TS_NORM_COPY>(a);
+    }
+    const int max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
+    for (int cyc = 0; cyc < max_cycles; cyc++) {
+      enqueue_cycle(kdim, xd, bd);
+      PGX_CUDA(cudaGetLastError());
+      PGX_CUDA(cudaMemcpyAsync(hs_pin, st, head, cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaStreamSynchronize(stream));
+      if (hs_pin->done || hs_pin->iter >= maxits) break;
+    }
+    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, rdev, nullptr, mk_skip());
+    {
+      auto a = ts_args<double, double, double>(n, mk_skip());
+      a.in = rdev;
+      a.epi = EPI_STORE;
+      a.dst = scal;
+      ts<double, double, double, TS_NORM_COPY>(a);
+    }
+    PGX_CUDA(cudaEventRecord(ev1, stream));
+    PGX_CUDA(cudaMemcpyAsync(hs_pin, st, head, cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaMemcpyAsync(r2_pin, scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    const FgmresDev hs = *hs_pin;
+    const double r2 = *r2_pin;
+    const int rc = check_err();
+    float ms = 0.f;
+    PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+    if (hs.normb < DBL_EPSILON) PGX_CUDA(cudaMemsetAsync(xd, 0, sizeof(double) * n, stream));
+    if (location == PGX_LOCATION_HOST)
+      PGX_CUDA(cudaMemcpyAsync(x, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    if (res) {
+      res->status = rc;
+      res->iters = hs.iter;
+      res->rel_res = hs.normb > 0 ? hs.normr / hs.normb : 0.0;
+      res->true_rel_res = hs.normb > 0 ? sqrt(r2) / hs.normb : 0.0;
+      res->solve_ms = ms;
+      res->launches = 0;  // kernels enqueued one by one are not counted here
+    }
+    if (rc == PGX_SUCCESS && !(std::isfinite(hs.normr)))
+      return fail(PGX_ERROR_NOT_FINITE, "FGMRES residual is not finite");
+    return rc;
+  }
 };
 
 }  // namespace pgx
 
 // ===================================================================== C ABI
 using namespace pgx;
+
+// Krylov basis of pgx_gemslr_solve_static: a fixed pool in the module's
+// global memory, so that solve needs no allocation.  Host code may not use
+// the array's name as a device address; each device's address comes from
+// cudaGetSymbolAddress on that device's first call.
+static __device__ __align__(256) unsigned char g_static_basis[PGX_STATIC_BASIS_BYTES];
+static void* g_static_basis_addr[64];
+static std::mutex g_static_basis_mu;
+
+static int static_basis(int device, void** out) {
+  if (device < 0 || device >= 64) return fail(PGX_ERROR_INVALID_PARAM, "device %d outside [0, 64)", device);
+  std::lock_guard<std::mutex> lock(g_static_basis_mu);
+  if (!g_static_basis_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_basis);
+    if (e != cudaSuccess)
+      return fail(PGX_ERROR_CUDA, "cudaGetSymbolAddress(static Krylov pool): %s", cudaGetErrorString(e));
+    g_static_basis_addr[device] = p;
+  }
+  *out = g_static_basis_addr[device];
+  return PGX_SUCCESS;
+}
 
 struct pgx_gemslr_s {
   Import im;
@@ -2053,6 +2192,23 @@ int pgx_gemslr_precond_apply(pgx_handle h, double* z, const double* v, int32_t l
   if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "apply before commit");
   PGX_CUDA(cudaSetDevice(h->device));
   return h->eng->apply(z, v, location);
+}
+
+int pgx_gemslr_solve_static(pgx_handle h, double* x, const double* b, int32_t location, const double* params,
+                            pgx_result* result) {
+  if (!h || !x || !b) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "solve before commit");
+  if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
+    return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+  if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "solve while a server drives the slots");
+  int kdim, maxits, atol;
+  double tol;
+  read_solver_params(params, kdim, maxits, tol, atol);
+  PGX_CUDA(cudaSetDevice(h->device));
+  void* pool = nullptr;
+  PGX_TRY(static_basis(h->device, &pool));
+  return h->eng->solve_fixed_basis(x, b, location, kdim, maxits, tol, atol, pool, PGX_STATIC_BASIS_BYTES,
+                                   result);
 }
 
 int pgx_gemslr_set_slots(pgx_handle h, int32_t nslots) {
