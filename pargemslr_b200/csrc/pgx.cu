@@ -421,11 +421,22 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
 // (end of the consumer's level - q < ring); otherwise as the row index, read
 // back from global memory.  Returns PGX_ERROR_INVALID_PARAM (and builds
 // nothing) when the factor couples two subdomains.
+template <typename T, typename CC>
+static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::vector<int>& dom, DTri<T>& d,
+                          cudaStream_t s, const std::vector<double>* dinv, std::vector<int>* slot_of_row,
+                          const std::vector<int>* upper_slot_of_row);
 template <typename T>
 static int upload_tri_comp(Arena& ar, const HostCsr& h, bool upper, const std::vector<int>& dom, DTri<T>& d,
                            cudaStream_t s, const std::vector<double>* dinv, std::vector<int>* slot_of_row,
                            const std::vector<int>* upper_slot_of_row) {
-  using CC = CompCfg<T>;
+  return upload_tri_sub<T, CompCfg<T>>(ar, h, upper, dom, d, s, dinv, slot_of_row, upper_slot_of_row);
+}
+
+// The layout for a per-subdomain kernel whose shared-memory sizes are CC's.
+template <typename T, typename CC>
+static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::vector<int>& dom, DTri<T>& d,
+                          cudaStream_t s, const std::vector<double>* dinv, std::vector<int>* slot_of_row,
+                          const std::vector<int>* upper_slot_of_row) {
   const int n = h.rows;
   std::vector<int> lptr, order, lev;
   PGX_TRY(build_levels(upper, n, h.rp.data(), h.cj.data(), lptr, order, &lev));
@@ -461,17 +472,18 @@ static int upload_tri_comp(Arena& ar, const HostCsr& h, bool upper, const std::v
   auto pad4 = [](std::vector<int>& v, int fill) {
     while (v.size() % 4) v.push_back(fill);
   };
-  // far operands of each row: producers at least `ring` positions before the
-  // end of the row's level
+  const int ROWCAP = CC::rows - 4, NNZCAP = CC::nnz - 4;
+  // near operands stay in the shared ring until the consumer reads them:
+  // within `ring` positions of the end of the consumer's level
+  auto is_near = [&](int r, int qj) { return lvl_end[r] - qj < CC::ring; };
   std::vector<int> nfar(n, 0);
   for (int r = 0; r < n; r++)
     for (int k = h.rp[r]; k < h.rp[r + 1]; k++)
-      if (lvl_end[r] - posc[h.cj[k]] >= CC::ring) nfar[r]++;
+      if (!is_near(r, posc[h.cj[k]])) nfar[r]++;
   for (int r = 0; r < n; r++)
     if (nfar[r] > CC::far) return PGX_ERROR_INVALID_PARAM;
   std::vector<int> ord, rp, cj, lvb, meta, comp_ch0(1, 0), far_col;
   std::vector<double> va;
-  const int ROWCAP = CC::rows - 4, NNZCAP = CC::nnz - 4;
   auto push_meta = [&](int pos0) {
     meta.insert(meta.end(), {(int)ord.size(), (int)rp.size(), (int)cj.size(), (int)lvb.size(), pos0,
                              (int)far_col.size(), 0, 0});
@@ -503,7 +515,7 @@ static int upload_tri_comp(Arena& ar, const HostCsr& h, bool upper, const std::v
         for (int k = h.rp[r]; k < h.rp[r + 1]; k++) {
           const int j = h.cj[k];
           const int qj = posc[j];
-          if (lvl_end[r] - qj < CC::ring) {
+          if (is_near(r, qj)) {
             cj.push_back(-((qj & (CC::ring - 1)) + 1));
           } else {
             // far: gathered while the previous chunk is solved, so it must
@@ -1131,7 +1143,9 @@ struct Engine : EngineBase {
     if (M.rows == 0) return;
     const int S = M.S;
     const int gpb = 256 / S;
-    const int grid = grid_for(M.rows, gpb, 148 * 16);
+    // one group per row, every row in flight at once: the gathers of x need
+    // many loads outstanding per SM
+    const int grid = grid_for(M.rows, gpb, 1 << 30);
     const int *rp2 = M2 ? M2->rp : nullptr, *cj2 = M2 ? M2->cj : nullptr;
     const TA* va2 = M2 ? M2->va : nullptr;
 #define PGX_SPMV(SS)                                                                                  \
@@ -2416,7 +2430,7 @@ int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double
   if (!Ad || !x || !y) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   if (Ad->rows == 0) return PGX_SUCCESS;
   const int S = pick_lanes(Ad->nnz, Ad->rows);
-  const int grid = grid_for(Ad->rows, 256 / S, 148 * 16);
+  const int grid = grid_for(Ad->rows, 256 / S, 1 << 30);
   Skip sk = mk_skip();
 #define PGX_SPMV1(SS)                                                                                        \
   spmv_kernel<double, double, double, double, SS><<<grid, 256>>>(Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, \

@@ -435,20 +435,28 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
 // the median distance between a row and the rows it needs is ~10^3
 // positions and almost all are within 10^4.  So one CTA walks a whole
 // subdomain (trsv_comp_kernel below).
-constexpr int kCompThreads = 1024;
+#ifndef PGX_COMP_THREADS
+#define PGX_COMP_THREADS 1024
+#endif
+// 1024 threads: one CTA per SM; 512 threads: two CTAs per SM (registers and
+// shared memory sized for it), for many concurrent solves
+constexpr int kCompThreads = PGX_COMP_THREADS;
+constexpr int kCompMinBlocks = kCompThreads >= 1024 ? 1 : 2;
+constexpr int kUnroll = 4;  // operands per lane loaded before any is used
 template <typename T>
 struct CompCfg {
-  static constexpr int ring = 8192;                           // 32 KB (f32) / 64 KB (f64)
-  static constexpr int far = 1024;                            // far operands per chunk (per buffer)
-  static constexpr int nnz = sizeof(T) == 8 ? 4096 : 8192;    // per chunk buffer
-  static constexpr int rows = sizeof(T) == 8 ? 768 : 1024;    // per chunk buffer (incl. padding)
+  static constexpr bool big = kCompThreads >= 1024;
+  static constexpr int ring = big ? 8192 : 4096;              // 32/16 KB (f32), 64/32 KB (f64)
+  static constexpr int far = big ? 1024 : 512;                // far operands per chunk (per buffer)
+  static constexpr int nnz = sizeof(T) == 8 ? (big ? 4096 : 2048) : (big ? 8192 : 4096);  // per chunk buffer
+  static constexpr int rows = sizeof(T) == 8 ? (big ? 768 : 384) : (big ? 1024 : 512);   // incl. padding
   // per buffer: va[nnz] T | sb[rows] T | sd[rows] T | cj[nnz] int | ord[rows] int | rp[rows+4] int | lvb[rows+4] int
   static constexpr size_t buf_bytes =
       sizeof(T) * (size_t)(nnz + 2 * rows) + sizeof(int) * (size_t)(nnz + rows + 2 * (rows + 4));
   // ring and the two far-operand buffers are one array: operand index -(c+1)
   static constexpr size_t bytes = sizeof(T) * (size_t)(ring + 2 * far) + 2 * buf_bytes;
-  static_assert(bytes <= 227 * 1024, "per-subdomain solve exceeds the shared memory of one CTA");
-  static_assert(far <= 1024 && rows <= 1024, "one gather per thread of a 1024-thread CTA");
+  static_assert(bytes * kCompMinBlocks <= 227 * 1024, "per-subdomain solve exceeds the shared memory of an SM");
+  static_assert(far <= kCompThreads && rows <= kCompThreads, "one gather per thread");
 };
 
 // Per-chunk metadata, two int4 per chunk: {row0, rp0, nnz0, lv0} and
@@ -551,7 +559,7 @@ __device__ __forceinline__ void comp_stage_bulk(const CompBuf<T>& b, const Chunk
 // publishes the chunk's results and waits for its copies.  No CTA waits on
 // another: no tickets, no deadlock.
 template <typename T, int S, bool UPPER>
-__global__ void __launch_bounds__(kCompThreads) trsv_comp_kernel(
+__global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_kernel(
     int n, const int* __restrict__ comp_ch0,  // ncomp+1: chunk range of each subdomain
     CompArrays g, const T* __restrict__ va, const T* __restrict__ dslot, T* yslot, const T* rhs,
     const double* __restrict__ rhs_scale, T* y, T* x, int* err, Skip skip) {
@@ -593,26 +601,45 @@ __global__ void __launch_bounds__(kCompThreads) trsv_comp_kernel(
     const int pos0 = m0.pos0;
     const int nl = m1.lv0 - m0.lv0;
     bool gathered = false;
+    int a = b.lvb[0], e = nl > 1 ? b.lvb[1] : a;
     for (int lv = 0; lv + 1 < nl; lv++) {
-      const int a = b.lvb[lv], e = b.lvb[lv + 1];
       if (a >= e) break;  // padding after the last boundary
+      const int e_next = lv + 2 < nl ? b.lvb[lv + 2] : e;
       for (int i = a + group; i < e; i += ngroups) {
-        T acc = 0;
         const int k1 = b.rp[i], k2 = b.rp[i + 1];
-        for (int k = k1 + sl; k < k2; k += S) {
-          const int q = -b.cj[k] - 1;
-          if ((unsigned)q < (unsigned)RF)
-            acc += b.va[k] * ring[q];
-          else
-            atomicOr(err, kErrIndex);
+        const T bi_ = b.sb[i];
+        const T di_ = UPPER ? b.sd[i] : T(0);
+        // up to kUnroll operands per lane with independent loads, then the rest
+        T acc = 0;
+        unsigned bad = 0;
+        int q[kUnroll];
+        T v[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+          const int k = k1 + sl + u * S;
+          q[u] = k < k2 ? -b.cj[k] - 1 : 0;
+          v[u] = k < k2 ? b.va[k] : T(0);
         }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+          if (k1 + sl + u * S < k2) {  // never read an unwritten ring slot
+            bad |= (unsigned)q[u] >= (unsigned)RF;
+            acc += v[u] * ring[min((unsigned)q[u], (unsigned)(RF - 1))];
+          }
+        }
+        for (int k = k1 + sl + kUnroll * S; k < k2; k += S) {
+          const int qq = -b.cj[k] - 1;
+          bad |= (unsigned)qq >= (unsigned)RF;
+          acc += b.va[k] * ring[min((unsigned)qq, (unsigned)(RF - 1))];
+        }
+        if (bad) atomicOr(err, kErrIndex);
         acc = group_reduce(acc, S, lane);
         if (sl == 0) {
           T o;
           if (UPPER) {
-            o = (b.sb[i] - acc) * b.sd[i];
+            o = (bi_ - acc) * di_;
           } else {
-            T bb = b.sb[i];
+            T bb = bi_;
             if (rhs_scale) bb = (T)((double)bb * rs);
             o = bb - acc;
           }
@@ -631,6 +658,8 @@ __global__ void __launch_bounds__(kCompThreads) trsv_comp_kernel(
             atomicOr(err, kErrIndex);
         }
       }
+      a = e;
+      e = e_next;
     }
     if (!gathered) {
       if (rhs_row >= 0) cp_async_elem(&nb.sb[tid], &rhs[rhs_row]);
