@@ -7,9 +7,10 @@ with x_true = 2u - 1 seeded; 4 GeMSLR levels, ILUT drop 1e-3 / 200 per row,
 rank 16 per level, inner Schur FGMRES on level 0 (tol 1e-2, 5 steps),
 FGMRES(50) to relative residual 1e-8.  The preconditioner is built once by
 this library's host setup (pgx_gemslr_setup, untimed).  A "step" is one
-batch of --slots right-hand sides (b_r = A x_r, x_r seeded), each solved
-completely from x0 = 0, concurrently in that many solve slots over the one
-resident preconditioner (pgx_gemslr_solve_batch); value = solves/s.
+batch of --batch right-hand sides (b_r = A x_r, x_r seeded), each solved
+completely from x0 = 0, concurrently over the one resident preconditioner
+(pgx_gemslr_solve_batch): slot 0 takes one, every further slot --lanes of
+them in lockstep (their triangular passes merged); value = solves/s.
 
   python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp64]
   python bench.py --impl reference ...   (the reference CPU solver, oracle/_ref)
@@ -213,14 +214,17 @@ def run_pgx(args):
     torch.cuda.set_device(local)
     p = P.workload_params(WORKLOAD)
     A, n, _, _ = build_problem()
-    R = args.slots
-    # one step = R right-hand sides b_r = A x_r (x_r seeded), solved concurrently in R slots
+    R = args.batch
+    # one step = R right-hand sides b_r = A x_r (x_r seeded), solved concurrently: slot 0 takes one,
+    # every further slot `lanes` at once
+    nslots = 1 + -(-(R - 1) // args.lanes)
     xts = np.stack([problems.x_true(n, SEED + r) for r in range(R)])
     B = np.stack([problems.spmv(A, xts[r]) for r in range(R)])
     t0 = time.time()
     h = GemslrHandle.from_matrix(A, p, precision=args.precision, device=local)
     setup_s = time.time() - t0
-    h.set_slots(R)
+    h.set_lanes(args.lanes)
+    h.set_slots(nslots)
     dev = torch.device("cuda", local)
     B_dev = torch.from_numpy(B).to(dev)
     X_dev = torch.zeros_like(B_dev)
@@ -279,6 +283,7 @@ def run_pgx(args):
         e2e_ms.append(ev_a.elapsed_time(ev_b))
     e2e_total = max_over_ranks(sum(e2e_ms) / 1e3, dev)
     h.set_slots(1)
+    h.set_lanes(1)
 
     # the plain FP64 path for comparison: FP64 preconditioner, one solve at a time
     plain = None
@@ -318,7 +323,8 @@ def run_pgx(args):
         "config": {"workload": "3D 7-point Laplacian %d^3 (n=%d), 4 levels, ILUT 1e-3/200, rank 16, "
                                "inner Schur FGMRES(5) tol 1e-2, FGMRES(50) to 1e-8, x0 = 0" % (GRID[0], n),
                    "precision": args.precision, "setup": "pgx_gemslr_setup (this library), untimed",
-                   "solves_per_step": R, "slots": R, "setup_s": round(setup_s, 2),
+                   "solves_per_step": R, "slots": nslots, "lanes_per_slot": args.lanes,
+                   "setup_s": round(setup_s, 2),
                    "iters": [min(iters), max(iters)], "true_rel_res_max": max(rel), "x_err_max": x_err,
                    "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                                   "what": "device time of each solve inside the batch (its slot's events)"},
@@ -360,7 +366,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["pgx", "reference"], default="pgx")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--slots", type=int, default=32, help="right-hand sides solved concurrently per step")
+    ap.add_argument("--batch", type=int, default=96, help="right-hand sides solved concurrently per step")
+    ap.add_argument("--lanes", type=int, default=4, choices=[1, 2, 4],
+                    help="right-hand sides each slot advances in lockstep")
     ap.add_argument("--no-fp64-plain", action="store_true", help="skip the plain FP64 comparison solves")
     ap.add_argument("--ref-iters", type=int, default=3, help="FGMRES iterations in one reference CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -229,6 +229,13 @@ typedef struct pgx_server_s *pgx_server;
 /* Number of solve slots (1..256; slot 0 is the handle itself).  Refused while
  * a server created on the handle is live. */
 int pgx_gemslr_set_slots(pgx_handle handle, int32_t nslots);
+/* Right-hand sides each additional slot (slots 1..) advances together: 1, 2
+ * or 4.  A multi-lane slot keeps one FGMRES state per lane and runs the
+ * triangular passes of all its lanes in one kernel, so each factor entry is
+ * read once for all of them; every other step runs per lane with the
+ * single-solve arithmetic, so results do not change with the lane count.
+ * The slots are rebuilt; refused while a server is live. */
+int pgx_gemslr_set_lanes(pgx_handle handle, int32_t lanes);
 /* Device bytes one additional slot needs for FGMRES(kdim). */
 int pgx_gemslr_slot_bytes(pgx_handle handle, int32_t kdim, int64_t *bytes);
 

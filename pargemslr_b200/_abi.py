@@ -42,7 +42,7 @@ EXPORTS = (
     "pgx_csr_spmv_device", "pgx_gemslr_setup", "pgx_gemslr_kernel_stats",
     "pgx_gemslr_set_slots", "pgx_gemslr_slot_bytes", "pgx_gemslr_solve_batch",
     "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
-    "pgx_gemslr_solve_static",
+    "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes",
 )
 
 
@@ -104,6 +104,7 @@ def lib() -> C.CDLL:
     L.pgx_gemslr_setup.argtypes = [C.POINTER(vp), C.POINTER(Csr), vp, i32]
     L.pgx_gemslr_kernel_stats.argtypes = [vp, i32, i32, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.pgx_gemslr_set_slots.argtypes = [vp, i32]
+    L.pgx_gemslr_set_lanes.argtypes = [vp, i32]
     L.pgx_gemslr_slot_bytes.argtypes = [vp, i32, C.POINTER(i64)]
     L.pgx_gemslr_solve_batch.argtypes = [vp, i32, vp, i64, vp, i64, i32, vp, vp]
     L.pgx_server_create.argtypes = [vp, vp, C.POINTER(vp)]

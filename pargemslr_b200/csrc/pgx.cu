@@ -24,6 +24,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <array>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -653,8 +654,28 @@ struct EngineBase {
   virtual int make_clone(std::unique_ptr<EngineBase>& out) = 0;
   virtual int solve_fixed_basis(double* x, const double* b, int location, int kdim, int maxits, double tol,
                                 int atol, void* pool, size_t pool_bytes, pgx_result* res) = 0;
+  // right-hand sides the slot advances together; poll() then fills lanes()
+  // results
+  virtual int lanes() const { return 1; }
+  // another slot over the same factors advancing `lanes` right-hand sides together
+  virtual int make_lanes_clone(Import& im, int lanes, std::unique_ptr<EngineBase>& out) {
+    (void)im;
+    (void)lanes;
+    (void)out;
+    return fail(PGX_ERROR_FUNCTION_CALL, "slots are cloned from the handle itself");
+  }
+  virtual int begin_many(int count, double* const* x, const double* const* b, int location, int kdim, int maxits,
+                         double tol, int atol) {
+    if (count != 1) return fail(PGX_ERROR_INVALID_PARAM, "this slot solves one right-hand side at a time");
+    return begin(x[0], b[0], location, kdim, maxits, tol, atol);
+  }
 };
 
+
+template <typename P>
+struct Engine;
+template <typename P>
+int make_batch_slot(Engine<P>& own, Import& im, int lanes, std::unique_ptr<EngineBase>& out);
 
 template <typename P>
 struct Engine : EngineBase {
@@ -1538,6 +1559,48 @@ struct Engine : EngineBase {
 
   int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol) override {
     if (phase != IDLE) return fail(PGX_ERROR_FUNCTION_CALL, "slot busy");
+    double* xd = nullptr;
+    const double* bd = nullptr;
+    PGX_TRY(begin_prologue(x, b, location, kdim, maxits, tol, atol, &xd, &bd));
+    s_max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
+    if (s_max_cycles > 0 && (!cycle_exec || g_kdim != kdim || g_x != xd || g_b != bd)) {
+      drop_graph();
+      cudaGraph_t g = nullptr;
+      PGX_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_cycle(kdim, xd, bd);
+      cudaError_t ce = cudaStreamEndCapture(stream, &g);
+      if (ce != cudaSuccess) return fail(PGX_ERROR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      size_t nodes = 0;
+      cudaGraphGetNodes(g, nullptr, &nodes);
+      cycle_nodes = (int)nodes;
+      ce = cudaGraphInstantiate(&cycle_exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) {
+        cycle_exec = nullptr;
+        return fail(PGX_ERROR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      }
+      g_kdim = kdim;
+      g_x = xd;
+      g_b = bd;
+    }
+    s_cyc = 0;
+    s_maxits = maxits;
+    s_launches = 5;  // ||b||, residual, ||r0||, final residual and its norm
+    s_location = location;
+    s_xd = xd;
+    s_bd = bd;
+    s_xuser = x;
+    phase = RUNNING;
+    const int rc = launch_cycle_or_finish(false);
+    if (rc != PGX_SUCCESS) phase = IDLE;
+    return rc;
+  }
+
+  // The start of a solve up to the first restart cycle (fgmres.hpp:263-360):
+  // inputs to the device, the FGMRES header, ||b||, r0 = b - A x0 and ||r0||.
+  // *xd and *bd receive the device vectors the cycles work on.
+  int begin_prologue(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+                     double** xd_out, const double** bd_out) {
     if (kdim < 1 || kdim > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", kdim, KMAX);
     if (maxits < 0) return fail(PGX_ERROR_INVALID_PARAM, "maxits %d < 0", maxits);
     if (location == PGX_LOCATION_HOST) {
@@ -1583,38 +1646,9 @@ struct Engine : EngineBase {
       a.st = st;
       ts<double, double, double, TS_NORM_COPY>(a);
     }
-    s_max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
-    if (s_max_cycles > 0 && (!cycle_exec || g_kdim != kdim || g_x != xd || g_b != bd)) {
-      drop_graph();
-      cudaGraph_t g = nullptr;
-      PGX_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-      enqueue_cycle(kdim, xd, bd);
-      cudaError_t ce = cudaStreamEndCapture(stream, &g);
-      if (ce != cudaSuccess) return fail(PGX_ERROR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
-      size_t nodes = 0;
-      cudaGraphGetNodes(g, nullptr, &nodes);
-      cycle_nodes = (int)nodes;
-      ce = cudaGraphInstantiate(&cycle_exec, g, 0);
-      cudaGraphDestroy(g);
-      if (ce != cudaSuccess) {
-        cycle_exec = nullptr;
-        return fail(PGX_ERROR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-      }
-      g_kdim = kdim;
-      g_x = xd;
-      g_b = bd;
-    }
-    s_cyc = 0;
-    s_maxits = maxits;
-    s_launches = 5;  // ||b||, residual, ||r0||, final residual and its norm
-    s_location = location;
-    s_xd = xd;
-    s_bd = bd;
-    s_xuser = x;
-    phase = RUNNING;
-    const int rc = launch_cycle_or_finish(false);
-    if (rc != PGX_SUCCESS) phase = IDLE;
-    return rc;
+    *xd_out = xd;
+    *bd_out = bd;
+    return PGX_SUCCESS;
   }
 
   // after a cycle: either the next cycle or the final FP64 residual check
@@ -1627,7 +1661,15 @@ struct Engine : EngineBase {
       PGX_CUDA(cudaEventRecord(ev_poll, stream));
       return PGX_SUCCESS;
     }
-    // FP64 true residual ||b - A x|| / ||b||
+    PGX_TRY(enqueue_finish());
+    PGX_CUDA(cudaEventRecord(ev_poll, stream));
+    phase = FINISHING;
+    return PGX_SUCCESS;
+  }
+
+  // the FP64 true residual ||b - A x|| / ||b|| and the copies of the state
+  // header and the residual norm back to the host
+  int enqueue_finish() {
     spmv<double, double, double, double>(A, s_xd, -1.0, nullptr, nullptr, 0.0, s_bd, 1.0, rdev, nullptr, mk_skip());
     {
       auto a = ts_args<double, double, double>(n, mk_skip());
@@ -1639,8 +1681,6 @@ struct Engine : EngineBase {
     PGX_CUDA(cudaEventRecord(ev1, stream));
     PGX_CUDA(cudaMemcpyAsync(hs_pin, st, offsetof(FgmresDev, sc), cudaMemcpyDeviceToHost, stream));
     PGX_CUDA(cudaMemcpyAsync(r2_pin, scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
-    PGX_CUDA(cudaEventRecord(ev_poll, stream));
-    phase = FINISHING;
     return PGX_SUCCESS;
   }
 
@@ -1679,6 +1719,12 @@ struct Engine : EngineBase {
     // FINISHING: the state header and the residual norm are on the host
     phase = IDLE;
     *finished = true;
+    return collect_result(res);
+  }
+
+  // after enqueue_finish has landed: zero right-hand side, x back to the
+  // host, the outcome
+  int collect_result(pgx_result* res) {
     const FgmresDev hs = *hs_pin;
     const double r2 = *r2_pin;
     const int rc = check_err();
@@ -1716,6 +1762,13 @@ struct Engine : EngineBase {
     auto* e = new Engine<P>();
     out.reset(e);
     return e->clone_from(*this);
+  }
+
+  // batched factor layouts shared by this handle's multi-lane slots, by lane count
+  std::shared_ptr<void> batch_layout[5];
+  int make_lanes_clone(Import& im, int lanes, std::unique_ptr<EngineBase>& out) override {
+    if (lanes == 1) return make_clone(out);
+    return make_batch_slot<P>(*this, im, lanes, out);
   }
 
   // FGMRES with the Krylov basis in memory handed in by the caller (the
@@ -1834,6 +1887,509 @@ struct Engine : EngineBase {
   }
 };
 
+// Per-level layout of the triangular factors for R right-hand sides at once
+// (the CompCfgR chunking), built once per handle and read by every R-lane
+// slot.  Levels whose factors do not fit that layout keep each lane's own
+// single-right-hand-side kernels.
+template <typename P, int R>
+struct BatchLayout {
+  Arena ar;
+  std::vector<DTri<P>> L, U;
+};
+
+// A solve slot that advances R right-hand sides in lockstep: R lanes, each
+// with its own FGMRES state and work vectors (clones of the owner), share one
+// stream and one captured restart cycle.  The triangular passes of the
+// preconditioner are merged over the lanes (trsv_comp_batch_kernel: each
+// factor entry is read once for R vectors); every other kernel runs once per
+// lane exactly as in Engine, so each lane's arithmetic is that of a single
+// solve and its result matches it bit for bit.
+template <typename P, int R>
+struct BatchEngine : EngineBase {
+  Engine<P>* owner = nullptr;
+  std::shared_ptr<BatchLayout<P, R>> lay;
+  std::unique_ptr<Engine<P>> lane[R];
+  cudaStream_t stream = nullptr;
+  Arena wk;
+  std::vector<std::array<P*, R>> yslot;  // per level, in the R-layout's slot order
+  int n = 0, nlev = 0;
+  cudaGraphExec_t cycle_exec = nullptr;
+  int cycle_nodes = 0, g_kdim = -1;
+  std::array<const void*, R> g_x{}, g_b{};
+  enum { IDLE = 0, RUNNING = 1, FINISHING = 2 };
+  int phase = IDLE, count = 0, s_cyc = 0, s_max_cycles = 0, s_maxits = 0;
+
+  ~BatchEngine() override {
+    if (stream) cudaStreamSynchronize(stream);
+    if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
+    for (int r = 1; r < R; r++)
+      if (lane[r]) lane[r]->stream = nullptr;  // lane 0 owns the shared stream
+  }
+
+  int setup(Engine<P>& own, Import& im, std::shared_ptr<BatchLayout<P, R>> shared) {
+    const int bytes = (int)CompCfgR<P, R>::bytes;
+#define PGX_BATTR(SS)                                                                                        \
+  PGX_CUDA(cudaFuncSetAttribute(trsv_comp_batch_kernel<P, SS, false, R>,                                     \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));                        \
+  PGX_CUDA(cudaFuncSetAttribute(trsv_comp_batch_kernel<P, SS, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                bytes))
+    PGX_BATTR(2);
+    PGX_BATTR(4);
+    PGX_BATTR(8);
+    PGX_BATTR(16);
+    PGX_BATTR(32);
+#undef PGX_BATTR
+    owner = &own;
+    n = own.n;
+    nlev = own.nlev;
+    for (int r = 0; r < R; r++) {
+      lane[r].reset(new Engine<P>());
+      PGX_TRY(lane[r]->clone_from(own));
+    }
+    stream = lane[0]->stream;
+    for (int r = 1; r < R; r++) {
+      PGX_CUDA(cudaStreamSynchronize(lane[r]->stream));
+      PGX_CUDA(cudaStreamDestroy(lane[r]->stream));
+      lane[r]->stream = stream;
+    }
+    if (shared) {
+      lay = shared;
+    } else {
+      lay = std::make_shared<BatchLayout<P, R>>();
+      lay->L.resize(nlev);
+      lay->U.resize(nlev);
+      for (int l = 0; l < nlev; l++) {
+        HostLevel& h = im.levels[l];
+        if (h.L.rows == 0 || !own.lv[l].L.comp) continue;
+        std::vector<int> uslot_of_row;
+        using CC = CompCfgR<P, R>;
+        int rc = upload_tri_sub<P, CC>(lay->ar, h.U, true, h.dom_ptr, lay->U[l], stream, &h.dinv, &uslot_of_row,
+                                       nullptr);
+        if (rc == PGX_SUCCESS)
+          rc = upload_tri_sub<P, CC>(lay->ar, h.L, false, h.dom_ptr, lay->L[l], stream, nullptr, nullptr,
+                                     &uslot_of_row);
+        if (rc != PGX_SUCCESS) {
+          lay->L[l] = DTri<P>();
+          lay->U[l] = DTri<P>();
+        }
+      }
+    }
+    yslot.resize(nlev);
+    for (int l = 0; l < nlev; l++)
+      for (int r = 0; r < R; r++) {
+        yslot[l][r] = nullptr;
+        if (lay->U[l].comp) PGX_TRY(wk.zeros(&yslot[l][r], (size_t)lay->U[l].nslots, stream));
+      }
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    return PGX_SUCCESS;
+  }
+
+  int lanes() const override { return R; }
+  int64_t slot_bytes(int kdim) const override {
+    int64_t b = (int64_t)wk.bytes;
+    for (int r = 0; r < R; r++) b += lane[r]->slot_bytes(kdim);
+    return b;
+  }
+  int64_t device_bytes(int kdim) const override { return slot_bytes(kdim); }
+
+  static SkipR<R> all(const std::array<Skip, R>& s) {
+    SkipR<R> o;
+    for (int r = 0; r < R; r++) o.s[r] = s[r];
+    return o;
+  }
+
+  // one triangular pass of level l for every lane
+  void trsv_b(int l, bool upper, const std::array<const P*, R>& rhs, const std::array<P*, R>& y,
+              const std::array<P*, R>& x, const std::array<Skip, R>& sk) {
+    const DTri<P>& T = upper ? lay->U[l] : lay->L[l];
+    if (!T.comp) {
+      for (int r = 0; r < R; r++) {
+        DLevel<P>& d = lane[r]->lv[l];
+        lane[r]->trsv(upper ? d.U : d.L, upper, upper ? d.dinv : nullptr, rhs[r], nullptr, y[r], x[r], sk[r],
+                      d.yslot);
+      }
+      return;
+    }
+    if (T.n == 0) return;
+    const size_t bytes = CompCfgR<P, R>::bytes;
+    CompArrays ca;
+    ca.meta = (const int4*)T.cmeta;
+    ca.ord = T.ord;
+    ca.rp = T.rp;
+    ca.cj = T.cj;
+    ca.lvb = T.lvb;
+    ca.uslot = T.uslot;
+    ca.far_col = T.far_col;
+    PtrR<P, R> prhs, py, px, pys;
+    for (int r = 0; r < R; r++) {
+      prhs.p[r] = const_cast<P*>(rhs[r]);
+      py.p[r] = y[r];
+      px.p[r] = x[r];
+      pys.p[r] = yslot[l][r];
+    }
+    const SkipR<R> skr = all(sk);
+    int* err = lane[0]->err;
+#define PGX_TRSVB(SS)                                                                                         \
+  if (upper)                                                                                                  \
+    trsv_comp_batch_kernel<P, SS, true, R><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, ca, T.va, \
+                                                                                     T.dslot, pys, prhs, py, px, \
+                                                                                     err, skr);               \
+  else                                                                                                        \
+    trsv_comp_batch_kernel<P, SS, false, R><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, ca, T.va, \
+                                                                                      T.dslot, pys, prhs, py, px, \
+                                                                                      err, skr)
+    switch (T.S) {
+      case 2: PGX_TRSVB(2); break;
+      case 4: PGX_TRSVB(4); break;
+      case 8: PGX_TRSVB(8); break;
+      case 16: PGX_TRSVB(16); break;
+      default: PGX_TRSVB(32); break;
+    }
+#undef PGX_TRSVB
+  }
+
+  void solve_b_b(int l, const std::array<const P*, R>& rhs, const std::array<P*, R>& x,
+                 const std::array<Skip, R>& sk) {
+    std::array<P*, R> y;
+    std::array<const P*, R> none;
+    for (int r = 0; r < R; r++) {
+      y[r] = lane[r]->lv[l].y;
+      none[r] = nullptr;
+    }
+    trsv_b(l, false, rhs, y, x, sk);
+    trsv_b(l, true, none, y, x, sk);
+  }
+
+  // Engine::solve_level for every lane
+  void solve_level_b(int l, const std::array<P*, R>& x, const std::array<const P*, R>& rhs,
+                     const std::array<Skip, R>& sk) {
+    if (l == nlev - 1) {
+      solve_b_b(l, rhs, x, sk);
+      return;
+    }
+    const int nl = lane[0]->lv[l].nl;
+    std::array<P*, R> zu, zl, xl;
+    std::array<const P*, R> czu, czl;
+    for (int r = 0; r < R; r++) {
+      zu[r] = lane[r]->lv[l].z;
+      zl[r] = zu[r] + nl;
+      xl[r] = x[r] + nl;
+      czu[r] = zu[r];
+      czl[r] = zl[r];
+    }
+    solve_b_b(l, rhs, zu, sk);
+    for (int r = 0; r < R; r++) {
+      DLevel<P>& d = lane[r]->lv[l];
+      lane[r]->template spmv<P, P, P, P>(d.E, zu[r], (P)-1, nullptr, nullptr, (P)0, rhs[r] + nl, (P)1, zl[r], nullptr,
+                                         sk[r]);
+    }
+    if (l == 0 && lane[0]->inner) {
+      inner_solve_b(xl, czl, sk);
+    } else {
+      for (int r = 0; r < R; r++)
+        if (lane[r]->lv[l].rank > 0) lane[r]->lowrank_inplace(l, zl[r], sk[r]);
+      solve_level_b(l + 1, xl, czl, sk);
+    }
+    for (int r = 0; r < R; r++) {
+      DLevel<P>& d = lane[r]->lv[l];
+      lane[r]->template spmv<P, P, P, P>(d.F, xl[r], (P)-1, nullptr, nullptr, (P)0, rhs[r], (P)1, zu[r], nullptr,
+                                         sk[r]);
+    }
+    solve_b_b(l, czu, x, sk);
+  }
+
+  // Engine::inner_solve for every lane
+  void inner_solve_b(const std::array<P*, R>& xl, const std::array<const P*, R>& zl,
+                     const std::array<Skip, R>& outer) {
+    const int m0 = lane[0]->lv[0].m;
+    const long long ld = m0;
+    const int kin = lane[0]->inner_maxits;
+    for (int r = 0; r < R; r++) {
+      Engine<P>& e = *lane[r];
+      auto a = Engine<P>::template ts_args<P, P, P>(m0, outer[r]);
+      a.in = zl[r];
+      a.out = e.Vin;
+      a.epi = EPI_INIT_INNER;
+      a.st = e.st_in;
+      e.template ts<P, P, P, TS_NORM_COPY>(a);
+    }
+    for (int j = 0; j < kin; j++) {
+      std::array<Skip, R> it;
+      std::array<P*, R> zj, xlr, szu, swu;
+      std::array<const P*, R> cxlr, cszu;
+      for (int r = 0; r < R; r++) {
+        Engine<P>& e = *lane[r];
+        DLevel<P>& d0 = e.lv[0];
+        it[r] = mk_skip(outer[r].f0, outer[r].f1, &e.st_in->cycle_done);
+        P* vj = e.Vin + (long long)j * ld;
+        zj[r] = e.Zin + (long long)j * ld;
+        if (d0.rank > 0) {
+          auto a = Engine<P>::template ts_args<P, P, P>(m0, it[r]);
+          a.ncols = d0.rank;
+          a.V = d0.W;
+          a.ldv = m0;
+          a.in = vj;
+          a.in_scale = &e.st_in->sc[j];
+          a.epi = EPI_STORE;
+          a.dst = d0.lrt;
+          e.template ts<P, P, P, TS_DOT>(a);
+        }
+        {
+          auto u = Engine<P>::template ts_args<P, P, P>(m0, it[r]);
+          u.ncols = d0.rank;
+          u.M = d0.WH;
+          u.ldm = m0;
+          u.coef = d0.lrt;
+          u.in = vj;
+          u.in_scale = &e.st_in->sc[j];
+          u.out = d0.xlr;
+          e.template ts<P, P, P, TS_UPDATE>(u);
+        }
+        xlr[r] = d0.xlr;
+        cxlr[r] = d0.xlr;
+        szu[r] = e.s_zu;
+        swu[r] = e.s_wu;
+        cszu[r] = e.s_zu;
+      }
+      solve_level_b(1, zj, cxlr, it);
+      for (int r = 0; r < R; r++) {
+        Engine<P>& e = *lane[r];
+        e.template spmv<P, P, P, P>(e.lv[0].F, zj[r], (P)1, nullptr, nullptr, (P)0, (const P*)nullptr, (P)0, szu[r],
+                                    nullptr, it[r]);
+      }
+      solve_b_b(0, cszu, swu, it);
+      for (int r = 0; r < R; r++) {
+        Engine<P>& e = *lane[r];
+        P* wj = e.Vin + (long long)(j + 1) * ld;
+        e.template spmv<P, P, P, P>(e.C0, zj[r], (P)1, &e.lv[0].E, swu[r], (P)-1, (const P*)nullptr, (P)0, wj,
+                                    nullptr, it[r]);
+        e.template arnoldi_step<P, P>(e.Vin, ld, j, e.st_in, m0, it[r]);
+      }
+    }
+    for (int r = 0; r < R; r++) {
+      Engine<P>& e = *lane[r];
+      auto u = Engine<P>::template ts_args<P, P, P>(m0, outer[r]);
+      u.ncols_dev = &e.st_in->i;
+      u.M = e.Zin;
+      u.ldm = ld;
+      u.coef = e.st_in->rs;
+      u.in = nullptr;
+      u.out = xl[r];
+      e.template ts<P, P, P, TS_UPDATE>(u);
+    }
+  }
+
+  // Engine::enqueue_cycle for every lane, preconditioner applies merged
+  void enqueue_cycle_b(int kdim, const std::array<double*, R>& xd, const std::array<const double*, R>& bd) {
+    const long long ld = n;
+    std::array<Skip, R> sk;
+    for (int r = 0; r < R; r++) sk[r] = mk_skip(&lane[r]->st->done, &lane[r]->st->cycle_done);
+    const int grid = grid_for(n, 256, 148 * 16);
+    for (int j = 0; j < kdim; j++) {
+      std::array<P*, R> xt;
+      std::array<const P*, R> rt;
+      for (int r = 0; r < R; r++) {
+        Engine<P>& e = *lane[r];
+        gather_kernel<double, P><<<grid, 256, 0, stream>>>(n, e.pperm, e.V + (long long)j * ld, &e.st->sc[j], e.rt,
+                                                           sk[r]);
+        xt[r] = e.xt;
+        rt[r] = e.rt;
+      }
+      solve_level_b(0, xt, rt, sk);
+      for (int r = 0; r < R; r++) {
+        Engine<P>& e = *lane[r];
+        P* zj = e.Z + (long long)j * ld;
+        scatter_kernel<P, P><<<grid, 256, 0, stream>>>(n, e.qperm ? e.qperm : e.pperm, e.xt, zj, sk[r]);
+        e.template spmv<double, P, double, double>(e.A, zj, 1.0, nullptr, nullptr, 0.0, (const double*)nullptr, 0.0,
+                                                   e.V + (long long)(j + 1) * ld, nullptr, sk[r]);
+        e.template arnoldi_step<double, double>(e.V, ld, j, e.st, n, sk[r]);
+      }
+    }
+    for (int r = 0; r < R; r++) {
+      Engine<P>& e = *lane[r];
+      auto u = Engine<P>::template ts_args<P, P, double>(n, mk_skip());
+      u.ncols_dev = &e.st->i;
+      u.M = e.Z;
+      u.ldm = ld;
+      u.coef = e.st->rs;
+      u.in = xd[r];
+      u.out = xd[r];
+      e.template ts<P, P, double, TS_UPDATE>(u);
+      e.template spmv<double, double, double, double>(e.A, xd[r], -1.0, nullptr, nullptr, 0.0, bd[r], 1.0, e.V,
+                                                      nullptr, mk_skip(&e.st->done));
+      fgmres_cycle_reset_kernel<<<1, 1, 0, stream>>>(e.st, mk_skip());
+    }
+  }
+
+  int begin_many(int cnt, double* const* x, const double* const* b, int location, int kdim, int maxits, double tol,
+                 int atol) override {
+    if (phase != IDLE) return fail(PGX_ERROR_FUNCTION_CALL, "slot busy");
+    if (cnt < 1 || cnt > R) return fail(PGX_ERROR_INVALID_PARAM, "%d right-hand sides for a %d-lane slot", cnt, R);
+    std::array<double*, R> xd;
+    std::array<const double*, R> bd;
+    for (int r = 0; r < R; r++) {
+      Engine<P>& e = *lane[r];
+      if (r < cnt) {
+        PGX_TRY(e.begin_prologue(x[r], b[r], location, kdim, maxits, tol, atol, &xd[r], &bd[r]));
+        e.s_location = location;
+        e.s_xuser = x[r];
+      } else {
+        // an idle lane solves b = 0 (finished at once) on its own vectors
+        PGX_CUDA(cudaMemsetAsync(e.bdev, 0, sizeof(double) * n, stream));
+        PGX_CUDA(cudaMemsetAsync(e.xdev, 0, sizeof(double) * n, stream));
+        PGX_TRY(e.begin_prologue(e.xdev, e.bdev, PGX_LOCATION_DEVICE, kdim, maxits, tol, atol, &xd[r], &bd[r]));
+        e.s_location = PGX_LOCATION_DEVICE;
+        e.s_xuser = e.xdev;
+      }
+      e.s_xd = xd[r];
+      e.s_bd = bd[r];
+      e.s_launches = 5;
+    }
+    s_max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
+    bool same = cycle_exec && g_kdim == kdim;
+    for (int r = 0; r < R; r++) same = same && g_x[r] == xd[r] && g_b[r] == bd[r];
+    if (s_max_cycles > 0 && !same) {
+      if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
+      cycle_exec = nullptr;
+      cudaGraph_t g = nullptr;
+      PGX_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_cycle_b(kdim, xd, bd);
+      cudaError_t ce = cudaStreamEndCapture(stream, &g);
+      if (ce != cudaSuccess) return fail(PGX_ERROR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      size_t nodes = 0;
+      cudaGraphGetNodes(g, nullptr, &nodes);
+      cycle_nodes = (int)nodes;
+      ce = cudaGraphInstantiate(&cycle_exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) {
+        cycle_exec = nullptr;
+        return fail(PGX_ERROR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      }
+      g_kdim = kdim;
+      for (int r = 0; r < R; r++) {
+        g_x[r] = xd[r];
+        g_b[r] = bd[r];
+      }
+    }
+    count = cnt;
+    s_cyc = 0;
+    s_maxits = maxits;
+    phase = RUNNING;
+    const int rc = launch_cycle_or_finish(false);
+    if (rc != PGX_SUCCESS) phase = IDLE;
+    return rc;
+  }
+
+  int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol) override {
+    double* xs[1] = {x};
+    const double* bs[1] = {b};
+    return begin_many(1, xs, bs, location, kdim, maxits, tol, atol);
+  }
+
+  int launch_cycle_or_finish(bool last_done) {
+    cudaEvent_t evp = lane[0]->ev_poll;
+    if (!last_done && s_cyc < s_max_cycles) {
+      PGX_CUDA(cudaGraphLaunch(cycle_exec, stream));
+      s_cyc++;
+      for (int r = 0; r < R; r++) {
+        lane[r]->s_launches += cycle_nodes / R;
+        PGX_CUDA(cudaMemcpyAsync(lane[r]->hs_pin, lane[r]->st, offsetof(FgmresDev, sc), cudaMemcpyDeviceToHost,
+                                 stream));
+      }
+      PGX_CUDA(cudaEventRecord(evp, stream));
+      return PGX_SUCCESS;
+    }
+    for (int r = 0; r < R; r++) PGX_TRY(lane[r]->enqueue_finish());
+    PGX_CUDA(cudaEventRecord(evp, stream));
+    phase = FINISHING;
+    return PGX_SUCCESS;
+  }
+
+  int poll(bool block, bool* finished, pgx_result* res) override {
+    *finished = false;
+    if (phase == IDLE) {
+      *finished = true;
+      return PGX_SUCCESS;
+    }
+    cudaEvent_t evp = lane[0]->ev_poll;
+    cudaError_t q = block ? cudaEventSynchronize(evp) : cudaEventQuery(evp);
+    if (q == cudaErrorNotReady) return PGX_SUCCESS;
+    if (q != cudaSuccess) {
+      phase = IDLE;
+      *finished = true;
+      return fail(PGX_ERROR_CUDA, "cudaEventQuery: %s", cudaGetErrorString(q));
+    }
+    if (phase == RUNNING) {
+      bool over = true;
+      for (int r = 0; r < R; r++) {
+        const FgmresDev& hs = *lane[r]->hs_pin;
+        over = over && (hs.done || hs.iter >= s_maxits);
+      }
+      const int rc = launch_cycle_or_finish(over);
+      if (rc != PGX_SUCCESS) {
+        phase = IDLE;
+        *finished = true;
+      }
+      return rc;
+    }
+    phase = IDLE;
+    *finished = true;
+    int first = PGX_SUCCESS;
+    for (int r = 0; r < R; r++) {
+      pgx_result tmp;
+      const int rc = lane[r]->collect_result(r < count && res ? &tmp : nullptr);
+      if (r < count && res) res[r] = tmp;
+      if (r < count && rc != PGX_SUCCESS && first == PGX_SUCCESS) first = rc;
+    }
+    return first;
+  }
+
+  int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+            pgx_result* res) override {
+    PGX_TRY(begin(x, b, location, kdim, maxits, tol, atol));
+    bool finished = false;
+    std::array<pgx_result, R> rr;
+    while (!finished) PGX_TRY(poll(true, &finished, rr.data()));
+    if (res) *res = rr[0];
+    return PGX_SUCCESS;
+  }
+
+  int kernel_stats(int, int, int, double*, double*, int*) override {
+    return fail(PGX_ERROR_FUNCTION_CALL, "kernel statistics are taken on the handle itself");
+  }
+  int build_lowrank_level(Import&, int, int, int, unsigned long long) override {
+    return fail(PGX_ERROR_FUNCTION_CALL, "setup runs on the handle itself");
+  }
+  int apply(double*, const double*, int) override {
+    return fail(PGX_ERROR_FUNCTION_CALL, "the preconditioner is applied on the handle itself");
+  }
+  int make_clone(std::unique_ptr<EngineBase>&) override {
+    return fail(PGX_ERROR_FUNCTION_CALL, "slots are cloned from the handle itself");
+  }
+  int solve_fixed_basis(double*, const double*, int, int, int, double, int, void*, size_t, pgx_result*) override {
+    return fail(PGX_ERROR_FUNCTION_CALL, "the static-basis solve runs on the handle itself");
+  }
+};
+
+template <typename P, int R>
+static int make_batch_slot_r(Engine<P>& own, Import& im, std::unique_ptr<EngineBase>& out) {
+  auto* e = new BatchEngine<P, R>();
+  out.reset(e);
+  auto shared = std::static_pointer_cast<BatchLayout<P, R>>(own.batch_layout[R]);
+  PGX_TRY(e->setup(own, im, shared));
+  if (!shared) own.batch_layout[R] = e->lay;
+  return PGX_SUCCESS;
+}
+
+template <typename P>
+int make_batch_slot(Engine<P>& own, Import& im, int lanes, std::unique_ptr<EngineBase>& out) {
+  switch (lanes) {
+    case 2: return make_batch_slot_r<P, 2>(own, im, out);
+    case 4: return make_batch_slot_r<P, 4>(own, im, out);
+    default: return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: one of 1, 2, 4", lanes);
+  }
+}
+
 }  // namespace pgx
 
 // ===================================================================== C ABI
@@ -1867,6 +2423,7 @@ struct pgx_gemslr_s {
   std::vector<std::unique_ptr<EngineBase>> extra;  // slots 1..: borrow them
   int device = 0;
   int servers = 0;  // live pgx_server objects driving the slots
+  int lanes = 1;    // right-hand sides each extra slot advances together
   int nslots() const { return eng ? 1 + (int)extra.size() : 0; }
   EngineBase* slot(int i) { return i == 0 ? eng.get() : extra[i - 1].get(); }
   ~pgx_gemslr_s() {
@@ -1888,7 +2445,7 @@ struct pgx_server_s {
     int64_t id;
   };
   std::deque<Req> queue;
-  std::vector<int64_t> slot_id;  // request in each slot, -1 if the slot is free
+  std::vector<std::vector<int64_t>> slot_ids;  // requests in each slot (one per lane), empty if free
   std::deque<std::pair<int64_t, pgx_result>> done;
 };
 
@@ -2234,17 +2791,30 @@ int pgx_gemslr_set_slots(pgx_handle h, int32_t nslots) {
   while ((int)h->extra.size() > nslots - 1) h->extra.pop_back();
   while ((int)h->extra.size() < nslots - 1) {
     std::unique_ptr<EngineBase> e;
-    const int rc = h->eng->make_clone(e);
+    const int rc = h->eng->make_lanes_clone(h->im, h->lanes, e);
     if (rc != PGX_SUCCESS) return rc;
     h->extra.push_back(std::move(e));
   }
   return PGX_SUCCESS;
 }
 
+int pgx_gemslr_set_lanes(pgx_handle h, int32_t lanes) {
+  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+  if (lanes != 1 && lanes != 2 && lanes != 4) return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: one of 1, 2, 4", lanes);
+  if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "lanes cannot change while a server is live");
+  if (lanes == h->lanes) return PGX_SUCCESS;
+  PGX_CUDA(cudaSetDevice(h->device));
+  const int nslots = h->nslots();
+  h->extra.clear();
+  h->lanes = lanes;
+  return pgx_gemslr_set_slots(h, nslots);
+}
+
 int pgx_gemslr_slot_bytes(pgx_handle h, int32_t kdim, int64_t* bytes) {
   if (!h || !bytes) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
-  *bytes = h->eng->slot_bytes(kdim);
+  *bytes = h->extra.empty() ? h->eng->slot_bytes(kdim) : h->extra.back()->slot_bytes(kdim);
   return PGX_SUCCESS;
 }
 
@@ -2262,7 +2832,8 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
   PGX_CUDA(cudaSetDevice(h->device));
   if (results) memset(results, 0, sizeof(pgx_result) * (size_t)nrhs);
   const int ns = h->nslots();
-  std::vector<int> busy(ns, -1);
+  // busy[s]: the right-hand sides slot s is solving (one per lane)
+  std::vector<std::vector<int>> busy(ns);
   int next = 0, remaining = nrhs, first_err = PGX_SUCCESS;
   std::string first_msg;
   auto note = [&](int rc) {
@@ -2271,33 +2842,44 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
       first_msg = g_last_error;
     }
   };
+  std::vector<pgx_result> res(4);
   while (remaining > 0) {
     bool progressed = false;
     for (int sidx = 0; sidx < ns; sidx++) {
       EngineBase* e = h->slot(sidx);
-      if (busy[sidx] < 0 && next < nrhs) {
-        const int r = next++;
-        const int rc = e->begin(X + (size_t)r * ldx, B + (size_t)r * ldb, location, kdim, maxits, tol, atol);
+      if (busy[sidx].empty() && next < nrhs) {
+        const int cnt = std::min(e->lanes(), nrhs - next);
+        double* xs[4];
+        const double* bs[4];
+        for (int k = 0; k < cnt; k++) {
+          xs[k] = X + (size_t)(next + k) * ldx;
+          bs[k] = B + (size_t)(next + k) * ldb;
+        }
+        const int rc = e->begin_many(cnt, xs, bs, location, kdim, maxits, tol, atol);
         progressed = true;
         if (rc != PGX_SUCCESS) {
-          if (results) results[r].status = rc;
+          for (int k = 0; k < cnt; k++)
+            if (results) results[next + k].status = rc;
           note(rc);
-          remaining--;
+          next += cnt;
+          remaining -= cnt;
           continue;
         }
-        busy[sidx] = r;
+        for (int k = 0; k < cnt; k++) busy[sidx].push_back(next + k);
+        next += cnt;
       }
-      if (busy[sidx] >= 0) {
+      if (!busy[sidx].empty()) {
         bool fin = false;
-        pgx_result res;
-        memset(&res, 0, sizeof(res));
-        const int rc = e->poll(false, &fin, &res);
+        for (auto& r : res) memset(&r, 0, sizeof(r));
+        const int rc = e->poll(false, &fin, res.data());
         if (rc != PGX_SUCCESS || fin) {
-          if (rc != PGX_SUCCESS) res.status = rc;
-          if (results) results[busy[sidx]] = res;
-          note(res.status);
-          busy[sidx] = -1;
-          remaining--;
+          for (size_t k = 0; k < busy[sidx].size(); k++) {
+            if (rc != PGX_SUCCESS && res[k].status == PGX_SUCCESS) res[k].status = rc;
+            if (results) results[busy[sidx][k]] = res[k];
+            note(res[k].status);
+          }
+          remaining -= (int)busy[sidx].size();
+          busy[sidx].clear();
           progressed = true;
         }
       }
@@ -2315,7 +2897,7 @@ int pgx_server_create(pgx_handle h, const double* params, pgx_server* out) {
   srv->h = h;
   srv->has_params = params != nullptr;
   if (params) memcpy(srv->params, params, sizeof(srv->params));
-  srv->slot_id.assign(h->nslots(), -1);
+  srv->slot_ids.assign(h->nslots(), std::vector<int64_t>());
   h->servers++;
   *out = srv;
   return PGX_SUCCESS;
@@ -2338,33 +2920,48 @@ int pgx_server_step(pgx_server srv, int32_t* n_active, int32_t* n_queued) {
   double tol;
   read_solver_params(srv->has_params ? srv->params : nullptr, kdim, maxits, tol, atol);
   int active = 0;
+  pgx_result res[4];
   for (int sidx = 0; sidx < h->nslots(); sidx++) {
     EngineBase* e = h->slot(sidx);
-    if (srv->slot_id[sidx] < 0 && !srv->queue.empty()) {
-      // the oldest waiting request goes to the free slot
-      const pgx_server_s::Req r = srv->queue.front();
-      srv->queue.pop_front();
-      const int rc = e->begin(r.x, r.b, r.location, kdim, maxits, tol, atol);
+    std::vector<int64_t>& ids = srv->slot_ids[sidx];
+    if (ids.empty() && !srv->queue.empty()) {
+      // the oldest waiting requests (one per lane, same memory location) go to the free slot
+      double* xs[4];
+      const double* bs[4];
+      const int loc = srv->queue.front().location;
+      int cnt = 0;
+      while (cnt < e->lanes() && !srv->queue.empty() && srv->queue.front().location == loc) {
+        const pgx_server_s::Req r = srv->queue.front();
+        srv->queue.pop_front();
+        xs[cnt] = r.x;
+        bs[cnt] = r.b;
+        ids.push_back(r.id);
+        cnt++;
+      }
+      const int rc = e->begin_many(cnt, xs, bs, loc, kdim, maxits, tol, atol);
       if (rc != PGX_SUCCESS) {
-        pgx_result res;
-        memset(&res, 0, sizeof(res));
-        res.status = rc;
-        srv->done.push_back({r.id, res});
+        for (int64_t id : ids) {
+          pgx_result bad;
+          memset(&bad, 0, sizeof(bad));
+          bad.status = rc;
+          srv->done.push_back({id, bad});
+        }
+        ids.clear();
         continue;
       }
-      srv->slot_id[sidx] = r.id;
     }
-    if (srv->slot_id[sidx] >= 0) {
+    if (!ids.empty()) {
       bool fin = false;
-      pgx_result res;
-      memset(&res, 0, sizeof(res));
-      const int rc = e->poll(false, &fin, &res);
+      memset(res, 0, sizeof(res));
+      const int rc = e->poll(false, &fin, res);
       if (rc != PGX_SUCCESS || fin) {
-        if (rc != PGX_SUCCESS) res.status = rc;
-        srv->done.push_back({srv->slot_id[sidx], res});
-        srv->slot_id[sidx] = -1;
+        for (size_t k = 0; k < ids.size(); k++) {
+          if (rc != PGX_SUCCESS && res[k].status == PGX_SUCCESS) res[k].status = rc;
+          srv->done.push_back({ids[k], res[k]});
+        }
+        ids.clear();
       } else {
-        active++;
+        active += (int)ids.size();
       }
     }
   }
@@ -2390,11 +2987,12 @@ int pgx_server_destroy(pgx_server srv) {
   if (!srv) return PGX_SUCCESS;
   cudaSetDevice(srv->h->device);
   // finish the in-flight solves so that no slot is left in the middle of a cycle
+  pgx_result res[4];
   for (int sidx = 0; sidx < srv->h->nslots(); sidx++) {
-    if (srv->slot_id[sidx] < 0) continue;
+    if (srv->slot_ids[sidx].empty()) continue;
     bool fin = false;
     while (!fin)
-      if (srv->h->slot(sidx)->poll(true, &fin, nullptr) != PGX_SUCCESS) break;
+      if (srv->h->slot(sidx)->poll(true, &fin, res) != PGX_SUCCESS) break;
   }
   srv->h->servers--;
   delete srv;

@@ -33,6 +33,19 @@ struct Skip {
   }
 };
 
+// Skip flags of R solves advancing together: a kernel shared by them returns
+// only when every one of them is skipped.
+template <int R>
+struct SkipR {
+  Skip s[R];
+  __device__ __forceinline__ bool on() const {
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      if (!s[r].on()) return false;
+    return true;
+  }
+};
+
 // ---------------------------------------------------------------- FGMRES
 // Device-resident state of one flexible GMRES solve (FlexGmresClass::Solve,
 // ParGeMSLR SRC/solvers/fgmres.hpp:263-558).  H is column-major (KMAX+1) x KMAX.
@@ -674,6 +687,218 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_kernel
       const T o = ring[(pos0 + i) & (C::ring - 1)];
       out[r] = o;
       if (!UPPER) yslot[((const int*)b.sd)[i]] = o;
+    }
+    if (ch + 1 < c1) {
+      cp_async_wait_all();
+      __syncthreads();
+    }
+    m0 = m1;
+    m1 = m2;
+    m2 = m3;
+  }
+}
+
+// --------------------- per-subdomain triangular solve, several right-hand sides
+// trsv_comp_batch_kernel: trsv_comp_kernel for R right-hand sides at once.
+// The factor's rows, columns and values are staged and read once per chunk
+// and applied to all R vectors; the ring holds R values per schedule
+// position (one vector load per operand).  Shared-memory sizes shrink with R
+// (CompCfgR), so the layout is built for the R it serves.
+template <typename T, int R>
+struct __align__(sizeof(T) * R <= 16 ? sizeof(T) * R : 16) VecR {
+  T v[R];
+};
+template <typename T, int R>
+struct PtrR {
+  T* p[R];
+};
+template <typename T, int R>
+struct CompCfgR {
+  static constexpr bool d = sizeof(T) == 8;
+  static constexpr int ring = R <= 1 ? CompCfg<T>::ring : (d ? (R == 2 ? 4096 : 2048) : (R == 2 ? 8192 : 4096));
+  static constexpr int far = R <= 1 ? CompCfg<T>::far : (d ? (R == 2 ? 512 : 256) : (R == 2 ? 1024 : 512));
+  static constexpr int nnz = R <= 1 ? CompCfg<T>::nnz : (d ? (R == 2 ? 3072 : 2048) : (R == 2 ? 5632 : 4096));
+  static constexpr int rows = R <= 1 ? CompCfg<T>::rows : (d ? (R == 2 ? 768 : 512) : (R == 2 ? 1024 : 768));
+  // per buffer: va[nnz] T | sb[R][rows] T | sd[rows] T | cj[nnz] int | ord[rows] int | rp[rows+4] int | lvb[rows+4] int
+  static constexpr size_t buf_bytes =
+      sizeof(T) * (size_t)(nnz + (R + 1) * rows) + sizeof(int) * (size_t)(nnz + rows + 2 * (rows + 4));
+  static constexpr size_t bytes = sizeof(T) * R * (size_t)(ring + 2 * far) + 2 * buf_bytes;
+  static_assert(bytes <= 227 * 1024, "batched per-subdomain solve exceeds the shared memory of one CTA");
+  static_assert(far <= kCompThreads && rows <= kCompThreads, "one gather per thread");
+};
+
+template <typename T, int R>
+struct CompBufR {
+  T *va, *sb, *sd;  // sb: R arrays of `rows`
+  int *cj, *ord, *rp, *lvb;
+};
+template <typename T, int R>
+__device__ __forceinline__ CompBufR<T, R> comp_buf_r(unsigned char* base, int which) {
+  using C = CompCfgR<T, R>;
+  unsigned char* b = base + sizeof(T) * R * (size_t)(C::ring + 2 * C::far) + (size_t)which * C::buf_bytes;
+  CompBufR<T, R> o;
+  o.va = (T*)b;
+  o.sb = o.va + C::nnz;
+  o.sd = o.sb + R * C::rows;
+  o.cj = (int*)(o.sd + C::rows);
+  o.ord = o.cj + C::nnz;
+  o.rp = o.ord + C::rows;
+  o.lvb = o.rp + C::rows + 4;
+  return o;
+}
+
+template <typename T, int R, bool UPPER>
+__device__ __forceinline__ void comp_stage_bulk_r(const CompBufR<T, R>& b, const ChunkMeta& m, const ChunkMeta& me,
+                                                  const CompArrays& g, const T* __restrict__ va,
+                                                  const T* __restrict__ dslot, const PtrR<T, R>& yslot) {
+  using C = CompCfgR<T, R>;
+  stage16(b.va, va + m.nnz0, (me.nnz0 - m.nnz0) * (int)sizeof(T));
+  stage16(b.cj, g.cj + m.nnz0, (me.nnz0 - m.nnz0) * 4);
+  stage16(b.ord, g.ord + m.row0, (me.row0 - m.row0) * 4);
+  stage16(b.rp, g.rp + m.rp0, (me.rp0 - m.rp0) * 4);
+  stage16(b.lvb, g.lvb + m.lv0, (me.lv0 - m.lv0) * 4);
+  if (UPPER) {
+    stage16(b.sd, dslot + m.row0, (me.row0 - m.row0) * (int)sizeof(T));
+#pragma unroll
+    for (int r = 0; r < R; r++) stage16(b.sb + r * C::rows, yslot.p[r] + m.row0, (me.row0 - m.row0) * (int)sizeof(T));
+  } else {
+    stage16(b.sd, g.uslot + m.row0, (me.row0 - m.row0) * 4);
+  }
+}
+
+template <typename T, int S, bool UPPER, int R>
+__global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_kernel(
+    int n, const int* __restrict__ comp_ch0, CompArrays g, const T* __restrict__ va, const T* __restrict__ dslot,
+    PtrR<T, R> yslot, PtrR<T, R> rhs, PtrR<T, R> y, PtrR<T, R> x, int* err, SkipR<R> skip) {
+  if (skip.on()) return;
+  using C = CompCfgR<T, R>;
+  using V = VecR<T, R>;
+  constexpr int RF = C::ring + 2 * C::far;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* ring = (V*)smem_raw;  // ring, then far buffer 0, then far buffer 1
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int c0 = comp_ch0[blockIdx.x], c1 = comp_ch0[blockIdx.x + 1];
+  const PtrR<T, R> out = UPPER ? x : y;
+  if (c0 >= c1) return;
+  ChunkMeta m0 = load_meta(g.meta, c0), m1 = load_meta(g.meta, c0 + 1);
+  ChunkMeta m2 = c0 + 2 <= c1 ? load_meta(g.meta, c0 + 2) : m1;
+  {
+    const CompBufR<T, R> b = comp_buf_r<T, R>(smem_raw, 0);
+    comp_stage_bulk_r<T, R, UPPER>(b, m0, m1, g, va, dslot, yslot);
+    if (!UPPER && tid < m1.row0 - m0.row0) {
+      const int rr = __ldg(&g.ord[m0.row0 + tid]);
+      if (rr >= 0) {
+#pragma unroll
+        for (int r = 0; r < R; r++) cp_async_elem(&b.sb[r * C::rows + tid], &rhs.p[r][rr]);
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+  const int sl = tid & (S - 1), group = tid / S, ngroups = kCompThreads / S;
+  for (int ch = c0; ch < c1; ch++) {
+    const int bi = (ch - c0) & 1;
+    const CompBufR<T, R> nb = comp_buf_r<T, R>(smem_raw, bi ^ 1);
+    int rhs_row = -1, far_col = -1;
+    if (ch + 1 < c1) {
+      comp_stage_bulk_r<T, R, UPPER>(nb, m1, m2, g, va, dslot, yslot);
+      if (!UPPER && tid < m2.row0 - m1.row0) rhs_row = __ldg(&g.ord[m1.row0 + tid]);
+      if (tid < m2.far0 - m1.far0) far_col = __ldg(&g.far_col[m1.far0 + tid]);
+    }
+    const ChunkMeta m3 = ch + 3 <= c1 ? load_meta(g.meta, ch + 3) : m2;
+    const CompBufR<T, R> b = comp_buf_r<T, R>(smem_raw, bi);
+    const int pos0 = m0.pos0;
+    const int nl = m1.lv0 - m0.lv0;
+    bool gathered = false;
+    int a = b.lvb[0], e = nl > 1 ? b.lvb[1] : a;
+    for (int lv = 0; lv + 1 < nl; lv++) {
+      if (a >= e) break;
+      const int e_next = lv + 2 < nl ? b.lvb[lv + 2] : e;
+      for (int i = a + group; i < e; i += ngroups) {
+        const int k1 = b.rp[i], k2 = b.rp[i + 1];
+        T acc[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) acc[r] = 0;
+        unsigned bad = 0;
+        int q[kUnroll];
+        T v[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+          const int k = k1 + sl + u * S;
+          q[u] = k < k2 ? -b.cj[k] - 1 : 0;
+          v[u] = k < k2 ? b.va[k] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+          if (k1 + sl + u * S < k2) {
+            bad |= (unsigned)q[u] >= (unsigned)RF;
+            const V w = ring[min((unsigned)q[u], (unsigned)(RF - 1))];
+#pragma unroll
+            for (int r = 0; r < R; r++) acc[r] += v[u] * w.v[r];
+          }
+        }
+        for (int k = k1 + sl + kUnroll * S; k < k2; k += S) {
+          const int qq = -b.cj[k] - 1;
+          bad |= (unsigned)qq >= (unsigned)RF;
+          const V w = ring[min((unsigned)qq, (unsigned)(RF - 1))];
+          const T vv = b.va[k];
+#pragma unroll
+          for (int r = 0; r < R; r++) acc[r] += vv * w.v[r];
+        }
+        if (bad) atomicOr(err, kErrIndex);
+#pragma unroll
+        for (int r = 0; r < R; r++) acc[r] = group_reduce(acc[r], S, lane);
+        if (sl == 0) {
+          V o;
+          const T di_ = UPPER ? b.sd[i] : T(0);
+#pragma unroll
+          for (int r = 0; r < R; r++) {
+            const T bb = b.sb[r * C::rows + i];
+            o.v[r] = UPPER ? (bb - acc[r]) * di_ : bb - acc[r];
+          }
+          ring[(pos0 + i) & (C::ring - 1)] = o;
+        }
+      }
+      __syncthreads();
+      if (!gathered) {
+        gathered = true;
+        if (rhs_row >= 0) {
+#pragma unroll
+          for (int r = 0; r < R; r++) cp_async_elem(&nb.sb[r * C::rows + tid], &rhs.p[r][rhs_row]);
+        }
+        if (far_col >= 0) {
+          if ((unsigned)far_col < (unsigned)n) {
+            V* fv = &ring[C::ring + (bi ^ 1) * C::far + tid];
+#pragma unroll
+            for (int r = 0; r < R; r++) cp_async_elem(&fv->v[r], &out.p[r][far_col]);
+          } else {
+            atomicOr(err, kErrIndex);
+          }
+        }
+      }
+      a = e;
+      e = e_next;
+    }
+    if (!gathered) {
+      if (rhs_row >= 0) {
+#pragma unroll
+        for (int r = 0; r < R; r++) cp_async_elem(&nb.sb[r * C::rows + tid], &rhs.p[r][rhs_row]);
+      }
+      if (far_col >= 0 && (unsigned)far_col < (unsigned)n) {
+        V* fv = &ring[C::ring + (bi ^ 1) * C::far + tid];
+#pragma unroll
+        for (int r = 0; r < R; r++) cp_async_elem(&fv->v[r], &out.p[r][far_col]);
+      }
+    }
+    for (int i = tid; i < m1.row0 - m0.row0; i += blockDim.x) {
+      const int rr = b.ord[i];
+      if (rr < 0) continue;
+      const V o = ring[(pos0 + i) & (C::ring - 1)];
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        out.p[r][rr] = o.v[r];
+        if (!UPPER) yslot.p[r][((const int*)b.sd)[i]] = o.v[r];
+      }
     }
     if (ch + 1 < c1) {
       cp_async_wait_all();

@@ -152,6 +152,10 @@ class GemslrHandle:
         """Solve slots for concurrent solves (pgx_gemslr_set_slots); slot 0 is the handle."""
         _abi.check(_abi.lib().pgx_gemslr_set_slots(self._h, nslots))
 
+    def set_lanes(self, lanes: int) -> None:
+        """Right-hand sides each additional slot advances together (1, 2 or 4; pgx_gemslr_set_lanes)."""
+        _abi.check(_abi.lib().pgx_gemslr_set_lanes(self._h, lanes))
+
     def slot_bytes(self, kdim: int) -> int:
         """Device bytes of one additional slot for FGMRES(kdim)."""
         b = C.c_int64(0)

@@ -46,6 +46,36 @@ def test_batch_equals_single_solves(precision):
     h.close()
 
 
+@pytest.mark.parametrize("precision,lanes", [("mixed", 2), ("mixed", 4), ("fp64", 4)])
+def test_multilane_slots_equal_single_solves(precision, lanes):
+    """Lanes share the triangular passes; every other step is per lane, so bits match."""
+    from pargemslr_b200.handle import GemslrHandle
+    p = P.workload_params("lap3d_128")
+    A, n, B = _system(nrhs=7, seed=13)
+    h = GemslrHandle.from_matrix(A, p, precision=precision)
+    singles = [h.solve(b, params=p) for b in B]
+    h.set_lanes(lanes)
+    h.set_slots(3)
+    X, res = h.solve_batch(B, params=p)
+    for r, (x1, r1) in enumerate(singles):
+        assert res[r]["status"] == 0
+        assert res[r]["iters"] == r1["iters"], (r, res[r]["iters"], r1["iters"])
+        np.testing.assert_array_equal(X[r], x1)
+    srv = h.server(p)
+    xs = {}
+    for rid in (5, 1, 6, 0, 3, 2, 4):
+        xs[rid] = np.zeros(n)
+        srv.submit(xs[rid], B[rid], rid)
+    done = srv.run()
+    assert sorted(i for i, _ in done) == list(range(7))
+    for rid, rr in done:
+        assert rr["status"] == 0
+        np.testing.assert_array_equal(xs[rid], singles[rid][0])
+    srv.close()
+    h.set_lanes(1)
+    h.close()
+
+
 def test_server_matches_single_solves_in_any_order():
     from pargemslr_b200.handle import GemslrHandle
     p = P.workload_params("lap3d_128")
