@@ -114,14 +114,15 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+def ncu_traffic(lanes: int):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary (None if not captured)."""
     path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f)
+            d = json.load(f)
     except (OSError, ValueError):
         return None
+    return d.get("lanes%d" % lanes)
 
 
 def max_over_ranks(value: float, device) -> float:
@@ -282,6 +283,17 @@ def run_pgx(args):
         ev_b.synchronize()
         e2e_ms.append(ev_a.elapsed_time(ev_b))
     e2e_total = max_over_ranks(sum(e2e_ms) / 1e3, dev)
+
+    # roofline of the dominant kernel: the level-0 triangular passes, merged over
+    # the lanes of a multi-lane slot (the kernel the batch spends its time in)
+    torch.cuda.nvtx.range_push("kernel_stats")  # plain stream launches, outside any graph
+    if args.lanes > 1:
+        blo_ms, blo_bytes = h.kernel_stats(3, 0, reps=5)
+        bup_ms, bup_bytes = h.kernel_stats(4, 0, reps=5)
+    lo_ms, lo_bytes = h.kernel_stats(0, 0, reps=5)
+    up_ms, up_bytes = h.kernel_stats(1, 0, reps=5)
+    spmv_ms, spmv_bytes = h.kernel_stats(2, 0, reps=5)
+    torch.cuda.nvtx.range_pop()
     h.set_slots(1)
     h.set_lanes(1)
 
@@ -304,17 +316,19 @@ def run_pgx(args):
         plain = {"solves_per_s": len(pm) / (sum(pm) / 1e3), "ms_per_solve": sum(pm) / len(pm), "iters": pit,
                  "what": "FP64 preconditioner, one solve at a time (pgx_gemslr_solve), same setup and RHS"}
 
-    # roofline of the dominant kernel: the level-0 triangular passes
-    torch.cuda.nvtx.range_push("kernel_stats")  # plain stream launches, outside any graph
-    lo_ms, lo_bytes = h.kernel_stats(0, 0, reps=5)
-    up_ms, up_bytes = h.kernel_stats(1, 0, reps=5)
-    spmv_ms, spmv_bytes = h.kernel_stats(2, 0, reps=5)
-    torch.cuda.nvtx.range_pop()
     peak, peak_kind = measured_peak_hbm()
-    tri_bytes = (lo_bytes + up_bytes) / 2.0
-    tri_ms = (lo_ms + up_ms) / 2.0
+    single = {"bytes_per_launch": (lo_bytes + up_bytes) / 2.0, "ms_per_launch": (lo_ms + up_ms) / 2.0}
+    single["achieved"] = single["bytes_per_launch"] / (single["ms_per_launch"] * 1e-3) / 1e9
+    if args.lanes > 1:
+        kname = ("trsv_comp_batch_kernel (level-0 ILU L and U passes merged over %d lanes, mean; one CTA per "
+                 "subdomain)" % args.lanes)
+        tri_bytes = (blo_bytes + bup_bytes) / 2.0
+        tri_ms = (blo_ms + bup_ms) / 2.0
+    else:
+        kname = "trsv_comp_kernel (level-0 ILU L and U passes, mean; one CTA per subdomain)"
+        tri_bytes, tri_ms = single["bytes_per_launch"], single["ms_per_launch"]
     achieved = tri_bytes / (tri_ms * 1e-3) / 1e9
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(args.lanes)
     line = {
         "metric": metric_name(), "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -335,9 +349,10 @@ def run_pgx(args):
                 "d2h_bytes_per_step": 8 * n * R},
         "gpu_launches": int(sum(launches)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "kernel": "trsv_comp_kernel (level-0 ILU L and U passes, mean; one CTA per subdomain)",
+                     "peak_kind": peak_kind, "kernel": kname, "single_lane": single,
                      "bytes_per_launch": tri_bytes, "ms_per_launch": tri_ms,
                      "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                     "traffic_source": traffic.get("how") if traffic else None,
                      "spmv": {"achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "ms": spmv_ms}},
         "clocks": clk,
     }

@@ -267,7 +267,9 @@ int pgx_gemslr_precond_apply(pgx_handle handle, double *z, const double *v, int3
 /* Measurement: average device time (CUDA events on the handle's stream,
  * over `reps` launches) and algorithmic bytes per launch of one building
  * block of the solve: which 0 = lower triangular pass of `level`, 1 = upper
- * triangular pass of `level`, 2 = outer CSR SpMV.  Algorithmic bytes count
+ * triangular pass of `level`, 2 = outer CSR SpMV, 3 / 4 = the lower / upper
+ * pass of `level` merged over the lanes of a multi-lane slot (vectors counted
+ * once per lane, the factor once).  Algorithmic bytes count
  * every operand once: nnz*(value+index) + row pointers + schedule + vectors
  * in and out. */
 int pgx_gemslr_kernel_stats(pgx_handle handle, int32_t which, int32_t level, int32_t reps, double *avg_ms,

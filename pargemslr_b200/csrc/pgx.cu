@@ -2354,8 +2354,46 @@ struct BatchEngine : EngineBase {
     return PGX_SUCCESS;
   }
 
-  int kernel_stats(int, int, int, double*, double*, int*) override {
-    return fail(PGX_ERROR_FUNCTION_CALL, "kernel statistics are taken on the handle itself");
+  // device time and algorithmic bytes of the merged lower (which 0) or upper
+  // (which 1) pass of `level` over all R lanes; the factor is counted once,
+  // the vectors once per lane
+  int kernel_stats(int which, int level, int reps, double* avg_ms, double* bytes, int* launches) override {
+    if (reps < 1) reps = 1;
+    if (which < 0 || which > 1) return fail(PGX_ERROR_INVALID_OPTION, "unknown kernel %d", which);
+    if (level < 0 || level >= nlev) return fail(PGX_ERROR_INVALID_PARAM, "level out of range");
+    std::array<Skip, R> sk;
+    std::array<const P*, R> rt, none;
+    std::array<P*, R> y, xt;
+    for (int r = 0; r < R; r++) {
+      sk[r] = mk_skip();
+      rt[r] = lane[r]->rt;
+      none[r] = nullptr;
+      y[r] = lane[r]->lv[level].y;
+      xt[r] = lane[r]->xt;
+    }
+    const DTri<P>& T = which == 0 ? lay->L[level] : lay->U[level];
+    const int nl = lane[0]->lv[level].nl;
+    const double vb = sizeof(P);
+    const double nnz = (double)(which == 0 ? lane[0]->lv[level].L.nnz_total : lane[0]->lv[level].U.nnz_total);
+    *bytes = nnz * (vb + 4.0) + 4.0 * (nl + 1) + 4.0 * nl + R * 2.0 * vb * nl + (which == 1 ? vb * nl : 0.0);
+    *launches = T.comp ? 1 : R;
+    cudaEvent_t e0 = lane[0]->ev0, e1 = lane[0]->ev1;
+    float total = 0.f;
+    for (int rep = 0; rep < reps; rep++) {
+      if (which == 0) PGX_CUDA(cudaEventRecord(e0, stream));
+      trsv_b(level, false, rt, y, xt, sk);
+      if (which == 0) PGX_CUDA(cudaEventRecord(e1, stream));
+      if (which == 1) PGX_CUDA(cudaEventRecord(e0, stream));
+      trsv_b(level, true, none, y, xt, sk);
+      if (which == 1) PGX_CUDA(cudaEventRecord(e1, stream));
+      PGX_CUDA(cudaStreamSynchronize(stream));
+      float ms = 0.f;
+      PGX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      total += ms;
+    }
+    PGX_TRY(lane[0]->check_err());
+    *avg_ms = total / reps;
+    return PGX_SUCCESS;
   }
   int build_lowrank_level(Import&, int, int, int, unsigned long long) override {
     return fail(PGX_ERROR_FUNCTION_CALL, "setup runs on the handle itself");
@@ -3005,6 +3043,12 @@ int pgx_gemslr_kernel_stats(pgx_handle h, int32_t which, int32_t level, int32_t 
   if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
   PGX_CUDA(cudaSetDevice(h->device));
   int launches = 0;
+  if (which == 3 || which == 4) {
+    // the merged passes of a multi-lane slot
+    if (h->extra.empty() || h->extra.back()->lanes() < 2)
+      return fail(PGX_ERROR_FUNCTION_CALL, "no multi-lane slot (pgx_gemslr_set_lanes, pgx_gemslr_set_slots)");
+    return h->extra.back()->kernel_stats(which - 3, level, reps, avg_ms, bytes, &launches);
+  }
   return h->eng->kernel_stats(which, level, reps, avg_ms, bytes, &launches);
 }
 
