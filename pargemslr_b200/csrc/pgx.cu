@@ -150,6 +150,15 @@ static int pick_lanes(long long nnz, long long rows) {
   return 2;
 }
 
+// lanes per row of the CSR SpMV: about three nonzeros per lane keeps several
+// independent gathers of x in flight per thread
+static int spmv_lanes(long long nnz, long long rows) {
+  const double avg = rows > 0 ? (double)nnz / (double)rows : 0.0;
+  int S = 2;
+  while (S < 32 && 3.0 * S * 2 <= avg) S *= 2;
+  return S;
+}
+
 // -------------------------------------------------------- device memory
 struct Arena {
   std::vector<void*> ptrs;
@@ -204,7 +213,7 @@ static int upload_csr(Arena& ar, const HostCsr& h, DCsr<T>& d, cudaStream_t s) {
   d.rows = h.rows;
   d.cols = h.cols;
   d.nnz = h.nnz();
-  d.S = pick_lanes(d.nnz, d.rows);
+  d.S = spmv_lanes(d.nnz, d.rows);
   if (h.rows == 0) return PGX_SUCCESS;
   PGX_TRY(ar.upload(&d.rp, h.rp.data(), h.rp.size(), s));
   PGX_TRY(ar.upload(&d.cj, h.cj.data(), h.cj.size(), s));
@@ -1164,9 +1173,7 @@ struct Engine : EngineBase {
     if (M.rows == 0) return;
     const int S = M.S;
     const int gpb = 256 / S;
-    // one group per row, every row in flight at once: the gathers of x need
-    // many loads outstanding per SM
-    const int grid = grid_for(M.rows, gpb, 1 << 30);
+    const int grid = grid_for(M.rows, gpb, 148 * 16);
     const int *rp2 = M2 ? M2->rp : nullptr, *cj2 = M2 ? M2->cj : nullptr;
     const TA* va2 = M2 ? M2->va : nullptr;
 #define PGX_SPMV(SS)                                                                                  \
@@ -3071,8 +3078,8 @@ int pgx_build_levels(char uplo, int32_t n, const int32_t* rowptr, const int32_t*
 int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double beta, double* y) {
   if (!Ad || !x || !y) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   if (Ad->rows == 0) return PGX_SUCCESS;
-  const int S = pick_lanes(Ad->nnz, Ad->rows);
-  const int grid = grid_for(Ad->rows, 256 / S, 1 << 30);
+  const int S = spmv_lanes(Ad->nnz, Ad->rows);
+  const int grid = grid_for(Ad->rows, 256 / S, 148 * 16);
   Skip sk = mk_skip();
 #define PGX_SPMV1(SS)                                                                                        \
   spmv_kernel<double, double, double, double, SS><<<grid, 256>>>(Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, \

@@ -846,17 +846,50 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_
           for (int r = 0; r < R; r++) acc[r] += vv * w.v[r];
         }
         if (bad) atomicOr(err, kErrIndex);
+        // sum over the group's lanes for every lane value: reduce-scatter
+        // first (each step halves the values a lane carries), then a
+        // butterfly on one value.  Every partial sum adds the same two
+        // operands as group_reduce does, so the results are identical.
+        const unsigned gmask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane & ~(S - 1)));
+        if (R == 4 && S >= 4) {
+          const bool hb = (sl & (S >> 1)) != 0, qb = (sl & (S >> 2)) != 0;
+          T k0 = hb ? acc[2] : acc[0], k1 = hb ? acc[3] : acc[1];
+          const T s0 = hb ? acc[0] : acc[2], s1 = hb ? acc[1] : acc[3];
+          k0 += __shfl_xor_sync(gmask, s0, S >> 1);
+          k1 += __shfl_xor_sync(gmask, s1, S >> 1);
+          T kk = qb ? k1 : k0;
+          kk += __shfl_xor_sync(gmask, qb ? k0 : k1, S >> 2);
 #pragma unroll
-        for (int r = 0; r < R; r++) acc[r] = group_reduce(acc[r], S, lane);
-        if (sl == 0) {
-          V o;
-          const T di_ = UPPER ? b.sd[i] : T(0);
-#pragma unroll
-          for (int r = 0; r < R; r++) {
+          for (int off = S >> 3; off > 0; off >>= 1) kk += __shfl_xor_sync(gmask, kk, off);
+          if ((sl & ((S >> 2) - 1)) == 0) {
+            const int r = (hb ? 2 : 0) + (qb ? 1 : 0);
             const T bb = b.sb[r * C::rows + i];
-            o.v[r] = UPPER ? (bb - acc[r]) * di_ : bb - acc[r];
+            ring[(pos0 + i) & (C::ring - 1)].v[r] = UPPER ? (bb - kk) * b.sd[i] : bb - kk;
           }
-          ring[(pos0 + i) & (C::ring - 1)] = o;
+        } else if (R == 2 && S >= 2) {
+          const bool hb = (sl & (S >> 1)) != 0;
+          T kk = hb ? acc[1] : acc[0];
+          kk += __shfl_xor_sync(gmask, hb ? acc[0] : acc[1], S >> 1);
+#pragma unroll
+          for (int off = S >> 2; off > 0; off >>= 1) kk += __shfl_xor_sync(gmask, kk, off);
+          if ((sl & ((S >> 1) - 1)) == 0) {
+            const int r = hb ? 1 : 0;
+            const T bb = b.sb[r * C::rows + i];
+            ring[(pos0 + i) & (C::ring - 1)].v[r] = UPPER ? (bb - kk) * b.sd[i] : bb - kk;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; r++) acc[r] = group_reduce(acc[r], S, lane);
+          if (sl == 0) {
+            V o;
+            const T di_ = UPPER ? b.sd[i] : T(0);
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+              const T bb = b.sb[r * C::rows + i];
+              o.v[r] = UPPER ? (bb - acc[r]) * di_ : bb - acc[r];
+            }
+            ring[(pos0 + i) & (C::ring - 1)] = o;
+          }
         }
       }
       __syncthreads();
