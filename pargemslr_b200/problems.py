@@ -58,3 +58,62 @@ def spmv(A, x: np.ndarray) -> np.ndarray:
     y = np.zeros(len(rp) - 1)
     np.add.at(y, np.repeat(np.arange(len(rp) - 1), np.diff(rp)), va * x[cj])
     return y
+
+
+def _csr_from_rows(n: int, rows: np.ndarray, cols: np.ndarray, vals: np.ndarray):
+    order = np.lexsort((cols, rows))
+    r, c, v = rows[order], cols[order], vals[order]
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, r + 1, 1)
+    return np.cumsum(rp).astype(np.int32), c.astype(np.int32), v.astype(np.float64)
+
+
+def upwind_convdiff_2d(nx: int, ny: int, beta_x: float, beta_y: float):
+    """-Laplace(u) + beta . grad(u) on an nx x ny grid, h = 1/(n+1), first-order
+    upwind convection, Dirichlet boundary by truncation, scaled by h^2.
+
+    Nonsymmetric for beta != 0.  The reference's stencil is central, so this
+    generator is the project's own (rows in natural order, columns sorted).
+    """
+    n = nx * ny
+    hx, hy = 1.0 / (nx + 1), 1.0 / (ny + 1)
+    idx = np.arange(n, dtype=np.int64)
+    i = idx // nx
+    j = idx - i * nx
+    # upwind: for beta > 0 the convection term couples to the west/south neighbour
+    wx, wy = abs(beta_x) * hx, abs(beta_y) * hy
+    west = -1.0 - (wx if beta_x > 0 else 0.0)
+    east = -1.0 - (wx if beta_x < 0 else 0.0)
+    south = -1.0 - (wy if beta_y > 0 else 0.0)
+    north = -1.0 - (wy if beta_y < 0 else 0.0)
+    diag = 4.0 + wx + wy
+    parts = ((j > 0, -1, west), (j < nx - 1, 1, east), (i > 0, -nx, south), (i < ny - 1, nx, north),
+             (np.ones(n, bool), 0, diag))
+    rows = np.concatenate([idx[c] for c, _, _ in parts])
+    cols = np.concatenate([idx[c] + off for c, off, _ in parts])
+    vals = np.concatenate([np.full(int(c.sum()), v) for c, _, v in parts])
+    return _csr_from_rows(n, rows, cols, vals)
+
+
+def random_diag_dominant(n: int, seed: int, nnz_min: int = 7, nnz_max: int = 27, factor: float = 1.2):
+    """Nonsymmetric random sparse matrix: each row has a uniform number of
+    nonzeros in [nnz_min, nnz_max] (diagonal included) at random columns,
+    off-diagonal values ~ N(0, 1), and the diagonal set to `factor` times
+    the row's absolute off-diagonal sum."""
+    rng = np.random.default_rng(seed)
+    per_row = rng.integers(nnz_min - 1, nnz_max, size=n)  # off-diagonals per row
+    rows = np.repeat(np.arange(n, dtype=np.int64), per_row)
+    cols = rng.integers(0, n - 1, size=rows.size)
+    cols = cols + (cols >= rows)  # never the diagonal
+    vals = rng.standard_normal(rows.size)
+    # merge duplicate (row, col) pairs
+    key = rows * n + cols
+    key, inv = np.unique(key, return_inverse=True)
+    vals = np.bincount(inv, weights=vals)
+    rows, cols = key // n, key % n
+    diag = factor * np.bincount(rows, weights=np.abs(vals), minlength=n)
+    diag[diag == 0] = 1.0
+    allr = np.concatenate([rows, np.arange(n)])
+    allc = np.concatenate([cols, np.arange(n)])
+    allv = np.concatenate([vals, diag])
+    return _csr_from_rows(n, allr, allc, allv)

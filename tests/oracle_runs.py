@@ -33,11 +33,20 @@ def param_args(p: np.ndarray):
     return out
 
 
+def _file_digest(path: Optional[str]) -> Optional[str]:
+    if path is None:
+        return None
+    with open(path, "rb") as f:
+        return hashlib.sha1(f.read()).hexdigest()
+
+
 def run(lap=None, csr_file: Optional[str] = None, params: Optional[np.ndarray] = None, xtrue: Optional[np.ndarray] = None,
-        apply_k: int = 0, solve: bool = True, dump: bool = True, threads: int = 1, tag: str = "") -> Dict[str, object]:
+        apply_k: int = 0, solve: bool = True, dump: bool = True, threads: int = 1, tag: str = "",
+        rhs_file: Optional[str] = None) -> Dict[str, object]:
     """Run the reference once; returns paths and parsed results."""
-    key = hashlib.sha1(repr((lap, csr_file, None if params is None else params.tobytes(),
-                             None if xtrue is None else xtrue.tobytes(), apply_k, solve, dump, threads, tag))
+    key = hashlib.sha1(repr((lap, _file_digest(csr_file), None if params is None else params.tobytes(),
+                             None if xtrue is None else xtrue.tobytes(), apply_k, solve, dump, threads, tag,
+                             _file_digest(rhs_file)))
                        .encode()).hexdigest()[:16]
     out = os.path.join(CACHE, key)
     done = os.path.join(out, "result.txt")
@@ -48,7 +57,9 @@ def run(lap=None, csr_file: Optional[str] = None, params: Optional[np.ndarray] =
             cmd += ["--lap", *[str(v) for v in lap]]
         else:
             cmd += ["--csr", csr_file]
-        if xtrue is not None:
+        if rhs_file is not None:
+            cmd += ["--rhs", rhs_file]
+        elif xtrue is not None:
             xf = os.path.join(out, "xtrue.bin")
             pgxd.write(xf, {"x_true": np.ascontiguousarray(xtrue, np.float64)})
             cmd += ["--xtrue", xf]
@@ -70,7 +81,7 @@ def run(lap=None, csr_file: Optional[str] = None, params: Optional[np.ndarray] =
                 res[k] = [float(t) for t in v.split(",")]
             else:
                 res[k] = float(v) if any(c in v for c in ".e") else int(v)
-    res["setup"] = os.path.join(out, "setup.bin")
+    res["setup"] = os.path.join(out, "setup.bin") if dump else None
     res["problem"] = os.path.join(out, "problem.bin")
     if solve:
         res["solution"] = pgxd.read(os.path.join(out, "solution.bin"))
