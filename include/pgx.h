@@ -284,6 +284,15 @@ int pgx_gemslr_kernel_stats(pgx_handle handle, int32_t which, int32_t level, int
 int pgx_build_levels(char uplo, int32_t n, const int32_t *rowptr, const int32_t *colidx,
                      int32_t *nlevels, int32_t *level_ptr, int32_t *order);
 
+/* Read a coordinate Matrix Market file with real or integer values, general
+ * or symmetric (the files CooMatrixClass::ReadFromMMFile /
+ * CooMatrixReadFromFile accept, matrixops.cpp:11134), into 0-based CSR with
+ * columns sorted within each row and duplicates summed; a symmetric file's
+ * off-diagonal entries are mirrored.  The arrays are allocated by the
+ * library: release them with pgx_csr_free.  Errors: PGX_ERROR_IO. */
+int pgx_csr_read_mm(const char *path, pgx_csr *A);
+int pgx_csr_free(pgx_csr *A);
+
 /* y = alpha * A x + beta * y on device pointers (CSR SpMV kernel). */
 int pgx_csr_spmv_device(const pgx_csr *A_device, double alpha, const double *x, double beta, double *y);
 

@@ -42,7 +42,7 @@ EXPORTS = (
     "pgx_csr_spmv_device", "pgx_gemslr_setup", "pgx_gemslr_kernel_stats",
     "pgx_gemslr_set_slots", "pgx_gemslr_slot_bytes", "pgx_gemslr_solve_batch",
     "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
-    "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes",
+    "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes", "pgx_csr_read_mm", "pgx_csr_free",
 )
 
 
@@ -105,6 +105,8 @@ def lib() -> C.CDLL:
     L.pgx_gemslr_kernel_stats.argtypes = [vp, i32, i32, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.pgx_gemslr_set_slots.argtypes = [vp, i32]
     L.pgx_gemslr_set_lanes.argtypes = [vp, i32]
+    L.pgx_csr_read_mm.argtypes = [C.c_char_p, C.POINTER(Csr)]
+    L.pgx_csr_free.argtypes = [C.POINTER(Csr)]
     L.pgx_gemslr_slot_bytes.argtypes = [vp, i32, C.POINTER(i64)]
     L.pgx_gemslr_solve_batch.argtypes = [vp, i32, vp, i64, vp, i64, i32, vp, vp]
     L.pgx_server_create.argtypes = [vp, vp, C.POINTER(vp)]
@@ -153,3 +155,18 @@ def build_levels(uplo: str, rp: np.ndarray, cj: np.ndarray):
     check(lib().pgx_build_levels(uplo.encode(), n, ptr(rp), ptr(cj) if cj.size else None, C.byref(nlev),
                                  ptr(lptr), ptr(order)))
     return lptr[: nlev.value + 1].copy(), order[:n].copy()
+
+
+def read_mm(path: str):
+    """(rowptr, colidx, values) of a Matrix Market file read by the library (pgx_csr_read_mm)."""
+    L = lib()
+    A = Csr()
+    check(L.pgx_csr_read_mm(path.encode(), C.byref(A)))
+    try:
+        n, nnz = A.rows, A.nnz
+        rp = np.ctypeslib.as_array(C.cast(A.rowptr, C.POINTER(C.c_int32)), (n + 1,)).copy()
+        cj = np.ctypeslib.as_array(C.cast(A.colidx, C.POINTER(C.c_int32)), (max(nnz, 1),))[:nnz].copy()
+        va = np.ctypeslib.as_array(C.cast(A.values, C.POINTER(C.c_double)), (max(nnz, 1),))[:nnz].copy()
+        return rp, cj, va, (A.rows, A.cols)
+    finally:
+        L.pgx_csr_free(C.byref(A))

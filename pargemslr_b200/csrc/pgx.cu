@@ -3075,6 +3075,43 @@ int pgx_build_levels(char uplo, int32_t n, const int32_t* rowptr, const int32_t*
   return PGX_SUCCESS;
 }
 
+int pgx_csr_read_mm(const char* path, pgx_csr* A) {
+  if (!path || !A) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  memset(A, 0, sizeof(*A));
+  setup::Csr c;
+  std::string err;
+  if (setup::read_matrix_market(path, c, err)) return fail(PGX_ERROR_IO, "%s: %s", path, err.c_str());
+  const size_t nnz = c.cj.size();
+  int32_t* rp = (int32_t*)malloc(sizeof(int32_t) * c.rp.size());
+  int32_t* cj = (int32_t*)malloc(sizeof(int32_t) * std::max<size_t>(nnz, 1));
+  double* va = (double*)malloc(sizeof(double) * std::max<size_t>(nnz, 1));
+  if (!rp || !cj || !va) {
+    free(rp);
+    free(cj);
+    free(va);
+    return fail(PGX_ERROR_OOM, "host allocation for %zu nonzeros", nnz);
+  }
+  std::copy(c.rp.begin(), c.rp.end(), rp);
+  std::copy(c.cj.begin(), c.cj.end(), cj);
+  std::copy(c.va.begin(), c.va.end(), va);
+  A->rows = c.rows;
+  A->cols = c.cols;
+  A->nnz = (int64_t)nnz;
+  A->rowptr = rp;
+  A->colidx = cj;
+  A->values = va;
+  return PGX_SUCCESS;
+}
+
+int pgx_csr_free(pgx_csr* A) {
+  if (!A) return PGX_SUCCESS;
+  free((void*)A->rowptr);
+  free((void*)A->colidx);
+  free((void*)A->values);
+  memset(A, 0, sizeof(*A));
+  return PGX_SUCCESS;
+}
+
 int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double beta, double* y) {
   if (!Ad || !x || !y) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   if (Ad->rows == 0) return PGX_SUCCESS;

@@ -25,6 +25,9 @@
 #include <cstring>
 #include <numeric>
 #include <queue>
+#include <cstdio>
+#include <string>
+#include <cctype>
 #include <vector>
 
 #include "pgx_setup.h"
@@ -438,6 +441,100 @@ Csr permuted_block(int n, const int* rp, const int* cj, const double* va, const 
     b.rp[r - r0 + 1] = (int)b.cj.size();
   }
   return b;
+}
+
+// ------------------------------------------------------------ Matrix Market
+// Coordinate Matrix Market files with real or integer values, general or
+// symmetric, as CooMatrixReadFromFile accepts them (ParGeMSLR
+// SRC/matrices/matrixops.cpp:11134-11210): indices 1-based in the file; a
+// symmetric file lists one triangle and each off-diagonal entry is mirrored.
+// The result is CSR with columns sorted within each row and duplicate
+// entries summed.
+int read_matrix_market(const char* path, Csr& out, std::string& err) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) {
+    err = std::string("cannot open ") + path;
+    return 1;
+  }
+  struct Closer {
+    FILE* f;
+    ~Closer() { std::fclose(f); }
+  } closer{f};
+  char line[1024];
+  if (!std::fgets(line, sizeof(line), f)) {
+    err = "empty file";
+    return 1;
+  }
+  std::string banner(line);
+  for (auto& c : banner) c = (char)std::tolower((unsigned char)c);
+  if (banner.rfind("%%matrixmarket", 0) != 0) {
+    err = "no Matrix Market banner";
+    return 1;
+  }
+  if (banner.find("matrix") == std::string::npos || banner.find("coordinate") == std::string::npos) {
+    err = "only coordinate matrices are supported";
+    return 1;
+  }
+  if (banner.find("real") == std::string::npos && banner.find("integer") == std::string::npos) {
+    err = "only real or integer values are supported";
+    return 1;
+  }
+  const bool sym = banner.find("symmetric") != std::string::npos && banner.find("skew") == std::string::npos;
+  if (banner.find("general") == std::string::npos && !sym) {
+    err = "only general or symmetric matrices are supported";
+    return 1;
+  }
+  long long M = 0, N = 0, nz = 0;
+  while (std::fgets(line, sizeof(line), f)) {
+    if (line[0] == '%') continue;
+    if (std::sscanf(line, "%lld %lld %lld", &M, &N, &nz) == 3) break;
+  }
+  if (M <= 0 || N <= 0 || nz < 0 || M > INT32_MAX || N > INT32_MAX) {
+    err = "invalid size line";
+    return 1;
+  }
+  std::vector<long long> key;
+  std::vector<double> val;
+  key.reserve((size_t)(sym ? 2 * nz : nz));
+  val.reserve(key.capacity());
+  for (long long k = 0; k < nz; k++) {
+    long long I, J;
+    double v;
+    if (std::fscanf(f, "%lld %lld %lf", &I, &J, &v) != 3) {
+      err = "entry " + std::to_string(k + 1) + " unreadable";
+      return 1;
+    }
+    if (I < 1 || I > M || J < 1 || J > N) {
+      err = "entry " + std::to_string(k + 1) + " out of range";
+      return 1;
+    }
+    key.push_back((I - 1) * N + (J - 1));
+    val.push_back(v);
+    if (sym && I != J) {
+      key.push_back((J - 1) * N + (I - 1));
+      val.push_back(v);
+    }
+  }
+  std::vector<size_t> ord(key.size());
+  std::iota(ord.begin(), ord.end(), (size_t)0);
+  std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return key[a] < key[b]; });
+  out = Csr();
+  out.rows = (int)M;
+  out.cols = (int)N;
+  out.rp.assign((size_t)M + 1, 0);
+  long long last = -1;
+  for (size_t t : ord) {
+    if (key[t] == last) {
+      out.va.back() += val[t];
+      continue;
+    }
+    last = key[t];
+    out.cj.push_back((int)(key[t] % N));
+    out.va.push_back(val[t]);
+    out.rp[(size_t)(key[t] / N) + 1]++;
+  }
+  for (long long r = 0; r < M; r++) out.rp[r + 1] += out.rp[r];
+  return 0;
 }
 
 }  // namespace setup

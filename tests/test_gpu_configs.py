@@ -125,3 +125,25 @@ def test_random_sparse_requests_arriving_while_others_run():
         x_ref = ref["solution"]["x"]
         assert np.linalg.norm(singles[0][0] - x_ref) / np.linalg.norm(x_ref) <= 1e-6
     h.close()
+
+
+def test_matrix_market_file_to_solution(tmp_path):
+    """A matrix read from a Matrix Market file (pgx_csr_read_mm) set up and solved on the GPU."""
+    import scipy.io
+    import scipy.sparse as sp
+    from pargemslr_b200 import _abi
+    from pargemslr_b200.handle import GemslrHandle
+    rp, cj, va = problems.upwind_convdiff_2d(70, 50, 20.0, 8.0)
+    n = rp.size - 1
+    path = str(tmp_path / "convdiff.mtx")
+    scipy.io.mmwrite(path, sp.csr_matrix((va, cj, rp), shape=(n, n)))
+    rp2, cj2, va2, shape = _abi.read_mm(path)
+    assert shape == (n, n)
+    p = _convdiff_params()
+    xt = problems.x_true(n, 3)
+    b = problems.spmv((rp2, cj2, va2), xt)
+    h = GemslrHandle.from_matrix((rp2, cj2, va2), p, precision="fp64")
+    x, r = h.solve(b, params=p)
+    assert r["status"] == 0 and r["true_rel_res"] <= 1e-8
+    assert np.linalg.norm(x - xt) / np.linalg.norm(xt) <= 1e-6
+    h.close()
