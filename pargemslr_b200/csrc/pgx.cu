@@ -2876,6 +2876,24 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
   read_solver_params(params, kdim, maxits, tol, atol);
   PGX_CUDA(cudaSetDevice(h->device));
   if (results) memset(results, 0, sizeof(pgx_result) * (size_t)nrhs);
+  // host columns are checked before any is assigned, so that a bad one does
+  // not take the other lanes of its slot down with it
+  std::vector<int> order;
+  order.reserve((size_t)nrhs);
+  int first_bad = -1;
+  for (int r = 0; r < nrhs; r++) {
+    bool ok = true;
+    if (location == PGX_LOCATION_HOST) {
+      const double* bc = B + (size_t)r * ldb;
+      for (int i = 0; i < h->im.n && ok; i++) ok = std::isfinite(bc[i]);
+    }
+    if (ok) {
+      order.push_back(r);
+    } else {
+      if (results) results[r].status = PGX_ERROR_NOT_FINITE;
+      if (first_bad < 0) first_bad = r;
+    }
+  }
   const int ns = h->nslots();
   // busy[s]: the right-hand sides slot s is solving (one per lane)
   std::vector<std::vector<int>> busy(ns);
@@ -2888,29 +2906,35 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
     }
   };
   std::vector<pgx_result> res(4);
+  if (first_bad >= 0) {
+    fail(PGX_ERROR_NOT_FINITE, "b(:, %d) is not finite", first_bad);
+    note(PGX_ERROR_NOT_FINITE);
+  }
+  const int nok = (int)order.size();
+  remaining = nok;
   while (remaining > 0) {
     bool progressed = false;
     for (int sidx = 0; sidx < ns; sidx++) {
       EngineBase* e = h->slot(sidx);
-      if (busy[sidx].empty() && next < nrhs) {
-        const int cnt = std::min(e->lanes(), nrhs - next);
+      if (busy[sidx].empty() && next < nok) {
+        const int cnt = std::min(e->lanes(), nok - next);
         double* xs[4];
         const double* bs[4];
         for (int k = 0; k < cnt; k++) {
-          xs[k] = X + (size_t)(next + k) * ldx;
-          bs[k] = B + (size_t)(next + k) * ldb;
+          xs[k] = X + (size_t)order[next + k] * ldx;
+          bs[k] = B + (size_t)order[next + k] * ldb;
         }
         const int rc = e->begin_many(cnt, xs, bs, location, kdim, maxits, tol, atol);
         progressed = true;
         if (rc != PGX_SUCCESS) {
           for (int k = 0; k < cnt; k++)
-            if (results) results[next + k].status = rc;
+            if (results) results[order[next + k]].status = rc;
           note(rc);
           next += cnt;
           remaining -= cnt;
           continue;
         }
-        for (int k = 0; k < cnt; k++) busy[sidx].push_back(next + k);
+        for (int k = 0; k < cnt; k++) busy[sidx].push_back(order[next + k]);
         next += cnt;
       }
       if (!busy[sidx].empty()) {
@@ -2953,6 +2977,10 @@ int pgx_server_submit(pgx_server srv, double* x, const double* b, int32_t locati
   if (request_id < 0) return fail(PGX_ERROR_INVALID_PARAM, "request id %lld < 0", (long long)request_id);
   if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
     return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+  if (location == PGX_LOCATION_HOST) {
+    for (int i = 0; i < srv->h->im.n; i++)
+      if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%d] is not finite", i);
+  }
   srv->queue.push_back({x, b, location, request_id});
   return PGX_SUCCESS;
 }

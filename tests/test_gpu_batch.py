@@ -103,16 +103,29 @@ def test_server_matches_single_solves_in_any_order():
     h.close()
 
 
-def test_batch_reports_a_bad_column():
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_batch_reports_a_bad_column(lanes):
+    from pargemslr_b200 import _abi
     from pargemslr_b200.handle import GemslrHandle
     p = P.workload_params("lap3d_128")
-    A, n, B = _system(grid=(12, 12, 12), nrhs=3)
+    A, n, B = _system(grid=(12, 12, 12), nrhs=5)
     h = GemslrHandle.from_matrix(A, p, precision="fp64")
+    h.set_lanes(lanes)
     h.set_slots(2)
     B[1, 7] = np.nan
     with pytest.raises(PgxError):
         h.solve_batch(B, params=p)
+    # the other columns are still solved, lanes shared with the bad one included
+    X = np.zeros_like(B)
+    res = (_abi.Result * 5)()
+    import ctypes as C
+    rc = _abi.lib().pgx_gemslr_solve_batch(h._h, 5, _abi.ptr(X), n, _abi.ptr(B), n, _abi.LOCATION_HOST,
+                                           _abi.ptr(p), C.cast(res, C.c_void_p))
+    assert rc == _abi.ERROR_NOT_FINITE
+    assert res[1].status == _abi.ERROR_NOT_FINITE
+    for r in (0, 2, 3, 4):
+        assert res[r].status == 0 and res[r].true_rel_res <= 1e-8
     B[1, 7] = 0.0
-    X, res = h.solve_batch(B, params=p)
-    assert all(r["status"] == 0 for r in res)
+    X, out = h.solve_batch(B, params=p)
+    assert all(r["status"] == 0 for r in out)
     h.close()
