@@ -225,7 +225,20 @@ def run_pgx(args):
     h = GemslrHandle.from_matrix(A, p, precision=args.precision, device=local)
     setup_s = time.time() - t0
     h.set_lanes(args.lanes)
-    h.set_slots(nslots)
+    from pargemslr_b200._abi import ERROR_OOM, PgxError
+    while True:
+        # each right-hand side in flight holds its own Krylov basis: on a GPU
+        # with less free memory, halve the batch until the slots fit
+        try:
+            h.set_slots(nslots)
+            break
+        except PgxError as exc:
+            if exc.code != ERROR_OOM or R <= args.lanes:
+                raise
+            h.set_slots(1)
+            R //= 2
+            nslots = 1 + -(-(R - 1) // args.lanes)
+            xts, B = xts[:R], B[:R]
     dev = torch.device("cuda", local)
     B_dev = torch.from_numpy(B).to(dev)
     X_dev = torch.zeros_like(B_dev)
