@@ -557,6 +557,9 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
     comp_ch0.push_back((int)meta.size() / 8);
   }
   push_meta(0);  // closes the last chunk
+  for (int c : cj)
+    if (c >= 0 || -c - 1 >= CC::ring + 2 * CC::far)
+      if (c != 0) return fail(PGX_ERROR_INVALID_PARAM, "per-subdomain layout: operand index out of range");
   // slot of every row in the flat row list; the upper pass's slots index its
   // dinv and the y the lower pass leaves behind
   std::vector<int> slot(n, -1);

@@ -456,6 +456,9 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
 constexpr int kCompThreads = PGX_COMP_THREADS;
 constexpr int kCompMinBlocks = kCompThreads >= 1024 ? 1 : 2;
 constexpr int kUnroll = 4;  // operands per lane loaded before any is used
+// Operand indices into the ring are checked once on the host when the layout
+// is built; the kernels clamp them into the shared array, so a damaged layout
+// can give wrong values but never an access outside shared memory.
 template <typename T>
 struct CompCfg {
   static constexpr bool big = kCompThreads >= 1024;
@@ -624,7 +627,6 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_kernel
         const T di_ = UPPER ? b.sd[i] : T(0);
         // up to kUnroll operands per lane with independent loads, then the rest
         T acc = 0;
-        unsigned bad = 0;
         int q[kUnroll];
         T v[kUnroll];
 #pragma unroll
@@ -636,16 +638,13 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_kernel
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
           if (k1 + sl + u * S < k2) {  // never read an unwritten ring slot
-            bad |= (unsigned)q[u] >= (unsigned)RF;
             acc += v[u] * ring[min((unsigned)q[u], (unsigned)(RF - 1))];
           }
         }
         for (int k = k1 + sl + kUnroll * S; k < k2; k += S) {
           const int qq = -b.cj[k] - 1;
-          bad |= (unsigned)qq >= (unsigned)RF;
           acc += b.va[k] * ring[min((unsigned)qq, (unsigned)(RF - 1))];
         }
-        if (bad) atomicOr(err, kErrIndex);
         acc = group_reduce(acc, S, lane);
         if (sl == 0) {
           T o;
@@ -819,7 +818,6 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_
         T acc[R];
 #pragma unroll
         for (int r = 0; r < R; r++) acc[r] = 0;
-        unsigned bad = 0;
         int q[kUnroll];
         T v[kUnroll];
 #pragma unroll
@@ -831,7 +829,6 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
           if (k1 + sl + u * S < k2) {
-            bad |= (unsigned)q[u] >= (unsigned)RF;
             const V w = ring[min((unsigned)q[u], (unsigned)(RF - 1))];
 #pragma unroll
             for (int r = 0; r < R; r++) acc[r] += v[u] * w.v[r];
@@ -839,13 +836,11 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_
         }
         for (int k = k1 + sl + kUnroll * S; k < k2; k += S) {
           const int qq = -b.cj[k] - 1;
-          bad |= (unsigned)qq >= (unsigned)RF;
           const V w = ring[min((unsigned)qq, (unsigned)(RF - 1))];
           const T vv = b.va[k];
 #pragma unroll
           for (int r = 0; r < R; r++) acc[r] += vv * w.v[r];
         }
-        if (bad) atomicOr(err, kErrIndex);
         // sum over the group's lanes for every lane value: reduce-scatter
         // first (each step halves the values a lane carries), then a
         // butterfly on one value.  Every partial sum adds the same two
