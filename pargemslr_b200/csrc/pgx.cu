@@ -2917,7 +2917,9 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
   remaining = nok;
   while (remaining > 0) {
     bool progressed = false;
-    for (int sidx = 0; sidx < ns; sidx++) {
+    // the additional (possibly multi-lane) slots first, the handle's own last
+    for (int t = 0; t < ns; t++) {
+      const int sidx = (t + 1) % ns;
       EngineBase* e = h->slot(sidx);
       if (busy[sidx].empty() && next < nok) {
         const int cnt = std::min(e->lanes(), nok - next);
@@ -2997,7 +2999,10 @@ int pgx_server_step(pgx_server srv, int32_t* n_active, int32_t* n_queued) {
   read_solver_params(srv->has_params ? srv->params : nullptr, kdim, maxits, tol, atol);
   int active = 0;
   pgx_result res[4];
-  for (int sidx = 0; sidx < h->nslots(); sidx++) {
+  const int ns = h->nslots();
+  // the additional (possibly multi-lane) slots first, the handle's own last
+  for (int t = 0; t < ns; t++) {
+    const int sidx = (t + 1) % ns;
     EngineBase* e = h->slot(sidx);
     std::vector<int64_t>& ids = srv->slot_ids[sidx];
     if (ids.empty() && !srv->queue.empty()) {
