@@ -731,9 +731,8 @@ struct CompBufR {
   T *va, *sb, *sd;  // sb: R arrays of `rows`
   int *cj, *ord, *rp, *lvb;
 };
-template <typename T, int R>
+template <typename T, int R, typename C = CompCfgR<T, R>>
 __device__ __forceinline__ CompBufR<T, R> comp_buf_r(unsigned char* base, int which) {
-  using C = CompCfgR<T, R>;
   unsigned char* b = base + sizeof(T) * R * (size_t)(C::ring + 2 * C::far) + (size_t)which * C::buf_bytes;
   CompBufR<T, R> o;
   o.va = (T*)b;
@@ -746,11 +745,10 @@ __device__ __forceinline__ CompBufR<T, R> comp_buf_r(unsigned char* base, int wh
   return o;
 }
 
-template <typename T, int R, bool UPPER>
+template <typename T, int R, bool UPPER, typename C = CompCfgR<T, R>>
 __device__ __forceinline__ void comp_stage_bulk_r(const CompBufR<T, R>& b, const ChunkMeta& m, const ChunkMeta& me,
                                                   const CompArrays& g, const T* __restrict__ va,
                                                   const T* __restrict__ dslot, const PtrR<T, R>& yslot) {
-  using C = CompCfgR<T, R>;
   stage16(b.va, va + m.nnz0, (me.nnz0 - m.nnz0) * (int)sizeof(T));
   stage16(b.cj, g.cj + m.nnz0, (me.nnz0 - m.nnz0) * 4);
   stage16(b.ord, g.ord + m.row0, (me.row0 - m.row0) * 4);
@@ -765,12 +763,11 @@ __device__ __forceinline__ void comp_stage_bulk_r(const CompBufR<T, R>& b, const
   }
 }
 
-template <typename T, int S, bool UPPER, int R>
+template <typename T, int S, bool UPPER, int R, typename C = CompCfgR<T, R>>
 __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_kernel(
     int n, const int* __restrict__ comp_ch0, CompArrays g, const T* __restrict__ va, const T* __restrict__ dslot,
     PtrR<T, R> yslot, PtrR<T, R> rhs, PtrR<T, R> y, PtrR<T, R> x, int* err, SkipR<R> skip) {
   if (skip.on()) return;
-  using C = CompCfgR<T, R>;
   using V = VecR<T, R>;
   constexpr int RF = C::ring + 2 * C::far;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -782,8 +779,8 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_
   ChunkMeta m0 = load_meta(g.meta, c0), m1 = load_meta(g.meta, c0 + 1);
   ChunkMeta m2 = c0 + 2 <= c1 ? load_meta(g.meta, c0 + 2) : m1;
   {
-    const CompBufR<T, R> b = comp_buf_r<T, R>(smem_raw, 0);
-    comp_stage_bulk_r<T, R, UPPER>(b, m0, m1, g, va, dslot, yslot);
+    const CompBufR<T, R> b = comp_buf_r<T, R, C>(smem_raw, 0);
+    comp_stage_bulk_r<T, R, UPPER, C>(b, m0, m1, g, va, dslot, yslot);
     if (!UPPER && tid < m1.row0 - m0.row0) {
       const int rr = __ldg(&g.ord[m0.row0 + tid]);
       if (rr >= 0) {
@@ -797,15 +794,15 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_
   const int sl = tid & (S - 1), group = tid / S, ngroups = kCompThreads / S;
   for (int ch = c0; ch < c1; ch++) {
     const int bi = (ch - c0) & 1;
-    const CompBufR<T, R> nb = comp_buf_r<T, R>(smem_raw, bi ^ 1);
+    const CompBufR<T, R> nb = comp_buf_r<T, R, C>(smem_raw, bi ^ 1);
     int rhs_row = -1, far_col = -1;
     if (ch + 1 < c1) {
-      comp_stage_bulk_r<T, R, UPPER>(nb, m1, m2, g, va, dslot, yslot);
+      comp_stage_bulk_r<T, R, UPPER, C>(nb, m1, m2, g, va, dslot, yslot);
       if (!UPPER && tid < m2.row0 - m1.row0) rhs_row = __ldg(&g.ord[m1.row0 + tid]);
       if (tid < m2.far0 - m1.far0) far_col = __ldg(&g.far_col[m1.far0 + tid]);
     }
     const ChunkMeta m3 = ch + 3 <= c1 ? load_meta(g.meta, ch + 3) : m2;
-    const CompBufR<T, R> b = comp_buf_r<T, R>(smem_raw, bi);
+    const CompBufR<T, R> b = comp_buf_r<T, R, C>(smem_raw, bi);
     const int pos0 = m0.pos0;
     const int nl = m1.lv0 - m0.lv0;
     bool gathered = false;
