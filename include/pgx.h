@@ -167,7 +167,8 @@ int pgx_gemslr_destroy(pgx_handle handle);
 int pgx_gemslr_setup(pgx_handle *handle, const pgx_csr *A, const double *params, int32_t precision);
 
 /* Bytes of device memory the committed handle holds (factors, matrices,
- * Krylov basis for kdim, work vectors); used for admission control. */
+ * Krylov basis for kdim, work vectors), every solve slot and the multi-lane
+ * factor layouts included; used for admission control. */
 int pgx_gemslr_device_bytes(pgx_handle handle, int32_t kdim, int64_t *bytes);
 
 /* FGMRES(kdim) solve of A x = b right-preconditioned by GeMSLR

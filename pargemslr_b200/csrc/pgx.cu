@@ -669,6 +669,9 @@ struct EngineBase {
   // right-hand sides the slot advances together; poll() then fills lanes()
   // results
   virtual int lanes() const { return 1; }
+  // device bytes of the multi-lane factor layouts this handle keeps, and their release
+  virtual int64_t layout_bytes() const { return 0; }
+  virtual void release_layouts() {}
   // another slot over the same factors advancing `lanes` right-hand sides together
   virtual int make_lanes_clone(Import& im, int lanes, std::unique_ptr<EngineBase>& out) {
     (void)im;
@@ -1776,6 +1779,10 @@ struct Engine : EngineBase {
 
   // batched factor layouts shared by this handle's multi-lane slots, by lane count
   std::shared_ptr<void> batch_layout[5];
+  int64_t layout_bytes() const override;
+  void release_layouts() override {
+    for (auto& l : batch_layout) l.reset();
+  }
   int make_lanes_clone(Import& im, int lanes, std::unique_ptr<EngineBase>& out) override {
     if (lanes == 1) return make_clone(out);
     return make_batch_slot<P>(*this, im, lanes, out);
@@ -2430,6 +2437,14 @@ static int make_batch_slot_r(Engine<P>& own, Import& im, std::unique_ptr<EngineB
 }
 
 template <typename P>
+int64_t Engine<P>::layout_bytes() const {
+  int64_t b = 0;
+  if (batch_layout[2]) b += (int64_t)std::static_pointer_cast<BatchLayout<P, 2>>(batch_layout[2])->ar.bytes;
+  if (batch_layout[4]) b += (int64_t)std::static_pointer_cast<BatchLayout<P, 4>>(batch_layout[4])->ar.bytes;
+  return b;
+}
+
+template <typename P>
 int make_batch_slot(Engine<P>& own, Import& im, int lanes, std::unique_ptr<EngineBase>& out) {
   switch (lanes) {
     case 2: return make_batch_slot_r<P, 2>(own, im, out);
@@ -2774,7 +2789,10 @@ int pgx_gemslr_destroy(pgx_handle h) {
 int pgx_gemslr_device_bytes(pgx_handle h, int32_t kdim, int64_t* bytes) {
   if (!h || !bytes) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
-  *bytes = h->eng->device_bytes(kdim);
+  // factors and the handle's own slot, the other slots, the multi-lane layouts
+  int64_t b = h->eng->device_bytes(kdim) + h->eng->layout_bytes();
+  for (auto& e : h->extra) b += e->slot_bytes(kdim);
+  *bytes = b;
   return PGX_SUCCESS;
 }
 
@@ -2855,6 +2873,7 @@ int pgx_gemslr_set_lanes(pgx_handle h, int32_t lanes) {
   PGX_CUDA(cudaSetDevice(h->device));
   const int nslots = h->nslots();
   h->extra.clear();
+  h->eng->release_layouts();  // rebuilt on demand for the new lane count
   h->lanes = lanes;
   return pgx_gemslr_set_slots(h, nslots);
 }

@@ -54,8 +54,12 @@ def test_multilane_slots_equal_single_solves(precision, lanes):
     A, n, B = _system(nrhs=7, seed=13)
     h = GemslrHandle.from_matrix(A, p, precision=precision)
     singles = [h.solve(b, params=p) for b in B]
+    kd = int(p[P.SOLVER_KDIM])
+    base = h.device_bytes(kd)
     h.set_lanes(lanes)
     h.set_slots(3)
+    # two more slots of `lanes` right-hand sides each, plus their factor layout
+    assert h.device_bytes(kd) >= base + 2 * h.slot_bytes(kd)
     X, res = h.solve_batch(B, params=p)
     for r, (x1, r1) in enumerate(singles):
         assert res[r]["status"] == 0
