@@ -623,8 +623,6 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_kernel
       const int e_next = lv + 2 < nl ? b.lvb[lv + 2] : e;
       for (int i = a + group; i < e; i += ngroups) {
         const int k1 = b.rp[i], k2 = b.rp[i + 1];
-        const T bi_ = b.sb[i];
-        const T di_ = UPPER ? b.sd[i] : T(0);
         // up to kUnroll operands per lane with independent loads, then the rest
         T acc = 0;
         int q[kUnroll];
@@ -647,11 +645,12 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_kernel
         }
         acc = group_reduce(acc, S, lane);
         if (sl == 0) {
+          // only the writing lane reads the row's right-hand side and inverse diagonal
           T o;
           if (UPPER) {
-            o = (bi_ - acc) * di_;
+            o = (b.sb[i] - acc) * b.sd[i];
           } else {
-            T bb = bi_;
+            T bb = b.sb[i];
             if (rhs_scale) bb = (T)((double)bb * rs);
             o = bb - acc;
           }
