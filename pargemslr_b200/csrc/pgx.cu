@@ -150,6 +150,14 @@ static int pick_lanes(long long nnz, long long rows) {
   return 2;
 }
 
+// true if every entry is finite (host memory; OpenMP over large vectors)
+static bool all_finite(const double* b, long long n) {
+  int bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static) if (n >= (1LL << 16))
+  for (long long i = 0; i < n; i++) bad |= !std::isfinite(b[i]);
+  return !bad;
+}
+
 // lanes per row of the CSR SpMV: about three nonzeros per lane keeps several
 // independent gathers of x in flight per thread
 static int spmv_lanes(long long nnz, long long rows) {
@@ -661,7 +669,9 @@ struct EngineBase {
   // a solve slot: begin() enqueues the start of a solve and its first
   // restart cycle, poll() advances it by at most one cycle
   virtual int64_t slot_bytes(int kdim) const = 0;
-  virtual int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol) = 0;
+  // prechecked: a host b was already checked for NaN/Inf by the caller
+  virtual int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+                    bool prechecked = false) = 0;
   virtual int poll(bool block, bool* finished, pgx_result* res) = 0;
   virtual int make_clone(std::unique_ptr<EngineBase>& out) = 0;
   virtual int solve_fixed_basis(double* x, const double* b, int location, int kdim, int maxits, double tol,
@@ -680,9 +690,9 @@ struct EngineBase {
     return fail(PGX_ERROR_FUNCTION_CALL, "slots are cloned from the handle itself");
   }
   virtual int begin_many(int count, double* const* x, const double* const* b, int location, int kdim, int maxits,
-                         double tol, int atol) {
+                         double tol, int atol, bool prechecked = false) {
     if (count != 1) return fail(PGX_ERROR_INVALID_PARAM, "this slot solves one right-hand side at a time");
-    return begin(x[0], b[0], location, kdim, maxits, tol, atol);
+    return begin(x[0], b[0], location, kdim, maxits, tol, atol, prechecked);
   }
 };
 
@@ -1570,11 +1580,12 @@ struct Engine : EngineBase {
   const double* s_bd = nullptr;
   double* s_xuser = nullptr;
 
-  int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol) override {
+  int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+            bool prechecked = false) override {
     if (phase != IDLE) return fail(PGX_ERROR_FUNCTION_CALL, "slot busy");
     double* xd = nullptr;
     const double* bd = nullptr;
-    PGX_TRY(begin_prologue(x, b, location, kdim, maxits, tol, atol, &xd, &bd));
+    PGX_TRY(begin_prologue(x, b, location, kdim, maxits, tol, atol, &xd, &bd, prechecked));
     s_max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
     if (s_max_cycles > 0 && (!cycle_exec || g_kdim != kdim || g_x != xd || g_b != bd)) {
       drop_graph();
@@ -1613,13 +1624,11 @@ struct Engine : EngineBase {
   // inputs to the device, the FGMRES header, ||b||, r0 = b - A x0 and ||r0||.
   // *xd and *bd receive the device vectors the cycles work on.
   int begin_prologue(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
-                     double** xd_out, const double** bd_out) {
+                     double** xd_out, const double** bd_out, bool prechecked = false) {
     if (kdim < 1 || kdim > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", kdim, KMAX);
     if (maxits < 0) return fail(PGX_ERROR_INVALID_PARAM, "maxits %d < 0", maxits);
-    if (location == PGX_LOCATION_HOST) {
-      for (int i = 0; i < n; i++)
-        if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%d] is not finite", i);
-    }
+    if (location == PGX_LOCATION_HOST && !prechecked && !all_finite(b, n))
+      return fail(PGX_ERROR_NOT_FINITE, "b is not finite");
     PGX_TRY(ensure_krylov(kdim));
     double* xd = x;
     const double* bd = b;
@@ -2239,7 +2248,7 @@ struct BatchEngine : EngineBase {
   }
 
   int begin_many(int cnt, double* const* x, const double* const* b, int location, int kdim, int maxits, double tol,
-                 int atol) override {
+                 int atol, bool prechecked = false) override {
     if (phase != IDLE) return fail(PGX_ERROR_FUNCTION_CALL, "slot busy");
     if (cnt < 1 || cnt > R) return fail(PGX_ERROR_INVALID_PARAM, "%d right-hand sides for a %d-lane slot", cnt, R);
     std::array<double*, R> xd;
@@ -2247,7 +2256,7 @@ struct BatchEngine : EngineBase {
     for (int r = 0; r < R; r++) {
       Engine<P>& e = *lane[r];
       if (r < cnt) {
-        PGX_TRY(e.begin_prologue(x[r], b[r], location, kdim, maxits, tol, atol, &xd[r], &bd[r]));
+        PGX_TRY(e.begin_prologue(x[r], b[r], location, kdim, maxits, tol, atol, &xd[r], &bd[r], prechecked));
         e.s_location = location;
         e.s_xuser = x[r];
       } else {
@@ -2297,10 +2306,11 @@ struct BatchEngine : EngineBase {
     return rc;
   }
 
-  int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol) override {
+  int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+            bool prechecked = false) override {
     double* xs[1] = {x};
     const double* bs[1] = {b};
-    return begin_many(1, xs, bs, location, kdim, maxits, tol, atol);
+    return begin_many(1, xs, bs, location, kdim, maxits, tol, atol, prechecked);
   }
 
   int launch_cycle_or_finish(bool last_done) {
@@ -2904,11 +2914,7 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
   order.reserve((size_t)nrhs);
   int first_bad = -1;
   for (int r = 0; r < nrhs; r++) {
-    bool ok = true;
-    if (location == PGX_LOCATION_HOST) {
-      const double* bc = B + (size_t)r * ldb;
-      for (int i = 0; i < h->im.n && ok; i++) ok = std::isfinite(bc[i]);
-    }
+    const bool ok = location != PGX_LOCATION_HOST || all_finite(B + (size_t)r * ldb, h->im.n);
     if (ok) {
       order.push_back(r);
     } else {
@@ -2948,7 +2954,7 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
           xs[k] = X + (size_t)order[next + k] * ldx;
           bs[k] = B + (size_t)order[next + k] * ldb;
         }
-        const int rc = e->begin_many(cnt, xs, bs, location, kdim, maxits, tol, atol);
+        const int rc = e->begin_many(cnt, xs, bs, location, kdim, maxits, tol, atol, true);
         progressed = true;
         if (rc != PGX_SUCCESS) {
           for (int k = 0; k < cnt; k++)
@@ -3001,10 +3007,8 @@ int pgx_server_submit(pgx_server srv, double* x, const double* b, int32_t locati
   if (request_id < 0) return fail(PGX_ERROR_INVALID_PARAM, "request id %lld < 0", (long long)request_id);
   if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
     return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
-  if (location == PGX_LOCATION_HOST) {
-    for (int i = 0; i < srv->h->im.n; i++)
-      if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%d] is not finite", i);
-  }
+  if (location == PGX_LOCATION_HOST && !all_finite(b, srv->h->im.n))
+    return fail(PGX_ERROR_NOT_FINITE, "b is not finite");
   srv->queue.push_back({x, b, location, request_id});
   return PGX_SUCCESS;
 }
@@ -3038,7 +3042,7 @@ int pgx_server_step(pgx_server srv, int32_t* n_active, int32_t* n_queued) {
         ids.push_back(r.id);
         cnt++;
       }
-      const int rc = e->begin_many(cnt, xs, bs, loc, kdim, maxits, tol, atol);
+      const int rc = e->begin_many(cnt, xs, bs, loc, kdim, maxits, tol, atol, true);
       if (rc != PGX_SUCCESS) {
         for (int64_t id : ids) {
           pgx_result bad;
