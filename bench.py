@@ -228,7 +228,7 @@ def run_pgx(args):
     from pargemslr_b200._abi import ERROR_OOM, PgxError
     while True:
         # each right-hand side in flight holds its own Krylov basis: on a GPU
-        # with less free memory, halve the batch until the slots fit
+        # with less free memory, shrink the batch until the slots fit
         try:
             h.set_slots(nslots)
             break
@@ -236,7 +236,7 @@ def run_pgx(args):
             if exc.code != ERROR_OOM or R <= args.lanes:
                 raise
             h.set_slots(1)
-            R //= 2
+            R = max(args.lanes, R - 4 * args.lanes)
             nslots = 1 + -(-(R - 1) // args.lanes)
             xts, B = xts[:R], B[:R]
     dev = torch.device("cuda", local)
