@@ -1,0 +1,130 @@
+// Host checks of the GeMSLR setup routines (setup.cpp): the nested-
+// dissection level structure, ILUT and the Matrix Market reader.  Built and
+// run by tests/test_setup_host.py; prints "ok" lines and exits 0 on success.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+#include "../pargemslr_b200/csrc/pgx_setup.h"
+
+using namespace pgx::setup;
+
+static int failures = 0;
+#define CHECK(cond, ...)                  \
+  do {                                    \
+    if (!(cond)) {                        \
+      std::printf("FAIL: " __VA_ARGS__);  \
+      std::printf("\n");                  \
+      failures++;                         \
+    }                                     \
+  } while (0)
+
+// 7-point Laplacian of an N^3 grid (x fastest), CSR with sorted columns
+static void laplace3d(int N, std::vector<int>& rp, std::vector<int>& cj, std::vector<double>& va) {
+  rp.assign(1, 0);
+  cj.clear();
+  va.clear();
+  auto id = [&](int x, int y, int z) { return (z * N + y) * N + x; };
+  for (int z = 0; z < N; z++)
+    for (int y = 0; y < N; y++)
+      for (int x = 0; x < N; x++) {
+        const int cols[7] = {z > 0 ? id(x, y, z - 1) : -1, y > 0 ? id(x, y - 1, z) : -1, x > 0 ? id(x - 1, y, z) : -1,
+                             id(x, y, z), x < N - 1 ? id(x + 1, y, z) : -1, y < N - 1 ? id(x, y + 1, z) : -1,
+                             z < N - 1 ? id(x, y, z + 1) : -1};
+        for (int c : cols)
+          if (c >= 0) {
+            cj.push_back(c);
+            va.push_back(c == id(x, y, z) ? 6.0 : -1.0);
+          }
+        rp.push_back((int)cj.size());
+      }
+}
+
+int main(int argc, char** argv) {
+  const int N = 14, n = N * N * N;
+  std::vector<int> rp, cj;
+  std::vector<double> va;
+  laplace3d(N, rp, cj, va);
+  Graph g = symmetric_graph(n, rp.data(), cj.data());
+
+  // 1. levels: a permutation; within a level, subdomains do not couple
+  Ordering o = gemslr_ordering(g, 4, 10, true);
+  std::vector<int> seen(n, 0), iperm(n);
+  for (int i = 0; i < n; i++) {
+    CHECK(o.perm[i] >= 0 && o.perm[i] < n, "perm entry out of range");
+    seen[o.perm[i]]++;
+    iperm[o.perm[i]] = i;
+  }
+  for (int i = 0; i < n; i++) CHECK(seen[i] == 1, "perm is not a permutation");
+  const int nlev = (int)o.lev_ptr.size() - 1;
+  CHECK(nlev >= 2 && o.lev_ptr[0] == 0 && o.lev_ptr[nlev] == n, "level pointers");
+  int coupled = 0;
+  for (int l = 0; l < nlev; l++) {
+    const int s = o.lev_ptr[l], e = o.lev_ptr[l + 1];
+    const std::vector<int>& dom = o.dom_ptr[l];
+    CHECK(dom.front() == 0 && dom.back() == e - s, "domain pointers of level %d", l);
+    std::vector<int> comp(e - s);
+    for (size_t c = 0; c + 1 < dom.size(); c++)
+      for (int r = dom[c]; r < dom[c + 1]; r++) comp[r] = (int)c;
+    for (int r = s; r < e; r++) {
+      const int old = o.perm[r];
+      for (int k = rp[old]; k < rp[old + 1]; k++) {
+        const int q = iperm[cj[k]];
+        if (q >= s && q < e && comp[q - s] != comp[r - s]) coupled++;
+      }
+    }
+  }
+  CHECK(coupled == 0, "%d couplings between subdomains of one level", coupled);
+  std::printf("ok levels: %d levels, level 0 has %zu subdomains\n", nlev, o.dom_ptr[0].size() - 1);
+
+  // 2. ILUT with no dropping on a small block is the exact LU: (L + I) (U + D) reproduces B
+  const int s0 = o.lev_ptr[0], c0e = s0 + o.dom_ptr[0][1];
+  Csr B = permuted_block(n, rp.data(), cj.data(), va.data(), o.perm, iperm, s0, c0e, s0, c0e);
+  Factor f;
+  CHECK(ilut(B.rows, B.rp.data(), B.cj.data(), B.va.data(), 0.0, B.rows, f) == 0, "ilut failed");
+  const int m = B.rows;
+  std::vector<double> dense((size_t)m * m, 0.0);
+  for (int i = 0; i < m; i++) {
+    // row i of L+I times (U + D): sum_k L(i,k) Urow(k) + Urow(i)
+    std::vector<double> row((size_t)m, 0.0);
+    auto add_urow = [&](int k, double s) {
+      row[k] += s / f.dinv[k];
+      for (int t = f.U.rp[k]; t < f.U.rp[k + 1]; t++) row[f.U.cj[t]] += s * f.U.va[t];
+    };
+    add_urow(i, 1.0);
+    for (int t = f.L.rp[i]; t < f.L.rp[i + 1]; t++) add_urow(f.L.cj[t], f.L.va[t]);
+    for (int k = B.rp[i]; k < B.rp[i + 1]; k++) row[B.cj[k]] -= B.va[k];
+    double err = 0.0;
+    for (double v : row) err = std::fmax(err, std::fabs(v));
+    CHECK(err < 1e-10, "row %d of LU - B: %g", i, err);
+  }
+  for (int i = 0; i < m; i++)
+    for (int t = f.L.rp[i]; t < f.L.rp[i + 1]; t++) CHECK(f.L.cj[t] < i, "L not strictly lower");
+  std::printf("ok ilut: exact LU of a %d-row subdomain block\n", m);
+
+  // 3. with dropping, the factors keep at most lfil entries per row part
+  Factor g2;
+  CHECK(ilut(B.rows, B.rp.data(), B.cj.data(), B.va.data(), 1e-2, 5, g2) == 0, "ilut(1e-2, 5) failed");
+  int longest = 0;
+  for (int i = 0; i < m; i++) {
+    longest = std::max(longest, g2.L.rp[i + 1] - g2.L.rp[i]);
+    longest = std::max(longest, g2.U.rp[i + 1] - g2.U.rp[i]);
+  }
+  CHECK(longest <= 5, "row part with %d entries > lfil 5", longest);
+  std::printf("ok ilut: fill limit respected (longest row part %d)\n", longest);
+
+  // 4. Matrix Market: symmetric file mirrored, duplicates summed
+  if (argc > 1) {
+    Csr mm;
+    std::string err;
+    CHECK(read_matrix_market(argv[1], mm, err) == 0, "read_matrix_market: %s", err.c_str());
+    CHECK(mm.rows == 3 && mm.cols == 3, "mm size");
+    const std::vector<int> erp = {0, 2, 3, 5}, ecj = {0, 2, 1, 0, 2};
+    const std::vector<double> eva = {3.5, -1.0, 2.0, -1.0, 4.0};
+    CHECK(mm.rp == erp && mm.cj == ecj && mm.va == eva, "mm contents");
+    std::printf("ok matrix market\n");
+  }
+  return failures ? 1 : 0;
+}
