@@ -261,6 +261,15 @@ int pgx_server_step(pgx_server server, int32_t *n_active, int32_t *n_queued);
 int pgx_server_collect(pgx_server server, int32_t max, int64_t *ids, pgx_result *results, int32_t *n);
 int pgx_server_destroy(pgx_server server);
 
+/* Serve on a thread of the library's own: pgx_server_start runs the step
+ * loop above on a background thread until pgx_server_stop (or destroy).
+ * While it runs, pgx_server_submit and pgx_server_collect may be called from
+ * any thread, and pgx_server_step is refused.  An error met by the thread is
+ * returned by pgx_server_stop; the affected requests are collected with it
+ * in their status. */
+int pgx_server_start(pgx_server server);
+int pgx_server_stop(pgx_server server);
+
 /* Apply the preconditioner once, z = M^-1 v (GemslrClass::Solve,
  * gemslr.cpp:3431-3472), on host or device vectors. */
 int pgx_gemslr_precond_apply(pgx_handle handle, double *z, const double *v, int32_t location);

@@ -43,6 +43,7 @@ EXPORTS = (
     "pgx_gemslr_set_slots", "pgx_gemslr_slot_bytes", "pgx_gemslr_solve_batch",
     "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
     "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes", "pgx_csr_read_mm", "pgx_csr_free",
+    "pgx_server_start", "pgx_server_stop",
 )
 
 
@@ -114,6 +115,8 @@ def lib() -> C.CDLL:
     L.pgx_server_step.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
     L.pgx_server_collect.argtypes = [vp, i32, vp, vp, C.POINTER(i32)]
     L.pgx_server_destroy.argtypes = [vp]
+    L.pgx_server_start.argtypes = [vp]
+    L.pgx_server_stop.argtypes = [vp]
     L.pgx_gemslr_solve_static.argtypes = [vp, vp, vp, i32, vp, vp]
     for name in EXPORTS:
         if name != "pgx_last_error":

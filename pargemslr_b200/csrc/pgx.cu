@@ -27,6 +27,9 @@
 #include <array>
 #include <deque>
 #include <memory>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -2520,6 +2523,14 @@ struct pgx_server_s {
   std::deque<Req> queue;
   std::vector<std::vector<int64_t>> slot_ids;  // requests in each slot (one per lane), empty if free
   std::deque<std::pair<int64_t, pgx_result>> done;
+  // the serving thread (pgx_server_start): mu guards the queue, the slots
+  // and the finished list; the thread sleeps on cv while nothing is pending
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread worker;
+  std::atomic<bool> running{false};
+  int worker_rc = 0;
+  std::string worker_msg;
 };
 
 extern "C" {
@@ -3009,12 +3020,15 @@ int pgx_server_submit(pgx_server srv, double* x, const double* b, int32_t locati
     return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
   if (location == PGX_LOCATION_HOST && !all_finite(b, srv->h->im.n))
     return fail(PGX_ERROR_NOT_FINITE, "b is not finite");
-  srv->queue.push_back({x, b, location, request_id});
+  {
+    std::lock_guard<std::mutex> lock(srv->mu);
+    srv->queue.push_back({x, b, location, request_id});
+  }
+  srv->cv.notify_one();
   return PGX_SUCCESS;
 }
 
-int pgx_server_step(pgx_server srv, int32_t* n_active, int32_t* n_queued) {
-  if (!srv) return fail(PGX_ERROR_INVALID_PARAM, "null server");
+static int server_step_locked(pgx_server srv, int32_t* n_active, int32_t* n_queued) {
   pgx_handle h = srv->h;
   PGX_CUDA(cudaSetDevice(h->device));
   int kdim, maxits, atol;
@@ -3074,8 +3088,56 @@ int pgx_server_step(pgx_server srv, int32_t* n_active, int32_t* n_queued) {
   return PGX_SUCCESS;
 }
 
+int pgx_server_step(pgx_server srv, int32_t* n_active, int32_t* n_queued) {
+  if (!srv) return fail(PGX_ERROR_INVALID_PARAM, "null server");
+  if (srv->running) return fail(PGX_ERROR_FUNCTION_CALL, "the server steps on its own thread (pgx_server_stop first)");
+  std::lock_guard<std::mutex> lock(srv->mu);
+  return server_step_locked(srv, n_active, n_queued);
+}
+
+int pgx_server_start(pgx_server srv) {
+  if (!srv) return fail(PGX_ERROR_INVALID_PARAM, "null server");
+  if (srv->running) return fail(PGX_ERROR_FUNCTION_CALL, "the server thread is already running");
+  srv->worker_rc = PGX_SUCCESS;
+  srv->running = true;
+  srv->worker = std::thread([srv]() {
+    while (srv->running) {
+      int32_t active = 0, queued = 0;
+      {
+        std::lock_guard<std::mutex> lock(srv->mu);
+        const int rc = server_step_locked(srv, &active, &queued);
+        if (rc != PGX_SUCCESS && srv->worker_rc == PGX_SUCCESS) {
+          srv->worker_rc = rc;
+          srv->worker_msg = g_last_error;
+        }
+      }
+      if (active == 0 && queued == 0) {
+        // idle: wait for a submission (or stop), waking now and then regardless
+        std::unique_lock<std::mutex> lock(srv->mu);
+        srv->cv.wait_for(lock, std::chrono::milliseconds(2),
+                         [srv]() { return !srv->running || !srv->queue.empty(); });
+      } else {
+        // solves in flight: look again shortly without holding the lock
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+      }
+    }
+  });
+  return PGX_SUCCESS;
+}
+
+int pgx_server_stop(pgx_server srv) {
+  if (!srv) return fail(PGX_ERROR_INVALID_PARAM, "null server");
+  if (!srv->running) return PGX_SUCCESS;
+  srv->running = false;
+  srv->cv.notify_all();
+  if (srv->worker.joinable()) srv->worker.join();
+  if (srv->worker_rc != PGX_SUCCESS) return fail(srv->worker_rc, "server thread: %s", srv->worker_msg.c_str());
+  return PGX_SUCCESS;
+}
+
 int pgx_server_collect(pgx_server srv, int32_t max, int64_t* ids, pgx_result* results, int32_t* n) {
   if (!srv || !n) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  std::lock_guard<std::mutex> lock(srv->mu);
   int k = 0;
   while (k < max && !srv->done.empty()) {
     if (ids) ids[k] = srv->done.front().first;
@@ -3089,6 +3151,7 @@ int pgx_server_collect(pgx_server srv, int32_t max, int64_t* ids, pgx_result* re
 
 int pgx_server_destroy(pgx_server srv) {
   if (!srv) return PGX_SUCCESS;
+  pgx_server_stop(srv);
   cudaSetDevice(srv->h->device);
   // finish the in-flight solves so that no slot is left in the middle of a cycle
   pgx_result res[4];

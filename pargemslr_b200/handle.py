@@ -248,6 +248,14 @@ class Server:
             out.append((int(ids[i]), _result(res[i])))
         return out
 
+    def start(self) -> None:
+        """Serve on a background thread of the library (pgx_server_start): submit/collect from any thread."""
+        _abi.check(_abi.lib().pgx_server_start(self._s))
+
+    def stop(self) -> None:
+        """Stop the background thread (pgx_server_stop); in-flight solves can be finished with step/run."""
+        _abi.check(_abi.lib().pgx_server_stop(self._s))
+
     def run(self):
         """Step until the queue and the slots are empty; returns every collected (id, result)."""
         done = []

@@ -133,3 +133,36 @@ def test_batch_reports_a_bad_column(lanes):
     X, out = h.solve_batch(B, params=p)
     assert all(r["status"] == 0 for r in out)
     h.close()
+
+
+def test_server_on_its_own_thread():
+    """Requests submitted while the library's serving thread runs; each result equals a single solve."""
+    import time
+    from pargemslr_b200.handle import GemslrHandle
+    p = P.workload_params("lap3d_128")
+    A, n, B = _system(nrhs=6, seed=17)
+    h = GemslrHandle.from_matrix(A, p, precision="mixed")
+    singles = [h.solve(b, params=p)[0] for b in B]
+    h.set_lanes(2)
+    h.set_slots(2)
+    srv = h.server(p)
+    srv.start()
+    with pytest.raises(PgxError):
+        srv.step()  # the thread owns the stepping
+    xs = [np.zeros(n) for _ in range(len(B))]
+    got = {}
+    for rid in range(len(B)):
+        srv.submit(xs[rid], B[rid], rid)
+        time.sleep(0.01)
+        got.update(dict(srv.collect()))
+    t0 = time.time()
+    while len(got) < len(B) and time.time() - t0 < 120:
+        time.sleep(0.005)
+        got.update(dict(srv.collect()))
+    srv.stop()
+    assert sorted(got) == list(range(len(B)))
+    for rid, res in got.items():
+        assert res["status"] == 0 and res["true_rel_res"] <= 1e-8
+        np.testing.assert_array_equal(xs[rid], singles[rid])
+    srv.close()
+    h.close()
