@@ -2,7 +2,7 @@
 
 The reference (oracle) runs GemslrClass::Setup and FlexGmresClass::Solve on
 the CPU; its post-setup structures are imported through the C ABI and the
-same right-hand side is solved on the GPU.  Bars (north-star parity):
+same right-hand side is solved on the GPU.  Bars:
   FP64 path:  iterations within +-1 of the reference, FP64 true relative
               residual <= 1e-8, ||x - x_ref|| / ||x_ref|| <= 1e-6;
   mixed path: iterations at most 15% above the reference (plus one), FP64
