@@ -1762,17 +1762,18 @@ struct Engine : EngineBase {
     if (s_location == PGX_LOCATION_HOST)
       PGX_CUDA(cudaMemcpyAsync(s_xuser, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
     PGX_CUDA(cudaStreamSynchronize(stream));
+    int out = rc;
+    if (out == PGX_SUCCESS && !(std::isfinite(hs.normr)))
+      out = fail(PGX_ERROR_NOT_FINITE, "FGMRES residual is not finite");
     if (res) {
-      res->status = rc;
+      res->status = out;
       res->iters = hs.iter;
       res->rel_res = hs.normb > 0 ? hs.normr / hs.normb : 0.0;
       res->true_rel_res = hs.normb > 0 ? sqrt(r2) / hs.normb : 0.0;
       res->solve_ms = ms;
       res->launches = s_launches;
     }
-    if (rc == PGX_SUCCESS && !(std::isfinite(hs.normr)))
-      return fail(PGX_ERROR_NOT_FINITE, "FGMRES residual is not finite");
-    return rc;
+    return out;
   }
 
   int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
@@ -2364,14 +2365,14 @@ struct BatchEngine : EngineBase {
     }
     phase = IDLE;
     *finished = true;
-    int first = PGX_SUCCESS;
+    // each lane's outcome (a NaN in one right-hand side, say) is in its own
+    // result; the return value is kept for failures of the slot as a whole
     for (int r = 0; r < R; r++) {
       pgx_result tmp;
-      const int rc = lane[r]->collect_result(r < count && res ? &tmp : nullptr);
+      lane[r]->collect_result(r < count && res ? &tmp : nullptr);
       if (r < count && res) res[r] = tmp;
-      if (r < count && rc != PGX_SUCCESS && first == PGX_SUCCESS) first = rc;
     }
-    return first;
+    return PGX_SUCCESS;
   }
 
   int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,

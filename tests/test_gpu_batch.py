@@ -166,3 +166,32 @@ def test_server_on_its_own_thread():
         np.testing.assert_array_equal(xs[rid], singles[rid])
     srv.close()
     h.close()
+
+
+def test_nonfinite_device_column_retires_only_its_request():
+    """A NaN in one device right-hand side ends that solve with PGX_ERROR_NOT_FINITE; its lane mates finish normally."""
+    import ctypes as C
+    import torch
+    from pargemslr_b200 import _abi
+    from pargemslr_b200.handle import GemslrHandle
+    p = P.workload_params("lap3d_128")
+    p[P.SOLVER_MAXITS] = 20
+    A, n, B = _system(grid=(12, 12, 12), nrhs=4, seed=23)
+    h = GemslrHandle.from_matrix(A, p, precision="mixed")
+    singles = [h.solve(b, params=p)[0] for b in B]
+    h.set_lanes(4)
+    h.set_slots(2)
+    Bd = torch.tensor(B, device="cuda")
+    Bd[2, 5] = float("nan")
+    Xd = torch.zeros_like(Bd)
+    torch.cuda.synchronize()
+    res = (_abi.Result * 4)()
+    rc = _abi.lib().pgx_gemslr_solve_batch(h._h, 4, Xd.data_ptr(), n, Bd.data_ptr(), n, _abi.LOCATION_DEVICE,
+                                           _abi.ptr(p), C.cast(res, C.c_void_p))
+    assert rc == _abi.ERROR_NOT_FINITE
+    assert res[2].status == _abi.ERROR_NOT_FINITE
+    X = Xd.cpu().numpy()
+    for r in (0, 1, 3):
+        assert res[r].status == 0 and res[r].true_rel_res <= 1e-8
+        np.testing.assert_array_equal(X[r], singles[r])
+    h.close()
