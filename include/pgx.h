@@ -303,6 +303,26 @@ int pgx_build_levels(char uplo, int32_t n, const int32_t *rowptr, const int32_t 
 int pgx_csr_read_mm(const char *path, pgx_csr *A);
 int pgx_csr_free(pgx_csr *A);
 
+/* ---- parameter arrays ----------------------------------------------------
+ * The double[PGX_PARAMS_SIZE] array every entry point above takes is the one
+ * SetWithParameterArray reads (index names in SRC/utils/utils.hpp:77-297).
+ * pgx_params_default fills it as PargemslrSetDefaultParameterArray does
+ * (SRC/utils/utils.cpp:30-126).  pgx_params_read_file then overwrites the
+ * slots a driver's parameter file names, as that driver's
+ * read_inputs_from_file does, line k of the file setting its fixed slots:
+ *   PGX_INPUTS_SEQUENTIAL  TESTS/sequential/inputs (io.cpp:336-725)
+ *   PGX_INPUTS_PARALLEL    TESTS/parallel/inputs (io_par.cpp:359-819)
+ *   PGX_INPUTS_HYPRE       TESTS/hypre/inputs (pargemslr_hypre_interface.cpp:391-820)
+ * Errors: PGX_ERROR_IO for a file that cannot be opened or an unknown keyword
+ * (the line is named in pgx_last_error; the lines before it stay applied, as
+ * in the reference); PGX_ERROR_INVALID_PARAM for an unknown format. */
+#define PGX_PARAMS_SIZE 180
+#define PGX_INPUTS_SEQUENTIAL 0
+#define PGX_INPUTS_PARALLEL   1
+#define PGX_INPUTS_HYPRE      2
+int pgx_params_default(double *params);
+int pgx_params_read_file(const char *path, int32_t format, double *params);
+
 /* y = alpha * A x + beta * y on device pointers (CSR SpMV kernel). */
 int pgx_csr_spmv_device(const pgx_csr *A_device, double alpha, const double *x, double beta, double *y);
 

@@ -43,7 +43,7 @@ EXPORTS = (
     "pgx_gemslr_set_slots", "pgx_gemslr_slot_bytes", "pgx_gemslr_solve_batch",
     "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
     "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes", "pgx_csr_read_mm", "pgx_csr_free",
-    "pgx_server_start", "pgx_server_stop",
+    "pgx_server_start", "pgx_server_stop", "pgx_params_default", "pgx_params_read_file",
 )
 
 
@@ -118,6 +118,8 @@ def lib() -> C.CDLL:
     L.pgx_server_start.argtypes = [vp]
     L.pgx_server_stop.argtypes = [vp]
     L.pgx_gemslr_solve_static.argtypes = [vp, vp, vp, i32, vp, vp]
+    L.pgx_params_default.argtypes = [vp]
+    L.pgx_params_read_file.argtypes = [C.c_char_p, i32, vp]
     for name in EXPORTS:
         if name != "pgx_last_error":
             getattr(L, name).restype = C.c_int
@@ -158,6 +160,24 @@ def build_levels(uplo: str, rp: np.ndarray, cj: np.ndarray):
     check(lib().pgx_build_levels(uplo.encode(), n, ptr(rp), ptr(cj) if cj.size else None, C.byref(nlev),
                                  ptr(lptr), ptr(order)))
     return lptr[: nlev.value + 1].copy(), order[:n].copy()
+
+
+INPUTS_FORMATS = {"sequential": 0, "parallel": 1, "hypre": 2}
+
+
+def params_default() -> np.ndarray:
+    """The default parameter array built by the library (pgx_params_default)."""
+    p = np.zeros(180, dtype=np.float64)
+    check(lib().pgx_params_default(ptr(p)))
+    return p
+
+
+def params_read_file(path: str, fmt: str, base: np.ndarray = None) -> np.ndarray:
+    """`base` (default: the library's defaults) with the slots a parameter file names overwritten
+    (pgx_params_read_file); fmt is "sequential", "parallel" or "hypre"."""
+    p = params_default() if base is None else np.array(base, dtype=np.float64, copy=True)
+    check(lib().pgx_params_read_file(path.encode(), INPUTS_FORMATS[fmt], ptr(p)))
+    return p
 
 
 def read_mm(path: str):

@@ -38,6 +38,7 @@
 
 #include "../../include/pgx.h"
 #include "pgx_device.cuh"
+#include "pgx_params.h"
 #include "pgx_setup.h"
 
 namespace pgx {
@@ -3232,6 +3233,20 @@ int pgx_csr_free(pgx_csr* A) {
   free((void*)A->colidx);
   free((void*)A->values);
   memset(A, 0, sizeof(*A));
+  return PGX_SUCCESS;
+}
+
+int pgx_params_default(double* params) {
+  if (!params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  params::set_defaults(params);
+  return PGX_SUCCESS;
+}
+
+int pgx_params_read_file(const char* path, int32_t format, double* params) {
+  if (!path || !params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  std::string err;
+  const int rc = params::read_file(path, format, params, err);
+  if (rc) return fail(rc, "%s", err.c_str());
   return PGX_SUCCESS;
 }
 

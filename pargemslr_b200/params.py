@@ -4,7 +4,9 @@ ParGeMSLR drives every solver and preconditioner from one ``double
 params[180]`` array whose slots are named ``PARGEMSLR_IO_*``
 (ParGeMSLR SRC/utils/utils.hpp:77-297).  Drivers fill it with
 ``PargemslrSetDefaultParameterArray`` (SRC/utils/utils.cpp:30-126), then
-overwrite slots from a positional text file (TESTS/sequential/io.cpp:336-560).
+overwrite slots from a positional text file (TESTS/sequential/io.cpp:336-725,
+TESTS/parallel/io_par.cpp:359-819, TESTS/hypre/pargemslr_hypre_interface.cpp:391-820);
+``read_inputs_file`` reads those files with the library's native reader.
 The same array is accepted by this package's ``SetWithParameterArray`` and by
 the C ABI, so a driver keeps its parameter handling unchanged.
 """
@@ -230,6 +232,13 @@ def sequential_inputs_params() -> np.ndarray:
     p[ADVANCED_GLOBAL_SOLVE] = 0           # LU
     p[GENERAL_PRINT_LEVEL] = 1
     return p
+
+
+def read_inputs_file(path: str, fmt: str = "sequential", base: np.ndarray | None = None) -> np.ndarray:
+    """A driver parameter file read onto ``base`` (default: the defaults), as the reference driver of
+    that format reads it; fmt is "sequential", "parallel" or "hypre" (pgx_params_read_file)."""
+    from pargemslr_b200 import _abi
+    return _abi.params_read_file(path, fmt, base)
 
 
 def workload_params(name: str) -> np.ndarray:
