@@ -171,6 +171,13 @@ int pgx_gemslr_setup(pgx_handle *handle, const pgx_csr *A, const double *params,
  * factor layouts included; used for admission control. */
 int pgx_gemslr_device_bytes(pgx_handle handle, int32_t kdim, int64_t *bytes);
 
+/* Nonzeros of the preconditioner, counted as ParallelGemslrClass::GetNumNonzeros
+ * counts them (parallel_gemslr.cpp:7609-7632 over 1022-1056): nnz_bsolver sums
+ * the ILU factors of every level's B blocks, n_l + nnz(L_l) + nnz(U_l)
+ * (IluClass, ilu.cpp:2149); nnz_lr sums W_l and WH_l, m_l x r_l entries each.
+ * Host-side, valid once every level is set; either pointer may be NULL. */
+int pgx_gemslr_nnz(pgx_handle handle, int64_t *nnz_bsolver, int64_t *nnz_lr);
+
 /* FGMRES(kdim) solve of A x = b right-preconditioned by GeMSLR
  * (FlexGmresClass::Solve, fgmres.hpp:263-558).  params is the reference's
  * double[180] parameter array (PARGEMSLR_IO_*, utils.hpp:77-297) from which

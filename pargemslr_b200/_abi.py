@@ -44,6 +44,7 @@ EXPORTS = (
     "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
     "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes", "pgx_csr_read_mm", "pgx_csr_free",
     "pgx_server_start", "pgx_server_stop", "pgx_params_default", "pgx_params_read_file",
+    "pgx_gemslr_nnz",
 )
 
 
@@ -119,6 +120,7 @@ def lib() -> C.CDLL:
     L.pgx_server_stop.argtypes = [vp]
     L.pgx_gemslr_solve_static.argtypes = [vp, vp, vp, i32, vp, vp]
     L.pgx_params_default.argtypes = [vp]
+    L.pgx_gemslr_nnz.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     L.pgx_params_read_file.argtypes = [C.c_char_p, i32, vp]
     for name in EXPORTS:
         if name != "pgx_last_error":

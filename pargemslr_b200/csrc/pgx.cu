@@ -3236,6 +3236,22 @@ int pgx_csr_free(pgx_csr* A) {
   return PGX_SUCCESS;
 }
 
+int pgx_gemslr_nnz(pgx_handle h, int64_t* nnz_bsolver, int64_t* nnz_lr) {
+  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+  const Import& im = h->im;
+  if (im.nlev < 1) return fail(PGX_ERROR_FUNCTION_CALL, "levels not set");
+  int64_t nb = 0, nl = 0;
+  for (int l = 0; l < im.nlev; l++) {
+    const HostLevel& hl = im.levels[l];
+    if (!hl.set) return fail(PGX_ERROR_FUNCTION_CALL, "level %d not set", l);
+    nb += (int64_t)(im.lev_ptr[l + 1] - im.lev_ptr[l]) + hl.L.nnz() + hl.U.nnz();
+    nl += 2 * (int64_t)(im.n - im.lev_ptr[l + 1]) * hl.rank;
+  }
+  if (nnz_bsolver) *nnz_bsolver = nb;
+  if (nnz_lr) *nnz_lr = nl;
+  return PGX_SUCCESS;
+}
+
 int pgx_params_default(double* params) {
   if (!params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   params::set_defaults(params);
