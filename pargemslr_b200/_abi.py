@@ -47,6 +47,14 @@ EXPORTS = (
     "pgx_gemslr_nnz",
 )
 
+# every symbol include/pgx_hypre.h declares (the reference's hypre plugin interface)
+HYPRE_EXPORTS = (
+    "pgx_hypre_init_gpu", "pgx_hypre_finalize_gpu", "pgx_hypre_csr_matrix_create", "pgx_hypre_csr_matrix_destroy",
+    "pgx_hypre_csr_matrix_view", "pgx_hypre_gemslr_create", "pgx_hypre_gemslr_destroy",
+    "pgx_hypre_gemslr_set_params", "pgx_hypre_gemslr_set_precision", "pgx_hypre_gemslr_setup",
+    "pgx_hypre_gemslr_solve", "pgx_hypre_gemslr_handle", "pgx_hypre_params_from_file", "pgx_hypre_params_destroy",
+)
+
 
 class PgxError(RuntimeError):
     def __init__(self, code: int, msg: str):
@@ -122,9 +130,29 @@ def lib() -> C.CDLL:
     L.pgx_params_default.argtypes = [vp]
     L.pgx_gemslr_nnz.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     L.pgx_params_read_file.argtypes = [C.c_char_p, i32, vp]
-    for name in EXPORTS:
+    for name in EXPORTS + HYPRE_EXPORTS:
         if name != "pgx_last_error":
             getattr(L, name).restype = C.c_int
+    lg = C.c_long
+    L.pgx_hypre_init_gpu.argtypes = [C.c_int]
+    L.pgx_hypre_finalize_gpu.argtypes = []
+    L.pgx_hypre_csr_matrix_create.argtypes = [lg, lg, lg, lg, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, C.c_int, vp,
+                                              C.c_int]
+    L.pgx_hypre_csr_matrix_create.restype = vp
+    L.pgx_hypre_csr_matrix_destroy.argtypes = [vp]
+    L.pgx_hypre_csr_matrix_view.argtypes = [vp, C.POINTER(Csr)]
+    L.pgx_hypre_gemslr_create.argtypes = []
+    L.pgx_hypre_gemslr_create.restype = vp
+    L.pgx_hypre_gemslr_destroy.argtypes = [vp]
+    L.pgx_hypre_gemslr_set_params.argtypes = [vp, vp]
+    L.pgx_hypre_gemslr_set_precision.argtypes = [vp, C.c_int]
+    L.pgx_hypre_gemslr_setup.argtypes = [vp, vp, vp, vp]
+    L.pgx_hypre_gemslr_solve.argtypes = [vp, vp, vp, vp]
+    L.pgx_hypre_gemslr_handle.argtypes = [vp]
+    L.pgx_hypre_gemslr_handle.restype = vp
+    L.pgx_hypre_params_from_file.argtypes = [C.c_char_p]
+    L.pgx_hypre_params_from_file.restype = C.POINTER(C.c_double)
+    L.pgx_hypre_params_destroy.argtypes = [vp]
     _lib = L
     return L
 

@@ -38,6 +38,7 @@
 
 #include "../../include/pgx.h"
 #include "pgx_device.cuh"
+#include "pgx_internal.h"
 #include "pgx_params.h"
 #include "pgx_setup.h"
 
@@ -54,6 +55,11 @@ static int fail(int code, const char* fmt, ...) {
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
   g_last_error = buf;
+  return code;
+}
+
+int set_error(int code, const char* msg) {
+  g_last_error = msg;
   return code;
 }
 

@@ -1,4 +1,4 @@
-"""The C-ABI library loads and exports every symbol include/pgx.h declares (no GPU)."""
+"""The C-ABI library loads and exports every symbol include/pgx.h and include/pgx_hypre.h declare (no GPU)."""
 import os
 import re
 
@@ -7,19 +7,20 @@ from pargemslr_b200 import _abi
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared():
-    with open(os.path.join(ROOT, "include", "pgx.h")) as f:
+def declared(header="pgx.h"):
+    with open(os.path.join(ROOT, "include", header)) as f:
         text = f.read()
-    return sorted(set(re.findall(r"^(?:int|const char \*)\s*\**(pgx_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:int|const char \*|void \*|double \*|pgx_handle)\s*(pgx_\w+)\s*\(", text, re.M)))
 
 
 def test_header_and_binding_agree():
     assert declared() == sorted(_abi.EXPORTS)
+    assert declared("pgx_hypre.h") == sorted(_abi.HYPRE_EXPORTS)
 
 
 def test_library_exports_every_declared_symbol():
     L = _abi.lib()
-    missing = [s for s in declared() if not hasattr(L, s)]
+    missing = [s for s in declared() + declared("pgx_hypre.h") if not hasattr(L, s)]
     assert not missing, missing
 
 
