@@ -14,6 +14,7 @@ them in lockstep (their triangular passes merged); value = solves/s.
 
   python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp64]
   python bench.py --impl reference ...   (the reference CPU solver, oracle/_ref)
+  python bench.py --impl reference --ref-mode throughput   (one single-threaded reference per host thread)
 
 Under torchrun (N > 1) every rank solves its own replica on its own GPU; the
 solve does not shard, so there is no collective in the data path; the
@@ -144,32 +145,69 @@ def build_problem():
     return A, n, b, xt
 
 
-def cpu_sample(n_threads: int, iters: int, steps: int = 1):
-    """Time the reference CPU solver (oracle/_ref) on the same workload."""
+def _ref_command(out: str, xtrue_path: str, n_threads: int, iters: int, steps: int):
     driver = os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver")
-    if not os.path.exists(driver):
-        return None, "oracle/_ref/pgx_ref_driver not built"
     p = P.workload_params(WORKLOAD)
-    out = tempfile.mkdtemp(prefix="pgx_ref_")
-    A, n, b, xt = build_problem()
-    pgxd.write(os.path.join(out, "xtrue.bin"), {"x_true": xt})
-    cmd = [driver, "--out", out, "--lap", *[str(g) for g in GRID], "0", "0", "0", "0", "--xtrue",
-           os.path.join(out, "xtrue.bin"), "--threads", str(n_threads), "--solve", "--max-iters-timed", str(iters),
-           "--repeat", str(steps)]
+    cmd = [driver, "--out", out, "--lap", *[str(g) for g in GRID], "0", "0", "0", "0", "--xtrue", xtrue_path,
+           "--threads", str(n_threads), "--solve", "--max-iters-timed", str(iters), "--repeat", str(steps)]
     for i, v in enumerate(p):
         cmd += ["--param", f"{i}={float(v)!r}"]
     env = dict(os.environ, OMP_NUM_THREADS=str(n_threads), OPENBLAS_NUM_THREADS="1")
-    t0 = time.time()
-    subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
-    wall = time.time() - t0
+    return cmd, env
+
+
+def _ref_result(out: str, wall: float):
     res = {}
     with open(os.path.join(out, "result.txt")) as f:
         for line in f:
             k, v = line.strip().split("=", 1)
             res[k] = v
     times = [float(t) for t in res["solve_times"].split(",")]
-    its = int(res["iters"])
-    return {"times": times, "iters": its, "setup_s": float(res["setup_s"]), "wall_s": wall}, None
+    return {"times": times, "iters": int(res["iters"]), "setup_s": float(res["setup_s"]), "wall_s": wall}
+
+
+def _ref_inputs():
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver")):
+        return None
+    d = tempfile.mkdtemp(prefix="pgx_ref_")
+    A, n, b, xt = build_problem()
+    path = os.path.join(d, "xtrue.bin")
+    pgxd.write(path, {"x_true": xt})
+    return d, path
+
+
+def cpu_sample(n_threads: int, iters: int, steps: int = 1):
+    """Time the reference CPU solver (oracle/_ref) on the same workload: one process on n_threads threads."""
+    inp = _ref_inputs()
+    if inp is None:
+        return None, "oracle/_ref/pgx_ref_driver not built"
+    out, xtrue_path = inp
+    cmd, env = _ref_command(out, xtrue_path, n_threads, iters, steps)
+    t0 = time.time()
+    subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
+    return _ref_result(out, time.time() - t0), None
+
+
+def cpu_sample_procs(procs: int, iters: int, steps: int = 1):
+    """Throughput form of the reference baseline: `procs` single-threaded reference processes at once, each
+    setting up and solving the same workload on its own, as independent solves on the host's cores would run.
+    Returns one result per process."""
+    inp = _ref_inputs()
+    if inp is None:
+        return None, "oracle/_ref/pgx_ref_driver not built"
+    d, xtrue_path = inp
+    runs = []
+    t0 = time.time()
+    for k in range(procs):
+        out = os.path.join(d, f"p{k}")
+        os.makedirs(out)
+        cmd, env = _ref_command(out, xtrue_path, 1, iters, steps)
+        runs.append((out, subprocess.Popen(cmd, env=env, stdout=subprocess.DEVNULL)))
+    codes = [proc.wait() for _, proc in runs]
+    wall = time.time() - t0
+    if any(codes):
+        return None, f"reference processes exited with {codes}"
+    return [_ref_result(out, wall) for out, _ in runs], None
 
 
 def run_reference(args):
@@ -178,21 +216,35 @@ def run_reference(args):
         return
     threads = os.cpu_count() or 1
     steps = args.warmup + args.steps
-    r, why = cpu_sample(threads, args.ref_iters, steps)
-    if r is None:
-        print(json.dumps({"impl": "reference", "unavailable": why}))
-        return
-    per_iter = [t / max(r["iters"], 1) for t in r["times"][args.warmup:]]
-    t_solve = statistics.mean(per_iter) * REF_ITERS
-    value = 1.0 / t_solve
-    sample = (f"reference FGMRES+GemslrClass (oracle/_ref), first {r['iters']} iterations of the 128^3 solve per "
-              f"step on {threads} threads, scaled to the full {REF_ITERS}-iteration solve")
+    if args.ref_mode == "throughput":
+        rs, why = cpu_sample_procs(threads, args.ref_iters, steps)
+        if rs is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        # each process's solves/s from its timed steps, summed over the processes running at once
+        value = sum(1.0 / (statistics.mean(t / max(r["iters"], 1) for t in r["times"][args.warmup:]) * REF_ITERS)
+                    for r in rs)
+        t_solve = 1.0 / value
+        r = rs[0]
+        sample = (f"reference FGMRES+GemslrClass (oracle/_ref), {threads} single-threaded processes at once, each "
+                  f"timing the first {r['iters']} iterations of its own {GRID[0]}^3 solve per step, scaled to the full "
+                  f"{REF_ITERS}-iteration solve; solves/s summed over the processes")
+    else:
+        r, why = cpu_sample(threads, args.ref_iters, steps)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        per_iter = [t / max(r["iters"], 1) for t in r["times"][args.warmup:]]
+        t_solve = statistics.mean(per_iter) * REF_ITERS
+        value = 1.0 / t_solve
+        sample = (f"reference FGMRES+GemslrClass (oracle/_ref), first {r['iters']} iterations of the {GRID[0]}^3 "
+                  f"solve per step on {threads} threads, scaled to the full {REF_ITERS}-iteration solve")
     line = {
         "impl": "reference", "metric": metric_name(), "value": value, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_solve * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "3D 7-point Laplacian 128^3, 4 levels, ILUT 1e-3/200, rank 16, FGMRES(50), 1e-8",
-                   "setup_s": r["setup_s"]},
+        "config": {"workload": f"3D 7-point Laplacian {GRID[0]}^3, 4 levels, ILUT 1e-3/200, rank 16, FGMRES(50), "
+                               "1e-8", "setup_s": r["setup_s"], "ref_mode": args.ref_mode},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -399,6 +451,9 @@ def main():
                     help="right-hand sides each slot advances in lockstep")
     ap.add_argument("--no-fp64-plain", action="store_true", help="skip the plain FP64 comparison solves")
     ap.add_argument("--ref-iters", type=int, default=3, help="FGMRES iterations in one reference CPU sample")
+    ap.add_argument("--ref-mode", choices=["latency", "throughput"], default="latency",
+                    help="reference arm: one process on all host threads (latency), or one single-threaded "
+                         "process per host thread at once (throughput)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=128,
                     help="cube edge of the Laplacian (128 is the headline workload; smaller grids for profiling)")
