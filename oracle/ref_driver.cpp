@@ -393,6 +393,12 @@ int main(int argc, char **argv)
    FILE *res = std::fopen((out + "/result.txt").c_str(), "w");
    std::fprintf(res, "n=%d\nnnz=%ld\nsetup_s=%.9g\nthreads=%d\nnlev=%d\n", n, A.GetNumNonzeros(), t_setup, threads,
                 precond._nlev_used);
+   {
+      /* the preconditioner's own nonzero count (GemslrClass::GetNumNonzeros, gemslr.cpp:4127) */
+      long int nnz_bsolver = 0, nnz_lr = 0;
+      precond.GetNumNonzeros(nnz_bsolver, nnz_lr);
+      std::fprintf(res, "nnz_bsolver=%ld\nnnz_lr=%ld\n", nnz_bsolver, nnz_lr);
+   }
 
    if (apply_k > 0)
    {

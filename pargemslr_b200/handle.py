@@ -24,6 +24,53 @@ def init(device: int = 0) -> None:
         _initialized_device = device
 
 
+def import_structures(st: GemslrStructures, precision: str = "fp64") -> C.c_void_p:
+    """A handle holding the structures, set level by level (pgx_gemslr_create / set_*), not yet committed
+    to the device; the caller commits or destroys it."""
+    prec = {"fp64": _abi.PRECISION_FP64, "mixed": _abi.PRECISION_MIXED}[precision]
+    L = _abi.lib()
+    h = C.c_void_p()
+    _abi.check(L.pgx_gemslr_create(C.byref(h), st.n, prec))
+    keep: list = []
+    try:
+        A = _abi.csr_struct(*st.A, keep=keep)
+        _abi.check(L.pgx_gemslr_set_matrix(h, C.byref(A)))
+        pp = np.ascontiguousarray(st.pperm, np.int32)
+        qp = None if st.qperm is None else np.ascontiguousarray(st.qperm, np.int32)
+        keep.extend([pp, qp])
+        _abi.check(L.pgx_gemslr_set_perm(h, _abi.ptr(pp), _abi.ptr(qp)))
+        lp = np.ascontiguousarray(st.lev_ptr, np.int32)
+        keep.append(lp)
+        _abi.check(L.pgx_gemslr_set_levels(h, st.nlev, _abi.ptr(lp)))
+        for l, lv in enumerate(st.levels):
+            desc = _abi.Level()
+            dom = np.ascontiguousarray(lv.dom_ptr, np.int32)
+            dinv = np.ascontiguousarray(lv.dinv, np.float64)
+            keep.extend([dom, dinv])
+            desc.ncomp = lv.ncomp
+            desc.dom_ptr = _abi.ptr(dom)
+            desc.L = _abi.csr_struct(*lv.L, keep=keep)
+            desc.U = _abi.csr_struct(*lv.U, keep=keep)
+            desc.dinv = _abi.ptr(dinv)
+            desc.B = _abi.csr_struct(*lv.B, keep=keep)
+            if lv.E is not None:
+                desc.E = _abi.csr_struct(*lv.E, keep=keep)
+                desc.F = _abi.csr_struct(*lv.F, keep=keep)
+            desc.rank = lv.rank
+            if lv.rank > 0:
+                W = np.ascontiguousarray(lv.W, np.float64)
+                WH = np.ascontiguousarray(lv.WH, np.float64)
+                keep.extend([W, WH])
+                desc.W = _abi.ptr(W)
+                desc.WH = _abi.ptr(WH)
+            _abi.check(L.pgx_gemslr_set_level(h, l, C.byref(desc)))
+        _abi.check(L.pgx_gemslr_set_inner(h, st.inner_enable, st.inner_maxits, st.inner_tol))
+    except Exception:
+        L.pgx_gemslr_destroy(h)
+        raise
+    return h
+
+
 class GemslrHandle:
     """GeMSLR-preconditioned FGMRES on one GPU, built from post-setup structures.
 
@@ -35,48 +82,12 @@ class GemslrHandle:
         init(device)
         self.n = st.n
         self.precision = precision
-        prec = {"fp64": _abi.PRECISION_FP64, "mixed": _abi.PRECISION_MIXED}[precision]
-        L = _abi.lib()
-        h = C.c_void_p()
-        _abi.check(L.pgx_gemslr_create(C.byref(h), st.n, prec))
-        self._h = h
-        keep: list = []
+        self._h = None
+        self._h = import_structures(st, precision)
         try:
-            A = _abi.csr_struct(*st.A, keep=keep)
-            _abi.check(L.pgx_gemslr_set_matrix(h, C.byref(A)))
-            pp = np.ascontiguousarray(st.pperm, np.int32)
-            qp = None if st.qperm is None else np.ascontiguousarray(st.qperm, np.int32)
-            keep.extend([pp, qp])
-            _abi.check(L.pgx_gemslr_set_perm(h, _abi.ptr(pp), _abi.ptr(qp)))
-            lp = np.ascontiguousarray(st.lev_ptr, np.int32)
-            keep.append(lp)
-            _abi.check(L.pgx_gemslr_set_levels(h, st.nlev, _abi.ptr(lp)))
-            for l, lv in enumerate(st.levels):
-                desc = _abi.Level()
-                dom = np.ascontiguousarray(lv.dom_ptr, np.int32)
-                dinv = np.ascontiguousarray(lv.dinv, np.float64)
-                keep.extend([dom, dinv])
-                desc.ncomp = lv.ncomp
-                desc.dom_ptr = _abi.ptr(dom)
-                desc.L = _abi.csr_struct(*lv.L, keep=keep)
-                desc.U = _abi.csr_struct(*lv.U, keep=keep)
-                desc.dinv = _abi.ptr(dinv)
-                desc.B = _abi.csr_struct(*lv.B, keep=keep)
-                if lv.E is not None:
-                    desc.E = _abi.csr_struct(*lv.E, keep=keep)
-                    desc.F = _abi.csr_struct(*lv.F, keep=keep)
-                desc.rank = lv.rank
-                if lv.rank > 0:
-                    W = np.ascontiguousarray(lv.W, np.float64)
-                    WH = np.ascontiguousarray(lv.WH, np.float64)
-                    keep.extend([W, WH])
-                    desc.W = _abi.ptr(W)
-                    desc.WH = _abi.ptr(WH)
-                _abi.check(L.pgx_gemslr_set_level(h, l, C.byref(desc)))
-            _abi.check(L.pgx_gemslr_set_inner(h, st.inner_enable, st.inner_maxits, st.inner_tol))
-            _abi.check(L.pgx_gemslr_commit(h))
+            _abi.check(_abi.lib().pgx_gemslr_commit(self._h))
         except Exception:
-            L.pgx_gemslr_destroy(h)
+            _abi.lib().pgx_gemslr_destroy(self._h)
             self._h = None
             raise
 

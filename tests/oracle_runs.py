@@ -46,7 +46,7 @@ def run(lap=None, csr_file: Optional[str] = None, params: Optional[np.ndarray] =
     """Run the reference once; returns paths and parsed results."""
     key = hashlib.sha1(repr((lap, _file_digest(csr_file), None if params is None else params.tobytes(),
                              None if xtrue is None else xtrue.tobytes(), apply_k, solve, dump, threads, tag,
-                             _file_digest(rhs_file)))
+                             _file_digest(rhs_file), _file_digest(DRIVER)))
                        .encode()).hexdigest()[:16]
     out = os.path.join(CACHE, key)
     done = os.path.join(out, "result.txt")

@@ -107,3 +107,40 @@ def test_oracle_planted_error_is_detected():
     g = O.GemslrOracle(setup)
     n = g.n
     assert not np.array_equal(g.solve(ap["in"][:n]), ap["out"][:n])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_preconditioner_nonzeros_match_reference(case):
+    """pgx_gemslr_nnz on the reference's exported setup, against the reference's own count.
+
+    ILU part: every B block's ILU holds n_c + nnz(L_c) + nnz(U_c) (ilu.cpp:2149), summed over blocks and levels in
+    both GemslrClass::GetNumNonzeros (gemslr.cpp:4127) and ParallelGemslrClass::GetNumNonzeros
+    (parallel_gemslr.cpp:7609).  Low-rank part: the parallel class, which the library follows, counts W_l and WH_l
+    (m_l x r_l each); the sequential class the oracle runs counts W_l and H_l (r_l x r_l)."""
+    import ctypes as C
+
+    from pargemslr_b200 import _abi
+    from pargemslr_b200.handle import import_structures
+    from pargemslr_b200.structures import from_dump
+    setup, _, _, _, _, meta = load(case)
+    n, nlev = int(setup["n"][0]), int(setup["nlev"][0])
+    lev_ptr = setup["lev_ptr"]
+    ilu = sum(setup[f"L{l}.B{c}.D"].size + setup[f"L{l}.B{c}.L.j"].size + setup[f"L{l}.B{c}.U.j"].size
+              for l in range(nlev) for c in range(int(setup[f"L{l}.ncomp"][0])))
+    ranks = [int(setup[f"L{l}.lrc"][0]) if f"L{l}.lrc" in setup else 0 for l in range(nlev)]
+    m = [n - int(lev_ptr[l + 1]) for l in range(nlev)]
+    h = import_structures(from_dump(os.path.join(GOLDEN, case, "setup.bin")))
+    try:
+        nb, nl = C.c_int64(), C.c_int64()
+        _abi.check(_abi.lib().pgx_gemslr_nnz(h, C.byref(nb), C.byref(nl)))
+    finally:
+        _abi.lib().pgx_gemslr_destroy(h)
+    assert nb.value == ilu
+    assert nl.value == sum(2 * m[l] * ranks[l] for l in range(nlev))
+    from tests import oracle_runs
+    if oracle_runs.available():
+        lap = tuple(float(v) for v in meta["lap"].split())
+        lap = (int(lap[0]), int(lap[1]), int(lap[2])) + lap[3:]
+        ref = oracle_runs.run(lap=lap, params=P.workload_params(meta["workload"]), solve=False, dump=False)
+        assert ref["nnz_bsolver"] == nb.value
+        assert ref["nnz_lr"] == sum(m[l] * ranks[l] + ranks[l] ** 2 for l in range(nlev))
