@@ -329,6 +329,12 @@ int pgx_csr_free(pgx_csr *A);
 #define PGX_INPUTS_HYPRE      2
 int pgx_params_default(double *params);
 int pgx_params_read_file(const char *path, int32_t format, double *params);
+/* The command-line overrides the drivers' read_inputs applies
+ * (TESTS/sequential/io.cpp:729-748): "-tol V", "-kdim N", "-maxits N" among
+ * argv[0..argc-1], each taking the first occurrence whose next argument does
+ * not start with '-', read with atof / atoi (PargemslrReadInputArg,
+ * SRC/utils/utils.cpp:389-416). */
+int pgx_params_read_args(int32_t argc, const char *const *argv, double *params);
 
 /* y = alpha * A x + beta * y on device pointers (CSR SpMV kernel). */
 int pgx_csr_spmv_device(const pgx_csr *A_device, double alpha, const double *x, double beta, double *y);

@@ -44,7 +44,7 @@ EXPORTS = (
     "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
     "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes", "pgx_csr_read_mm", "pgx_csr_free",
     "pgx_server_start", "pgx_server_stop", "pgx_params_default", "pgx_params_read_file",
-    "pgx_gemslr_nnz",
+    "pgx_gemslr_nnz", "pgx_params_read_args",
 )
 
 # every symbol include/pgx_hypre.h declares (the reference's hypre plugin interface)
@@ -130,6 +130,7 @@ def lib() -> C.CDLL:
     L.pgx_params_default.argtypes = [vp]
     L.pgx_gemslr_nnz.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     L.pgx_params_read_file.argtypes = [C.c_char_p, i32, vp]
+    L.pgx_params_read_args.argtypes = [i32, C.POINTER(C.c_char_p), vp]
     for name in EXPORTS + HYPRE_EXPORTS:
         if name != "pgx_last_error":
             getattr(L, name).restype = C.c_int
@@ -207,6 +208,15 @@ def params_read_file(path: str, fmt: str, base: np.ndarray = None) -> np.ndarray
     (pgx_params_read_file); fmt is "sequential", "parallel" or "hypre"."""
     p = params_default() if base is None else np.array(base, dtype=np.float64, copy=True)
     check(lib().pgx_params_read_file(path.encode(), INPUTS_FORMATS[fmt], ptr(p)))
+    return p
+
+
+def params_read_args(args, base: np.ndarray = None) -> np.ndarray:
+    """`base` (default: the library's defaults) with a driver's -tol / -kdim / -maxits arguments applied
+    (pgx_params_read_args)."""
+    p = params_default() if base is None else np.array(base, dtype=np.float64, copy=True)
+    argv = (C.c_char_p * max(len(args), 1))(*[a.encode() for a in args])
+    check(lib().pgx_params_read_args(len(args), argv, ptr(p)))
     return p
 
 

@@ -5,6 +5,7 @@
 //   sequential  read_inputs_from_file  TESTS/sequential/io.cpp:336-725      (38 lines)
 //   parallel    read_inputs_from_file  TESTS/parallel/io_par.cpp:359-819    (35 lines)
 //   hypre       read_inputs_from_file  TESTS/hypre/pargemslr_hypre_interface.cpp:391-820 (31 lines)
+//   arguments   read_inputs            TESTS/sequential/io.cpp:729-748
 //
 // A file is read line by line; line k has a fixed meaning in each format.  A
 // numeric line fills its slots with the numbers found at its start, left to
@@ -299,6 +300,28 @@ void set_defaults(double* p) {
   p[RESIDUAL_ITERS] = 1;
   p[PRINT_LEVEL] = 1;
   p[POLY_ORDER] = 3;
+}
+
+// The command-line overrides of the drivers' read_inputs
+// (TESTS/sequential/io.cpp:729-748, TESTS/parallel/io_par.cpp:822-843): "-tol
+// V", "-kdim N", "-maxits N".  A flag counts when its next argument exists
+// and does not start with '-'; the first such occurrence wins.  Values are
+// read as atof / atoi read them (PargemslrReadInputArg, SRC/utils/utils.cpp:389-416).
+void read_args(int argc, const char* const* argv, double* p) {
+  struct Flag {
+    const char* name;
+    int slot;
+    bool integer;
+  };
+  static const Flag flags[] = {{"tol", TOL, false}, {"kdim", KDIM, true}, {"maxits", MAXITS, true}};
+  for (const Flag& f : flags) {
+    for (int i = 0; i < argc; i++) {
+      if (!argv[i] || argv[i][0] != '-' || strcmp(argv[i] + 1, f.name) != 0) continue;
+      if (i + 1 >= argc || !argv[i + 1] || argv[i + 1][0] == '-') continue;
+      p[f.slot] = f.integer ? (double)atoi(argv[i + 1]) : atof(argv[i + 1]);
+      break;
+    }
+  }
 }
 
 int read_file(const char* path, int format, double* p, std::string& err) {

@@ -3272,6 +3272,12 @@ int pgx_params_read_file(const char* path, int32_t format, double* params) {
   return PGX_SUCCESS;
 }
 
+int pgx_params_read_args(int32_t argc, const char* const* argv, double* params) {
+  if (!params || argc < 0 || (argc > 0 && !argv)) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  params::read_args(argc, argv, params);
+  return PGX_SUCCESS;
+}
+
 int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double beta, double* y) {
   if (!Ad || !x || !y) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   if (Ad->rows == 0) return PGX_SUCCESS;

@@ -110,3 +110,11 @@ def run_reference(fmt: str, path: str, fill: float | None = None):
     rc = int(out[k].split()[1])
     vals = np.array([float.fromhex(line.split()[1]) for line in out[k + 1:k + 181]])
     return rc, vals
+
+
+def run_reference_args(argv):
+    """(status, 180 values) from the sequential driver's read_inputs on argv, over the defaults."""
+    cmd = [os.path.join(REF_DIR, "params_ref_sequential"), "--args", *argv]
+    out = subprocess.run(cmd, capture_output=True, text=True, check=True).stdout.split("\n")
+    k = max(i for i, line in enumerate(out) if line.startswith("rc "))
+    return int(out[k].split()[1]), np.array([float.fromhex(line.split()[1]) for line in out[k + 1:k + 181]])

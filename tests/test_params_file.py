@@ -134,3 +134,38 @@ def test_errors(tmp_path):
     empty = _write(tmp_path, "e", "")
     for fmt in F.FORMATS:
         np.testing.assert_array_equal(_abi.params_read_file(empty, fmt), _abi.params_default())
+
+
+ARG_CASES = [
+    # (argv, {slot: value}) as the drivers' read_inputs applies them
+    (["-tol", "1e-3", "-kdim", "30", "-maxits", "77"], {13: 1e-3, 11: 30, 12: 77}),
+    (["-maxits", "-5", "x", "-maxits", "12"], {12: 12}),  # a value starting with '-' is skipped
+    (["-kdim", "2.9e1", "-kdim", "40"], {11: 2}),  # atoi reads the leading digits; the first use wins
+    (["--tol", "5", "tol", "6", "-tol"], {}),  # neither "--tol" nor a bare name nor a trailing flag counts
+    (["-tol", "abc"], {13: 0.0}),  # atof of a non-number
+    ([], {}),
+]
+
+
+@pytest.mark.parametrize("argv,changed", ARG_CASES)
+def test_command_line_arguments(argv, changed):
+    want = _abi.params_default()
+    for slot, v in changed.items():
+        want[slot] = v
+    np.testing.assert_array_equal(_abi.params_read_args(argv), want)
+    if F.reference_available("sequential"):
+        rc, ref = F.run_reference_args(argv)
+        assert rc == 0
+        np.testing.assert_array_equal(ref, want)
+
+
+def test_random_command_lines_live():
+    if not F.reference_available("sequential"):
+        pytest.skip("oracle/_ref parsers not built")
+    import random
+    rng = random.Random(17)
+    toks = ["-tol", "-kdim", "-maxits", "-x", "--tol", "tol", "1e-3", "-1", "42", "3.5", "abc", "", "7e", "0x10"]
+    for _ in range(200):
+        argv = [rng.choice(toks) for _ in range(rng.randint(0, 8))]
+        rc, ref = F.run_reference_args(argv)
+        np.testing.assert_array_equal(_abi.params_read_args(argv), ref, err_msg=repr(argv))
