@@ -310,6 +310,16 @@ int pgx_build_levels(char uplo, int32_t n, const int32_t *rowptr, const int32_t 
 int pgx_csr_read_mm(const char *path, pgx_csr *A);
 int pgx_csr_free(pgx_csr *A);
 
+/* Read a vector stored as a coordinate Matrix Market file of M rows (the
+ * right-hand sides of the reference's matrix lists, e.g. gr_30_30_b.mtx), as
+ * SequentialVectorClass::ReadFromMMFile reads it (vectorops.cpp:1116-1180):
+ * M entries, zero except x[I - idxin] = value for each listed entry "I J
+ * value", a later entry replacing an earlier one, J not used.  *n receives M;
+ * x may be NULL to ask for M only, otherwise it needs capacity >= M entries.
+ * Errors: PGX_ERROR_IO (unreadable file or entry, index out of range);
+ * PGX_ERROR_INVALID_PARAM (capacity below M). */
+int pgx_vector_read_mm(const char *path, int32_t idxin, int32_t capacity, double *x, int32_t *n);
+
 /* ---- parameter arrays ----------------------------------------------------
  * The double[PGX_PARAMS_SIZE] array every entry point above takes is the one
  * SetWithParameterArray reads (index names in SRC/utils/utils.hpp:77-297).

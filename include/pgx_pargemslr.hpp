@@ -75,6 +75,21 @@ class ParallelVectorClass {
     for (int i = 0; i < n_; i++) data_[i] = v;
     return PGX_SUCCESS;
   }
+  /* A vector in a coordinate Matrix Market file (SequentialVectorClass::
+   * ReadFromMMFile, sequential_vector.hpp:572); idxin is the file's index
+   * base.  The vector becomes an owned host vector. */
+  int ReadFromMMFile(const char* vecfile, int idxin) {
+    int32_t n = 0;
+    int rc = pgx_vector_read_mm(vecfile, idxin, 0, nullptr, &n);
+    if (rc) return rc;
+    own_.assign((size_t)n, 0.0);
+    rc = pgx_vector_read_mm(vecfile, idxin, n, own_.data(), &n);
+    if (rc) return rc;
+    data_ = own_.data();
+    n_ = n;
+    location_ = kMemoryHost;
+    return PGX_SUCCESS;
+  }
   double* GetData() const { return data_; }
   int GetLengthLocal() const { return n_; }
   long int GetLengthGlobal() const { return n_; }

@@ -44,7 +44,7 @@ EXPORTS = (
     "pgx_server_create", "pgx_server_submit", "pgx_server_step", "pgx_server_collect", "pgx_server_destroy",
     "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes", "pgx_csr_read_mm", "pgx_csr_free",
     "pgx_server_start", "pgx_server_stop", "pgx_params_default", "pgx_params_read_file",
-    "pgx_gemslr_nnz", "pgx_params_read_args",
+    "pgx_gemslr_nnz", "pgx_params_read_args", "pgx_vector_read_mm",
 )
 
 # every symbol include/pgx_hypre.h declares (the reference's hypre plugin interface)
@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
     L.pgx_gemslr_nnz.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     L.pgx_params_read_file.argtypes = [C.c_char_p, i32, vp]
     L.pgx_params_read_args.argtypes = [i32, C.POINTER(C.c_char_p), vp]
+    L.pgx_vector_read_mm.argtypes = [C.c_char_p, i32, i32, vp, C.POINTER(i32)]
     for name in EXPORTS + HYPRE_EXPORTS:
         if name != "pgx_last_error":
             getattr(L, name).restype = C.c_int
@@ -218,6 +219,16 @@ def params_read_args(args, base: np.ndarray = None) -> np.ndarray:
     argv = (C.c_char_p * max(len(args), 1))(*[a.encode() for a in args])
     check(lib().pgx_params_read_args(len(args), argv, ptr(p)))
     return p
+
+
+def read_mm_vector(path: str, idxin: int = 1) -> np.ndarray:
+    """A vector stored as a coordinate Matrix Market file, read by the library (pgx_vector_read_mm)."""
+    L = lib()
+    n = C.c_int32(0)
+    check(L.pgx_vector_read_mm(path.encode(), idxin, 0, None, C.byref(n)))
+    x = np.zeros(n.value)
+    check(L.pgx_vector_read_mm(path.encode(), idxin, n.value, ptr(x), C.byref(n)))
+    return x
 
 
 def read_mm(path: str):

@@ -3258,6 +3258,18 @@ int pgx_gemslr_nnz(pgx_handle h, int64_t* nnz_bsolver, int64_t* nnz_lr) {
   return PGX_SUCCESS;
 }
 
+int pgx_vector_read_mm(const char* path, int32_t idxin, int32_t capacity, double* x, int32_t* n) {
+  if (!path || !n) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  std::vector<double> v;
+  std::string err;
+  if (setup::read_matrix_market_vector(path, idxin, v, err)) return fail(PGX_ERROR_IO, "%s: %s", path, err.c_str());
+  *n = (int32_t)v.size();
+  if (!x) return PGX_SUCCESS;
+  if (capacity < *n) return fail(PGX_ERROR_INVALID_PARAM, "capacity %d below the vector's %d entries", capacity, *n);
+  std::copy(v.begin(), v.end(), x);
+  return PGX_SUCCESS;
+}
+
 int pgx_params_default(double* params) {
   if (!params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   params::set_defaults(params);

@@ -35,6 +35,7 @@ Graph symmetric_graph(int n, const int* rp, const int* cj);
 Ordering gemslr_ordering(const Graph& g, int nlev, int minsep, bool local_rcm);
 int ilut(int n, const int* rp, const int* cj, const double* va, double droptol, int lfil, Factor& f);
 int read_matrix_market(const char* path, Csr& out, std::string& err);
+int read_matrix_market_vector(const char* path, int idxin, std::vector<double>& x, std::string& err);
 Csr permuted_block(int n, const int* rp, const int* cj, const double* va, const std::vector<int>& perm,
                    const std::vector<int>& iperm, int r0, int r1, int c0, int c1);
 

@@ -444,6 +444,46 @@ Csr permuted_block(int n, const int* rp, const int* cj, const double* va, const 
 }
 
 // ------------------------------------------------------------ Matrix Market
+// The banner and size line of a coordinate Matrix Market file with real or
+// integer values; for a matrix, general or symmetric (sym set for the latter).
+static bool mm_header(FILE* f, bool matrix_symmetry, bool& sym, long long& M, long long& N, long long& nz,
+                      std::string& err) {
+  char line[1024];
+  if (!std::fgets(line, sizeof(line), f)) {
+    err = "empty file";
+    return false;
+  }
+  std::string banner(line);
+  for (auto& c : banner) c = (char)std::tolower((unsigned char)c);
+  if (banner.rfind("%%matrixmarket", 0) != 0) {
+    err = "no Matrix Market banner";
+    return false;
+  }
+  if (banner.find("matrix") == std::string::npos || banner.find("coordinate") == std::string::npos) {
+    err = "only coordinate matrices are supported";
+    return false;
+  }
+  if (banner.find("real") == std::string::npos && banner.find("integer") == std::string::npos) {
+    err = "only real or integer values are supported";
+    return false;
+  }
+  sym = banner.find("symmetric") != std::string::npos && banner.find("skew") == std::string::npos;
+  if (matrix_symmetry && banner.find("general") == std::string::npos && !sym) {
+    err = "only general or symmetric matrices are supported";
+    return false;
+  }
+  M = N = nz = 0;
+  while (std::fgets(line, sizeof(line), f)) {
+    if (line[0] == '%') continue;
+    if (std::sscanf(line, "%lld %lld %lld", &M, &N, &nz) == 3) break;
+  }
+  if (M <= 0 || N <= 0 || nz < 0 || M > INT32_MAX || N > INT32_MAX) {
+    err = "invalid size line";
+    return false;
+  }
+  return true;
+}
+
 // Coordinate Matrix Market files with real or integer values, general or
 // symmetric, as CooMatrixReadFromFile accepts them (ParGeMSLR
 // SRC/matrices/matrixops.cpp:11134-11210): indices 1-based in the file; a
@@ -460,39 +500,9 @@ int read_matrix_market(const char* path, Csr& out, std::string& err) {
     FILE* f;
     ~Closer() { std::fclose(f); }
   } closer{f};
-  char line[1024];
-  if (!std::fgets(line, sizeof(line), f)) {
-    err = "empty file";
-    return 1;
-  }
-  std::string banner(line);
-  for (auto& c : banner) c = (char)std::tolower((unsigned char)c);
-  if (banner.rfind("%%matrixmarket", 0) != 0) {
-    err = "no Matrix Market banner";
-    return 1;
-  }
-  if (banner.find("matrix") == std::string::npos || banner.find("coordinate") == std::string::npos) {
-    err = "only coordinate matrices are supported";
-    return 1;
-  }
-  if (banner.find("real") == std::string::npos && banner.find("integer") == std::string::npos) {
-    err = "only real or integer values are supported";
-    return 1;
-  }
-  const bool sym = banner.find("symmetric") != std::string::npos && banner.find("skew") == std::string::npos;
-  if (banner.find("general") == std::string::npos && !sym) {
-    err = "only general or symmetric matrices are supported";
-    return 1;
-  }
+  bool sym = false;
   long long M = 0, N = 0, nz = 0;
-  while (std::fgets(line, sizeof(line), f)) {
-    if (line[0] == '%') continue;
-    if (std::sscanf(line, "%lld %lld %lld", &M, &N, &nz) == 3) break;
-  }
-  if (M <= 0 || N <= 0 || nz < 0 || M > INT32_MAX || N > INT32_MAX) {
-    err = "invalid size line";
-    return 1;
-  }
+  if (!mm_header(f, true, sym, M, N, nz, err)) return 1;
   std::vector<long long> key;
   std::vector<double> val;
   key.reserve((size_t)(sym ? 2 * nz : nz));
@@ -534,6 +544,41 @@ int read_matrix_market(const char* path, Csr& out, std::string& err) {
     out.rp[(size_t)(key[t] / N) + 1]++;
   }
   for (long long r = 0; r < M; r++) out.rp[r + 1] += out.rp[r];
+  return 0;
+}
+
+// A vector in a coordinate Matrix Market file, as SequentialVectorReadFromFile
+// reads one (ParGeMSLR SRC/vectors/vectorops.cpp:1116-1180): M entries, zero
+// except x[I - idxin] = value for each listed entry, a later entry replacing
+// an earlier one; the column index is not used.
+int read_matrix_market_vector(const char* path, int idxin, std::vector<double>& x, std::string& err) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) {
+    err = std::string("cannot open ") + path;
+    return 1;
+  }
+  struct Closer {
+    FILE* f;
+    ~Closer() { std::fclose(f); }
+  } closer{f};
+  bool sym = false;
+  long long M = 0, N = 0, nz = 0;
+  if (!mm_header(f, false, sym, M, N, nz, err)) return 1;
+  x.assign((size_t)M, 0.0);
+  for (long long k = 0; k < nz; k++) {
+    long long I, J;
+    double v;
+    if (std::fscanf(f, "%lld %lld %lf", &I, &J, &v) != 3) {
+      err = "entry " + std::to_string(k + 1) + " unreadable";
+      return 1;
+    }
+    const long long r = I - idxin;
+    if (r < 0 || r >= M) {
+      err = "entry " + std::to_string(k + 1) + " out of range";
+      return 1;
+    }
+    x[(size_t)r] = v;
+  }
   return 0;
 }
 

@@ -115,6 +115,24 @@ def test_driver_rejects_a_bad_parameter_file(tmp_path):
     assert rc == 1 and kv["params"] == str(_abi.ERROR_IO) and "line 3" in text
 
 
+def test_vector_from_matrix_market(tmp_path):
+    """ParallelVectorClass::ReadFromMMFile reads a right-hand-side file as the reference's vector reader does."""
+    vec = tmp_path / "b.mtx"
+    vec.write_text("%%MatrixMarket matrix coordinate real general\n5 1 3\n2 1 0.5\n5 1 -2\n2 1 4\n")
+    src = tmp_path / "v.cpp"
+    src.write_text('#include <cstdio>\n#include "pgx_pargemslr.hpp"\n'
+                   "int main(int, char** argv) { pgx::ParallelVectorClass<double> b;\n"
+                   "  int rc = b.ReadFromMMFile(argv[1], 1); printf(\"%d %d\", rc, b.GetLengthLocal());\n"
+                   "  for (int i = 0; i < b.GetLengthLocal(); i++) printf(\" %g\", b.GetData()[i]);\n"
+                   "  printf(\" %d\\n\", b.ReadFromMMFile(\"/nonexistent.mtx\", 1)); return 0; }\n")
+    exe = str(tmp_path / "v")
+    lib = os.path.dirname(_abi.LIB_PATH)
+    subprocess.run(["g++", "-std=c++11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", exe,
+                    "-L", lib, "-lpgx", f"-Wl,-rpath,{lib}"], check=True)
+    out = subprocess.run([exe, str(vec)], capture_output=True, text=True, check=True).stdout.split()
+    assert out == ["0", "5", "0", "4", "0", "0", "-2", str(_abi.ERROR_IO)]
+
+
 def test_single_precision_types_do_not_compile(tmp_path):
     src = tmp_path / "f.cpp"
     src.write_text('#include "pgx_pargemslr.hpp"\nint main() { pgx::ParallelVectorClass<float> v; return 0; }\n')
