@@ -115,15 +115,16 @@ void* pgx_hypre_csr_matrix_create(long int nrow_global, long int ncol_global, lo
                                   long int ncol_start, int nrow_local, int ncol_local, int* diag_i, int* diag_j,
                                   double* diag_data, int* offd_i, int* /*offd_j*/, double* /*offd_data*/,
                                   int n_offd_map, long int* /*offd_map*/, int data_location) {
-  std::unique_ptr<HypreMatrix> m(new (std::nothrow) HypreMatrix());
-  if (!m) {
-    err(PGX_ERROR_OOM, "host allocation");
+  try {
+    std::unique_ptr<HypreMatrix> m(new HypreMatrix());
+    if (build_matrix(*m, nrow_global, ncol_global, nrow_start, ncol_start, nrow_local, ncol_local, diag_i, diag_j,
+                     diag_data, offd_i, n_offd_map, data_location))
+      return nullptr;
+    return m.release();
+  } catch (const std::bad_alloc&) {
+    err(PGX_ERROR_OOM, "host allocation for the matrix failed");
     return nullptr;
   }
-  if (build_matrix(*m, nrow_global, ncol_global, nrow_start, ncol_start, nrow_local, ncol_local, diag_i, diag_j,
-                   diag_data, offd_i, n_offd_map, data_location))
-    return nullptr;
-  return m.release();
 }
 
 int pgx_hypre_csr_matrix_destroy(void* matrix) {

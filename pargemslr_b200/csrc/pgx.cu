@@ -30,7 +30,9 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <exception>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <type_traits>
@@ -61,6 +63,22 @@ static int fail(int code, const char* fmt, ...) {
 int set_error(int code, const char* msg) {
   g_last_error = msg;
   return code;
+}
+
+// Runs an entry point's body so that no C++ exception crosses the C ABI: a
+// failed host allocation becomes PGX_ERROR_OOM, any other exception
+// PGX_ERROR_FUNCTION_CALL, each with its message.
+template <class F>
+static int guarded(const char* what, F&& body) {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return fail(PGX_ERROR_OOM, "%s: host allocation failed", what);
+  } catch (const std::exception& e) {
+    return fail(PGX_ERROR_FUNCTION_CALL, "%s: %s", what, e.what());
+  } catch (...) {
+    return fail(PGX_ERROR_FUNCTION_CALL, "%s: unexpected exception", what);
+  }
 }
 
 #define PGX_CUDA(call)                                                                       \
@@ -2560,23 +2578,27 @@ const char* pgx_last_error(void) { return g_last_error.c_str(); }
 int pgx_version(void) { return 100; }
 
 int pgx_gemslr_create(pgx_handle* handle, int32_t n, int32_t precision) {
-  if (!handle) return fail(PGX_ERROR_INVALID_PARAM, "null handle pointer");
-  *handle = nullptr;
-  if (n <= 0) return fail(PGX_ERROR_INVALID_PARAM, "n must be positive");
-  if (precision != PGX_PRECISION_FP64 && precision != PGX_PRECISION_MIXED)
-    return fail(PGX_ERROR_INVALID_OPTION, "unknown precision %d", precision);
-  pgx_gemslr_s* h = new pgx_gemslr_s();
-  h->im.n = n;
-  h->im.precision = precision;
-  h->device = g_device;
-  *handle = h;
-  return PGX_SUCCESS;
+  return guarded("pgx_gemslr_create", [&]() -> int {
+    if (!handle) return fail(PGX_ERROR_INVALID_PARAM, "null handle pointer");
+    *handle = nullptr;
+    if (n <= 0) return fail(PGX_ERROR_INVALID_PARAM, "n must be positive");
+    if (precision != PGX_PRECISION_FP64 && precision != PGX_PRECISION_MIXED)
+      return fail(PGX_ERROR_INVALID_OPTION, "unknown precision %d", precision);
+    pgx_gemslr_s* h = new pgx_gemslr_s();
+    h->im.n = n;
+    h->im.precision = precision;
+    h->device = g_device;
+    *handle = h;
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_gemslr_set_matrix(pgx_handle h, const pgx_csr* A) {
-  if (!h || !A) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  if (A->rows != h->im.n || A->cols != h->im.n) return fail(PGX_ERROR_INVALID_PARAM, "A must be n x n");
-  return copy_csr(A, h->im.A, "A");
+  return guarded("pgx_gemslr_set_matrix", [&]() -> int {
+    if (!h || !A) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    if (A->rows != h->im.n || A->cols != h->im.n) return fail(PGX_ERROR_INVALID_PARAM, "A must be n x n");
+    return copy_csr(A, h->im.A, "A");
+  });
 }
 
 static int check_perm(const int32_t* p, int n, const char* what) {
@@ -2589,70 +2611,76 @@ static int check_perm(const int32_t* p, int n, const char* what) {
 }
 
 int pgx_gemslr_set_perm(pgx_handle h, const int32_t* pperm, const int32_t* qperm) {
-  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
-  const int n = h->im.n;
-  if (pperm) {
-    PGX_TRY(check_perm(pperm, n, "pperm"));
-    h->im.pperm.assign(pperm, pperm + n);
-  } else {
-    h->im.pperm.resize(n);
-    for (int i = 0; i < n; i++) h->im.pperm[i] = i;
-  }
-  h->im.qperm.clear();
-  if (qperm) {
-    PGX_TRY(check_perm(qperm, n, "qperm"));
-    h->im.qperm.assign(qperm, qperm + n);
-  }
-  return PGX_SUCCESS;
+  return guarded("pgx_gemslr_set_perm", [&]() -> int {
+    if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+    const int n = h->im.n;
+    if (pperm) {
+      PGX_TRY(check_perm(pperm, n, "pperm"));
+      h->im.pperm.assign(pperm, pperm + n);
+    } else {
+      h->im.pperm.resize(n);
+      for (int i = 0; i < n; i++) h->im.pperm[i] = i;
+    }
+    h->im.qperm.clear();
+    if (qperm) {
+      PGX_TRY(check_perm(qperm, n, "qperm"));
+      h->im.qperm.assign(qperm, qperm + n);
+    }
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_gemslr_set_levels(pgx_handle h, int32_t nlev, const int32_t* lev_ptr) {
-  if (!h || !lev_ptr) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  if (nlev < 1) return fail(PGX_ERROR_INVALID_PARAM, "nlev must be >= 1");
-  if (lev_ptr[0] != 0 || lev_ptr[nlev] != h->im.n) return fail(PGX_ERROR_INVALID_PARAM, "lev_ptr must span [0, n]");
-  for (int l = 0; l < nlev; l++)
-    if (lev_ptr[l + 1] <= lev_ptr[l]) return fail(PGX_ERROR_INVALID_PARAM, "level %d is empty", l);
-  h->im.nlev = nlev;
-  h->im.lev_ptr.assign(lev_ptr, lev_ptr + nlev + 1);
-  h->im.levels.assign(nlev, HostLevel());
-  return PGX_SUCCESS;
+  return guarded("pgx_gemslr_set_levels", [&]() -> int {
+    if (!h || !lev_ptr) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    if (nlev < 1) return fail(PGX_ERROR_INVALID_PARAM, "nlev must be >= 1");
+    if (lev_ptr[0] != 0 || lev_ptr[nlev] != h->im.n) return fail(PGX_ERROR_INVALID_PARAM, "lev_ptr must span [0, n]");
+    for (int l = 0; l < nlev; l++)
+      if (lev_ptr[l + 1] <= lev_ptr[l]) return fail(PGX_ERROR_INVALID_PARAM, "level %d is empty", l);
+    h->im.nlev = nlev;
+    h->im.lev_ptr.assign(lev_ptr, lev_ptr + nlev + 1);
+    h->im.levels.assign(nlev, HostLevel());
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_gemslr_set_level(pgx_handle h, int32_t level, const pgx_level* d) {
-  if (!h || !d) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  Import& im = h->im;
-  if (level < 0 || level >= im.nlev) return fail(PGX_ERROR_INVALID_PARAM, "level %d out of range", level);
-  const int nl = im.lev_ptr[level + 1] - im.lev_ptr[level];
-  const int m = im.n - im.lev_ptr[level + 1];
-  const bool last = level == im.nlev - 1;
-  HostLevel hl;
-  hl.ncomp = d->ncomp;
-  if (d->dom_ptr && d->ncomp > 0) hl.dom_ptr.assign(d->dom_ptr, d->dom_ptr + d->ncomp + 1);
-  PGX_TRY(copy_csr(&d->L, hl.L, "L"));
-  PGX_TRY(copy_csr(&d->U, hl.U, "U"));
-  PGX_TRY(copy_csr(&d->B, hl.B, "B"));
-  if (hl.L.rows != nl || hl.L.cols != nl || hl.U.rows != nl || hl.U.cols != nl)
-    return fail(PGX_ERROR_INVALID_PARAM, "level %d: L/U must be %d x %d", level, nl, nl);
-  if (!d->dinv) return fail(PGX_ERROR_INVALID_PARAM, "level %d: missing dinv", level);
-  hl.dinv.assign(d->dinv, d->dinv + nl);
-  if (!hl.B.empty() && (hl.B.rows != nl || hl.B.cols != nl))
-    return fail(PGX_ERROR_INVALID_PARAM, "level %d: B must be %d x %d", level, nl, nl);
-  if (!last) {
-    PGX_TRY(copy_csr(&d->E, hl.E, "E"));
-    PGX_TRY(copy_csr(&d->F, hl.F, "F"));
-    if (hl.E.rows != m || hl.E.cols != nl) return fail(PGX_ERROR_INVALID_PARAM, "level %d: E must be %d x %d", level, m, nl);
-    if (hl.F.rows != nl || hl.F.cols != m) return fail(PGX_ERROR_INVALID_PARAM, "level %d: F must be %d x %d", level, nl, m);
-    if (d->rank < 0 || d->rank > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "level %d: rank %d outside [0, %d]", level, d->rank, KMAX);
-    hl.rank = d->rank;
-    if (hl.rank > 0) {
-      if (!d->W || !d->WH) return fail(PGX_ERROR_INVALID_PARAM, "level %d: missing W/WH", level);
-      hl.W.assign(d->W, d->W + (size_t)m * hl.rank);
-      hl.WH.assign(d->WH, d->WH + (size_t)m * hl.rank);
+  return guarded("pgx_gemslr_set_level", [&]() -> int {
+    if (!h || !d) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    Import& im = h->im;
+    if (level < 0 || level >= im.nlev) return fail(PGX_ERROR_INVALID_PARAM, "level %d out of range", level);
+    const int nl = im.lev_ptr[level + 1] - im.lev_ptr[level];
+    const int m = im.n - im.lev_ptr[level + 1];
+    const bool last = level == im.nlev - 1;
+    HostLevel hl;
+    hl.ncomp = d->ncomp;
+    if (d->dom_ptr && d->ncomp > 0) hl.dom_ptr.assign(d->dom_ptr, d->dom_ptr + d->ncomp + 1);
+    PGX_TRY(copy_csr(&d->L, hl.L, "L"));
+    PGX_TRY(copy_csr(&d->U, hl.U, "U"));
+    PGX_TRY(copy_csr(&d->B, hl.B, "B"));
+    if (hl.L.rows != nl || hl.L.cols != nl || hl.U.rows != nl || hl.U.cols != nl)
+      return fail(PGX_ERROR_INVALID_PARAM, "level %d: L/U must be %d x %d", level, nl, nl);
+    if (!d->dinv) return fail(PGX_ERROR_INVALID_PARAM, "level %d: missing dinv", level);
+    hl.dinv.assign(d->dinv, d->dinv + nl);
+    if (!hl.B.empty() && (hl.B.rows != nl || hl.B.cols != nl))
+      return fail(PGX_ERROR_INVALID_PARAM, "level %d: B must be %d x %d", level, nl, nl);
+    if (!last) {
+      PGX_TRY(copy_csr(&d->E, hl.E, "E"));
+      PGX_TRY(copy_csr(&d->F, hl.F, "F"));
+      if (hl.E.rows != m || hl.E.cols != nl) return fail(PGX_ERROR_INVALID_PARAM, "level %d: E must be %d x %d", level, m, nl);
+      if (hl.F.rows != nl || hl.F.cols != m) return fail(PGX_ERROR_INVALID_PARAM, "level %d: F must be %d x %d", level, nl, m);
+      if (d->rank < 0 || d->rank > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "level %d: rank %d outside [0, %d]", level, d->rank, KMAX);
+      hl.rank = d->rank;
+      if (hl.rank > 0) {
+        if (!d->W || !d->WH) return fail(PGX_ERROR_INVALID_PARAM, "level %d: missing W/WH", level);
+        hl.W.assign(d->W, d->W + (size_t)m * hl.rank);
+        hl.WH.assign(d->WH, d->WH + (size_t)m * hl.rank);
+      }
     }
-  }
-  hl.set = true;
-  im.levels[level] = std::move(hl);
-  return PGX_SUCCESS;
+    hl.set = true;
+    im.levels[level] = std::move(hl);
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_gemslr_set_inner(pgx_handle h, int32_t enable, int32_t maxits, double tol) {
@@ -2713,98 +2741,100 @@ static HostCsr to_host(const setup::Csr& b) {
 }
 
 int pgx_gemslr_setup(pgx_handle* handle, const pgx_csr* A, const double* params, int32_t precision) {
-  if (!handle || !A || !params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  *handle = nullptr;
-  if (A->rows != A->cols) return fail(PGX_ERROR_INVALID_PARAM, "A must be square");
-  pgx_handle h = nullptr;
-  PGX_TRY(pgx_gemslr_create(&h, A->rows, precision));
-  std::unique_ptr<pgx_gemslr_s> guard(h);
-  Import& im = h->im;
-  PGX_TRY(copy_csr(A, im.A, "A"));
-  const int n = im.n;
-  // parameters (PARGEMSLR_IO_* slots, SRC/utils/utils.hpp:77-297)
-  const int nlev_req = std::max(1, (int)params[20]);
-  const int perm_opt = (int)params[58];
-  const double tolB = params[40], tolC = params[44];
-  const int lfilB = std::max(1, (int)params[48]), lfilC = std::max(1, (int)params[50]);
-  const int rank1 = std::max(0, (int)params[74]), rank2 = std::max(0, (int)params[75]);
-  const double rfac1 = params[78] > 0 ? params[78] : 1.0, rfac2 = params[79] > 0 ? params[79] : 1.0;
-  const int lr_its = std::max(1, (int)params[90]);
-  im.inner_enable = params[130] != 0.0;
-  im.inner_tol = params[131];
-  im.inner_maxits = std::max(1, (int)params[132]);
-  if (im.inner_maxits > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "inner maxits above %d", KMAX);
-  // 1. levels and ordering
-  setup::Graph g = setup::symmetric_graph(n, im.A.rp.data(), im.A.cj.data());
-  setup::Ordering ord = setup::gemslr_ordering(g, nlev_req, 10, perm_opt != 0);
-  const int nlev = (int)ord.lev_ptr.size() - 1;
-  std::vector<int> iperm(n);
-  for (int i = 0; i < n; i++) iperm[ord.perm[i]] = i;
-  im.pperm = ord.perm;
-  im.qperm.clear();
-  PGX_TRY(pgx_gemslr_set_levels(h, nlev, ord.lev_ptr.data()));
-  // 2. blocks and ILUT factors per level (subdomains in parallel)
-  for (int l = 0; l < nlev; l++) {
-    HostLevel& hl = im.levels[l];
-    const int start = ord.lev_ptr[l], end = ord.lev_ptr[l + 1], nl = end - start;
-    const std::vector<int>& dom = ord.dom_ptr[l];
-    const int ncomp = (int)dom.size() - 1;
-    const bool last = l == nlev - 1;
-    std::vector<setup::Csr> B(ncomp);
-    std::vector<setup::Factor> F(ncomp);
-    std::vector<int> rc(ncomp, 0);
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int c = 0; c < ncomp; c++) {
-      const int r0 = start + dom[c], r1 = start + dom[c + 1];
-      B[c] = setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm, r0, r1, r0, r1);
-      rc[c] = setup::ilut(B[c].rows, B[c].rp.data(), B[c].cj.data(), B[c].va.data(), last ? tolC : tolB,
-                          last ? lfilC : lfilB, F[c]);
+  return guarded("pgx_gemslr_setup", [&]() -> int {
+    if (!handle || !A || !params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    *handle = nullptr;
+    if (A->rows != A->cols) return fail(PGX_ERROR_INVALID_PARAM, "A must be square");
+    pgx_handle h = nullptr;
+    PGX_TRY(pgx_gemslr_create(&h, A->rows, precision));
+    std::unique_ptr<pgx_gemslr_s> guard(h);
+    Import& im = h->im;
+    PGX_TRY(copy_csr(A, im.A, "A"));
+    const int n = im.n;
+    // parameters (PARGEMSLR_IO_* slots, SRC/utils/utils.hpp:77-297)
+    const int nlev_req = std::max(1, (int)params[20]);
+    const int perm_opt = (int)params[58];
+    const double tolB = params[40], tolC = params[44];
+    const int lfilB = std::max(1, (int)params[48]), lfilC = std::max(1, (int)params[50]);
+    const int rank1 = std::max(0, (int)params[74]), rank2 = std::max(0, (int)params[75]);
+    const double rfac1 = params[78] > 0 ? params[78] : 1.0, rfac2 = params[79] > 0 ? params[79] : 1.0;
+    const int lr_its = std::max(1, (int)params[90]);
+    im.inner_enable = params[130] != 0.0;
+    im.inner_tol = params[131];
+    im.inner_maxits = std::max(1, (int)params[132]);
+    if (im.inner_maxits > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "inner maxits above %d", KMAX);
+    // 1. levels and ordering
+    setup::Graph g = setup::symmetric_graph(n, im.A.rp.data(), im.A.cj.data());
+    setup::Ordering ord = setup::gemslr_ordering(g, nlev_req, 10, perm_opt != 0);
+    const int nlev = (int)ord.lev_ptr.size() - 1;
+    std::vector<int> iperm(n);
+    for (int i = 0; i < n; i++) iperm[ord.perm[i]] = i;
+    im.pperm = ord.perm;
+    im.qperm.clear();
+    PGX_TRY(pgx_gemslr_set_levels(h, nlev, ord.lev_ptr.data()));
+    // 2. blocks and ILUT factors per level (subdomains in parallel)
+    for (int l = 0; l < nlev; l++) {
+      HostLevel& hl = im.levels[l];
+      const int start = ord.lev_ptr[l], end = ord.lev_ptr[l + 1], nl = end - start;
+      const std::vector<int>& dom = ord.dom_ptr[l];
+      const int ncomp = (int)dom.size() - 1;
+      const bool last = l == nlev - 1;
+      std::vector<setup::Csr> B(ncomp);
+      std::vector<setup::Factor> F(ncomp);
+      std::vector<int> rc(ncomp, 0);
+  #pragma omp parallel for schedule(dynamic, 1)
+      for (int c = 0; c < ncomp; c++) {
+        const int r0 = start + dom[c], r1 = start + dom[c + 1];
+        B[c] = setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm, r0, r1, r0, r1);
+        rc[c] = setup::ilut(B[c].rows, B[c].rp.data(), B[c].cj.data(), B[c].va.data(), last ? tolC : tolB,
+                            last ? lfilC : lfilB, F[c]);
+      }
+      for (int c = 0; c < ncomp; c++)
+        if (rc[c]) return fail(PGX_ERROR_ILU_EMPTY_ROW, "ILUT met an empty row (level %d, subdomain %d)", l, c);
+      hl.ncomp = ncomp;
+      hl.dom_ptr = dom;
+      hl.L = HostCsr();
+      hl.U = HostCsr();
+      hl.B = HostCsr();
+      for (HostCsr* M : {&hl.L, &hl.U, &hl.B}) {
+        M->rows = M->cols = nl;
+        M->rp.assign(1, 0);
+      }
+      hl.dinv.clear();
+      for (int c = 0; c < ncomp; c++) {
+        append_block(hl.L, F[c].L, dom[c]);
+        append_block(hl.U, F[c].U, dom[c]);
+        append_block(hl.B, B[c], dom[c]);
+        hl.dinv.insert(hl.dinv.end(), F[c].dinv.begin(), F[c].dinv.end());
+      }
+      if (!last) {
+        hl.E = to_host(setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm, end,
+                                             n, start, end));
+        hl.F = to_host(setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm,
+                                             start, end, end, n));
+      }
+      hl.rank = 0;
+      hl.set = true;
     }
-    for (int c = 0; c < ncomp; c++)
-      if (rc[c]) return fail(PGX_ERROR_ILU_EMPTY_ROW, "ILUT met an empty row (level %d, subdomain %d)", l, c);
-    hl.ncomp = ncomp;
-    hl.dom_ptr = dom;
-    hl.L = HostCsr();
-    hl.U = HostCsr();
-    hl.B = HostCsr();
-    for (HostCsr* M : {&hl.L, &hl.U, &hl.B}) {
-      M->rows = M->cols = nl;
-      M->rp.assign(1, 0);
+    // 3. low-rank corrections, bottom-up, on the GPU in FP64
+    PGX_CUDA(cudaSetDevice(h->device));
+    if (nlev >= 2 && (rank1 > 0 || rank2 > 0)) {
+      const int inner = im.inner_enable;
+      im.inner_enable = 0;
+      auto* e = new Engine<double>();
+      std::unique_ptr<EngineBase> eng(e);
+      PGX_TRY(e->commit(im));
+      for (int l = nlev - 2; l >= 0; l--) {
+        const int k = (int)((l == 0 ? rank1 : rank2) * (l == 0 ? rfac1 : rfac2));
+        PGX_TRY(e->build_lowrank_level(im, l, k, lr_its, 0x5EEDULL + (unsigned long long)l));
+      }
+      im.inner_enable = inner;
     }
-    hl.dinv.clear();
-    for (int c = 0; c < ncomp; c++) {
-      append_block(hl.L, F[c].L, dom[c]);
-      append_block(hl.U, F[c].U, dom[c]);
-      append_block(hl.B, B[c], dom[c]);
-      hl.dinv.insert(hl.dinv.end(), F[c].dinv.begin(), F[c].dinv.end());
-    }
-    if (!last) {
-      hl.E = to_host(setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm, end,
-                                           n, start, end));
-      hl.F = to_host(setup::permuted_block(n, im.A.rp.data(), im.A.cj.data(), im.A.va.data(), ord.perm, iperm,
-                                           start, end, end, n));
-    }
-    hl.rank = 0;
-    hl.set = true;
-  }
-  // 3. low-rank corrections, bottom-up, on the GPU in FP64
-  PGX_CUDA(cudaSetDevice(h->device));
-  if (nlev >= 2 && (rank1 > 0 || rank2 > 0)) {
-    const int inner = im.inner_enable;
-    im.inner_enable = 0;
-    auto* e = new Engine<double>();
-    std::unique_ptr<EngineBase> eng(e);
-    PGX_TRY(e->commit(im));
-    for (int l = nlev - 2; l >= 0; l--) {
-      const int k = (int)((l == 0 ? rank1 : rank2) * (l == 0 ? rfac1 : rfac2));
-      PGX_TRY(e->build_lowrank_level(im, l, k, lr_its, 0x5EEDULL + (unsigned long long)l));
-    }
-    im.inner_enable = inner;
-  }
-  // 4. the solve engine in the requested precision
-  PGX_TRY(pgx_gemslr_commit(h));
-  *handle = guard.release();
-  return PGX_SUCCESS;
+    // 4. the solve engine in the requested precision
+    PGX_TRY(pgx_gemslr_commit(h));
+    *handle = guard.release();
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_gemslr_destroy(pgx_handle h) {
@@ -3191,46 +3221,50 @@ int pgx_gemslr_kernel_stats(pgx_handle h, int32_t which, int32_t level, int32_t 
 
 int pgx_build_levels(char uplo, int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_t* nlevels,
                      int32_t* level_ptr, int32_t* order) {
-  if (n < 0 || (n > 0 && (!rowptr || !nlevels || !level_ptr || !order)))
-    return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  if (uplo != 'L' && uplo != 'U') return fail(PGX_ERROR_INVALID_OPTION, "uplo must be 'L' or 'U'");
-  for (int i = 0; i < n; i++)
-    for (int k = rowptr[i]; k < rowptr[i + 1]; k++)
-      if (colidx[k] < 0 || colidx[k] >= n) return fail(PGX_ERROR_INVALID_PARAM, "column index out of range");
-  std::vector<int> lptr, ord;
-  PGX_TRY(build_levels(uplo == 'U', n, rowptr, colidx, lptr, ord));
-  *nlevels = (int)lptr.size() - 1;
-  std::copy(lptr.begin(), lptr.end(), level_ptr);
-  std::copy(ord.begin(), ord.end(), order);
-  return PGX_SUCCESS;
+  return guarded("pgx_build_levels", [&]() -> int {
+    if (n < 0 || (n > 0 && (!rowptr || !nlevels || !level_ptr || !order)))
+      return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    if (uplo != 'L' && uplo != 'U') return fail(PGX_ERROR_INVALID_OPTION, "uplo must be 'L' or 'U'");
+    for (int i = 0; i < n; i++)
+      for (int k = rowptr[i]; k < rowptr[i + 1]; k++)
+        if (colidx[k] < 0 || colidx[k] >= n) return fail(PGX_ERROR_INVALID_PARAM, "column index out of range");
+    std::vector<int> lptr, ord;
+    PGX_TRY(build_levels(uplo == 'U', n, rowptr, colidx, lptr, ord));
+    *nlevels = (int)lptr.size() - 1;
+    std::copy(lptr.begin(), lptr.end(), level_ptr);
+    std::copy(ord.begin(), ord.end(), order);
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_csr_read_mm(const char* path, pgx_csr* A) {
-  if (!path || !A) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  memset(A, 0, sizeof(*A));
-  setup::Csr c;
-  std::string err;
-  if (setup::read_matrix_market(path, c, err)) return fail(PGX_ERROR_IO, "%s: %s", path, err.c_str());
-  const size_t nnz = c.cj.size();
-  int32_t* rp = (int32_t*)malloc(sizeof(int32_t) * c.rp.size());
-  int32_t* cj = (int32_t*)malloc(sizeof(int32_t) * std::max<size_t>(nnz, 1));
-  double* va = (double*)malloc(sizeof(double) * std::max<size_t>(nnz, 1));
-  if (!rp || !cj || !va) {
-    free(rp);
-    free(cj);
-    free(va);
-    return fail(PGX_ERROR_OOM, "host allocation for %zu nonzeros", nnz);
-  }
-  std::copy(c.rp.begin(), c.rp.end(), rp);
-  std::copy(c.cj.begin(), c.cj.end(), cj);
-  std::copy(c.va.begin(), c.va.end(), va);
-  A->rows = c.rows;
-  A->cols = c.cols;
-  A->nnz = (int64_t)nnz;
-  A->rowptr = rp;
-  A->colidx = cj;
-  A->values = va;
-  return PGX_SUCCESS;
+  return guarded("pgx_csr_read_mm", [&]() -> int {
+    if (!path || !A) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    memset(A, 0, sizeof(*A));
+    setup::Csr c;
+    std::string err;
+    if (setup::read_matrix_market(path, c, err)) return fail(PGX_ERROR_IO, "%s: %s", path, err.c_str());
+    const size_t nnz = c.cj.size();
+    int32_t* rp = (int32_t*)malloc(sizeof(int32_t) * c.rp.size());
+    int32_t* cj = (int32_t*)malloc(sizeof(int32_t) * std::max<size_t>(nnz, 1));
+    double* va = (double*)malloc(sizeof(double) * std::max<size_t>(nnz, 1));
+    if (!rp || !cj || !va) {
+      free(rp);
+      free(cj);
+      free(va);
+      return fail(PGX_ERROR_OOM, "host allocation for %zu nonzeros", nnz);
+    }
+    std::copy(c.rp.begin(), c.rp.end(), rp);
+    std::copy(c.cj.begin(), c.cj.end(), cj);
+    std::copy(c.va.begin(), c.va.end(), va);
+    A->rows = c.rows;
+    A->cols = c.cols;
+    A->nnz = (int64_t)nnz;
+    A->rowptr = rp;
+    A->colidx = cj;
+    A->values = va;
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_csr_free(pgx_csr* A) {
@@ -3243,31 +3277,35 @@ int pgx_csr_free(pgx_csr* A) {
 }
 
 int pgx_gemslr_nnz(pgx_handle h, int64_t* nnz_bsolver, int64_t* nnz_lr) {
-  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
-  const Import& im = h->im;
-  if (im.nlev < 1) return fail(PGX_ERROR_FUNCTION_CALL, "levels not set");
-  int64_t nb = 0, nl = 0;
-  for (int l = 0; l < im.nlev; l++) {
-    const HostLevel& hl = im.levels[l];
-    if (!hl.set) return fail(PGX_ERROR_FUNCTION_CALL, "level %d not set", l);
-    nb += (int64_t)(im.lev_ptr[l + 1] - im.lev_ptr[l]) + hl.L.nnz() + hl.U.nnz();
-    nl += 2 * (int64_t)(im.n - im.lev_ptr[l + 1]) * hl.rank;
-  }
-  if (nnz_bsolver) *nnz_bsolver = nb;
-  if (nnz_lr) *nnz_lr = nl;
-  return PGX_SUCCESS;
+  return guarded("pgx_gemslr_nnz", [&]() -> int {
+    if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+    const Import& im = h->im;
+    if (im.nlev < 1) return fail(PGX_ERROR_FUNCTION_CALL, "levels not set");
+    int64_t nb = 0, nl = 0;
+    for (int l = 0; l < im.nlev; l++) {
+      const HostLevel& hl = im.levels[l];
+      if (!hl.set) return fail(PGX_ERROR_FUNCTION_CALL, "level %d not set", l);
+      nb += (int64_t)(im.lev_ptr[l + 1] - im.lev_ptr[l]) + hl.L.nnz() + hl.U.nnz();
+      nl += 2 * (int64_t)(im.n - im.lev_ptr[l + 1]) * hl.rank;
+    }
+    if (nnz_bsolver) *nnz_bsolver = nb;
+    if (nnz_lr) *nnz_lr = nl;
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_vector_read_mm(const char* path, int32_t idxin, int32_t capacity, double* x, int32_t* n) {
-  if (!path || !n) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  std::vector<double> v;
-  std::string err;
-  if (setup::read_matrix_market_vector(path, idxin, v, err)) return fail(PGX_ERROR_IO, "%s: %s", path, err.c_str());
-  *n = (int32_t)v.size();
-  if (!x) return PGX_SUCCESS;
-  if (capacity < *n) return fail(PGX_ERROR_INVALID_PARAM, "capacity %d below the vector's %d entries", capacity, *n);
-  std::copy(v.begin(), v.end(), x);
-  return PGX_SUCCESS;
+  return guarded("pgx_vector_read_mm", [&]() -> int {
+    if (!path || !n) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    std::vector<double> v;
+    std::string err;
+    if (setup::read_matrix_market_vector(path, idxin, v, err)) return fail(PGX_ERROR_IO, "%s: %s", path, err.c_str());
+    *n = (int32_t)v.size();
+    if (!x) return PGX_SUCCESS;
+    if (capacity < *n) return fail(PGX_ERROR_INVALID_PARAM, "capacity %d below the vector's %d entries", capacity, *n);
+    std::copy(v.begin(), v.end(), x);
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_params_default(double* params) {
@@ -3277,17 +3315,21 @@ int pgx_params_default(double* params) {
 }
 
 int pgx_params_read_file(const char* path, int32_t format, double* params) {
-  if (!path || !params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  std::string err;
-  const int rc = params::read_file(path, format, params, err);
-  if (rc) return fail(rc, "%s", err.c_str());
-  return PGX_SUCCESS;
+  return guarded("pgx_params_read_file", [&]() -> int {
+    if (!path || !params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    std::string err;
+    const int rc = params::read_file(path, format, params, err);
+    if (rc) return fail(rc, "%s", err.c_str());
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_params_read_args(int32_t argc, const char* const* argv, double* params) {
-  if (!params || argc < 0 || (argc > 0 && !argv)) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  params::read_args(argc, argv, params);
-  return PGX_SUCCESS;
+  return guarded("pgx_params_read_args", [&]() -> int {
+    if (!params || argc < 0 || (argc > 0 && !argv)) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    params::read_args(argc, argv, params);
+    return PGX_SUCCESS;
+  });
 }
 
 int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double beta, double* y) {

@@ -505,7 +505,8 @@ int read_matrix_market(const char* path, Csr& out, std::string& err) {
   if (!mm_header(f, true, sym, M, N, nz, err)) return 1;
   std::vector<long long> key;
   std::vector<double> val;
-  key.reserve((size_t)(sym ? 2 * nz : nz));
+  // the header's count sizes nothing beyond what the file's entries fill
+  key.reserve((size_t)std::min<long long>(sym ? 2 * nz : nz, 1LL << 24));
   val.reserve(key.capacity());
   for (long long k = 0; k < nz; k++) {
     long long I, J;
@@ -564,7 +565,8 @@ int read_matrix_market_vector(const char* path, int idxin, std::vector<double>& 
   bool sym = false;
   long long M = 0, N = 0, nz = 0;
   if (!mm_header(f, false, sym, M, N, nz, err)) return 1;
-  x.assign((size_t)M, 0.0);
+  // entries first, so that a file whose entries do not match its header sizes nothing
+  std::vector<std::pair<long long, double>> ent;
   for (long long k = 0; k < nz; k++) {
     long long I, J;
     double v;
@@ -577,8 +579,10 @@ int read_matrix_market_vector(const char* path, int idxin, std::vector<double>& 
       err = "entry " + std::to_string(k + 1) + " out of range";
       return 1;
     }
-    x[(size_t)r] = v;
+    ent.emplace_back(r, v);
   }
+  x.assign((size_t)M, 0.0);
+  for (const auto& e : ent) x[(size_t)e.first] = e.second;
   return 0;
 }
 

@@ -138,3 +138,18 @@ def test_vector_capacity_is_checked(tmp_path):
     x = np.zeros(3)
     rc = _abi.lib().pgx_vector_read_mm(str(path).encode(), 1, 3, _abi.ptr(x), C.byref(n))
     assert rc == _abi.ERROR_INVALID_PARAM and n.value == 6
+
+
+def test_headers_that_promise_more_than_the_file_holds(tmp_path):
+    """A header's counts size nothing by themselves: a file claiming 10^15 entries, or a vector of 2^31 - 1 rows,
+    fails at its first missing or bad entry with the I/O error, without allocating for the claim."""
+    big = tmp_path / "big.mtx"
+    big.write_text("%%MatrixMarket matrix coordinate real general\n2000000000 2000000000 1000000000000000\n")
+    with pytest.raises(_abi.PgxError) as e:
+        _abi.read_mm(str(big))
+    assert e.value.code == _abi.ERROR_IO and "entry 1" in str(e.value)
+    vec = tmp_path / "vec.mtx"
+    vec.write_text("%%MatrixMarket matrix coordinate real general\n2147483647 1 2\n1 1 1.0\nx\n")
+    with pytest.raises(_abi.PgxError) as e:
+        _abi.read_mm_vector(str(vec))
+    assert e.value.code == _abi.ERROR_IO and "entry 2" in str(e.value)
