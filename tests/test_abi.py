@@ -41,3 +41,40 @@ def test_level_schedule_rejects_non_triangular_factor():
     cj = np.array([1, 0], np.int32)  # row 0 depends on row 1: not lower triangular
     with pytest.raises(_abi.PgxError):
         _abi.build_levels("L", rp, cj)
+
+
+def test_a_c_program_links_and_calls_the_library(tmp_path):
+    """The C ABI is usable from C: a C99 program that includes include/pgx.h and include/pgx_hypre.h, links
+    libpgx.so and calls host-side entry points."""
+    import shutil
+    import subprocess
+
+    import pytest
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    src = tmp_path / "host.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "pgx.h"
+#include "pgx_hypre.h"
+int main(void) {
+  double params[PGX_PARAMS_SIZE];
+  const char *argv[] = {"-kdim", "30"};
+  int32_t lp[2] = {0, 0}, order[1] = {0}, nlev = 0;
+  const int32_t rp[2] = {0, 0};
+  void *g;
+  if (pgx_params_default(params) != PGX_SUCCESS) return 1;
+  if (pgx_params_read_args(2, argv, params) != PGX_SUCCESS || params[11] != 30.0) return 2;
+  if (pgx_build_levels('L', 1, rp, NULL, &nlev, lp, order) != PGX_SUCCESS || nlev != 1) return 3;
+  g = pgx_hypre_gemslr_create();
+  if (!g || pgx_hypre_gemslr_destroy(g) != PGX_SUCCESS) return 4;
+  printf("version %d\n", pgx_version());
+  return 0;
+}
+''')
+    exe = str(tmp_path / "host")
+    lib = os.path.dirname(_abi.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-o", exe, "-L", lib, "-lpgx", f"-Wl,-rpath,{lib}"], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.startswith("version "), (out.returncode, out.stdout, out.stderr)
