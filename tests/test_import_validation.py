@@ -1,4 +1,4 @@
-"""The import route's refusals on the host: pgx_gemslr_create / set_* / commit, no GPU needed.
+"""The import route's refusals on the host: pgx_gemslr_create / set_* / commit and the solve side, no GPU needed.
 
 Every structure a caller hands over is checked before anything reaches the
 device, and a refusal returns the reference's error codes (101 invalid
@@ -155,5 +155,31 @@ def test_whole_import_succeeds_up_to_the_device():
         nb, nl = C.c_int64(), C.c_int64()
         _abi.check(L.pgx_gemslr_nnz(h, C.byref(nb), C.byref(nl)))
         assert nb.value > 0
+    finally:
+        L.pgx_gemslr_destroy(h)
+
+
+@pytest.mark.parametrize("call", ["solve", "apply", "static", "slots", "lanes", "device_bytes", "slot_bytes", "batch",
+                                  "server", "kernel_stats"])
+def test_solve_side_calls_before_commit(call):
+    """Every solve-side entry point refuses a handle whose structures are set but not committed (106)."""
+    h = import_structures(ST)
+    n = ST.n
+    x, b, res = np.zeros(n), np.ones(n), _abi.Result()
+    v, ms, by, s = C.c_int64(), C.c_double(), C.c_double(), C.c_void_p()
+    calls = {
+        "solve": lambda: L.pgx_gemslr_solve(h, _abi.ptr(x), _abi.ptr(b), 0, None, C.byref(res)),
+        "apply": lambda: L.pgx_gemslr_precond_apply(h, _abi.ptr(x), _abi.ptr(b), 0),
+        "static": lambda: L.pgx_gemslr_solve_static(h, _abi.ptr(x), _abi.ptr(b), 0, None, C.byref(res)),
+        "slots": lambda: L.pgx_gemslr_set_slots(h, 2),
+        "lanes": lambda: L.pgx_gemslr_set_lanes(h, 2),
+        "device_bytes": lambda: L.pgx_gemslr_device_bytes(h, 50, C.byref(v)),
+        "slot_bytes": lambda: L.pgx_gemslr_slot_bytes(h, 50, C.byref(v)),
+        "batch": lambda: L.pgx_gemslr_solve_batch(h, 1, _abi.ptr(x), n, _abi.ptr(b), n, 0, None, None),
+        "server": lambda: L.pgx_server_create(h, None, C.byref(s)),
+        "kernel_stats": lambda: L.pgx_gemslr_kernel_stats(h, 0, 0, 1, C.byref(ms), C.byref(by)),
+    }
+    try:
+        _refused(calls[call](), _abi.ERROR_FUNCTION_CALL, "commit")
     finally:
         L.pgx_gemslr_destroy(h)
