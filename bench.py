@@ -266,6 +266,8 @@ def run_pgx(args):
 
     torch.cuda.set_device(local)
     p = P.workload_params(WORKLOAD)
+    if args.local_order == "multicolor":
+        p[P.ILU_PERM_OPTION_GLOBAL] = p[P.ILU_PERM_OPTION_LOCAL] = P.REORDER_MULTICOLOR
     A, n, _, _ = build_problem()
     R = args.batch
     # one step = R right-hand sides b_r = A x_r (x_r seeded), solved concurrently: slot 0 takes one,
@@ -402,6 +404,7 @@ def run_pgx(args):
         "config": {"workload": "3D 7-point Laplacian %d^3 (n=%d), 4 levels, ILUT 1e-3/200, rank 16, "
                                "inner Schur FGMRES(5) tol 1e-2, FGMRES(50) to 1e-8, x0 = 0" % (GRID[0], n),
                    "precision": args.precision, "setup": "pgx_gemslr_setup (this library), untimed",
+                   "local_order": args.local_order,
                    "solves_per_step": R, "slots": nslots, "lanes_per_slot": args.lanes,
                    "setup_s": round(setup_s, 2),
                    "iters": [min(iters), max(iters)], "true_rel_res_max": max(rel), "x_err_max": x_err,
@@ -451,6 +454,9 @@ def main():
                     help="right-hand sides each slot advances in lockstep")
     ap.add_argument("--no-fp64-plain", action="store_true", help="skip the plain FP64 comparison solves")
     ap.add_argument("--ref-iters", type=int, default=3, help="FGMRES iterations in one reference CPU sample")
+    ap.add_argument("--local-order", choices=["rcm", "multicolor"], default="rcm",
+                    help="order inside subdomains for this library's setup: reverse Cuthill-McKee (the reference's "
+                         "option) or multicolor (red-black on this grid; fewer levels in the triangular passes)")
     ap.add_argument("--ref-mode", choices=["latency", "throughput"], default="latency",
                     help="reference arm: one process on all host threads (latency), or one single-threaded "
                          "process per host thread at once (throughput)")

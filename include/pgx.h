@@ -159,11 +159,17 @@ int pgx_gemslr_destroy(pgx_handle handle);
  * kGemslrLowrankSubspaceIteration, gemslr.cpp:2592-2656).  params is the
  * reference's double[180] array; the slots read are NLEV_GLOBAL (20),
  * ILU_DROPTOL_B/C_GLOBAL (40, 44), ILU_ROWNNZ_B/C_GLOBAL (48, 50),
- * ILU_PERM_OPTION_GLOBAL (58, 0 = none, otherwise RCM), LR_RANK1/2_GLOBAL
+ * ILU_PERM_OPTION_GLOBAL (58: 0 = none, PGX_REORDER_MULTICOLOR, otherwise RCM), LR_RANK1/2_GLOBAL
  * (74, 75), LR_RANK_FACTOR1/2_GLOBAL (78, 79), LR_MAXITS1_GLOBAL (90) and
  * SCHUR_ENABLE / SCHUR_ITER_TOL / SCHUR_MAXITS (130-132).  Replaces
  * GemslrClass::Setup (gemslr.cpp:1602-1711) when no reference library is
  * linked; partitions come from this library's own bisection, not METIS. */
+/* Slot 58 value for a greedy multicolor order inside every subdomain (red-black
+ * on a grid stencil), an option beyond the reference's orderings
+ * (kIluReorderingNo..Input = 0..5, ilu.hpp:92-100).  The rows of one color are
+ * uncoupled, which cuts the dependency levels of the ILU factors and so the
+ * length of the triangular passes. */
+#define PGX_REORDER_MULTICOLOR 6
 int pgx_gemslr_setup(pgx_handle *handle, const pgx_csr *A, const double *params, int32_t precision);
 
 /* Bytes of device memory the committed handle holds (factors, matrices,

@@ -2765,7 +2765,10 @@ int pgx_gemslr_setup(pgx_handle* handle, const pgx_csr* A, const double* params,
     if (im.inner_maxits > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "inner maxits above %d", KMAX);
     // 1. levels and ordering
     setup::Graph g = setup::symmetric_graph(n, im.A.rp.data(), im.A.cj.data());
-    setup::Ordering ord = setup::gemslr_ordering(g, nlev_req, 10, perm_opt != 0);
+    const setup::LocalOrder inside = perm_opt == 0                         ? setup::LocalOrder::kNone
+                                     : perm_opt == PGX_REORDER_MULTICOLOR ? setup::LocalOrder::kMulticolor
+                                                                          : setup::LocalOrder::kRcm;
+    setup::Ordering ord = setup::gemslr_ordering(g, nlev_req, 10, inside);
     const int nlev = (int)ord.lev_ptr.size() - 1;
     std::vector<int> iperm(n);
     for (int i = 0; i < n; i++) iperm[ord.perm[i]] = i;

@@ -32,7 +32,10 @@ struct Ordering {
 };
 
 Graph symmetric_graph(int n, const int* rp, const int* cj);
+// order inside every subdomain: as found, reverse Cuthill-McKee, or greedy multicolor
+enum class LocalOrder { kNone, kRcm, kMulticolor };
 Ordering gemslr_ordering(const Graph& g, int nlev, int minsep, bool local_rcm);
+Ordering gemslr_ordering(const Graph& g, int nlev, int minsep, LocalOrder local);
 int ilut(int n, const int* rp, const int* cj, const double* va, double droptol, int lfil, Factor& f);
 int read_matrix_market(const char* path, Csr& out, std::string& err);
 int read_matrix_market_vector(const char* path, int idxin, std::vector<double>& x, std::string& err);

@@ -112,6 +112,7 @@ PARTITION_RKWAY = 1
 REORDER_NO = 0
 REORDER_RCM = 1
 REORDER_AMD = 2
+REORDER_MULTICOLOR = 6  # this library's greedy multicolor order inside subdomains (PGX_REORDER_MULTICOLOR)
 LOWRANK_STD = 0
 LOWRANK_TR = 1
 LOWRANK_SUB = 2

@@ -1,6 +1,7 @@
 // Host checks of the GeMSLR setup routines (setup.cpp): the nested-
 // dissection level structure, ILUT and the Matrix Market reader.  Built and
 // run by tests/test_setup_host.py; prints "ok" lines and exits 0 on success.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -125,6 +126,55 @@ int main(int argc, char** argv) {
     const std::vector<double> eva = {3.5, -1.0, 2.0, -1.0, 4.0};
     CHECK(mm.rp == erp && mm.cj == ecj && mm.va == eva, "mm contents");
     std::printf("ok matrix market\n");
+  }
+  // 5. multicolor order inside subdomains: the same levels and subdomains as the RCM order; each level-0
+  //    subdomain is a few uncoupled runs of rows (two on this grid); its ILUT factor has far fewer dependency levels
+  {
+    Ordering om = gemslr_ordering(g, 4, 10, LocalOrder::kMulticolor);
+    std::vector<int> seen2(n, 0), iperm2(n);
+    for (int i = 0; i < n; i++) {
+      seen2[om.perm[i]]++;
+      iperm2[om.perm[i]] = i;
+    }
+    bool perm_ok = true;
+    for (int i = 0; i < n; i++) perm_ok = perm_ok && seen2[i] == 1;
+    CHECK(perm_ok, "multicolor perm is not a permutation");
+    CHECK(om.lev_ptr == o.lev_ptr && om.dom_ptr == o.dom_ptr, "multicolor changes the level structure");
+    int most_runs = 0;
+    const std::vector<int>& dom = om.dom_ptr[0];
+    for (size_t c = 0; c + 1 < dom.size(); c++) {
+      // count maximal runs of the subdomain's order in which no two rows couple
+      std::vector<int> run_of(n, -1);
+      int runs = 1;
+      for (int r = dom[c]; r < dom[c + 1]; r++) {
+        const int old = om.perm[r];
+        bool clash = false;
+        for (int k = rp[old]; k < rp[old + 1] && !clash; k++) clash = cj[k] != old && run_of[cj[k]] == runs;
+        if (clash) runs++;
+        run_of[old] = runs;
+      }
+      most_runs = std::max(most_runs, runs);
+    }
+    CHECK(most_runs <= 3, "a subdomain splits into %d uncoupled runs", most_runs);
+    auto depth = [](const Csr& L) {
+      std::vector<int> lev(L.rows, 0);
+      int mx = 0;
+      for (int i = 0; i < L.rows; i++) {
+        for (int k = L.rp[i]; k < L.rp[i + 1]; k++) lev[i] = std::max(lev[i], lev[L.cj[k]] + 1);
+        mx = std::max(mx, lev[i] + 1);
+      }
+      return mx;
+    };
+    const int e0 = dom[1];
+    Csr Bm = permuted_block(n, rp.data(), cj.data(), va.data(), om.perm, iperm2, 0, e0, 0, e0);
+    Csr Br = permuted_block(n, rp.data(), cj.data(), va.data(), o.perm, iperm, 0, e0, 0, e0);
+    Factor fm, fr;
+    CHECK(ilut(Bm.rows, Bm.rp.data(), Bm.cj.data(), Bm.va.data(), 1e-3, 200, fm) == 0, "ilut (multicolor)");
+    CHECK(ilut(Br.rows, Br.rp.data(), Br.cj.data(), Br.va.data(), 1e-3, 200, fr) == 0, "ilut (RCM)");
+    const int dm = depth(fm.L), dr = depth(fr.L);
+    CHECK(2 * dm < dr, "multicolor factor depth %d not below half the RCM depth %d", dm, dr);
+    std::printf("ok multicolor: at most %d uncoupled runs per subdomain; factor depth %d against %d (RCM)\n", most_runs,
+                dm, dr);
   }
   return failures ? 1 : 0;
 }

@@ -3,7 +3,8 @@
 The C++ harness tests/setup_harness.cpp is compiled against setup.cpp with
 g++ and checks the nested-dissection level structure (a permutation whose
 levels have uncoupled subdomains), ILUT (exact LU without dropping, the fill
-limit with it) and the Matrix Market reader.
+limit with it), the Matrix Market reader, and the multicolor order inside
+subdomains (same levels, uncoupled runs of rows, far fewer factor levels).
 """
 import os
 import shutil
@@ -27,7 +28,7 @@ def test_setup_routines(tmp_path):
                   "3 3 5\n1 1 1.5\n1 1 2\n3 1 -1\n2 2 2\n3 3 4\n")
     out = subprocess.run([exe, str(mm)], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
-    assert out.stdout.count("ok") == 4, out.stdout
+    assert out.stdout.count("ok") == 5, out.stdout
 
 
 EDGE_SCRIPT = r'''
@@ -62,6 +63,10 @@ elif case == "more_levels_than_rows":
 elif case == "rank_above_size":
     p[P.LR_RANK1_GLOBAL] = p[P.LR_RANK2_GLOBAL] = 500
     M = lap(12, 12)
+elif case == "multicolor_order":
+    p[P.ILU_PERM_OPTION_GLOBAL] = 6
+    a = problems.laplacian(20, 20, 20)
+    M = sp.csr_matrix((a[2], a[1], a[0]), shape=(8000, 8000))
 elif case == "empty_row":
     M = sp.lil_matrix((20, 20)); M.setdiag(2.0); M[5, 5] = 0.0
 M = sp.csr_matrix(M); M.eliminate_zeros(); M.sort_indices()
@@ -77,6 +82,7 @@ print("rc", L.pgx_gemslr_setup(C.byref(h), C.byref(A), _abi.ptr(p), 0), L.pgx_la
 @pytest.mark.parametrize("case,expect", [("one", 200), ("diagonal", 200), ("two_blocks", 200), ("path3", 200),
                                          ("star", 200), ("nonsymmetric_pattern", 200),
                                          ("more_levels_than_rows", 200), ("rank_above_size", 200),
+                                         ("multicolor_order", 200),
                                          ("empty_row", 103)])
 def test_host_setup_of_awkward_matrices(tmp_path, case, expect):
     """pgx_gemslr_setup on matrices a file could hold: the host part (levels, ILUT, coupling blocks) completes and
