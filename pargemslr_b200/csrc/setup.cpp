@@ -286,7 +286,8 @@ static std::vector<int> rcm(const Graph& g, const std::vector<int>& verts, std::
 // 128^3 Laplacian (259,072 rows, ILUT 1e-3 / 200) the factors have 1,117
 // dependency levels in red-black order against 4,809 in RCM order, with 27%
 // fewer nonzeros, and GMRES on the block with either ILU converges in the
-// same number of iterations.
+// same number of iterations.  On the 2D 5-point Laplacian (ILUT 1e-2 / 20)
+// the two orders give about the same number of levels.
 static std::vector<int> multicolor(const Graph& g, std::vector<int> verts, std::vector<int>& mark, int& tag,
                                    std::vector<int>& pos) {
   std::sort(verts.begin(), verts.end());
