@@ -165,6 +165,8 @@ def fgmres(matvec: Callable, precond: Optional[Callable], x: np.ndarray, rhs: np
         return {"iters": 0, "rel_res": 0.0, "hist": [1.0]}
     tolr = tol if absolute else tol * normb
     hist = [normr / normb]
+    r0 = normr
+    sines = []  # the Givens sine of every iteration, in order
     it = 0
     i = 0
     broke = False
@@ -195,6 +197,7 @@ def fgmres(matvec: Callable, precond: Optional[Callable], x: np.ndarray, rhs: np
                 break
             c[i - 1] = hii / gam
             s[i - 1] = hii1 / gam
+            sines.append(s[i - 1])
             rs[i] = -s[i - 1] * rs[i - 1]
             rs[i - 1] = c[i - 1] * rs[i - 1]
             set_h(i - 1, i - 1, c[i - 1] * hii + s[i - 1] * hii1)
@@ -218,7 +221,7 @@ def fgmres(matvec: Callable, precond: Optional[Callable], x: np.ndarray, rhs: np
         w = col(V, i)
         matvec(1.0, x, 0.0, w)
         axpy(-1.0, w, v)
-    return {"iters": it, "rel_res": normr / normb, "hist": hist}
+    return {"iters": it, "rel_res": normr / normb, "hist": hist, "r0": r0, "normb": normb, "givens_s": sines}
 
 
 class GemslrOracle:

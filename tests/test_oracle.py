@@ -144,3 +144,22 @@ def test_preconditioner_nonzeros_match_reference(case):
         ref = oracle_runs.run(lap=lap, params=P.workload_params(meta["workload"]), solve=False, dump=False)
         assert ref["nnz_bsolver"] == nb.value
         assert ref["nnz_lr"] == sum(m[l] * ranks[l] + ranks[l] ** 2 for l in range(nlev))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_residual_history_is_a_running_product_of_givens_sines(case):
+    """The Givens residual history FlexGmresClass records (GetRelativeResidual, fgmres.hpp:430-450) is, bit for
+    bit, a running product: P_0 = ||r_0||, P_j = |s_j| * P_(j-1) over all iterations (a restart keeps the estimate),
+    history_j = P_j / ||b||.  Checked on the reference binary's own recorded history, so a solver that keeps only
+    its sines can give the history back."""
+    setup, prob, _, sol, res, meta = load(case)
+    g = O.GemslrOracle(setup)
+    p = P.workload_params(meta["workload"])
+    _, r = g.fgmres_solve(prob["b"], int(p[P.SOLVER_KDIM]), int(p[P.SOLVER_MAXITS]), float(p[P.SOLVER_TOL]))
+    prod = r["r0"]
+    hist = [prod / r["normb"]]
+    for s in r["givens_s"]:
+        prod = abs(s) * prod
+        hist.append(prod / r["normb"])
+    np.testing.assert_array_equal(np.array(hist), np.array(r["hist"]))
+    assert same(np.array(hist), sol["rel_res_hist"], case, rtol=1e-12)
