@@ -168,9 +168,10 @@ int pgx_gemslr_destroy(pgx_handle handle);
  * on a grid stencil), an option beyond the reference's orderings
  * (kIluReorderingNo..Input = 0..5, ilu.hpp:92-100).  The rows of one color are
  * uncoupled.  On the 3D 7-point Laplacian (ILUT 1e-3 / 200) the ILU factors
- * then have about a quarter of the dependency levels of the RCM order, which
- * shortens the triangular passes; on the 2D 5-point one (ILUT 1e-2 / 20) the
- * level counts are about equal. */
+ * then have about a quarter of the dependency levels of the RCM order; the
+ * level-0 triangular passes of a one-lane solve at 128^3 ran 1.35x shorter on
+ * a B200, at 26 FGMRES iterations against 24.  On the 2D 5-point Laplacian
+ * (ILUT 1e-2 / 20) the level counts are about equal. */
 #define PGX_REORDER_MULTICOLOR 6
 int pgx_gemslr_setup(pgx_handle *handle, const pgx_csr *A, const double *params, int32_t precision);
 
