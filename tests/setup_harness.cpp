@@ -176,5 +176,74 @@ int main(int argc, char** argv) {
     std::printf("ok multicolor: at most %d uncoupled runs per subdomain; factor depth %d against %d (RCM)\n", most_runs,
                 dm, dr);
   }
+
+  // 6. the red-black split of a multicolor subdomain's factors: the leading (red) rows have empty L rows and U entries
+  //    only into later colors, so L y = b is y_r = b_r, y_b = L_bb^-1 (b_b - L_br b_r), and (D + U) x = y is
+  //    x_b = (D_b + U_bb)^-1 y_b, x_r = D_r^-1 (y_r - U_rb x_b); both equal the plain solves to rounding
+  {
+    Ordering om = gemslr_ordering(g, 4, 10, LocalOrder::kMulticolor);
+    std::vector<int> iperm2(n);
+    for (int i = 0; i < n; i++) iperm2[om.perm[i]] = i;
+    const int e0 = om.dom_ptr[0][1];
+    Csr Bm = permuted_block(n, rp.data(), cj.data(), va.data(), om.perm, iperm2, 0, e0, 0, e0);
+    Factor fm;
+    CHECK(ilut(Bm.rows, Bm.rp.data(), Bm.cj.data(), Bm.va.data(), 1e-3, 200, fm) == 0, "ilut (multicolor)");
+    const int m = Bm.rows;
+    int nred = 0;
+    while (nred < m && fm.L.rp[nred + 1] == fm.L.rp[nred]) nred++;
+    int red_red_u = 0;
+    for (int r = 0; r < nred; r++)
+      for (int k = fm.U.rp[r]; k < fm.U.rp[r + 1]; k++) red_red_u += fm.U.cj[k] < nred;
+    CHECK(nred > m / 3 && red_red_u == 0, "red rows %d of %d, %d red-red U entries", nred, m, red_red_u);
+    std::vector<double> b(m);
+    for (int i = 0; i < m; i++) b[i] = std::sin(0.37 * i + 0.1);
+    // plain solves
+    std::vector<double> y(m), x(m);
+    for (int i = 0; i < m; i++) {
+      double s = b[i];
+      for (int k = fm.L.rp[i]; k < fm.L.rp[i + 1]; k++) s -= fm.L.va[k] * y[fm.L.cj[k]];
+      y[i] = s;
+    }
+    for (int i = m - 1; i >= 0; i--) {
+      double s = y[i];
+      for (int k = fm.U.rp[i]; k < fm.U.rp[i + 1]; k++) s -= fm.U.va[k] * x[fm.U.cj[k]];
+      x[i] = s * fm.dinv[i];
+    }
+    // split solves
+    std::vector<double> ys(m), xs(m);
+    for (int i = 0; i < nred; i++) ys[i] = b[i];
+    for (int i = nred; i < m; i++) {  // b_b - L_br b_r, then the black-only forward solve
+      double s = b[i];
+      for (int k = fm.L.rp[i]; k < fm.L.rp[i + 1]; k++)
+        if (fm.L.cj[k] < nred) s -= fm.L.va[k] * b[fm.L.cj[k]];
+      ys[i] = s;
+    }
+    for (int i = nred; i < m; i++) {
+      double s = ys[i];
+      for (int k = fm.L.rp[i]; k < fm.L.rp[i + 1]; k++)
+        if (fm.L.cj[k] >= nred) s -= fm.L.va[k] * ys[fm.L.cj[k]];
+      ys[i] = s;
+    }
+    for (int i = m - 1; i >= nred; i--) {  // the black-only backward solve
+      double s = ys[i];
+      for (int k = fm.U.rp[i]; k < fm.U.rp[i + 1]; k++) s -= fm.U.va[k] * xs[fm.U.cj[k]];
+      xs[i] = s * fm.dinv[i];
+    }
+    for (int i = 0; i < nred; i++) {  // x_r = D_r^-1 (y_r - U_rb x_b)
+      double s = ys[i];
+      for (int k = fm.U.rp[i]; k < fm.U.rp[i + 1]; k++) s -= fm.U.va[k] * xs[fm.U.cj[k]];
+      xs[i] = s * fm.dinv[i];
+    }
+    double dy = 0, dx = 0, ny = 0, nx = 0;
+    for (int i = 0; i < m; i++) {
+      dy = std::max(dy, std::fabs(ys[i] - y[i]));
+      dx = std::max(dx, std::fabs(xs[i] - x[i]));
+      ny = std::max(ny, std::fabs(y[i]));
+      nx = std::max(nx, std::fabs(x[i]));
+    }
+    CHECK(dy <= 1e-13 * ny && dx <= 1e-13 * nx, "split solves differ: %.2e / %.2e", dy / ny, dx / nx);
+    std::printf("ok red-black split: %d red rows of %d; split solves within %.1e / %.1e of the plain ones\n", nred, m,
+                dy / ny, dx / nx);
+  }
   return failures ? 1 : 0;
 }

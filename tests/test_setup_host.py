@@ -4,7 +4,8 @@ The C++ harness tests/setup_harness.cpp is compiled against setup.cpp with
 g++ and checks the nested-dissection level structure (a permutation whose
 levels have uncoupled subdomains), ILUT (exact LU without dropping, the fill
 limit with it), the Matrix Market reader, and the multicolor order inside
-subdomains (same levels, uncoupled runs of rows, far fewer factor levels).
+subdomains (same levels, uncoupled runs of rows, far fewer factor levels,
+and the red-black split of its factors, which solves as the plain factors do).
 """
 import os
 import shutil
@@ -28,7 +29,7 @@ def test_setup_routines(tmp_path):
                   "3 3 5\n1 1 1.5\n1 1 2\n3 1 -1\n2 2 2\n3 3 4\n")
     out = subprocess.run([exe, str(mm)], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
-    assert out.stdout.count("ok") == 5, out.stdout
+    assert out.stdout.count("ok") == 6, out.stdout
 
 
 EDGE_SCRIPT = r'''
