@@ -128,7 +128,9 @@ int pgx_init(int device);
 int pgx_finalize(void);
 /* Message describing the calling thread's most recent error. */
 const char *pgx_last_error(void);
-/* Library version as major*10000 + minor*100 + patch. */
+/* Library version as major*10000 + minor*100 + patch (0.2.0 = 200 adds the
+ * parameter and Matrix Market vector readers, pgx_gemslr_nnz and the hypre
+ * interface of pgx_hypre.h). */
 int pgx_version(void);
 
 /* ---- GeMSLR solve handle (replaces GemslrClass + FlexGmresClass solve) ---

@@ -2575,7 +2575,7 @@ int pgx_finalize(void) { return PGX_SUCCESS; }
 
 const char* pgx_last_error(void) { return g_last_error.c_str(); }
 
-int pgx_version(void) { return 100; }
+int pgx_version(void) { return 200; }  // 0.2.0: input readers, C++ front end, hypre interface, nnz
 
 int pgx_gemslr_create(pgx_handle* handle, int32_t n, int32_t precision) {
   return guarded("pgx_gemslr_create", [&]() -> int {

@@ -77,4 +77,4 @@ int main(void) {
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), str(src),
                     "-o", exe, "-L", lib, "-lpgx", f"-Wl,-rpath,{lib}"], check=True)
     out = subprocess.run([exe], capture_output=True, text=True)
-    assert out.returncode == 0 and out.stdout.startswith("version "), (out.returncode, out.stdout, out.stderr)
+    assert out.returncode == 0 and out.stdout.strip() == "version 200", (out.returncode, out.stdout, out.stderr)
