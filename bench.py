@@ -5,15 +5,25 @@ Workload (the headline configuration): 3D 7-point Laplacian on a 128^3 grid
 (2,097,152 unknowns, 14.6M nonzeros, the reference's stencil), b = A x_true
 with x_true = 2u - 1 seeded; 4 GeMSLR levels, ILUT drop 1e-3 / 200 per row,
 rank 16 per level, inner Schur FGMRES on level 0 (tol 1e-2, 5 steps),
-FGMRES(50) to relative residual 1e-8.  The preconditioner is built once by
-this library's host setup (pgx_gemslr_setup, untimed).  A "step" is one
-batch of --batch right-hand sides (b_r = A x_r, x_r seeded), each solved
-completely from x0 = 0, concurrently over the one resident preconditioner
-(pgx_gemslr_solve_batch): slot 0 takes one, every further slot --lanes of
-them in lockstep (their triangular passes merged); value = solves/s.
+FGMRES(50) to relative residual 1e-8 from x0 = 0.
 
-  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp64]
-  python bench.py --impl reference ...   (the reference CPU solver, oracle/_ref)
+Setup (untimed).  By default the preconditioner is the reference's own:
+GemslrClass::Setup of the reference, compiled from its sources into
+oracle/_ref, runs once on all host threads, writes its post-setup structures,
+and they are imported through the C ABI (pgx_gemslr_set_*) exactly as a
+reference-side driver would hand them over.  The same run solves the first
+right-hand side on the CPU, which gives the reference's solution x_ref, its
+iteration count and the CPU baseline's time.  ``--setup own`` uses this
+library's host setup (pgx_gemslr_setup) instead.
+
+A "step" is one batch of --batch right-hand sides (b_r = A x_r, x_r seeded),
+each solved completely from x0 = 0, concurrently over the one resident
+preconditioner (pgx_gemslr_solve_batch): slot 0 takes one, every further slot
+--lanes of them in lockstep (their triangular passes merged); value =
+solves/s.
+
+  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp64] [--setup reference|own]
+  python bench.py --impl reference ...   (the reference CPU solver, oracle/_ref, full solves)
   python bench.py --impl reference --ref-mode throughput   (one single-threaded reference per host thread)
 
 Under torchrun (N > 1) every rank solves its own replica on its own GPU; the
@@ -29,7 +39,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -44,14 +53,21 @@ from pargemslr_b200._abi import LOCATION_DEVICE, LOCATION_HOST  # noqa: E402
 GRID = (128, 128, 128)
 WORKLOAD = "lap3d_128"
 SEED = 7
-# FGMRES iterations of the reference solver on this workload (measured with
-# oracle/_ref on the same parameters: 39 iterations, 72.9 s single-thread);
-# the CPU sample times the first iterations and scales by this count
-REF_ITERS = 39
 
 
 def metric_name() -> str:
     return "solves/s (GeMSLR-FGMRES(50), rel-res 1e-8, 3D Laplacian %d^3)" % GRID[0]
+
+
+def workload_config(setup: str) -> dict:
+    """The `config` both arms print: the same workload, so their lines compare like for like."""
+    n = GRID[0] * GRID[1] * GRID[2]
+    who = ("the reference's GemslrClass::Setup (oracle/_ref) on all host threads, untimed" if setup == "reference"
+           else "this library's host setup (pgx_gemslr_setup), untimed")
+    return {"workload": "3D 7-point Laplacian %d^3 (n=%d), 4 levels, ILUT 1e-3/200, rank 16, inner Schur FGMRES(5) "
+                        "tol 1e-2, FGMRES(50) to rel-res 1e-8 from x0 = 0, b = A x_true (x_true = 2u-1, seeded)"
+                        % (GRID[0], n),
+            "setup": who}
 
 
 class ClockSampler:
@@ -145,11 +161,17 @@ def build_problem():
     return A, n, b, xt
 
 
-def _ref_command(out: str, xtrue_path: str, n_threads: int, iters: int, steps: int):
-    driver = os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver")
+# ------------------------------------------------------------ reference leg
+def _ref_driver() -> str:
+    return os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver")
+
+
+def _ref_command(out: str, xtrue_path: str, n_threads: int, solves: int, dump: bool):
     p = P.workload_params(WORKLOAD)
-    cmd = [driver, "--out", out, "--lap", *[str(g) for g in GRID], "0", "0", "0", "0", "--xtrue", xtrue_path,
-           "--threads", str(n_threads), "--solve", "--max-iters-timed", str(iters), "--repeat", str(steps)]
+    cmd = [_ref_driver(), "--out", out, "--lap", *[str(g) for g in GRID], "0", "0", "0", "0", "--xtrue", xtrue_path,
+           "--threads", str(n_threads), "--solve", "--repeat", str(solves)]
+    if dump:
+        cmd.append("--dump")
     for i, v in enumerate(p):
         cmd += ["--param", f"{i}={float(v)!r}"]
     env = dict(os.environ, OMP_NUM_THREADS=str(n_threads), OPENBLAS_NUM_THREADS="1")
@@ -163,32 +185,36 @@ def _ref_result(out: str, wall: float):
             k, v = line.strip().split("=", 1)
             res[k] = v
     times = [float(t) for t in res["solve_times"].split(",")]
-    return {"times": times, "iters": int(res["iters"]), "setup_s": float(res["setup_s"]), "wall_s": wall}
+    return {"dir": out, "times": times, "iters": int(res["iters"]), "setup_s": float(res["setup_s"]),
+            "true_rel_res": float(res["true_rel_res"]), "wall_s": wall}
 
 
 def _ref_inputs():
-    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver")):
+    if not os.path.exists(_ref_driver()):
         return None
     d = tempfile.mkdtemp(prefix="pgx_ref_")
-    A, n, b, xt = build_problem()
+    n = GRID[0] * GRID[1] * GRID[2]
     path = os.path.join(d, "xtrue.bin")
-    pgxd.write(path, {"x_true": xt})
+    pgxd.write(path, {"x_true": problems.x_true(n, SEED)})
     return d, path
 
 
-def cpu_sample(n_threads: int, iters: int, steps: int = 1):
-    """Time the reference CPU solver (oracle/_ref) on the same workload: one process on n_threads threads."""
+def reference_run(n_threads: int, solves: int, dump: bool):
+    """The reference CPU solver (oracle/_ref) on the workload: its setup on n_threads threads, then `solves` full
+    FGMRES solves of b = A x_true (x_true seeded as the first right-hand side of the GPU arm), each from x0 = 0.
+    With dump, its post-setup structures are written for import (setup.bin), with b (problem.bin) and the solution
+    (solution.bin).  Returns (result, None) or (None, why)."""
     inp = _ref_inputs()
     if inp is None:
         return None, "oracle/_ref/pgx_ref_driver not built"
     out, xtrue_path = inp
-    cmd, env = _ref_command(out, xtrue_path, n_threads, iters, steps)
+    cmd, env = _ref_command(out, xtrue_path, n_threads, solves, dump)
     t0 = time.time()
     subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
     return _ref_result(out, time.time() - t0), None
 
 
-def cpu_sample_procs(procs: int, iters: int, steps: int = 1):
+def reference_runs_parallel(procs: int, solves: int):
     """Throughput form of the reference baseline: `procs` single-threaded reference processes at once, each
     setting up and solving the same workload on its own, as independent solves on the host's cores would run.
     Returns one result per process."""
@@ -201,7 +227,7 @@ def cpu_sample_procs(procs: int, iters: int, steps: int = 1):
     for k in range(procs):
         out = os.path.join(d, f"p{k}")
         os.makedirs(out)
-        cmd, env = _ref_command(out, xtrue_path, 1, iters, steps)
+        cmd, env = _ref_command(out, xtrue_path, 1, solves, False)
         runs.append((out, subprocess.Popen(cmd, env=env, stdout=subprocess.DEVNULL)))
     codes = [proc.wait() for _, proc in runs]
     wall = time.time() - t0
@@ -215,40 +241,72 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    steps = args.warmup + args.steps
+    solves = args.warmup + args.steps
     if args.ref_mode == "throughput":
-        rs, why = cpu_sample_procs(threads, args.ref_iters, steps)
+        rs, why = reference_runs_parallel(threads, solves)
         if rs is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return
-        # each process's solves/s from its timed steps, summed over the processes running at once
-        value = sum(1.0 / (statistics.mean(t / max(r["iters"], 1) for t in r["times"][args.warmup:]) * REF_ITERS)
-                    for r in rs)
+        # each process's solves/s over its timed solves, summed over the processes running at once
+        value = sum(1.0 / statistics.mean(r["times"][args.warmup:]) for r in rs)
         t_solve = 1.0 / value
         r = rs[0]
+        timed_s = max(sum(x["times"][args.warmup:]) for x in rs)
         sample = (f"reference FGMRES+GemslrClass (oracle/_ref), {threads} single-threaded processes at once, each "
-                  f"timing the first {r['iters']} iterations of its own {GRID[0]}^3 solve per step, scaled to the full "
-                  f"{REF_ITERS}-iteration solve; solves/s summed over the processes")
+                  f"its own setup and {solves} full {GRID[0]}^3 solves ({r['iters']} iterations each) of which the "
+                  f"last {args.steps} are timed; solves/s summed over the processes")
     else:
-        r, why = cpu_sample(threads, args.ref_iters, steps)
+        r, why = reference_run(threads, solves, dump=False)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return
-        per_iter = [t / max(r["iters"], 1) for t in r["times"][args.warmup:]]
-        t_solve = statistics.mean(per_iter) * REF_ITERS
+        timed = r["times"][args.warmup:]
+        t_solve = statistics.mean(timed)
         value = 1.0 / t_solve
-        sample = (f"reference FGMRES+GemslrClass (oracle/_ref), first {r['iters']} iterations of the {GRID[0]}^3 "
-                  f"solve per step on {threads} threads, scaled to the full {REF_ITERS}-iteration solve")
+        timed_s = sum(timed)
+        sample = (f"reference FGMRES+GemslrClass (oracle/_ref) on {threads} threads: {solves} full {GRID[0]}^3 "
+                  f"solves ({r['iters']} iterations, true rel-res {r['true_rel_res']:.2e}) after one setup, the "
+                  f"last {args.steps} timed")
     line = {
         "impl": "reference", "metric": metric_name(), "value": value, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_solve * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"3D 7-point Laplacian {GRID[0]}^3, 4 levels, ILUT 1e-3/200, rank 16, FGMRES(50), "
-                               "1e-8", "setup_s": r["setup_s"], "ref_mode": args.ref_mode},
+        "config": workload_config("reference"),
+        "detail": {"iters": r["iters"], "true_rel_res": r["true_rel_res"], "setup_s": r["setup_s"],
+                   "ref_mode": args.ref_mode, "timed_s": timed_s, "wall_s": r["wall_s"]},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ GPU arm
+def _batch(h, p, R, n, B_dev, X_dev, ev_a, ev_b):
+    import torch
+    X_dev.zero_()
+    torch.cuda.synchronize()
+    ev_a.record()
+    res = h.solve_batch_ptr(R, X_dev.data_ptr(), n, B_dev.data_ptr(), n, LOCATION_DEVICE, p)
+    ev_b.record()
+    ev_b.synchronize()
+    return res, ev_a.elapsed_time(ev_b)
+
+
+def _fit_slots(h, R, lanes):
+    """Slots for R right-hand sides in flight; each holds its own Krylov basis, so on a GPU with less free memory
+    the batch shrinks until the slots fit.  Returns (R, nslots)."""
+    from pargemslr_b200._abi import ERROR_OOM, PgxError
+    nslots = 1 + -(-(R - 1) // lanes)
+    while True:
+        try:
+            h.set_slots(nslots)
+            return R, nslots
+        except PgxError as exc:
+            if exc.code != ERROR_OOM or R <= lanes:
+                raise
+            h.set_slots(1)
+            R = max(lanes, R - 4 * lanes)
+            nslots = 1 + -(-(R - 1) // lanes)
 
 
 def run_pgx(args):
@@ -263,53 +321,48 @@ def run_pgx(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     from pargemslr_b200.handle import GemslrHandle
+    from pargemslr_b200.structures import from_dump
 
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     p = P.workload_params(WORKLOAD)
     if args.local_order == "multicolor":
+        if args.setup != "own":
+            raise SystemExit("--local-order multicolor needs --setup own (the reference's setup orders by RCM)")
         p[P.ILU_PERM_OPTION_GLOBAL] = p[P.ILU_PERM_OPTION_LOCAL] = P.REORDER_MULTICOLOR
     A, n, _, _ = build_problem()
+    threads = os.cpu_count() or 1
+
+    # --- setup (untimed) and the reference's own solve of the first right-hand side
+    t0 = time.time()
+    ref, ref_why, st = None, None, None
+    if args.setup == "reference":
+        ref, ref_why = reference_run(threads, 1, dump=True)
+        if ref is None:
+            raise SystemExit("--setup reference: " + ref_why)
+        st = from_dump(os.path.join(ref["dir"], "setup.bin"))
+        h = GemslrHandle(st, precision=args.precision, device=local)
+    else:
+        h = GemslrHandle.from_matrix(A, p, precision=args.precision, device=local)
+    setup_s = time.time() - t0
+
     R = args.batch
-    # one step = R right-hand sides b_r = A x_r (x_r seeded), solved concurrently: slot 0 takes one,
-    # every further slot `lanes` at once
-    nslots = 1 + -(-(R - 1) // args.lanes)
     xts = np.stack([problems.x_true(n, SEED + r) for r in range(R)])
     B = np.stack([problems.spmv(A, xts[r]) for r in range(R)])
-    t0 = time.time()
-    h = GemslrHandle.from_matrix(A, p, precision=args.precision, device=local)
-    setup_s = time.time() - t0
+    if ref is not None:
+        # right-hand side 0 is the reference's own b (its MatVec of the same x_true)
+        B[0] = pgxd.read(os.path.join(ref["dir"], "problem.bin"))["b"]
+        x_ref = pgxd.read(os.path.join(ref["dir"], "solution.bin"))["x"]
     h.set_lanes(args.lanes)
-    from pargemslr_b200._abi import ERROR_OOM, PgxError
-    while True:
-        # each right-hand side in flight holds its own Krylov basis: on a GPU
-        # with less free memory, shrink the batch until the slots fit
-        try:
-            h.set_slots(nslots)
-            break
-        except PgxError as exc:
-            if exc.code != ERROR_OOM or R <= args.lanes:
-                raise
-            h.set_slots(1)
-            R = max(args.lanes, R - 4 * args.lanes)
-            nslots = 1 + -(-(R - 1) // args.lanes)
-            xts, B = xts[:R], B[:R]
-    dev = torch.device("cuda", local)
+    R, nslots = _fit_slots(h, R, args.lanes)
+    xts, B = xts[:R], B[:R]
     B_dev = torch.from_numpy(B).to(dev)
     X_dev = torch.zeros_like(B_dev)
     ev_a = torch.cuda.Event(enable_timing=True)
     ev_b = torch.cuda.Event(enable_timing=True)
 
-    def device_step():
-        X_dev.zero_()
-        torch.cuda.synchronize()
-        ev_a.record()
-        res = h.solve_batch_ptr(R, X_dev.data_ptr(), n, B_dev.data_ptr(), n, LOCATION_DEVICE, p)
-        ev_b.record()
-        ev_b.synchronize()
-        return res, ev_a.elapsed_time(ev_b)
-
     for _ in range(args.warmup):
-        device_step()
+        _batch(h, p, R, n, B_dev, X_dev, ev_a, ev_b)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -317,14 +370,16 @@ def run_pgx(args):
     clocks.start()
     wall0 = time.perf_counter()
     ms, iters, rel, launches, lat = [], [], [], [], []
+    first = None
     torch.cuda.nvtx.range_push("timed")  # lets a profiler capture the timed region alone
     for _ in range(args.steps):
-        res, t_ms = device_step()
+        res, t_ms = _batch(h, p, R, n, B_dev, X_dev, ev_a, ev_b)
         ms.append(t_ms)
         lat.extend(r["solve_ms"] for r in res)
         iters.extend(r["iters"] for r in res)
         rel.extend(r["true_rel_res"] for r in res)
         launches.append(sum(r["launches"] for r in res))
+        first = res[0]
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
@@ -334,14 +389,26 @@ def run_pgx(args):
         dist.barrier()
     value = world * args.steps * R / (total_ms / 1e3)
     X = X_dev.cpu().numpy()
-    x_err = max(float(np.linalg.norm(X[r] - xts[r]) / np.linalg.norm(xts[r])) for r in range(R))
+    x_err = max(float(np.linalg.norm(X[r] - xts[r]) / np.linalg.norm(xts[r])) for r in range(1, R)) if R > 1 else None
+    parity = None
+    if ref is not None:
+        dref = float(np.linalg.norm(X[0] - x_ref) / np.linalg.norm(x_ref))
+        parity = {"what": "right-hand side 0 (the reference's b) against the reference's own FP64 CPU solve on "
+                          "the same imported setup",
+                  "iters": first["iters"], "iters_ref": ref["iters"], "true_rel_res": first["true_rel_res"],
+                  "true_rel_res_ref": ref["true_rel_res"], "x_vs_x_ref": dref,
+                  "iters_bar": ("+-1" if args.precision == "fp64" else "<= +15%"),
+                  "ok": bool(dref <= 1e-6 and first["true_rel_res"] <= 1e-8 and
+                             (abs(first["iters"] - ref["iters"]) <= 1 if args.precision == "fp64"
+                              else first["iters"] <= int(np.floor(1.15 * ref["iters"])) + 1))}
 
     # end to end through the host-buffer C ABI call: pinned host B and X, the
     # copies in and out are inside every timed call
     B_host = torch.from_numpy(B).pin_memory()
     X_host = torch.zeros((R, n), dtype=torch.float64).pin_memory()
     e2e_ms = []
-    for _ in range(args.steps):
+    e2e_steps = min(args.steps, 5)
+    for _ in range(e2e_steps):
         X_host.zero_()
         torch.cuda.synchronize()
         ev_a.record()
@@ -363,11 +430,15 @@ def run_pgx(args):
     torch.cuda.nvtx.range_pop()
     h.set_slots(1)
     h.set_lanes(1)
+    h.close()
+    del B_host, X_host
 
-    # the plain FP64 path for comparison: FP64 preconditioner, one solve at a time
-    plain = None
-    if world == 1 and not args.no_fp64_plain:
-        h64 = GemslrHandle.from_matrix(A, p, precision="fp64", device=local)
+    # the FP64 preconditioner on the same setup: batched at the same width (as
+    # many right-hand sides as fit), and one solve at a time
+    fp64_batched, plain = None, None
+    if world == 1 and not args.no_fp64 and args.precision == "mixed":
+        h64 = (GemslrHandle(st, precision="fp64", device=local) if st is not None
+               else GemslrHandle.from_matrix(A, p, precision="fp64", device=local))
         pm, pit = [], []
         for k in range(3):
             x1 = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -379,9 +450,22 @@ def run_pgx(args):
             if k > 0:  # the first solve is warm-up
                 pm.append(ev_a.elapsed_time(ev_b))
                 pit.append(r1["iters"])
-        h64.close()
         plain = {"solves_per_s": len(pm) / (sum(pm) / 1e3), "ms_per_solve": sum(pm) / len(pm), "iters": pit,
                  "what": "FP64 preconditioner, one solve at a time (pgx_gemslr_solve), same setup and RHS"}
+        h64.set_lanes(args.lanes)
+        R64, ns64 = _fit_slots(h64, R, args.lanes)
+        B64, X64 = B_dev[:R64], X_dev[:R64]
+        _batch(h64, p, R64, n, B64, X64, ev_a, ev_b)  # warm-up
+        bm, bit = [], []
+        for _ in range(2):
+            res64, t_ms = _batch(h64, p, R64, n, B64, X64, ev_a, ev_b)
+            bm.append(t_ms)
+            bit.extend(r["iters"] for r in res64)
+        fp64_batched = {"solves_per_s": 2 * R64 / (sum(bm) / 1e3), "solves_per_step": R64, "slots": ns64,
+                        "lanes_per_slot": args.lanes, "iters": [min(bit), max(bit)],
+                        "what": "FP64 preconditioner, batched like the headline (pgx_gemslr_solve_batch); the "
+                                "width is the headline's unless its Krylov bases (8+8 bytes per entry) do not fit"}
+        h64.close()
 
     peak, peak_kind = measured_peak_hbm()
     single = {"bytes_per_launch": (lo_bytes + up_bytes) / 2.0, "ms_per_launch": (lo_ms + up_ms) / 2.0}
@@ -396,24 +480,25 @@ def run_pgx(args):
         tri_bytes, tri_ms = single["bytes_per_launch"], single["ms_per_launch"]
     achieved = tri_bytes / (tri_ms * 1e-3) / 1e9
     traffic = ncu_traffic(args.lanes)
+    detail = {"precision": args.precision, "setup_kind": args.setup, "local_order": args.local_order,
+              "solves_per_step": R, "slots": nslots, "lanes_per_slot": args.lanes, "setup_s": round(setup_s, 2),
+              "iters": [min(iters), max(iters)], "true_rel_res_max": max(rel),
+              "x_err_max_vs_x_true": x_err, "parity_vs_reference": parity,
+              "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                             "what": "device time of each solve inside the batch (its slot's events)"},
+              "fp64_plain": plain, "fp64_batched": fp64_batched,
+              "mixed_over_fp64_batched": (value / fp64_batched["solves_per_s"]) if fp64_batched else None,
+              "mixed_over_fp64_plain": (value / plain["solves_per_s"]) if plain else None,
+              "l2": "inputs larger than L2 (level-0 factors alone are about 1 GB)",
+              "host_wall_s": wall, "e2e_steps": e2e_steps}
     line = {
         "metric": metric_name(), "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 preconditioner / f64 FGMRES" if args.precision == "mixed" else "f64",
         "data": "synthetic",
-        "config": {"workload": "3D 7-point Laplacian %d^3 (n=%d), 4 levels, ILUT 1e-3/200, rank 16, "
-                               "inner Schur FGMRES(5) tol 1e-2, FGMRES(50) to 1e-8, x0 = 0" % (GRID[0], n),
-                   "precision": args.precision, "setup": "pgx_gemslr_setup (this library), untimed",
-                   "local_order": args.local_order,
-                   "solves_per_step": R, "slots": nslots, "lanes_per_slot": args.lanes,
-                   "setup_s": round(setup_s, 2),
-                   "iters": [min(iters), max(iters)], "true_rel_res_max": max(rel), "x_err_max": x_err,
-                   "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                                  "what": "device time of each solve inside the batch (its slot's events)"},
-                   "fp64_plain": plain,
-                   "l2": "inputs larger than L2 (preconditioner %.2f GB)" % (h.device_bytes(50) / 1e9),
-                   "host_wall_s": wall},
-        "e2e": {"value": world * args.steps * R / e2e_total, "unit": "solves/s", "h2d_bytes_per_step": 16 * n * R,
+        "config": workload_config(args.setup),
+        "detail": detail,
+        "e2e": {"value": world * e2e_steps * R / e2e_total, "unit": "solves/s", "h2d_bytes_per_step": 16 * n * R,
                 "d2h_bytes_per_step": 8 * n * R},
         "gpu_launches": int(sum(launches)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -425,19 +510,19 @@ def run_pgx(args):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and GRID == (128, 128, 128):
-        cpu, why = cpu_sample(os.cpu_count() or 1, args.ref_iters, 1)
+        cpu = ref
+        if cpu is None:
+            cpu, _ = reference_run(threads, 1, dump=False)
         if cpu is None:
             line["cpu_baseline"] = None
         else:
-            t_solve = cpu["times"][-1] / max(cpu["iters"], 1) * REF_ITERS
             line["cpu_baseline"] = {
-                "value": 1.0 / t_solve, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "reference",
-                "sample": f"reference CPU solver (oracle/_ref), first {cpu['iters']} FGMRES iterations of the same "
-                          f"128^3 solve, scaled to its full {REF_ITERS}-iteration solve; reference setup "
-                          f"{cpu['setup_s']:.1f} s untimed"}
+                "value": 1.0 / cpu["times"][-1], "unit": "solves/s", "cores": threads, "kind": "reference",
+                "sample": f"reference CPU solver (oracle/_ref) on {threads} threads: one full solve of the first "
+                          f"right-hand side ({cpu['iters']} FGMRES iterations, true rel-res "
+                          f"{cpu['true_rel_res']:.2e}); its setup ({cpu['setup_s']:.1f} s) untimed"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    h.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -449,14 +534,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["pgx", "reference"], default="pgx")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--setup", choices=["reference", "own"], default="reference",
+                    help="whose setup builds the preconditioner: the reference's GemslrClass::Setup, imported through "
+                         "the C ABI (default), or this library's host setup")
     ap.add_argument("--batch", type=int, default=96, help="right-hand sides solved concurrently per step")
     ap.add_argument("--lanes", type=int, default=4, choices=[1, 2, 4],
                     help="right-hand sides each slot advances in lockstep")
-    ap.add_argument("--no-fp64-plain", action="store_true", help="skip the plain FP64 comparison solves")
-    ap.add_argument("--ref-iters", type=int, default=3, help="FGMRES iterations in one reference CPU sample")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-preconditioner comparison solves")
     ap.add_argument("--local-order", choices=["rcm", "multicolor"], default="rcm",
-                    help="order inside subdomains for this library's setup: reverse Cuthill-McKee (the reference's "
-                         "option) or multicolor (red-black on this grid; fewer levels in the triangular passes)")
+                    help="order inside subdomains for this library's setup (--setup own): reverse Cuthill-McKee "
+                         "(the reference's option) or multicolor (red-black on this grid)")
     ap.add_argument("--ref-mode", choices=["latency", "throughput"], default="latency",
                     help="reference arm: one process on all host threads (latency), or one single-threaded "
                          "process per host thread at once (throughput)")

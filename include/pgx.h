@@ -225,7 +225,11 @@ int pgx_gemslr_solve(pgx_handle handle, double *x, const double *b, int32_t loca
  * Every GPU on which the library is loaded holds the pool until the process
  * exits.  The first call on a device looks up the pool's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture
- * begins.  All calls on one device share the pool and each clears the part
+ * begins.  The address is kept for the life of the device's primary
+ * context: after cudaDeviceReset (or any teardown of that context) the
+ * library must not be used on that device again in the same process, as the
+ * kept address no longer belongs to the new context.  All calls on one
+ * device share the pool and each clears the part
  * it uses before the solve, but calls that overlap on the GPU (from several
  * host threads, on one or several handles of the same device) race on it:
  * the caller must serialise them.  result->launches is 0: the kernels are

@@ -1773,8 +1773,16 @@ struct Engine : EngineBase {
   }
 
   // after enqueue_finish has landed: zero right-hand side, x back to the
-  // host, the outcome
+  // host, the outcome.  *res is always written: on a CUDA error before the
+  // outcome is known it holds zeros and that error as its status.
   int collect_result(pgx_result* res) {
+    if (res) memset(res, 0, sizeof(*res));
+    const int out = collect_result_body(res);
+    if (res && res->status == PGX_SUCCESS) res->status = out;
+    return out;
+  }
+
+  int collect_result_body(pgx_result* res) {
     const FgmresDev hs = *hs_pin;
     const double r2 = *r2_pin;
     const int rc = check_err();
@@ -1919,26 +1927,12 @@ struct Engine : EngineBase {
     PGX_CUDA(cudaMemcpyAsync(hs_pin, st, head, cudaMemcpyDeviceToHost, stream));
     PGX_CUDA(cudaMemcpyAsync(r2_pin, scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
     PGX_CUDA(cudaStreamSynchronize(stream));
-    const FgmresDev hs = *hs_pin;
-    const double r2 = *r2_pin;
-    const int rc = check_err();
-    float ms = 0.f;
-    PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-    if (hs.normb < DBL_EPSILON) PGX_CUDA(cudaMemsetAsync(xd, 0, sizeof(double) * n, stream));
-    if (location == PGX_LOCATION_HOST)
-      PGX_CUDA(cudaMemcpyAsync(x, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
-    PGX_CUDA(cudaStreamSynchronize(stream));
-    if (res) {
-      res->status = rc;
-      res->iters = hs.iter;
-      res->rel_res = hs.normb > 0 ? hs.normr / hs.normb : 0.0;
-      res->true_rel_res = hs.normb > 0 ? sqrt(r2) / hs.normb : 0.0;
-      res->solve_ms = ms;
-      res->launches = 0;  // kernels enqueued one by one are not counted here
-    }
-    if (rc == PGX_SUCCESS && !(std::isfinite(hs.normr)))
-      return fail(PGX_ERROR_NOT_FINITE, "FGMRES residual is not finite");
-    return rc;
+    // the outcome exactly as pgx_gemslr_solve reports it
+    s_xd = xd;
+    s_location = location;
+    s_xuser = x;
+    s_launches = 0;  // kernels enqueued one by one are not counted here
+    return collect_result(res);
   }
 };
 
@@ -2392,12 +2386,15 @@ struct BatchEngine : EngineBase {
     *finished = true;
     // each lane's outcome (a NaN in one right-hand side, say) is in its own
     // result; the return value is kept for failures of the slot as a whole
+    // (a CUDA error: the lanes share one stream)
+    int slot_rc = PGX_SUCCESS;
     for (int r = 0; r < R; r++) {
       pgx_result tmp;
-      lane[r]->collect_result(r < count && res ? &tmp : nullptr);
+      const int rc = lane[r]->collect_result(&tmp);
       if (r < count && res) res[r] = tmp;
+      if ((rc == PGX_ERROR_CUDA || rc == PGX_ERROR_OOM) && slot_rc == PGX_SUCCESS) slot_rc = rc;
     }
-    return PGX_SUCCESS;
+    return slot_rc;
   }
 
   int solve(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,

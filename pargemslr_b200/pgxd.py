@@ -3,8 +3,7 @@
 Layout: the 4-byte magic ``PGXD`` followed by records
 ``[u32 name_len][name][u8 dtype][u64 count][count elements]`` with dtype
 0 = int32, 1 = float64, 2 = int64, 3 = float32, little-endian.  The same
-format is written by the reference-side exporter and by
-this package, so structures can be handed over as files as well as through
+format is written by the reference-side exporter and by this package, so structures can be handed over as files as well as through
 the C ABI.
 """
 from __future__ import annotations

@@ -20,9 +20,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+from oracle.paths import REFERENCE_TESTS as REF_TESTS  # noqa: E402
 from tests import params_fuzz as F  # noqa: E402
 
-REF_TESTS = "/root/reference/ParGeMSLR/TESTS"
 REF_FILES = [("sequential", "sequential/inputs"), ("sequential", "sequential/inputs_ilut"),
              ("parallel", "parallel/inputs"), ("parallel", "parallel/inputs_bj_ilu"), ("hypre", "hypre/inputs")]
 SEEDS = range(50)

@@ -23,6 +23,8 @@ CASES = {
     "lap2d_64": ((64, 64, 1, 0.0, 0.0, 0.0, 0.0), "lap2d_256"),
     "lap2d_256": ((256, 256, 1, 0.0, 0.0, 0.0, 0.0), "lap2d_256"),
     "lap3d_32": ((32, 32, 32, 0.0, 0.0, 0.0, 0.0), "lap3d_128"),
+    # the headline's parameters (4 levels, ILUT 1e-3/200, rank 16, inner Schur FGMRES) at 64^3
+    "lap3d_64": ((64, 64, 64, 0.0, 0.0, 0.0, 0.0), "lap3d_128"),
     "convdiff2d_96": ((96, 96, 1, 0.0, 0.3, -0.2, 0.0), "lap2d_256"),
 }
 
@@ -53,7 +55,7 @@ def handles():
         h.close()
 
 
-@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32"])
+@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32", "lap3d_64"])
 def test_precond_apply_fp64_matches_reference(handles, name):
     h, ref, _ = handles(name, "fp64")
     ap = ref["apply"]
@@ -66,7 +68,7 @@ def test_precond_apply_fp64_matches_reference(handles, name):
         assert err <= 1e-9, f"apply {k}: relative difference {err:.3e}"
 
 
-@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32", "convdiff2d_96"])
+@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32", "lap3d_64", "convdiff2d_96"])
 def test_solve_fp64_matches_reference(handles, name):
     h, ref, p = handles(name, "fp64")
     b = pgxd.read(ref["problem"])["b"]
@@ -78,7 +80,7 @@ def test_solve_fp64_matches_reference(handles, name):
     assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) <= 1e-6
 
 
-@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32", "convdiff2d_96"])
+@pytest.mark.parametrize("name", ["lap2d_64", "lap2d_256", "lap3d_32", "lap3d_64", "convdiff2d_96"])
 def test_solve_mixed_within_budget(handles, name):
     h, ref, p = handles(name, "mixed")
     b = pgxd.read(ref["problem"])["b"]

@@ -20,9 +20,10 @@ import scipy.sparse as sp
 from pargemslr_b200 import _abi
 from pargemslr_b200 import params as P
 from pargemslr_b200 import problems
+from oracle.paths import REFERENCE_TESTS
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_HYPRE_INPUTS = "/root/reference/ParGeMSLR/TESTS/hypre/inputs"
+REF_HYPRE_INPUTS = os.path.join(REFERENCE_TESTS, "hypre", "inputs")
 
 
 def _diag_first(A):

@@ -12,9 +12,10 @@ import pytest
 import scipy.io
 import scipy.sparse as sp
 
+from oracle.paths import REFERENCE_TESTS
 from pargemslr_b200 import _abi
 
-REF_MATRICES = "/root/reference/ParGeMSLR/TESTS/sequential/Matrices"
+REF_MATRICES = os.path.join(REFERENCE_TESTS, "sequential", "Matrices")
 
 
 def _check_against_scipy(path):

@@ -19,11 +19,12 @@ import pytest
 
 from pargemslr_b200 import _abi
 from pargemslr_b200 import params as P
+from oracle.paths import REFERENCE_TESTS
 from tests import params_fuzz as F
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = json.load(open(os.path.join(HERE, "golden", "params_files.json")))
-REF_TESTS = "/root/reference/ParGeMSLR/TESTS"
+REF_TESTS = REFERENCE_TESTS
 
 
 def _write(tmp_path, name, text):
