@@ -153,6 +153,14 @@ def max_over_ranks(value: float, device) -> float:
     return float(t.item())
 
 
+def log(msg: str) -> None:
+    """Progress of the phases on stderr (the JSON line alone goes to stdout)."""
+    print("[bench %.1fs] %s" % (time.time() - _T0, msg), file=sys.stderr, flush=True)
+
+
+_T0 = time.time()
+
+
 def build_problem():
     A = problems.laplacian(*GRID)
     n = A[0].size - 1
@@ -292,21 +300,67 @@ def _batch(h, p, R, n, B_dev, X_dev, ev_a, ev_b):
     return res, ev_a.elapsed_time(ev_b)
 
 
-def _fit_slots(h, R, lanes):
-    """Slots for R right-hand sides in flight; each holds its own Krylov basis, so on a GPU with less free memory
-    the batch shrinks until the slots fit.  Returns (R, nslots)."""
+def _fit_slots(h, R, lanes, basis_bytes_per_rhs):
+    """Slots for R right-hand sides in flight.  Each holds its own Krylov basis (allocated at its first solve, so
+    it is counted here against the device's free memory, with 4 GB to spare); on a GPU with less free memory the
+    batch shrinks until the slots fit.  Returns (R, nslots)."""
+    import torch
     from pargemslr_b200._abi import ERROR_OOM, PgxError
-    nslots = 1 + -(-(R - 1) // lanes)
     while True:
+        nslots = 1 + -(-(R - 1) // lanes)
         try:
             h.set_slots(nslots)
-            return R, nslots
         except PgxError as exc:
             if exc.code != ERROR_OOM or R <= lanes:
                 raise
             h.set_slots(1)
             R = max(lanes, R - 4 * lanes)
-            nslots = 1 + -(-(R - 1) // lanes)
+            continue
+        free, _ = torch.cuda.mem_get_info()
+        pending = (1 + (nslots - 1) * lanes) * basis_bytes_per_rhs
+        if pending + (4 << 30) <= free or R <= lanes:
+            return R, nslots
+        h.set_slots(1)
+        R = max(lanes, R - 4 * lanes)
+
+
+def _fp64_comparison(args, st, A, p, n, R, kdim, B_dev, X_dev, ev_a, ev_b, device):
+    """The FP64 preconditioner on the same setup and right-hand sides: one solve at a time, and batched like the
+    headline (as many right-hand sides in flight as fit)."""
+    import torch
+    from pargemslr_b200.handle import GemslrHandle
+    h64 = (GemslrHandle(st, precision="fp64", device=device) if st is not None
+           else GemslrHandle.from_matrix(A, p, precision="fp64", device=device))
+    try:
+        pm, pit = [], []
+        for k in range(3):
+            x1 = torch.zeros(n, dtype=torch.float64, device=B_dev.device)
+            torch.cuda.synchronize()
+            ev_a.record()
+            r1 = h64.solve_device(x1.data_ptr(), B_dev[k % R].data_ptr(), params=p)
+            ev_b.record()
+            ev_b.synchronize()
+            if k > 0:  # the first solve is warm-up
+                pm.append(ev_a.elapsed_time(ev_b))
+                pit.append(r1["iters"])
+        plain = {"solves_per_s": len(pm) / (sum(pm) / 1e3), "ms_per_solve": sum(pm) / len(pm), "iters": pit,
+                 "what": "FP64 preconditioner, one solve at a time (pgx_gemslr_solve), same setup and RHS"}
+        h64.set_lanes(args.lanes)
+        R64, ns64 = _fit_slots(h64, R, args.lanes, n * (kdim + 1) * 16)
+        B64, X64 = B_dev[:R64], X_dev[:R64]
+        _batch(h64, p, R64, n, B64, X64, ev_a, ev_b)  # warm-up
+        bm, bit = [], []
+        for _ in range(2):
+            res64, t_ms = _batch(h64, p, R64, n, B64, X64, ev_a, ev_b)
+            bm.append(t_ms)
+            bit.extend(r["iters"] for r in res64)
+        batched = {"solves_per_s": 2 * R64 / (sum(bm) / 1e3), "solves_per_step": R64, "slots": ns64,
+                   "lanes_per_slot": args.lanes, "iters": [min(bit), max(bit)],
+                   "what": "FP64 preconditioner, batched like the headline (pgx_gemslr_solve_batch); the width is "
+                           "the headline's unless its Krylov bases (8+8 bytes per entry) do not fit"}
+        return plain, batched
+    finally:
+        h64.close()
 
 
 def run_pgx(args):
@@ -340,11 +394,13 @@ def run_pgx(args):
         ref, ref_why = reference_run(threads, 1, dump=True)
         if ref is None:
             raise SystemExit("--setup reference: " + ref_why)
+        log("reference setup and solve: %.1f s (%d iterations)" % (ref["wall_s"], ref["iters"]))
         st = from_dump(os.path.join(ref["dir"], "setup.bin"))
         h = GemslrHandle(st, precision=args.precision, device=local)
     else:
         h = GemslrHandle.from_matrix(A, p, precision=args.precision, device=local)
     setup_s = time.time() - t0
+    log("handle committed")
 
     R = args.batch
     xts = np.stack([problems.x_true(n, SEED + r) for r in range(R)])
@@ -353,16 +409,19 @@ def run_pgx(args):
         # right-hand side 0 is the reference's own b (its MatVec of the same x_true)
         B[0] = pgxd.read(os.path.join(ref["dir"], "problem.bin"))["b"]
         x_ref = pgxd.read(os.path.join(ref["dir"], "solution.bin"))["x"]
+    kdim = int(p[P.SOLVER_KDIM])
     h.set_lanes(args.lanes)
-    R, nslots = _fit_slots(h, R, args.lanes)
+    R, nslots = _fit_slots(h, R, args.lanes, n * (kdim + 1) * (8 + (4 if args.precision == "mixed" else 8)))
     xts, B = xts[:R], B[:R]
     B_dev = torch.from_numpy(B).to(dev)
     X_dev = torch.zeros_like(B_dev)
     ev_a = torch.cuda.Event(enable_timing=True)
     ev_b = torch.cuda.Event(enable_timing=True)
 
+    log("%d right-hand sides in %d slots" % (R, nslots))
     for _ in range(args.warmup):
         _batch(h, p, R, n, B_dev, X_dev, ev_a, ev_b)
+    log("warm-up done")
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -417,6 +476,7 @@ def run_pgx(args):
         ev_b.synchronize()
         e2e_ms.append(ev_a.elapsed_time(ev_b))
     e2e_total = max_over_ranks(sum(e2e_ms) / 1e3, dev)
+    log("timed and e2e steps done: %.3f s per step" % (total_ms / args.steps / 1e3))
 
     # roofline of the dominant kernel: the level-0 triangular passes, merged over
     # the lanes of a multi-lane slot (the kernel the batch spends its time in)
@@ -435,48 +495,23 @@ def run_pgx(args):
 
     # the FP64 preconditioner on the same setup: batched at the same width (as
     # many right-hand sides as fit), and one solve at a time
-    fp64_batched, plain = None, None
+    fp64_batched, plain, fp64_error = None, None, None
     if world == 1 and not args.no_fp64 and args.precision == "mixed":
-        h64 = (GemslrHandle(st, precision="fp64", device=local) if st is not None
-               else GemslrHandle.from_matrix(A, p, precision="fp64", device=local))
-        pm, pit = [], []
-        for k in range(3):
-            x1 = torch.zeros(n, dtype=torch.float64, device=dev)
-            torch.cuda.synchronize()
-            ev_a.record()
-            r1 = h64.solve_device(x1.data_ptr(), B_dev[k % R].data_ptr(), params=p)
-            ev_b.record()
-            ev_b.synchronize()
-            if k > 0:  # the first solve is warm-up
-                pm.append(ev_a.elapsed_time(ev_b))
-                pit.append(r1["iters"])
-        plain = {"solves_per_s": len(pm) / (sum(pm) / 1e3), "ms_per_solve": sum(pm) / len(pm), "iters": pit,
-                 "what": "FP64 preconditioner, one solve at a time (pgx_gemslr_solve), same setup and RHS"}
-        h64.set_lanes(args.lanes)
-        R64, ns64 = _fit_slots(h64, R, args.lanes)
-        B64, X64 = B_dev[:R64], X_dev[:R64]
-        _batch(h64, p, R64, n, B64, X64, ev_a, ev_b)  # warm-up
-        bm, bit = [], []
-        for _ in range(2):
-            res64, t_ms = _batch(h64, p, R64, n, B64, X64, ev_a, ev_b)
-            bm.append(t_ms)
-            bit.extend(r["iters"] for r in res64)
-        fp64_batched = {"solves_per_s": 2 * R64 / (sum(bm) / 1e3), "solves_per_step": R64, "slots": ns64,
-                        "lanes_per_slot": args.lanes, "iters": [min(bit), max(bit)],
-                        "what": "FP64 preconditioner, batched like the headline (pgx_gemslr_solve_batch); the "
-                                "width is the headline's unless its Krylov bases (8+8 bytes per entry) do not fit"}
-        h64.close()
+        try:
+            plain, fp64_batched = _fp64_comparison(args, st, A, p, n, R, kdim, B_dev, X_dev, ev_a, ev_b, local)
+        except Exception as exc:  # the headline line is printed regardless
+            fp64_error = repr(exc)[:300]
 
     peak, peak_kind = measured_peak_hbm()
     single = {"bytes_per_launch": (lo_bytes + up_bytes) / 2.0, "ms_per_launch": (lo_ms + up_ms) / 2.0}
     single["achieved"] = single["bytes_per_launch"] / (single["ms_per_launch"] * 1e-3) / 1e9
     if args.lanes > 1:
-        kname = ("trsv_comp_batch_kernel (level-0 ILU L and U passes merged over %d lanes, mean; one CTA per "
+        kname = ("trsv_pipe_kernel (level-0 ILU L and U passes merged over %d lanes, mean; one CTA per "
                  "subdomain)" % args.lanes)
         tri_bytes = (blo_bytes + bup_bytes) / 2.0
         tri_ms = (blo_ms + bup_ms) / 2.0
     else:
-        kname = "trsv_comp_kernel (level-0 ILU L and U passes, mean; one CTA per subdomain)"
+        kname = "trsv_pipe_kernel (level-0 ILU L and U passes, mean; one CTA per subdomain)"
         tri_bytes, tri_ms = single["bytes_per_launch"], single["ms_per_launch"]
     achieved = tri_bytes / (tri_ms * 1e-3) / 1e9
     traffic = ncu_traffic(args.lanes)
@@ -486,7 +521,7 @@ def run_pgx(args):
               "x_err_max_vs_x_true": x_err, "parity_vs_reference": parity,
               "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                              "what": "device time of each solve inside the batch (its slot's events)"},
-              "fp64_plain": plain, "fp64_batched": fp64_batched,
+              "fp64_plain": plain, "fp64_batched": fp64_batched, "fp64_error": fp64_error,
               "mixed_over_fp64_batched": (value / fp64_batched["solves_per_s"]) if fp64_batched else None,
               "mixed_over_fp64_plain": (value / plain["solves_per_s"]) if plain else None,
               "l2": "inputs larger than L2 (level-0 factors alone are about 1 GB)",
@@ -527,6 +562,94 @@ def run_pgx(args):
         dist.destroy_process_group()
 
 
+def run_serve(args):
+    """Serving workload: a Poisson stream of requests over resident preconditioned matrices (pgx_pool_*).
+
+    `--serve-matrices` random nonsymmetric sparse systems with rows log-uniform in [--serve-rows-min,
+    --serve-rows-max] (7-27 nonzeros per row, off-diagonals N(0,1), diagonal 1.2 x the row's absolute off-diagonal
+    sum), each set up once (untimed) and kept resident; one pool with a device-memory budget of 90% of the free
+    memory admits requests by the bytes of their slot (work space and FGMRES(40) Krylov basis).  For every arrival
+    rate, --serve-requests requests arrive with exponential gaps, each for a matrix drawn uniformly with a seeded
+    U[-1,1] right-hand side (a few per matrix, reused), solved to rel-res 1e-8.  Latency is arrival to collection on
+    the host clock; throughput is requests finished over the span from the first arrival to the last finish."""
+    import torch
+    from pargemslr_b200.handle import GemslrHandle
+    from pargemslr_b200.serving import Pool
+
+    rng = np.random.default_rng(2026)
+    p = P.workload_params("serve")
+    lo, hi = args.serve_rows_min, args.serve_rows_max
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), size=args.serve_matrices)).astype(int)
+    hs, setup_s = [], 0.0
+    for i, n in enumerate(sizes):
+        A = problems.random_diag_dominant(int(n), 1000 + i)
+        t0 = time.time()
+        hs.append(GemslrHandle.from_matrix(A, p, precision=args.precision))
+        setup_s += time.time() - t0
+        log("matrix %d: n=%d set up" % (i, n))
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(0.9 * free)
+    pool = Pool(budget, p)
+    for h in hs:
+        pool.add(h)
+    rhs_per = 4
+    B = [[torch.from_numpy(np.random.default_rng(7 * i + k).uniform(-1, 1, h.n)).cuda() for k in range(rhs_per)]
+         for i, h in enumerate(hs)]
+    pool.start()
+    results = []
+    rid = 0
+    for rate in args.serve_rates:
+        gaps = rng.exponential(1.0 / rate, size=args.serve_requests)
+        members = rng.integers(0, len(hs), size=args.serve_requests)
+        arrivals = {}
+        xs = {}
+        lat, iters, ok = [], [], 0
+        t_start = time.perf_counter()
+        t_next = t_start
+        k = 0
+        last_done = t_start
+        while k < args.serve_requests or len(arrivals) > 0:
+            now = time.perf_counter()
+            while k < args.serve_requests and t_next <= now:
+                m = int(members[k])
+                xs[rid] = torch.zeros(hs[m].n, dtype=torch.float64, device="cuda")
+                pool.submit_ptr(m, xs[rid].data_ptr(), B[m][k % rhs_per].data_ptr(), LOCATION_DEVICE, rid)
+                arrivals[rid] = t_next
+                rid += 1
+                k += 1
+                if k < args.serve_requests:
+                    t_next += gaps[k]
+            for i, r in pool.collect():
+                t = time.perf_counter()
+                lat.append((t - arrivals.pop(i)) * 1e3)
+                iters.append(r["iters"])
+                ok += int(r["status"] == 0 and r["true_rel_res"] <= 1e-8)
+                xs.pop(i, None)
+                last_done = t
+            time.sleep(0.0002)
+        span = last_done - t_start
+        st = pool.stats()
+        results.append({"rate_per_s": rate, "requests": args.serve_requests, "solves_per_s": len(lat) / span,
+                        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "iters_mean": float(np.mean(iters)), "converged": ok, "slots": st["slots"],
+                        "peak_bytes": st["peak_bytes"]})
+        log("rate %s: %.1f solves/s p50 %.1f ms p99 %.1f ms" % (rate, results[-1]["solves_per_s"],
+                                                                results[-1]["p50_ms"], results[-1]["p99_ms"]))
+    pool.stop()
+    pool.close()
+    for h in hs:
+        h.close()
+    line = {"metric": "serving: solves/s and p50/p99 request latency under Poisson arrivals, rel-res 1e-8",
+            "unit": "solves/s", "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+            "dtype": "f32 preconditioner / f64 FGMRES" if args.precision == "mixed" else "f64",
+            "config": {"workload": "%d random nonsymmetric sparse systems, rows log-uniform in [%d, %d], 7-27 "
+                                   "nonzeros per row, 2 levels, ILUT 1e-2/20, rank 8, FGMRES(40) to 1e-8"
+                                   % (len(hs), lo, hi),
+                       "budget_bytes": budget, "setup_s": round(setup_s, 1), "rows": [int(v) for v in sizes]},
+            "value": max(r["solves_per_s"] for r in results), "rates": results}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -550,11 +673,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=128,
                     help="cube edge of the Laplacian (128 is the headline workload; smaller grids for profiling)")
+    ap.add_argument("--workload", choices=["laplacian", "serve"], default="laplacian",
+                    help="laplacian: the headline batch benchmark; serve: Poisson arrivals over resident matrices")
+    ap.add_argument("--serve-matrices", type=int, default=64)
+    ap.add_argument("--serve-rows-min", type=int, default=200000)
+    ap.add_argument("--serve-rows-max", type=int, default=2000000)
+    ap.add_argument("--serve-requests", type=int, default=2000, help="requests per arrival rate")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[50, 200, 500, 1000, 2000])
     args = ap.parse_args()
     global GRID
     GRID = (args.grid,) * 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_pgx(args)
 

@@ -198,6 +198,17 @@ int pgx_gemslr_nnz(pgx_handle handle, int64_t *nnz_bsolver, int64_t *nnz_lr);
 int pgx_gemslr_solve(pgx_handle handle, double *x, const double *b, int32_t location,
                      const double *params, pgx_result *result);
 
+/* FlexGmresClass::GetRelativeResidual (fgmres.hpp:683): the Givens
+ * relative residual estimates of the handle's last pgx_gemslr_solve or
+ * pgx_gemslr_solve_static: entry 0 is ||r0||/||b||, entry j the estimate
+ * after iteration j (fgmres.hpp:362-364, 450-452), and 0 for an iteration
+ * that broke down.  *count receives iterations + 1 (the reference's vector
+ * is maxits + 1 long and zero past the last iteration); a zero right-hand
+ * side, or an x0 that already solves the system, gives one entry, 0.  At most
+ * `capacity` entries are written to hist; hist may be NULL to ask for the
+ * count.  Solves of the other slots (batch, server) keep no history. */
+int pgx_gemslr_residual_history(pgx_handle handle, int32_t capacity, double *hist, int32_t *count);
+
 /* ---- solve without device allocation -------------------------------------
  * No counterpart in the reference: it exists for callers of this library
  * that must not allocate device memory at solve time.  pgx_gemslr_solve
@@ -292,6 +303,37 @@ int pgx_server_destroy(pgx_server server);
 int pgx_server_start(pgx_server server);
 int pgx_server_stop(pgx_server server);
 
+/* Serving pool: many resident preconditioned matrices behind one request
+ * queue and one device-memory budget.  No counterpart in the reference,
+ * which serves one matrix per process.  pgx_pool_add makes a committed
+ * handle a member (its factors, its own slot and that slot's Krylov basis
+ * count against the budget at once; refused with PGX_ERROR_OOM when they do
+ * not fit); while a handle is a member its slots belong to the pool and
+ * solve, set_slots, commit and destroy are refused.  pgx_pool_submit queues
+ * a request for member `index`.  pgx_pool_step advances every request in
+ * flight by at most one restart cycle, then admits waiting requests first
+ * fit in arrival order: a request runs in an idle slot of its member, or in
+ * a new slot (work space and FGMRES(kdim) basis, pgx_gemslr_slot_bytes) if
+ * the budget has room, if need be after releasing idle slots of other
+ * members, least recently used first; otherwise it waits.  The pool's FGMRES
+ * options come from `params` at creation (SOLVER_KDIM, MAXITS, TOL, ATOL).
+ * pgx_pool_start / stop run the step loop on a thread of the library's own
+ * (as pgx_server_start); pgx_pool_collect returns finished requests;
+ * pgx_pool_stats the bytes counted now and at most so far, and the number of
+ * slots; pgx_pool_destroy finishes the requests in flight and returns the
+ * handles to their owners. */
+typedef struct pgx_pool_s *pgx_pool;
+int pgx_pool_create(int64_t budget_bytes, const double *params, pgx_pool *pool);
+int pgx_pool_add(pgx_pool pool, pgx_handle handle, int32_t *index);
+int pgx_pool_submit(pgx_pool pool, int32_t index, double *x, const double *b, int32_t location,
+                    int64_t request_id);
+int pgx_pool_step(pgx_pool pool, int32_t *n_active, int32_t *n_queued);
+int pgx_pool_start(pgx_pool pool);
+int pgx_pool_stop(pgx_pool pool);
+int pgx_pool_collect(pgx_pool pool, int32_t max, int64_t *ids, pgx_result *results, int32_t *n);
+int pgx_pool_stats(pgx_pool pool, int64_t *bytes_in_use, int64_t *peak_bytes, int32_t *slots);
+int pgx_pool_destroy(pgx_pool pool);
+
 /* Apply the preconditioner once, z = M^-1 v (GemslrClass::Solve,
  * gemslr.cpp:3431-3472), on host or device vectors. */
 int pgx_gemslr_precond_apply(pgx_handle handle, double *z, const double *v, int32_t location);
@@ -306,6 +348,34 @@ int pgx_gemslr_precond_apply(pgx_handle handle, double *z, const double *v, int3
  * in and out. */
 int pgx_gemslr_kernel_stats(pgx_handle handle, int32_t which, int32_t level, int32_t reps, double *avg_ms,
                             double *bytes);
+
+/* A text description of slot `slot` of a committed handle (0 = the handle's
+ * own slot), one line per structure: for every level the kernel and layout
+ * of the L and U passes (per-subdomain pipeline, segmented or level-set;
+ * lanes per row, dependency levels, chunks) and the SpMV variant of A, E_l,
+ * F_l and C_0 (lanes per row or merge path); for a multi-lane slot its
+ * merged layouts.  Plays the part of the reference's setup report
+ * (GemslrClass print level).  *length receives the text's length; at most
+ * capacity - 1 characters and a terminating zero are written to buf, which
+ * may be NULL to ask for the length. */
+int pgx_gemslr_describe(pgx_handle handle, int32_t slot, char *buf, int32_t capacity, int32_t *length);
+
+/* Bounded waits.  No counterpart in the reference, whose triangular solves
+ * run on one host thread.  The triangular solves that cross subdomains
+ * (factors that are not block diagonal, or subdomains too large for one CTA)
+ * let a row wait on values other CTAs publish; every such wait gives up
+ * after `polls` polls of about 20 ns each (default 2^21), records the
+ * expiry, and the kernel finishes, so the solve returns PGX_ERROR_TIMEOUT
+ * instead of hanging and the CUDA context stays usable.
+ * pgx_gemslr_set_wait_limit sets the bound for every slot of a handle
+ * (captured restart cycles are rebuilt).  pgx_wait_selfcheck runs that
+ * triangular kernel, on the current device, over two rows of which the
+ * second waits on the first and only the second is scheduled: nothing ever
+ * publishes the value, so the wait can only end by its bound.  *status
+ * receives what a solve would report (PGX_ERROR_TIMEOUT when the bound
+ * worked) and *wait_ms the kernel's device time. */
+int pgx_gemslr_set_wait_limit(pgx_handle handle, int64_t polls);
+int pgx_wait_selfcheck(int64_t polls, int32_t *status, double *wait_ms);
 
 /* ---- building blocks (each is also used inside the solve) ---------------
  * The level-set schedule of a unit-lower (uplo 'L') or upper (uplo 'U')
@@ -361,8 +431,22 @@ int pgx_params_read_file(const char *path, int32_t format, double *params);
  * SRC/utils/utils.cpp:389-416). */
 int pgx_params_read_args(int32_t argc, const char *const *argv, double *params);
 
-/* y = alpha * A x + beta * y on device pointers (CSR SpMV kernel). */
+/* CSR SpMV, y = alpha * A x + beta * y (CsrMatrixClass::MatVec,
+ * matrixops.cpp:5139-5330), with the kernel every solve uses for A, E_l,
+ * F_l and C_0.  The variant is picked per matrix from its row-length
+ * histogram (pgx_csr_spmv_plan, host arrays): S lanes per row, with S the
+ * smallest power of two (2..32) for which the 90th-percentile row fits one
+ * batch of S * 4 unrolled loads; or the merge-path SpMV (every thread the
+ * same number of row ends plus nonzeros) when rows are skewed: the longest
+ * row is longer than 16 batches and rows longer than 4 batches hold more
+ * than a tenth of the nonzeros.  pgx_csr_spmv_device runs the plan's choice
+ * on device arrays; pgx_csr_spmv_device_variant forces one: 0 the plan's,
+ * 1 lanes per row, 2 merge path.  The two variants sum a row in different
+ * orders, so their results agree to rounding, not bit for bit. */
+int pgx_csr_spmv_plan(const pgx_csr *A, int32_t *lanes, int32_t *merge_path);
 int pgx_csr_spmv_device(const pgx_csr *A_device, double alpha, const double *x, double beta, double *y);
+int pgx_csr_spmv_device_variant(const pgx_csr *A_device, int32_t variant, double alpha, const double *x,
+                                double beta, double *y);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,10 @@ EXPORTS = (
     "pgx_gemslr_solve_static", "pgx_gemslr_set_lanes", "pgx_csr_read_mm", "pgx_csr_free",
     "pgx_server_start", "pgx_server_stop", "pgx_params_default", "pgx_params_read_file",
     "pgx_gemslr_nnz", "pgx_params_read_args", "pgx_vector_read_mm",
+    "pgx_gemslr_set_wait_limit", "pgx_wait_selfcheck", "pgx_gemslr_residual_history",
+    "pgx_csr_spmv_plan", "pgx_csr_spmv_device_variant", "pgx_gemslr_describe",
+    "pgx_pool_create", "pgx_pool_add", "pgx_pool_submit", "pgx_pool_step", "pgx_pool_start", "pgx_pool_stop",
+    "pgx_pool_collect", "pgx_pool_stats", "pgx_pool_destroy",
 )
 
 # every symbol include/pgx_hypre.h declares (the reference's hypre plugin interface)
@@ -132,6 +136,21 @@ def lib() -> C.CDLL:
     L.pgx_params_read_file.argtypes = [C.c_char_p, i32, vp]
     L.pgx_params_read_args.argtypes = [i32, C.POINTER(C.c_char_p), vp]
     L.pgx_vector_read_mm.argtypes = [C.c_char_p, i32, i32, vp, C.POINTER(i32)]
+    L.pgx_gemslr_set_wait_limit.argtypes = [vp, i64]
+    L.pgx_wait_selfcheck.argtypes = [i64, C.POINTER(i32), C.POINTER(dbl)]
+    L.pgx_gemslr_residual_history.argtypes = [vp, i32, vp, C.POINTER(i32)]
+    L.pgx_pool_create.argtypes = [i64, vp, C.POINTER(vp)]
+    L.pgx_pool_add.argtypes = [vp, vp, C.POINTER(i32)]
+    L.pgx_pool_submit.argtypes = [vp, i32, vp, vp, i32, i64]
+    L.pgx_pool_step.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.pgx_pool_start.argtypes = [vp]
+    L.pgx_pool_stop.argtypes = [vp]
+    L.pgx_pool_collect.argtypes = [vp, i32, vp, vp, C.POINTER(i32)]
+    L.pgx_pool_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32)]
+    L.pgx_pool_destroy.argtypes = [vp]
+    L.pgx_gemslr_describe.argtypes = [vp, i32, C.c_char_p, i32, C.POINTER(i32)]
+    L.pgx_csr_spmv_plan.argtypes = [C.POINTER(Csr), C.POINTER(i32), C.POINTER(i32)]
+    L.pgx_csr_spmv_device_variant.argtypes = [C.POINTER(Csr), i32, dbl, vp, dbl, vp]
     for name in EXPORTS + HYPRE_EXPORTS:
         if name != "pgx_last_error":
             getattr(L, name).restype = C.c_int

@@ -186,12 +186,57 @@ static bool all_finite(const double* b, long long n) {
   return !bad;
 }
 
-// lanes per row of the CSR SpMV: about three nonzeros per lane keeps several
-// independent gathers of x in flight per thread
-static int spmv_lanes(long long nnz, long long rows) {
+// The SpMV variant of a matrix, picked from its row-length histogram:
+//   lanes per row S: the 90th-percentile row fits in one unrolled load batch
+//     of the S lanes (S * kSpmvUnroll entries), so nine rows in ten need no
+//     second round of gathers;
+//   merge path instead of S lanes per row when the rows are skewed: the
+//     longest row is more than 16 batches long and rows longer than four
+//     batches hold more than a tenth of the nonzeros (a group of lanes would
+//     serialise them while the short rows leave lanes idle).
+struct SpmvPlan {
+  int S = 2;
+  bool merge = false;
+};
+static SpmvPlan spmv_plan(int rows, const int* rp) {
+  SpmvPlan p;
+  if (rows <= 0) return p;
+  std::vector<int> len(rows);
+  long long nnz = 0;
+  int mx = 0;
+  for (int r = 0; r < rows; r++) {
+    len[r] = rp[r + 1] - rp[r];
+    nnz += len[r];
+    mx = std::max(mx, len[r]);
+  }
+  std::vector<int> sorted(len);
+  const size_t q = (size_t)std::min<long long>(rows - 1, (long long)std::ceil(0.9 * rows) - 1);
+  std::nth_element(sorted.begin(), sorted.begin() + q, sorted.end());
+  const int p90 = sorted[q];
+  while (p.S < 32 && p.S * kSpmvUnroll < p90) p.S *= 2;
+  const int batch = p.S * kSpmvUnroll;
+  long long heavy = 0;
+  for (int r = 0; r < rows; r++)
+    if (len[r] > 4 * batch) heavy += len[r];
+  p.merge = mx > 16 * batch && heavy * 10 > nnz;
+  return p;
+}
+
+// merge-path threads (kMergeItems items each) for a rows x nnz matrix
+static int merge_threads(long long rows, long long nnz) { return (int)((rows + nnz + kMergeItems - 1) / kMergeItems); }
+
+// Lanes per row of the per-subdomain solve: about PGX_PIPE_NNZ_PER_LANE nonzeros
+// per lane, so that a row's operand loads are issued at once (kUnroll deep)
+// and a level of a few dozen rows needs one sweep of the CTA's groups.  The
+// choice depends on the factor alone, so every slot and lane count of a
+// handle sums each row in the same order.
+#ifndef PGX_PIPE_NNZ_PER_LANE
+#define PGX_PIPE_NNZ_PER_LANE 4
+#endif
+static int pipe_lanes(long long nnz, long long rows) {
   const double avg = rows > 0 ? (double)nnz / (double)rows : 0.0;
   int S = 2;
-  while (S < 32 && 3.0 * S * 2 <= avg) S *= 2;
+  while (S < 16 && avg > (double)PGX_PIPE_NNZ_PER_LANE * S) S *= 2;
   return S;
 }
 
@@ -239,6 +284,7 @@ struct Arena {
 template <typename T>
 struct DCsr {
   int rows = 0, cols = 0, S = 8;
+  bool merge = false;  // merge-path SpMV (skewed rows) instead of S lanes per row
   long long nnz = 0;
   int *rp = nullptr, *cj = nullptr;
   T* va = nullptr;
@@ -249,11 +295,20 @@ static int upload_csr(Arena& ar, const HostCsr& h, DCsr<T>& d, cudaStream_t s) {
   d.rows = h.rows;
   d.cols = h.cols;
   d.nnz = h.nnz();
-  d.S = spmv_lanes(d.nnz, d.rows);
   if (h.rows == 0) return PGX_SUCCESS;
+  const SpmvPlan plan = spmv_plan(h.rows, h.rp.data());
+  d.S = plan.S;
+  d.merge = plan.merge;
   PGX_TRY(ar.upload(&d.rp, h.rp.data(), h.rp.size(), s));
-  PGX_TRY(ar.upload(&d.cj, h.cj.data(), h.cj.size(), s));
-  PGX_TRY(ar.upload(&d.va, h.va.data(), h.va.size(), s));
+  // column indices and values padded to whole 4-entry blocks (column 0,
+  // value 0) for the 128-bit loads of the SpMV
+  const size_t padded = (h.cj.size() + 3) / 4 * 4;
+  std::vector<int> cj(h.cj);
+  std::vector<double> va(h.va);
+  cj.resize(std::max<size_t>(padded, 4), 0);
+  va.resize(std::max<size_t>(padded, 4), 0.0);
+  PGX_TRY(ar.upload(&d.cj, cj.data(), cj.size(), s));
+  PGX_TRY(ar.upload(&d.va, va.data(), va.size(), s));
   return PGX_SUCCESS;
 }
 
@@ -266,7 +321,7 @@ struct DTri {
   unsigned long long* ticket = nullptr;
   // segmented schedule (trsv_seg_kernel); seg == false uses trsv_kernel
   bool seg = false;
-  bool comp = false;  // one CTA per subdomain (trsv_comp_kernel)
+  bool comp = false;  // one CTA per subdomain (trsv_pipe_kernel)
   int nseg = 0, ncomp = 1;
   int *comp_ch0 = nullptr, *cmeta = nullptr, *far_col = nullptr;  // one-CTA-per-subdomain schedule
   T* dslot = nullptr;   // upper pass: inverse diagonal in slot order
@@ -459,7 +514,7 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
   return PGX_SUCCESS;
 }
 
-// Chunked per-subdomain schedule for trsv_comp_kernel: each subdomain's
+// Chunked per-subdomain schedule for trsv_pipe_kernel: each subdomain's
 // rows in level-set order, cut into chunks that fit the kernel's staging
 // buffers, subdomain after subdomain.  A dependency is encoded as the
 // negative ring slot -(q % ring + 1) when its schedule position q is close
@@ -475,7 +530,7 @@ template <typename T>
 static int upload_tri_comp(Arena& ar, const HostCsr& h, bool upper, const std::vector<int>& dom, DTri<T>& d,
                            cudaStream_t s, const std::vector<double>* dinv, std::vector<int>* slot_of_row,
                            const std::vector<int>* upper_slot_of_row) {
-  return upload_tri_sub<T, CompCfg<T>>(ar, h, upper, dom, d, s, dinv, slot_of_row, upper_slot_of_row);
+  return upload_tri_sub<T, PipeCfg<T, 1>>(ar, h, upper, dom, d, s, dinv, slot_of_row, upper_slot_of_row);
 }
 
 // The layout for a per-subdomain kernel whose shared-memory sizes are CC's.
@@ -537,7 +592,10 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
   for (int c = 0; c < ncomp; c++) {
     const auto& sc = sched[c];
     size_t p = 0;
-    int prev_start = 0, chunk_in_comp = 0;
+    // starts of the previous chunk and of the one before it: a chunk's far
+    // operands are gathered while the chunk two before it is solved, so they
+    // must lie before that chunk's start
+    int prev_start = 0, prev2_start = 0, chunk_in_comp = 0;
     while (p < sc.size()) {
       // one chunk: consecutive positions within the row, nonzero and far caps
       size_t e = p;
@@ -551,7 +609,7 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
         e++;
       }
       push_meta((int)p);
-      const int far_base = CC::ring + (chunk_in_comp & 1) * CC::far;
+      const int far_base = CC::ring + (chunk_in_comp % 3) * CC::far;
       const int far0 = (int)far_col.size();
       rp.push_back(0);
       int acc = 0;
@@ -564,9 +622,9 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
           if (is_near(r, qj)) {
             cj.push_back(-((qj & (CC::ring - 1)) + 1));
           } else {
-            // far: gathered while the previous chunk is solved, so it must
-            // have been published before that chunk began
-            if (qj >= prev_start) return PGX_ERROR_INVALID_PARAM;
+            // far: gathered while the chunk two before is solved, so it
+            // must have been published before that chunk began
+            if (qj >= prev2_start) return PGX_ERROR_INVALID_PARAM;
             cj.push_back(-(far_base + ((int)far_col.size() - far0) + 1));
             far_col.push_back(j);
           }
@@ -577,6 +635,7 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
       }
       pad4(ord, -1);
       pad4(rp, acc);
+      pad4(far_col, -1);
       while (cj.size() % 4) {
         cj.push_back(0);
         va.push_back(0.0);
@@ -586,6 +645,7 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
         if (lev[sc[q]] != lev[sc[q - 1]]) lvb.push_back((int)(q - p));
       lvb.push_back((int)(e - p));
       pad4(lvb, (int)(e - p));
+      prev2_start = prev_start;
       prev_start = (int)p;
       chunk_in_comp++;
       p = e;
@@ -594,8 +654,20 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
   }
   push_meta(0);  // closes the last chunk
   for (int c : cj)
-    if (c >= 0 || -c - 1 >= CC::ring + 2 * CC::far)
+    if (c >= 0 || -c - 1 >= CC::ring + 3 * CC::far)
       if (c != 0) return fail(PGX_ERROR_INVALID_PARAM, "per-subdomain layout: operand index out of range");
+  // every chunk is staged by bulk copies: each range starts on a 16-byte
+  // boundary, spans a multiple of 16 bytes and fits its staging buffer
+  for (size_t ch = 0; ch + 1 < meta.size() / 8; ch++) {
+    const int* m = &meta[ch * 8];
+    const int* e = &meta[(ch + 1) * 8];
+    const int nr = e[0] - m[0], np = e[1] - m[1], nz = e[2] - m[2], nv = e[3] - m[3], nf = e[5] - m[5];
+    const bool aligned = (m[0] | m[1] | m[2] | m[3] | m[5] | nr | np | nz | nv | nf) % 4 == 0;
+    const bool fits = nr > 0 && nr <= CC::rows && np <= CC::rows + 4 && nv <= CC::rows + 4 && nz <= CC::nnz &&
+                      nf <= CC::far && np > 0 && nv > 0 && nz >= 0 && nf >= 0;
+    if (!aligned || !fits)
+      return fail(PGX_ERROR_INVALID_PARAM, "per-subdomain layout: chunk %zu breaks the staging rules", ch);
+  }
   // slot of every row in the flat row list; the upper pass's slots index its
   // dinv and the y the lower pass leaves behind
   std::vector<int> slot(n, -1);
@@ -621,8 +693,7 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
   d.nlevels = (int)lptr.size() - 1;
   d.nseg = (int)meta.size() / 8 - 1;
   d.nnz_total = h.nnz();
-  // lanes per row: one level of an average chunk in one sweep of the workers
-  d.S = std::min(pick_lanes(h.nnz(), n), 16);
+  d.S = pipe_lanes(h.nnz(), n);
   d.nblocks = ncomp;
   PGX_TRY(ar.upload(&d.ord, ord.data(), ord.size(), s));
   PGX_TRY(ar.upload(&d.rp, rp.data(), rp.size(), s));
@@ -660,6 +731,32 @@ struct DLevel {
   P *z = nullptr, *xlr = nullptr;
   double* lrt = nullptr;
 };
+
+template <typename T>
+static std::string describe_tri(const char* what, const DTri<T>& t) {
+  char buf[256];
+  if (t.n == 0) {
+    snprintf(buf, sizeof(buf), "  %s: empty\n", what);
+  } else if (t.comp) {
+    snprintf(buf, sizeof(buf), "  %s: per-subdomain pipeline, %d CTAs, %d lanes per row, %d dependency levels, %d chunks, %lld nonzeros\n",
+             what, t.ncomp, t.S, t.nlevels, t.nseg, t.nnz_total);
+  } else if (t.seg) {
+    snprintf(buf, sizeof(buf), "  %s: segmented, %d segments, %d CTAs, %d lanes per row, %d dependency levels\n", what,
+             t.nseg, t.nblocks, t.S, t.nlevels);
+  } else {
+    snprintf(buf, sizeof(buf), "  %s: level-set, %d groups, %d CTAs, %d lanes per row, %d dependency levels\n", what,
+             t.ngroups, t.nblocks, t.S, t.nlevels);
+  }
+  return buf;
+}
+template <typename T>
+static std::string describe_csr(const char* what, const DCsr<T>& m) {
+  char buf[192];
+  if (m.rows == 0) return std::string();
+  snprintf(buf, sizeof(buf), "  %s: %d x %d, %lld nonzeros, SpMV %s\n", what, m.rows, m.cols, m.nnz,
+           m.merge ? "merge path" : (std::to_string(m.S) + " lanes per row").c_str());
+  return buf;
+}
 
 static inline Skip mk_skip(const int* a = nullptr, const int* b = nullptr, const int* c = nullptr) {
   Skip s;
@@ -717,6 +814,13 @@ struct EngineBase {
     (void)out;
     return fail(PGX_ERROR_FUNCTION_CALL, "slots are cloned from the handle itself");
   }
+  // polls before a triangular-solve dependency wait gives up; captured
+  // restart cycles are rebuilt with the new bound
+  virtual void set_wait_limit(int polls) = 0;
+  // relative Givens residual estimates of the slot's last solve
+  virtual std::vector<double> residual_history() const { return std::vector<double>(); }
+  // one line per structure: which kernel and layout each pass and SpMV uses
+  virtual std::string describe() const { return std::string(); }
   virtual int begin_many(int count, double* const* x, const double* const* b, int location, int kdim, int maxits,
                          double tol, int atol, bool prechecked = false) {
     if (count != 1) return fail(PGX_ERROR_INVALID_PARAM, "this slot solves one right-hand side at a time");
@@ -759,10 +863,21 @@ struct Engine : EngineBase {
   P *rt = nullptr, *xt = nullptr;
   double* partial = nullptr;
   unsigned int* counter = nullptr;
+  // merge-path SpMV carries of this slot (rows and partial sums, one per
+  // thread of the largest merge-path matrix); null if no matrix uses it
+  int* mcarry_row = nullptr;
+  double* mcarry_val = nullptr;
   int* err = nullptr;
+  int spin_limit = kSpinLimit;  // polls before a dependency wait gives up (pgx_gemslr_set_wait_limit)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_poll = nullptr;
   FgmresDev* hs_pin = nullptr;  // pinned copy of the FGMRES state header
   double* r2_pin = nullptr;     // pinned copy of the final residual norm
+  double* hist_pin = nullptr;   // pinned copy of one cycle's residual estimates
+  // Givens residual estimates of the last solve driven by begin()/poll() or
+  // the static-basis solve: ||r0||, then one per iteration
+  std::vector<double> history;
+  int hist_iters = 0;
+  double hist_normb = 0.0;
   // one FGMRES restart cycle captured as a CUDA graph, keyed by its arguments
   cudaGraphExec_t cycle_exec = nullptr;
   int cycle_nodes = 0;  // kernels in one captured cycle
@@ -786,10 +901,56 @@ struct Engine : EngineBase {
     if (ev_poll) cudaEventDestroy(ev_poll);
     if (hs_pin) cudaFreeHost(hs_pin);
     if (r2_pin) cudaFreeHost(r2_pin);
+    if (hist_pin) cudaFreeHost(hist_pin);
     if (stream) cudaStreamDestroy(stream);
   }
 
   bool use_seg = true;
+
+  // dynamic shared memory of the per-subdomain solve for R right-hand sides
+  template <int R>
+  static int set_pipe_smem() {
+    const int bytes = (int)PipeCfg<P, R>::bytes;
+#define PGX_PIPEATTR(SS)                                                                                     \
+  PGX_CUDA(cudaFuncSetAttribute(trsv_pipe_kernel<P, SS, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                bytes));                                                                     \
+  PGX_CUDA(cudaFuncSetAttribute(trsv_pipe_kernel<P, SS, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))
+    PGX_PIPEATTR(2);
+    PGX_PIPEATTR(4);
+    PGX_PIPEATTR(8);
+    PGX_PIPEATTR(16);
+#undef PGX_PIPEATTR
+    return PGX_SUCCESS;
+  }
+
+  // the per-subdomain solve of factor T for R right-hand sides
+  template <int R>
+  static void launch_pipe(const DTri<P>& T, bool upper, const PtrR<P, R>& yslot, const PtrR<P, R>& rhs,
+                          const PtrR<P, R>& y, const PtrR<P, R>& x, int* err, const SkipR<R>& sk, cudaStream_t st) {
+    const size_t bytes = PipeCfg<P, R>::bytes;
+    CompArrays ca;
+    ca.meta = (const int4*)T.cmeta;
+    ca.ord = T.ord;
+    ca.rp = T.rp;
+    ca.cj = T.cj;
+    ca.lvb = T.lvb;
+    ca.uslot = T.uslot;
+    ca.far_col = T.far_col;
+#define PGX_PIPE(SS)                                                                                             \
+  if (upper)                                                                                                     \
+    trsv_pipe_kernel<P, SS, true, R><<<T.ncomp, kPipeThreads, bytes, st>>>(T.n, T.comp_ch0, ca, T.va, T.dslot,    \
+                                                                           yslot, rhs, y, x, err, sk);           \
+  else                                                                                                           \
+    trsv_pipe_kernel<P, SS, false, R><<<T.ncomp, kPipeThreads, bytes, st>>>(T.n, T.comp_ch0, ca, T.va, T.dslot,   \
+                                                                            yslot, rhs, y, x, err, sk)
+    switch (T.S) {
+      case 2: PGX_PIPE(2); break;
+      case 4: PGX_PIPE(4); break;
+      case 8: PGX_PIPE(8); break;
+      default: PGX_PIPE(16); break;
+    }
+#undef PGX_PIPE
+  }
 
   int set_seg_smem() {
     const int bytes = (int)SegCfg<P>::bytes;
@@ -802,16 +963,7 @@ struct Engine : EngineBase {
     PGX_SEGATTR(16);
     PGX_SEGATTR(32);
 #undef PGX_SEGATTR
-    const int cbytes = (int)CompCfg<P>::bytes;
-#define PGX_COMPATTR(SS)                                                                                         \
-  PGX_CUDA(cudaFuncSetAttribute(trsv_comp_kernel<P, SS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, cbytes)); \
-  PGX_CUDA(cudaFuncSetAttribute(trsv_comp_kernel<P, SS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, cbytes))
-    PGX_COMPATTR(2);
-    PGX_COMPATTR(4);
-    PGX_COMPATTR(8);
-    PGX_COMPATTR(16);
-    PGX_COMPATTR(32);
-#undef PGX_COMPATTR
+    PGX_TRY(set_pipe_smem<1>());
     return PGX_SUCCESS;
   }
 
@@ -841,6 +993,7 @@ struct Engine : EngineBase {
     PGX_CUDA(cudaEventCreateWithFlags(&ev_poll, cudaEventDisableTiming));
     PGX_CUDA(cudaMallocHost((void**)&hs_pin, sizeof(FgmresDev)));
     PGX_CUDA(cudaMallocHost((void**)&r2_pin, sizeof(double)));
+    PGX_CUDA(cudaMallocHost((void**)&hist_pin, sizeof(double) * KMAX));
     memset(hs_pin, 0, sizeof(FgmresDev));
     *r2_pin = 0.0;
     return PGX_SUCCESS;
@@ -944,6 +1097,20 @@ struct Engine : EngineBase {
     PGX_TRY(wk.zeros(&partial, (size_t)(KMAX + 1) * kTsMaxBlocks, stream));
     PGX_TRY(wk.zeros(&counter, 1, stream));
     PGX_TRY(wk.zeros(&err, 1, stream));
+    int mthreads = 0;
+    auto need = [&](const DCsr<P>& M) {
+      if (M.merge) mthreads = std::max(mthreads, merge_threads(M.rows, M.nnz));
+    };
+    if (A.merge) mthreads = std::max(mthreads, merge_threads(A.rows, A.nnz));
+    for (int l = 0; l < nlev; l++) {
+      need(lv[l].E);
+      need(lv[l].F);
+    }
+    need(C0);
+    if (mthreads > 0) {
+      PGX_TRY(wk.alloc(&mcarry_row, (size_t)mthreads));
+      PGX_TRY(wk.alloc(&mcarry_val, (size_t)mthreads));
+    }
     return PGX_SUCCESS;
   }
 
@@ -962,6 +1129,7 @@ struct Engine : EngineBase {
     inner_maxits = s.inner_maxits;
     inner_tol = s.inner_tol;
     use_seg = s.use_seg;
+    spin_limit = s.spin_limit;
     PGX_TRY(init_stream());
     PGX_TRY(alloc_work());
     PGX_CUDA(cudaStreamSynchronize(stream));
@@ -1215,14 +1383,23 @@ struct Engine : EngineBase {
   void spmv(const DCsr<TA>& M, const TX* x, TC alpha, const DCsr<TA>* M2, const TX* x2, TC alpha2,
             const TY* b, TC beta, TY* y, const double* xscale, Skip sk) {
     if (M.rows == 0) return;
+    if (M.merge && !M2 && !xscale && mcarry_row) {
+      const int nt = merge_threads(M.rows, M.nnz);
+      merge_spmv_kernel<TA, TX, TY, TC><<<(nt + 255) / 256, 256, 0, stream>>>(
+          M.rows, (int)M.nnz, M.rp, M.cj, M.va, x, alpha, b, beta, y, mcarry_row, (TC*)mcarry_val, sk);
+      merge_spmv_fixup_kernel<TY, TC><<<grid_for(nt, 256, 148 * 8), 256, 0, stream>>>(nt, mcarry_row,
+                                                                                     (const TC*)mcarry_val, alpha,
+                                                                                     y, sk);
+      return;
+    }
     const int S = M.S;
     const int gpb = 256 / S;
     const int grid = grid_for(M.rows, gpb, 148 * 16);
     const int *rp2 = M2 ? M2->rp : nullptr, *cj2 = M2 ? M2->cj : nullptr;
     const TA* va2 = M2 ? M2->va : nullptr;
-#define PGX_SPMV(SS)                                                                                  \
-  spmv_kernel<TA, TX, TY, TC, SS><<<grid, 256, 0, stream>>>(M.rows, M.rp, M.cj, M.va, x, alpha, rp2, cj2, \
-                                                            va2, x2, alpha2, b, beta, y, xscale, sk)
+#define PGX_SPMV(SS)                                                                                        \
+  spmv_kernel<TA, TX, TY, TC, SS, true><<<grid, 256, 0, stream>>>(M.rows, M.rp, M.cj, M.va, x, alpha, rp2, cj2, \
+                                                                  va2, x2, alpha2, b, beta, y, xscale, sk)
     switch (S) {
       case 2: PGX_SPMV(2); break;
       case 4: PGX_SPMV(4); break;
@@ -1239,32 +1416,14 @@ struct Engine : EngineBase {
             Skip sk, P* yslot = nullptr) {
     if (T.n == 0) return;
     if (T.comp) {
-      const size_t bytes = CompCfg<P>::bytes;
-      CompArrays ca;
-      ca.meta = (const int4*)T.cmeta;
-      ca.ord = T.ord;
-      ca.rp = T.rp;
-      ca.cj = T.cj;
-      ca.lvb = T.lvb;
-      ca.uslot = T.uslot;
-      ca.far_col = T.far_col;
-#define PGX_TRSVCOMP(SS)                                                                                        \
-  if (upper)                                                                                                    \
-    trsv_comp_kernel<P, SS, true><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, ca, T.va, \
-                                                                            T.dslot, yslot, rhs, rhs_scale, y, x, \
-                                                                            err, sk);                             \
-  else                                                                                                          \
-    trsv_comp_kernel<P, SS, false><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, ca, T.va, \
-                                                                             T.dslot, yslot, rhs, rhs_scale, y,    \
-                                                                             x, err, sk)
-      switch (T.S) {
-        case 2: PGX_TRSVCOMP(2); break;
-        case 4: PGX_TRSVCOMP(4); break;
-        case 8: PGX_TRSVCOMP(8); break;
-        case 16: PGX_TRSVCOMP(16); break;
-        default: PGX_TRSVCOMP(32); break;
-      }
-#undef PGX_TRSVCOMP
+      PtrR<P, 1> pys, prhs, py, px;
+      pys.p[0] = yslot;
+      prhs.p[0] = const_cast<P*>(rhs);
+      py.p[0] = y;
+      px.p[0] = x;
+      SkipR<1> sr;
+      sr.s[0] = sk;
+      launch_pipe<1>(T, upper, pys, prhs, py, px, err, sr, stream);
       return;
     }
     if (T.seg) {
@@ -1273,11 +1432,11 @@ struct Engine : EngineBase {
   if (upper)                                                                                                  \
     trsv_seg_kernel<P, SS, true><<<T.nblocks, kSegThreads, bytes, stream>>>(                                  \
         T.n, T.nseg, T.seg_row0, T.seg_rp0, T.seg_nnz0, T.seg_lv0, T.seg_nlvb, T.ord, T.rp, T.cj, T.va, T.lvb,  \
-        dinv, rhs, rhs_scale, y, x, T.ticket, err, sk);                                                       \
+        dinv, rhs, rhs_scale, y, x, T.ticket, err, spin_limit, sk);                                           \
   else                                                                                                        \
     trsv_seg_kernel<P, SS, false><<<T.nblocks, kSegThreads, bytes, stream>>>(                                 \
         T.n, T.nseg, T.seg_row0, T.seg_rp0, T.seg_nnz0, T.seg_lv0, T.seg_nlvb, T.ord, T.rp, T.cj, T.va, T.lvb,  \
-        dinv, rhs, rhs_scale, y, x, T.ticket, err, sk)
+        dinv, rhs, rhs_scale, y, x, T.ticket, err, spin_limit, sk)
       switch (T.S) {
         case 2: PGX_TRSVSEG(2); break;
         case 4: PGX_TRSVSEG(4); break;
@@ -1291,10 +1450,12 @@ struct Engine : EngineBase {
 #define PGX_TRSV(SS)                                                                                   \
   if (upper)                                                                                           \
     trsv_kernel<P, SS, true><<<T.nblocks, 256, 0, stream>>>(T.n, T.ngroups, T.ord, T.rp, T.cj, T.va,    \
-                                                            dinv, rhs, rhs_scale, y, x, T.ticket, err, sk); \
+                                                            dinv, rhs, rhs_scale, y, x, T.ticket, err,  \
+                                                            spin_limit, sk);                            \
   else                                                                                                 \
     trsv_kernel<P, SS, false><<<T.nblocks, 256, 0, stream>>>(T.n, T.ngroups, T.ord, T.rp, T.cj, T.va,   \
-                                                             dinv, rhs, rhs_scale, y, x, T.ticket, err, sk)
+                                                             dinv, rhs, rhs_scale, y, x, T.ticket, err, \
+                                                             spin_limit, sk)
     switch (T.S) {
       case 2: PGX_TRSV(2); break;
       case 4: PGX_TRSV(4); break;
@@ -1483,6 +1644,7 @@ struct Engine : EngineBase {
     PGX_CUDA(cudaStreamSynchronize(stream));
     if (h & kErrIndex) return fail(PGX_ERROR_INVALID_PARAM, "device index check failed");
     if (h & kErrTimeout) return fail(PGX_ERROR_TIMEOUT, "triangular-solve dependency wait timed out");
+    if (h & kErrStage) return fail(PGX_ERROR_TIMEOUT, "triangular-solve staging wait timed out");
     return PGX_SUCCESS;
   }
 
@@ -1639,6 +1801,8 @@ struct Engine : EngineBase {
     s_maxits = maxits;
     s_launches = 5;  // ||b||, residual, ||r0||, final residual and its norm
     s_location = location;
+    history.clear();
+    hist_iters = 0;
     s_xd = xd;
     s_bd = bd;
     s_xuser = x;
@@ -1708,6 +1872,7 @@ struct Engine : EngineBase {
       s_launches += cycle_nodes;
       s_cyc++;
       PGX_CUDA(cudaMemcpyAsync(hs_pin, st, offsetof(FgmresDev, sc), cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaMemcpyAsync(hist_pin, st->hist, sizeof(double) * g_kdim, cudaMemcpyDeviceToHost, stream));
       PGX_CUDA(cudaEventRecord(ev_poll, stream));
       return PGX_SUCCESS;
     }
@@ -1758,6 +1923,7 @@ struct Engine : EngineBase {
     }
     if (phase == RUNNING) {
       const FgmresDev& hs = *hs_pin;
+      absorb_history(hs);
       const bool over = hs.done || hs.iter >= s_maxits;
       const int rc = launch_cycle_or_finish(over);
       if (rc != PGX_SUCCESS) {
@@ -1770,6 +1936,49 @@ struct Engine : EngineBase {
     phase = IDLE;
     *finished = true;
     return collect_result(res);
+  }
+
+  // the residual estimates of the cycle that just landed (hs: its state
+  // header, hist_pin: its per-column estimates)
+  void absorb_history(const FgmresDev& hs) {
+    if (history.empty()) history.push_back(hs.normr0);
+    const int fresh = std::min(hs.iter - hist_iters, KMAX);
+    for (int j = 0; j < fresh; j++) history.push_back(hist_pin[j]);
+    hist_iters = hs.iter;
+    hist_normb = hs.normb;
+  }
+
+  // the relative residual history (FlexGmresClass::GetRelativeResidual,
+  // fgmres.hpp:683): estimates over ||b||; a zero right-hand side gives [0]
+  std::string describe() const override {
+    std::string o;
+    char buf[160];
+    snprintf(buf, sizeof(buf), "n %d, %d levels, precision %s, inner Schur FGMRES %s\n", n, nlev,
+             std::is_same<P, float>::value ? "mixed" : "fp64", inner ? "on" : "off");
+    o += buf;
+    o += describe_csr("A", A);
+    for (int l = 0; l < nlev; l++) {
+      const DLevel<P>& d = lv[l];
+      snprintf(buf, sizeof(buf), "level %d: rows %d, trailing %d, rank %d\n", l, d.nl, d.m, d.rank);
+      o += buf;
+      o += describe_tri("L", d.L);
+      o += describe_tri("U", d.U);
+      o += describe_csr("E", d.E);
+      o += describe_csr("F", d.F);
+    }
+    o += describe_csr("C0", C0);
+    return o;
+  }
+
+  std::vector<double> residual_history() const override {
+    std::vector<double> out;
+    if (hist_normb < DBL_EPSILON || (history.size() == 1 && history[0] < DBL_EPSILON)) {
+      // zero right-hand side, or x0 already the solution: the reference keeps [0]
+      if (!history.empty()) out.push_back(0.0);
+      return out;
+    }
+    for (double v : history) out.push_back(v / hist_normb);
+    return out;
   }
 
   // after enqueue_finish has landed: zero right-hand side, x back to the
@@ -1821,6 +2030,12 @@ struct Engine : EngineBase {
     auto* e = new Engine<P>();
     out.reset(e);
     return e->clone_from(*this);
+  }
+
+  void set_wait_limit(int polls) override {
+    if (stream) cudaStreamSynchronize(stream);
+    spin_limit = polls;
+    drop_graph();
   }
 
   // batched factor layouts shared by this handle's multi-lane slots, by lane count
@@ -1908,11 +2123,16 @@ struct Engine : EngineBase {
       ts<double, double, double, TS_NORM_COPY>(a);
     }
     const int max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
+    history.clear();
+    hist_iters = 0;
+    hist_normb = 0.0;
     for (int cyc = 0; cyc < max_cycles; cyc++) {
       enqueue_cycle(kdim, xd, bd);
       PGX_CUDA(cudaGetLastError());
       PGX_CUDA(cudaMemcpyAsync(hs_pin, st, head, cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaMemcpyAsync(hist_pin, st->hist, sizeof(double) * kdim, cudaMemcpyDeviceToHost, stream));
       PGX_CUDA(cudaStreamSynchronize(stream));
+      absorb_history(*hs_pin);
       if (hs_pin->done || hs_pin->iter >= maxits) break;
     }
     spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, rdev, nullptr, mk_skip());
@@ -1937,7 +2157,7 @@ struct Engine : EngineBase {
 };
 
 // Per-level layout of the triangular factors for R right-hand sides at once
-// (the CompCfgR chunking), built once per handle and read by every R-lane
+// (the PipeCfg<P, R> chunking), built once per handle and read by every R-lane
 // slot.  Levels whose factors do not fit that layout keep each lane's own
 // single-right-hand-side kernels.
 template <typename P, int R>
@@ -1949,7 +2169,7 @@ struct BatchLayout {
 // A solve slot that advances R right-hand sides in lockstep: R lanes, each
 // with its own FGMRES state and work vectors (clones of the owner), share one
 // stream and one captured restart cycle.  The triangular passes of the
-// preconditioner are merged over the lanes (trsv_comp_batch_kernel: each
+// preconditioner are merged over the lanes (trsv_pipe_kernel with R lanes: each
 // factor entry is read once for R vectors); every other kernel runs once per
 // lane exactly as in Engine, so each lane's arithmetic is that of a single
 // solve and its result matches it bit for bit.
@@ -1976,18 +2196,7 @@ struct BatchEngine : EngineBase {
   }
 
   int setup(Engine<P>& own, Import& im, std::shared_ptr<BatchLayout<P, R>> shared) {
-    const int bytes = (int)CompCfgR<P, R>::bytes;
-#define PGX_BATTR(SS)                                                                                        \
-  PGX_CUDA(cudaFuncSetAttribute(trsv_comp_batch_kernel<P, SS, false, R>,                                     \
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));                        \
-  PGX_CUDA(cudaFuncSetAttribute(trsv_comp_batch_kernel<P, SS, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                bytes))
-    PGX_BATTR(2);
-    PGX_BATTR(4);
-    PGX_BATTR(8);
-    PGX_BATTR(16);
-    PGX_BATTR(32);
-#undef PGX_BATTR
+    PGX_TRY(Engine<P>::template set_pipe_smem<R>());
     owner = &own;
     n = own.n;
     nlev = own.nlev;
@@ -2011,7 +2220,7 @@ struct BatchEngine : EngineBase {
         HostLevel& h = im.levels[l];
         if (h.L.rows == 0 || !own.lv[l].L.comp) continue;
         std::vector<int> uslot_of_row;
-        using CC = CompCfgR<P, R>;
+        using CC = PipeCfg<P, R>;
         int rc = upload_tri_sub<P, CC>(lay->ar, h.U, true, h.dom_ptr, lay->U[l], stream, &h.dinv, &uslot_of_row,
                                        nullptr);
         if (rc == PGX_SUCCESS)
@@ -2020,6 +2229,10 @@ struct BatchEngine : EngineBase {
         if (rc != PGX_SUCCESS) {
           lay->L[l] = DTri<P>();
           lay->U[l] = DTri<P>();
+        } else {
+          // rows are summed as the handle's own slot sums them
+          lay->L[l].S = own.lv[l].L.S;
+          lay->U[l].S = own.lv[l].U.S;
         }
       }
     }
@@ -2034,6 +2247,26 @@ struct BatchEngine : EngineBase {
   }
 
   int lanes() const override { return R; }
+  std::string describe() const override {
+    std::string o = "slot of " + std::to_string(R) + " lanes\n";
+    for (int l = 0; l < nlev; l++) {
+      o += "level " + std::to_string(l) + ":\n";
+      if (lay->L[l].comp) {
+        o += describe_tri("L (merged over the lanes)", lay->L[l]);
+        o += describe_tri("U (merged over the lanes)", lay->U[l]);
+      } else {
+        o += "  L, U: each lane's own passes\n";
+      }
+    }
+    return o;
+  }
+  void set_wait_limit(int polls) override {
+    if (stream) cudaStreamSynchronize(stream);
+    for (int r = 0; r < R; r++) lane[r]->spin_limit = polls;
+    if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
+    cycle_exec = nullptr;
+    g_kdim = -1;
+  }
   int64_t slot_bytes(int kdim) const override {
     int64_t b = (int64_t)wk.bytes;
     for (int r = 0; r < R; r++) b += lane[r]->slot_bytes(kdim);
@@ -2060,15 +2293,6 @@ struct BatchEngine : EngineBase {
       return;
     }
     if (T.n == 0) return;
-    const size_t bytes = CompCfgR<P, R>::bytes;
-    CompArrays ca;
-    ca.meta = (const int4*)T.cmeta;
-    ca.ord = T.ord;
-    ca.rp = T.rp;
-    ca.cj = T.cj;
-    ca.lvb = T.lvb;
-    ca.uslot = T.uslot;
-    ca.far_col = T.far_col;
     PtrR<P, R> prhs, py, px, pys;
     for (int r = 0; r < R; r++) {
       prhs.p[r] = const_cast<P*>(rhs[r]);
@@ -2076,25 +2300,7 @@ struct BatchEngine : EngineBase {
       px.p[r] = x[r];
       pys.p[r] = yslot[l][r];
     }
-    const SkipR<R> skr = all(sk);
-    int* err = lane[0]->err;
-#define PGX_TRSVB(SS)                                                                                         \
-  if (upper)                                                                                                  \
-    trsv_comp_batch_kernel<P, SS, true, R><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, ca, T.va, \
-                                                                                     T.dslot, pys, prhs, py, px, \
-                                                                                     err, skr);               \
-  else                                                                                                        \
-    trsv_comp_batch_kernel<P, SS, false, R><<<T.ncomp, kCompThreads, bytes, stream>>>(T.n, T.comp_ch0, ca, T.va, \
-                                                                                      T.dslot, pys, prhs, py, px, \
-                                                                                      err, skr)
-    switch (T.S) {
-      case 2: PGX_TRSVB(2); break;
-      case 4: PGX_TRSVB(4); break;
-      case 8: PGX_TRSVB(8); break;
-      case 16: PGX_TRSVB(16); break;
-      default: PGX_TRSVB(32); break;
-    }
-#undef PGX_TRSVB
+    Engine<P>::template launch_pipe<R>(T, upper, pys, prhs, py, px, lane[0]->err, all(sk), stream);
   }
 
   void solve_b_b(int l, const std::array<const P*, R>& rhs, const std::array<P*, R>& x,
@@ -3204,6 +3410,380 @@ int pgx_server_destroy(pgx_server srv) {
   return PGX_SUCCESS;
 }
 
+int pgx_gemslr_residual_history(pgx_handle h, int32_t capacity, double* hist, int32_t* count) {
+  if (!h || !count) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+  if (hist && capacity < 0) return fail(PGX_ERROR_INVALID_PARAM, "capacity %d < 0", capacity);
+  const std::vector<double> r = h->eng->residual_history();
+  *count = (int32_t)r.size();
+  if (hist) std::copy(r.begin(), r.begin() + std::min<size_t>(r.size(), (size_t)capacity), hist);
+  return PGX_SUCCESS;
+}
+
+int pgx_gemslr_describe(pgx_handle h, int32_t slot, char* buf, int32_t capacity, int32_t* length) {
+  return guarded("pgx_gemslr_describe", [&]() -> int {
+    if (!h || !length) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+    if (slot < 0 || slot >= h->nslots()) return fail(PGX_ERROR_INVALID_PARAM, "slot %d outside [0, %d)", slot, h->nslots());
+    const std::string d = h->slot(slot)->describe();
+    *length = (int32_t)d.size();
+    if (buf && capacity > 0) {
+      const size_t k = std::min<size_t>(d.size(), (size_t)capacity - 1);
+      memcpy(buf, d.data(), k);
+      buf[k] = 0;
+    }
+    return PGX_SUCCESS;
+  });
+}
+
+int pgx_gemslr_set_wait_limit(pgx_handle h, int64_t polls) {
+  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+  if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+  if (polls < 1 || polls > INT32_MAX) return fail(PGX_ERROR_INVALID_PARAM, "wait limit %lld outside [1, 2^31)", (long long)polls);
+  if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "the wait limit cannot change while a server is live");
+  PGX_CUDA(cudaSetDevice(h->device));
+  for (int i = 0; i < h->nslots(); i++) h->slot(i)->set_wait_limit((int)polls);
+  return PGX_SUCCESS;
+}
+
+// A lower triangular pass of trsv_kernel over two rows in which row 1 depends
+// on row 0 but only row 1 is scheduled: nothing ever publishes row 0, so the
+// wait on it can only end by its bound.  Every index stays inside the arrays
+// below (one group of 16 two-lane rows, one nonzero).
+int pgx_wait_selfcheck(int64_t polls, int32_t* status, double* wait_ms) {
+  if (!status) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (polls < 1 || polls > INT32_MAX) return fail(PGX_ERROR_INVALID_PARAM, "wait limit %lld outside [1, 2^31)", (long long)polls);
+  PGX_CUDA(cudaSetDevice(g_device));
+  constexpr int S = 2, G = kWarp / S;
+  int ord[G], rp[G + 1], cj[1] = {0};
+  double va[1] = {1.0}, rhs[2] = {1.0, 2.0};
+  for (int i = 0; i < G; i++) ord[i] = i == 0 ? 1 : -1;
+  for (int i = 0; i <= G; i++) rp[i] = i == 0 ? 0 : 1;
+  Arena ar;
+  int *d_ord = nullptr, *d_rp = nullptr, *d_cj = nullptr, *d_err = nullptr;
+  double *d_va = nullptr, *d_rhs = nullptr, *d_y = nullptr, *d_x = nullptr;
+  unsigned long long* d_ticket = nullptr;
+  cudaStream_t s = nullptr;
+  PGX_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } sg{s};
+  PGX_TRY(ar.upload(&d_ord, ord, G, s));
+  PGX_TRY(ar.upload(&d_rp, rp, G + 1, s));
+  PGX_TRY(ar.upload(&d_cj, cj, 1, s));
+  PGX_TRY(ar.upload(&d_va, va, 1, s));
+  PGX_TRY(ar.upload(&d_rhs, rhs, 2, s));
+  PGX_TRY(ar.alloc(&d_y, 2));
+  PGX_TRY(ar.alloc(&d_x, 2));
+  PGX_TRY(ar.zeros(&d_ticket, 2, s));
+  PGX_TRY(ar.zeros(&d_err, 1, s));
+  sentinel_fill_kernel<double><<<1, 32, 0, s>>>(2, d_y);
+  PGX_CUDA(cudaGetLastError());
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  PGX_CUDA(cudaEventCreate(&e0));
+  PGX_CUDA(cudaEventCreate(&e1));
+  PGX_CUDA(cudaEventRecord(e0, s));
+  trsv_kernel<double, S, false><<<1, 256, 0, s>>>(2, 1, d_ord, d_rp, d_cj, d_va, nullptr, d_rhs, nullptr, d_y, d_x,
+                                                  d_ticket, d_err, (int)polls, mk_skip());
+  const cudaError_t le = cudaGetLastError();
+  PGX_CUDA(cudaEventRecord(e1, s));
+  const cudaError_t se = cudaStreamSynchronize(s);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (le != cudaSuccess) return fail(PGX_ERROR_CUDA, "wait self-check launch: %s", cudaGetErrorString(le));
+  if (se != cudaSuccess) return fail(PGX_ERROR_CUDA, "wait self-check: %s", cudaGetErrorString(se));
+  int herr = 0;
+  PGX_CUDA(cudaMemcpy(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  *status = (herr & kErrTimeout) ? PGX_ERROR_TIMEOUT : (herr & kErrIndex) ? PGX_ERROR_INVALID_PARAM : PGX_SUCCESS;
+  if (wait_ms) *wait_ms = ms;
+  return PGX_SUCCESS;
+}
+
+// --------------------------------------------------------------- serving pool
+// Many resident preconditioned matrices served from one device-memory budget.
+// Each member (a committed handle) keeps its factors resident; solve slots
+// are created for a member when a request of it finds none idle and the
+// budget has room for the slot's work space and Krylov basis, and idle slots
+// of other members are released (least recently used first) when it has
+// not.  Requests wait in one queue and are admitted first-fit in arrival
+// order.
+struct pgx_pool_s {
+  struct Slot {
+    std::unique_ptr<EngineBase> eng;  // null: the member's handle itself (slot 0)
+    int64_t bytes = 0;                // counted against the budget (0 for slot 0, counted with the factors)
+    int64_t req = -1;                 // request in flight, -1 when idle
+    uint64_t last_used = 0;
+    EngineBase* get(pgx_handle h) { return eng ? eng.get() : h->eng.get(); }
+  };
+  struct Member {
+    pgx_handle h = nullptr;
+    int64_t base_bytes = 0;  // factors, the handle's own slot and its basis
+    int64_t slot_bytes = 0;  // one more slot, work space and basis
+    std::vector<Slot> slots;
+  };
+  struct Req {
+    int member;
+    double* x;
+    const double* b;
+    int location;
+    int64_t id;
+  };
+  int64_t budget = 0, in_use = 0, peak = 0;
+  int kdim = 50, maxits = 100, atol = 0;
+  double tol = 1e-6;
+  int device = 0;
+  uint64_t tick = 0;
+  std::vector<Member> members;
+  std::deque<Req> queue;
+  std::deque<std::pair<int64_t, pgx_result>> done;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread worker;
+  std::atomic<bool> running{false};
+  int worker_rc = 0;
+  std::string worker_msg;
+};
+
+static int pool_release_idle(pgx_pool p, int64_t need, int keep_member) {
+  // free idle extra slots of other members, least recently used first, until
+  // `need` more bytes fit the budget
+  while (p->in_use + need > p->budget) {
+    int bm = -1, bs = -1;
+    uint64_t best = UINT64_MAX;
+    for (int m = 0; m < (int)p->members.size(); m++) {
+      if (m == keep_member) continue;
+      auto& sl = p->members[m].slots;
+      for (int i = 1; i < (int)sl.size(); i++)
+        if (sl[i].req < 0 && sl[i].last_used < best) {
+          best = sl[i].last_used;
+          bm = m;
+          bs = i;
+        }
+    }
+    if (bm < 0) return 0;
+    p->in_use -= p->members[bm].slots[bs].bytes;
+    p->members[bm].slots.erase(p->members[bm].slots.begin() + bs);
+  }
+  return 1;
+}
+
+static int pool_step_locked(pgx_pool p, int32_t* n_active, int32_t* n_queued) {
+  PGX_CUDA(cudaSetDevice(p->device));
+  // 1. advance the slots in flight
+  int active = 0;
+  for (auto& m : p->members)
+    for (auto& sl : m.slots) {
+      if (sl.req < 0) continue;
+      bool fin = false;
+      pgx_result res;
+      memset(&res, 0, sizeof(res));
+      const int rc = sl.get(m.h)->poll(false, &fin, &res);
+      if (rc != PGX_SUCCESS || fin) {
+        if (rc != PGX_SUCCESS && res.status == PGX_SUCCESS) res.status = rc;
+        p->done.push_back({sl.req, res});
+        sl.req = -1;
+        sl.last_used = ++p->tick;
+      } else {
+        active++;
+      }
+    }
+  // 2. admit waiting requests, first fit in arrival order
+  for (auto it = p->queue.begin(); it != p->queue.end();) {
+    pgx_pool_s::Member& m = p->members[it->member];
+    int slot = -1;
+    for (int i = 0; i < (int)m.slots.size(); i++)
+      if (m.slots[i].req < 0) {
+        slot = i;
+        break;
+      }
+    if (slot < 0 && pool_release_idle(p, m.slot_bytes, it->member)) {
+      pgx_pool_s::Slot ns;
+      const int rc = m.h->eng->make_lanes_clone(m.h->im, 1, ns.eng);
+      if (rc == PGX_SUCCESS) {
+        ns.bytes = m.slot_bytes;
+        p->in_use += ns.bytes;
+        p->peak = std::max(p->peak, p->in_use);
+        m.slots.push_back(std::move(ns));
+        slot = (int)m.slots.size() - 1;
+      } else if (rc != PGX_ERROR_OOM) {
+        return rc;
+      }
+    }
+    if (slot < 0) {
+      ++it;  // no room for this one now; a later, smaller one may fit
+      continue;
+    }
+    pgx_pool_s::Slot& sl = m.slots[slot];
+    const int rc = sl.get(m.h)->begin(it->x, it->b, it->location, p->kdim, p->maxits, p->tol, p->atol, true);
+    if (rc != PGX_SUCCESS) {
+      pgx_result bad;
+      memset(&bad, 0, sizeof(bad));
+      bad.status = rc;
+      p->done.push_back({it->id, bad});
+    } else {
+      sl.req = it->id;
+      active++;
+    }
+    it = p->queue.erase(it);
+  }
+  if (n_active) *n_active = active;
+  if (n_queued) *n_queued = (int32_t)p->queue.size();
+  return PGX_SUCCESS;
+}
+
+int pgx_pool_create(int64_t budget_bytes, const double* params, pgx_pool* out) {
+  return guarded("pgx_pool_create", [&]() -> int {
+    if (!out) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    *out = nullptr;
+    if (budget_bytes <= 0) return fail(PGX_ERROR_INVALID_PARAM, "budget %lld <= 0", (long long)budget_bytes);
+    pgx_pool_s* p = new pgx_pool_s();
+    p->budget = budget_bytes;
+    p->device = g_device;
+    read_solver_params(params, p->kdim, p->maxits, p->tol, p->atol);
+    if (p->kdim < 1 || p->kdim > KMAX) {
+      delete p;
+      return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", p->kdim, KMAX);
+    }
+    *out = p;
+    return PGX_SUCCESS;
+  });
+}
+
+int pgx_pool_add(pgx_pool p, pgx_handle h, int32_t* index) {
+  return guarded("pgx_pool_add", [&]() -> int {
+    if (!p || !h || !index) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
+    if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "the handle is already served");
+    if (h->device != p->device) return fail(PGX_ERROR_INVALID_PARAM, "handle and pool are on different devices");
+    std::lock_guard<std::mutex> lock(p->mu);
+    pgx_pool_s::Member m;
+    m.h = h;
+    m.base_bytes = h->eng->device_bytes(p->kdim) + h->eng->layout_bytes();
+    for (auto& e : h->extra) m.base_bytes += e->slot_bytes(p->kdim);
+    m.slot_bytes = h->eng->slot_bytes(p->kdim);
+    if (p->in_use + m.base_bytes > p->budget)
+      return fail(PGX_ERROR_OOM, "the handle needs %lld bytes; the pool has %lld of %lld left", (long long)m.base_bytes,
+                  (long long)(p->budget - p->in_use), (long long)p->budget);
+    m.slots.resize(1);  // the handle's own slot
+    p->in_use += m.base_bytes;
+    p->peak = std::max(p->peak, p->in_use);
+    h->servers++;
+    p->members.push_back(std::move(m));
+    *index = (int32_t)p->members.size() - 1;
+    return PGX_SUCCESS;
+  });
+}
+
+int pgx_pool_submit(pgx_pool p, int32_t index, double* x, const double* b, int32_t location, int64_t request_id) {
+  if (!p || !x || !b) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (request_id < 0) return fail(PGX_ERROR_INVALID_PARAM, "request id %lld < 0", (long long)request_id);
+  if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
+    return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+  {
+    std::lock_guard<std::mutex> lock(p->mu);
+    if (index < 0 || index >= (int)p->members.size())
+      return fail(PGX_ERROR_INVALID_PARAM, "member %d outside [0, %d)", index, (int)p->members.size());
+    if (location == PGX_LOCATION_HOST && !all_finite(b, p->members[index].h->im.n))
+      return fail(PGX_ERROR_NOT_FINITE, "b is not finite");
+    p->queue.push_back({index, x, b, location, request_id});
+  }
+  p->cv.notify_one();
+  return PGX_SUCCESS;
+}
+
+int pgx_pool_step(pgx_pool p, int32_t* n_active, int32_t* n_queued) {
+  if (!p) return fail(PGX_ERROR_INVALID_PARAM, "null pool");
+  if (p->running) return fail(PGX_ERROR_FUNCTION_CALL, "the pool steps on its own thread (pgx_pool_stop first)");
+  std::lock_guard<std::mutex> lock(p->mu);
+  return pool_step_locked(p, n_active, n_queued);
+}
+
+int pgx_pool_start(pgx_pool p) {
+  if (!p) return fail(PGX_ERROR_INVALID_PARAM, "null pool");
+  if (p->running) return fail(PGX_ERROR_FUNCTION_CALL, "the pool thread is already running");
+  p->worker_rc = PGX_SUCCESS;
+  p->running = true;
+  p->worker = std::thread([p]() {
+    while (p->running) {
+      int32_t active = 0, queued = 0;
+      {
+        std::lock_guard<std::mutex> lock(p->mu);
+        const int rc = pool_step_locked(p, &active, &queued);
+        if (rc != PGX_SUCCESS && p->worker_rc == PGX_SUCCESS) {
+          p->worker_rc = rc;
+          p->worker_msg = g_last_error;
+        }
+      }
+      if (active == 0 && queued == 0) {
+        std::unique_lock<std::mutex> lock(p->mu);
+        p->cv.wait_for(lock, std::chrono::milliseconds(2), [p]() { return !p->running || !p->queue.empty(); });
+      } else {
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+      }
+    }
+  });
+  return PGX_SUCCESS;
+}
+
+int pgx_pool_stop(pgx_pool p) {
+  if (!p) return fail(PGX_ERROR_INVALID_PARAM, "null pool");
+  if (!p->running) return PGX_SUCCESS;
+  p->running = false;
+  p->cv.notify_all();
+  if (p->worker.joinable()) p->worker.join();
+  if (p->worker_rc != PGX_SUCCESS) return fail(p->worker_rc, "pool thread: %s", p->worker_msg.c_str());
+  return PGX_SUCCESS;
+}
+
+int pgx_pool_collect(pgx_pool p, int32_t max, int64_t* ids, pgx_result* results, int32_t* n) {
+  if (!p || !n) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  std::lock_guard<std::mutex> lock(p->mu);
+  int k = 0;
+  while (k < max && !p->done.empty()) {
+    if (ids) ids[k] = p->done.front().first;
+    if (results) results[k] = p->done.front().second;
+    p->done.pop_front();
+    k++;
+  }
+  *n = k;
+  return PGX_SUCCESS;
+}
+
+int pgx_pool_stats(pgx_pool p, int64_t* bytes_in_use, int64_t* peak_bytes, int32_t* slots) {
+  if (!p) return fail(PGX_ERROR_INVALID_PARAM, "null pool");
+  std::lock_guard<std::mutex> lock(p->mu);
+  if (bytes_in_use) *bytes_in_use = p->in_use;
+  if (peak_bytes) *peak_bytes = p->peak;
+  if (slots) {
+    int c = 0;
+    for (auto& m : p->members) c += (int)m.slots.size();
+    *slots = c;
+  }
+  return PGX_SUCCESS;
+}
+
+int pgx_pool_destroy(pgx_pool p) {
+  if (!p) return PGX_SUCCESS;
+  pgx_pool_stop(p);
+  cudaSetDevice(p->device);
+  for (auto& m : p->members) {
+    for (auto& sl : m.slots) {
+      if (sl.req < 0) continue;
+      bool fin = false;
+      pgx_result res;
+      while (!fin)
+        if (sl.get(m.h)->poll(true, &fin, &res) != PGX_SUCCESS) break;
+    }
+    m.slots.clear();  // the extra slots read the handle's factors: release them first
+    m.h->servers--;
+  }
+  delete p;
+  return PGX_SUCCESS;
+}
+
 int pgx_gemslr_kernel_stats(pgx_handle h, int32_t which, int32_t level, int32_t reps, double* avg_ms,
                             double* bytes) {
   if (!h || !avg_ms || !bytes) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
@@ -3332,28 +3912,76 @@ int pgx_params_read_args(int32_t argc, const char* const* argv, double* params) 
   });
 }
 
-int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double beta, double* y) {
-  if (!Ad || !x || !y) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
-  if (Ad->rows == 0) return PGX_SUCCESS;
-  const int S = spmv_lanes(Ad->nnz, Ad->rows);
-  const int grid = grid_for(Ad->rows, 256 / S, 148 * 16);
-  Skip sk = mk_skip();
-#define PGX_SPMV1(SS)                                                                                        \
-  spmv_kernel<double, double, double, double, SS><<<grid, 256>>>(Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, \
-                                                                 x, alpha, nullptr, nullptr, nullptr, nullptr, \
-                                                                 0.0, beta != 0.0 ? y : nullptr, beta, y,      \
-                                                                 nullptr, sk)
-  switch (S) {
-    case 2: PGX_SPMV1(2); break;
-    case 4: PGX_SPMV1(4); break;
-    case 8: PGX_SPMV1(8); break;
-    case 16: PGX_SPMV1(16); break;
-    default: PGX_SPMV1(32); break;
-  }
+int pgx_csr_spmv_plan(const pgx_csr* A, int32_t* lanes, int32_t* merge_path) {
+  return guarded("pgx_csr_spmv_plan", [&]() -> int {
+    if (!A || (A->rows > 0 && !A->rowptr)) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    if (A->rows < 0) return fail(PGX_ERROR_INVALID_PARAM, "rows %d < 0", A->rows);
+    const SpmvPlan p = spmv_plan(A->rows, A->rowptr);
+    if (lanes) *lanes = p.S;
+    if (merge_path) *merge_path = p.merge ? 1 : 0;
+    return PGX_SUCCESS;
+  });
+}
+
+int pgx_csr_spmv_device_variant(const pgx_csr* Ad, int32_t variant, double alpha, const double* x, double beta,
+                                double* y) {
+  return guarded("pgx_csr_spmv_device_variant", [&]() -> int {
+    if (!Ad || !x || !y) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    if (variant < 0 || variant > 2) return fail(PGX_ERROR_INVALID_OPTION, "unknown SpMV variant %d", variant);
+    if (Ad->rows == 0) return PGX_SUCCESS;
+    if (Ad->nnz > INT32_MAX || (long long)Ad->rows + Ad->nnz > INT32_MAX)
+      return fail(PGX_ERROR_INVALID_PARAM, "matrix too large for 32-bit indices");
+    // the plan needs the row pointer on the host
+    std::vector<int> rp(Ad->rows + 1);
+    PGX_CUDA(cudaMemcpy(rp.data(), Ad->rowptr, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost));
+    const SpmvPlan p = spmv_plan(Ad->rows, rp.data());
+    const bool merge = variant == 2 || (variant == 0 && p.merge);
+    Skip sk = mk_skip();
+    const double* b = beta != 0.0 ? y : nullptr;
+    if (merge) {
+      const int nt = merge_threads(Ad->rows, Ad->nnz);
+      Arena tmp;
+      int* crow = nullptr;
+      double* cval = nullptr;
+      PGX_TRY(tmp.alloc(&crow, (size_t)nt));
+      PGX_TRY(tmp.alloc(&cval, (size_t)nt));
+      merge_spmv_kernel<double, double, double, double><<<(nt + 255) / 256, 256>>>(
+          Ad->rows, (int)Ad->nnz, Ad->rowptr, Ad->colidx, Ad->values, x, alpha, b, beta, y, crow, cval, sk);
+      merge_spmv_fixup_kernel<double, double><<<grid_for(nt, 256, 148 * 8), 256>>>(nt, crow, cval, alpha, y, sk);
+      PGX_CUDA(cudaGetLastError());
+      PGX_CUDA(cudaDeviceSynchronize());
+      return PGX_SUCCESS;
+    }
+    const int S = p.S;
+    const int grid = grid_for(Ad->rows, 256 / S, 148 * 16);
+    // caller-owned arrays: 128-bit loads only where both are 16-byte aligned
+    // and the nonzeros fill whole 4-entry blocks
+    const bool vec = ((uintptr_t)Ad->colidx % 16 == 0) && ((uintptr_t)Ad->values % 16 == 0) && Ad->nnz % 4 == 0;
+#define PGX_SPMV1(SS)                                                                                             \
+  if (vec)                                                                                                        \
+    spmv_kernel<double, double, double, double, SS, true><<<grid, 256>>>(                                         \
+        Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, x, alpha, nullptr, nullptr, nullptr, nullptr, 0.0, b, beta, \
+        y, nullptr, sk);                                                                                          \
+  else                                                                                                            \
+    spmv_kernel<double, double, double, double, SS, false><<<grid, 256>>>(                                        \
+        Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, x, alpha, nullptr, nullptr, nullptr, nullptr, 0.0, b, beta, \
+        y, nullptr, sk)
+    switch (S) {
+      case 2: PGX_SPMV1(2); break;
+      case 4: PGX_SPMV1(4); break;
+      case 8: PGX_SPMV1(8); break;
+      case 16: PGX_SPMV1(16); break;
+      default: PGX_SPMV1(32); break;
+    }
 #undef PGX_SPMV1
-  PGX_CUDA(cudaGetLastError());
-  PGX_CUDA(cudaDeviceSynchronize());
-  return PGX_SUCCESS;
+    PGX_CUDA(cudaGetLastError());
+    PGX_CUDA(cudaDeviceSynchronize());
+    return PGX_SUCCESS;
+  });
+}
+
+int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double beta, double* y) {
+  return pgx_csr_spmv_device_variant(Ad, 0, alpha, x, beta, y);
 }
 
 }  // extern "C"

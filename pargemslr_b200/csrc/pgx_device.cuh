@@ -17,11 +17,12 @@ constexpr int kWarp = 32;
 constexpr int KMAX = 128;          // largest Krylov dimension a handle accepts
 constexpr int kTsThreads = 512;    // block size of the tall-skinny kernels
 constexpr int kTsMaxBlocks = 296;  // 2 blocks per SM on a 148-SM B200
-constexpr int kSpinLimit = 1 << 21;  // bounded waits in the sync-free triangular solve
+constexpr int kSpinLimit = 1 << 21;  // default bound of the waits in the sync-free triangular solves
 
 // status bits written by kernels into the handle's error word
-constexpr int kErrTimeout = 1;
-constexpr int kErrIndex = 2;
+constexpr int kErrTimeout = 1;  // a dependency wait of a cross-subdomain triangular solve gave up
+constexpr int kErrIndex = 2;    // an index check failed
+constexpr int kErrStage = 4;    // a staging wait of the per-subdomain triangular solve gave up
 
 struct Skip {
   const int* f0;
@@ -62,6 +63,7 @@ struct FgmresDev {
   double tol;
   double normb;
   double normr;    // Givens residual estimate (reference: normr)
+  double normr0;   // ||r0|| at the start of the solve (first entry of the residual history)
   double eps;      // numeric_limits<RealDataType>::epsilon() of the solver
   int absolute;
   int pad;
@@ -71,6 +73,7 @@ struct FgmresDev {
   double coefB[KMAX + 1];  // re-orthogonalisation coefficients
   double c[KMAX], s[KMAX], rs[KMAX + 1], y[KMAX];
   double H[(KMAX + 1) * KMAX];
+  double hist[KMAX];  // Givens estimate after each column of the current cycle (0 at a breakdown)
 };
 
 template <typename T>
@@ -98,7 +101,80 @@ __device__ __forceinline__ T warp_reduce(T v) {
 // Follows CsrMatrixPMatVecHostTemplate (ParGeMSLR SRC/matrices/matrixops.cpp:5139)
 // for one matrix; the two-matrix form fuses the Schur operator
 // C x - E (B^-1 F x) of GemslrClass::SchurMatVec (gemslr.cpp:3799-3960).
-template <typename TA, typename TX, typename TY, typename TC, int S>
+// Each lane issues the loads of its first kSpmvUnroll column indices, then
+// of the x entries they name, before it multiplies: the gathers of x are in
+// flight together.  A lane sums its entries in increasing order either way.
+constexpr int kSpmvUnroll = 4;
+
+template <typename TA, typename TX, typename TC, int S>
+__device__ __forceinline__ TC row_dot(int k1, int k2, int lane, const int* __restrict__ cj, const TA* __restrict__ va,
+                                      const TX* __restrict__ x) {
+  int c[kSpmvUnroll];
+  TA v[kSpmvUnroll];
+#pragma unroll
+  for (int u = 0; u < kSpmvUnroll; u++) {
+    const int k = k1 + lane + u * S;
+    c[u] = k < k2 ? __ldg(&cj[k]) : -1;
+    v[u] = k < k2 ? __ldg(&va[k]) : TA(0);
+  }
+  TX xv[kSpmvUnroll];
+#pragma unroll
+  for (int u = 0; u < kSpmvUnroll; u++) xv[u] = c[u] >= 0 ? x[c[u]] : TX(0);
+  TC acc = 0;
+#pragma unroll
+  for (int u = 0; u < kSpmvUnroll; u++)
+    if (c[u] >= 0) acc += (TC)v[u] * (TC)xv[u];
+  for (int k = k1 + lane + kSpmvUnroll * S; k < k2; k += S) acc += (TC)__ldg(&va[k]) * (TC)x[__ldg(&cj[k])];
+  return acc;
+}
+
+// The same dot product with 128-bit loads: the row's entries [k1, k2) lie in
+// the aligned 4-entry blocks k1/4 .. (k2+3)/4 - 1; the S lanes take the
+// blocks in turn, each loading a block's column indices as one int4 and its
+// values as one float4 or two double2, and mask the entries outside the row.
+// Needs cj and va 16-byte aligned and padded to a whole last block (the
+// library's own uploads are).  A lane sums its entries in increasing order.
+template <typename TA>
+__device__ __forceinline__ void load_block4(const TA* __restrict__ p, TA* v);
+template <>
+__device__ __forceinline__ void load_block4<float>(const float* __restrict__ p, float* v) {
+  const float4 a = __ldg((const float4*)p);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+}
+template <>
+__device__ __forceinline__ void load_block4<double>(const double* __restrict__ p, double* v) {
+  const double2 a = __ldg((const double2*)p), b = __ldg((const double2*)p + 1);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+
+template <typename TA, typename TX, typename TC, int S>
+__device__ __forceinline__ TC row_dot_vec(int k1, int k2, int lane, const int* __restrict__ cj,
+                                          const TA* __restrict__ va, const TX* __restrict__ x) {
+  TC acc = 0;
+  const int b1 = (k2 + 3) >> 2;
+  for (int bb = (k1 >> 2) + lane; bb < b1; bb += S) {
+    const int kb = bb << 2;
+    const int4 c4 = __ldg((const int4*)cj + bb);
+    TA v[4];
+    load_block4<TA>(va + kb, v);
+    const int c[4] = {c4.x, c4.y, c4.z, c4.w};
+    TX xv[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) xv[u] = (kb + u >= k1 && kb + u < k2) ? x[c[u]] : TX(0);
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (kb + u >= k1 && kb + u < k2) acc += (TC)v[u] * (TC)xv[u];
+  }
+  return acc;
+}
+
+template <typename TA, typename TX, typename TY, typename TC, int S, bool VEC>
 __global__ void __launch_bounds__(256) spmv_kernel(
     int nrows, const int* __restrict__ rp1, const int* __restrict__ cj1, const TA* __restrict__ va1,
     const TX* __restrict__ x1, TC alpha, const int* __restrict__ rp2, const int* __restrict__ cj2,
@@ -111,14 +187,15 @@ __global__ void __launch_bounds__(256) spmv_kernel(
   const TC xs = xscale ? (TC)(*xscale) : (TC)1;
   for (int row = blockIdx.x * groups_per_block + threadIdx.x / S; row < nrows;
        row += gridDim.x * groups_per_block) {
-    TC acc = 0;
-    const int k1 = rp1[row], k2 = rp1[row + 1];
-    for (int k = k1 + lane; k < k2; k += S) acc += (TC)va1[k] * (TC)x1[cj1[k]];
+    const int k1 = __ldg(&rp1[row]), k2 = __ldg(&rp1[row + 1]);
+    TC acc = VEC ? row_dot_vec<TA, TX, TC, S>(k1, k2, lane, cj1, va1, x1)
+                 : row_dot<TA, TX, TC, S>(k1, k2, lane, cj1, va1, x1);
     acc = group_reduce(acc, S, wlane);
     TC acc2 = 0;
     if (rp2) {
-      const int q1 = rp2[row], q2 = rp2[row + 1];
-      for (int k = q1 + lane; k < q2; k += S) acc2 += (TC)va2[k] * (TC)x2[cj2[k]];
+      const int q1 = __ldg(&rp2[row]), q2 = __ldg(&rp2[row + 1]);
+      acc2 = VEC ? row_dot_vec<TA, TX, TC, S>(q1, q2, lane, cj2, va2, x2)
+                 : row_dot<TA, TX, TC, S>(q1, q2, lane, cj2, va2, x2);
       acc2 = group_reduce(acc2, S, wlane);
     }
     if (lane == 0) {
@@ -127,6 +204,86 @@ __global__ void __launch_bounds__(256) spmv_kernel(
       if (b) v += beta * (TC)b[row];
       y[row] = (TY)v;
     }
+  }
+}
+
+// ---------------------------------------------------- merge-path CSR SpMV
+// For matrices whose row lengths are skewed (a few very long rows among
+// short ones), the row-per-group kernel leaves most lanes idle on the short
+// rows and serialises the long ones.  The merge-path SpMV (Merrill and
+// Garland, "Merge-based parallel sparse matrix-vector multiplication", SC16)
+// gives every thread the same number of merge items, where the items are
+// the n row ends and the nnz nonzeros taken in merge order (a nonzero k of
+// row r comes before the end of row r).  A thread finds its start on the
+// merge path by a binary search on its diagonal, then consumes its items:
+// rows that end in its range are written at once; the partial sum of the
+// row it stops inside is its carry, added by merge_spmv_fixup_kernel.
+// y = alpha * A x + beta * b (b may be absent or alias y).
+constexpr int kMergeItems = 16;  // merge items per thread
+
+__device__ __forceinline__ void merge_path_search(int diag, const int* __restrict__ rp, int nrows, int nnz, int* row,
+                                                  int* k) {
+  // the number of row ends among the first `diag` merge items: the largest i
+  // with rp[i] (the end of row i-1) <= diag - i
+  int lo = max(diag - nnz, 0), hi = min(diag, nrows);
+  while (lo < hi) {
+    const int pivot = (lo + hi) >> 1;
+    if (__ldg(&rp[pivot + 1]) <= diag - pivot - 1)
+      lo = pivot + 1;
+    else
+      hi = pivot;
+  }
+  *row = min(lo, nrows);
+  *k = diag - *row;
+}
+
+template <typename TA, typename TX, typename TY, typename TC>
+__global__ void __launch_bounds__(256) merge_spmv_kernel(
+    int nrows, int nnz, const int* __restrict__ rp, const int* __restrict__ cj, const TA* __restrict__ va,
+    const TX* __restrict__ x, TC alpha, const TY* b, TC beta, TY* y, int* __restrict__ carry_row,
+    TC* __restrict__ carry_val, Skip skip) {
+  if (skip.on()) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)nrows + nnz;
+  const long long d0 = (long long)t * kMergeItems;
+  if (d0 >= total) return;
+  const int d1 = (int)min(d0 + kMergeItems, total);
+  int r, k, r1, k1;
+  merge_path_search((int)d0, rp, nrows, nnz, &r, &k);
+  merge_path_search(d1, rp, nrows, nnz, &r1, &k1);
+  TC acc = 0;
+  int rend = r < nrows ? __ldg(&rp[r + 1]) : nnz;
+  while (r < r1 || k < k1) {
+    if (r < nrows && k < rend && k < k1) {
+      acc += (TC)__ldg(&va[k]) * (TC)x[__ldg(&cj[k])];
+      k++;
+    } else {
+      // row r ends inside this range: its sum here plus the carries of the
+      // threads before it that stopped inside the row
+      TC v = alpha * acc;
+      if (b) v += beta * (TC)b[r];
+      y[r] = (TY)v;
+      acc = 0;
+      r++;
+      rend = r < nrows ? __ldg(&rp[r + 1]) : nnz;
+    }
+  }
+  carry_row[t] = r < nrows ? r : -1;
+  carry_val[t] = acc;
+}
+
+// y[row] += alpha * (carries of that row, in thread order): one thread per
+// run of equal rows, so the sum is deterministic
+template <typename TY, typename TC>
+__global__ void merge_spmv_fixup_kernel(int nthreads, const int* __restrict__ carry_row,
+                                        const TC* __restrict__ carry_val, TC alpha, TY* y, Skip skip) {
+  if (skip.on()) return;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += gridDim.x * blockDim.x) {
+    const int row = carry_row[t];
+    if (row < 0 || (t > 0 && carry_row[t - 1] == row)) continue;
+    TC s = 0;
+    for (int u = t; u < nthreads && carry_row[u] == row; u++) s += carry_val[u];
+    y[row] = (TY)((TC)y[row] + alpha * s);
   }
 }
 
@@ -154,7 +311,8 @@ __global__ void __launch_bounds__(256) spmv_kernel(
 // claimed earlier by warps that are running, so the waits always end.  The
 // last warp to leave resets the counter (ticket[0]) and the exit count
 // (ticket[1]) for the next launch, whatever the grid size.  Waits are
-// bounded; on expiry the kernel records kErrTimeout and finishes.
+// bounded by spin_limit polls (kSpinLimit unless the handle sets another);
+// on expiry the kernel records kErrTimeout and finishes.
 template <typename T>
 struct Sentinel;
 template <>
@@ -193,7 +351,8 @@ template <typename T, int S, bool UPPER>
 __global__ void __launch_bounds__(256) trsv_kernel(
     int n, int ngroups, const int* __restrict__ ord, const int* __restrict__ rp, const int* __restrict__ cj,
     const T* __restrict__ va, const T* __restrict__ dinv, const T* __restrict__ rhs,
-    const double* __restrict__ rhs_scale, T* y, T* x, unsigned long long* ticket, int* err, Skip skip) {
+    const double* __restrict__ rhs_scale, T* y, T* x, unsigned long long* ticket, int* err, int spin_limit,
+    Skip skip) {
   constexpr int G = kWarp / S;  // rows per warp
   if (skip.on()) return;
   const int lane = threadIdx.x & (kWarp - 1);
@@ -221,7 +380,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(
         if (Sentinel<T>::is(v)) {
           int spins = 0;
           do {
-            if (++spins > kSpinLimit || (*(volatile int*)err & kErrTimeout)) {
+            if (++spins > spin_limit || (*(volatile int*)err & kErrTimeout)) {
               atomicOr(err, kErrTimeout);
               v = 0;
               break;
@@ -307,7 +466,7 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
     const int* __restrict__ ord, const int* __restrict__ rp,  // rp: segment-relative row pointers
     const int* __restrict__ cj, const T* __restrict__ va, const int* __restrict__ lvb,  // lvb: segment-relative
     const T* __restrict__ dinv, const T* __restrict__ rhs, const double* __restrict__ rhs_scale, T* y, T* x,
-    unsigned long long* ticket, int* err, Skip skip) {
+    unsigned long long* ticket, int* err, int spin_limit, Skip skip) {
   if (skip.on()) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NNZ = SegCfg<T>::nnz;
@@ -402,7 +561,7 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
             if (Sentinel<T>::is(v)) {
               int spins = 0;
               do {
-                if (++spins > kSpinLimit || (*(volatile int*)err & kErrTimeout)) {
+                if (++spins > spin_limit || (*(volatile int*)err & kErrTimeout)) {
                   atomicOr(err, kErrTimeout);
                   v = 0;
                   break;
@@ -447,39 +606,58 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
 // ILU factor are short-range: for the RCM-ordered subdomains of a 3D problem
 // the median distance between a row and the rows it needs is ~10^3
 // positions and almost all are within 10^4.  So one CTA walks a whole
-// subdomain (trsv_comp_kernel below).
-#ifndef PGX_COMP_THREADS
-#define PGX_COMP_THREADS 1024
+// subdomain (trsv_pipe_kernel below), for R right-hand sides at once.
+#ifndef PGX_PIPE_THREADS
+#define PGX_PIPE_THREADS 512
 #endif
-// 1024 threads: one CTA per SM; 512 threads: two CTAs per SM (registers and
-// shared memory sized for it), for many concurrent solves
-constexpr int kCompThreads = PGX_COMP_THREADS;
-constexpr int kCompMinBlocks = kCompThreads >= 1024 ? 1 : 2;
-constexpr int kUnroll = 4;  // operands per lane loaded before any is used
-// Operand indices into the ring are checked once on the host when the layout
-// is built; the kernels clamp them into the shared array, so a damaged layout
-// can give wrong values but never an access outside shared memory.
-template <typename T>
-struct CompCfg {
-  static constexpr bool big = kCompThreads >= 1024;
-  static constexpr int ring = big ? 8192 : 4096;              // 32/16 KB (f32), 64/32 KB (f64)
-  static constexpr int far = big ? 1024 : 512;                // far operands per chunk (per buffer)
-  static constexpr int nnz = sizeof(T) == 8 ? (big ? 4096 : 2048) : (big ? 8192 : 4096);  // per chunk buffer
-  static constexpr int rows = sizeof(T) == 8 ? (big ? 768 : 384) : (big ? 1024 : 512);   // incl. padding
-  // per buffer: va[nnz] T | sb[rows] T | sd[rows] T | cj[nnz] int | ord[rows] int | rp[rows+4] int | lvb[rows+4] int
+// one CTA per subdomain; the SM's other thread slots stay free for other kernels
+constexpr int kPipeThreads = PGX_PIPE_THREADS;
+constexpr int kPipeStages = 4;     // chunks in flight: the one being solved and three being staged
+constexpr int kUnroll = 4;         // operands per lane loaded before any is used
+constexpr long long kMbarWaitCycles = 1ll << 31;  // bound of a wait on a staging barrier: about 1 s
+
+template <typename T, int R>
+struct __align__(sizeof(T) * R <= 16 ? sizeof(T) * R : 16) VecR {
+  T v[R];
+};
+template <typename T, int R>
+struct PtrR {
+  T* p[R];
+};
+
+// Shared-memory plan of the pipelined solve for value type T and R
+// right-hand sides: a ring of the last `ring` results (R values per schedule
+// position) followed by three far-operand buffers of `far` entries, then
+// kPipeStages staging buffers of one chunk each (at most `nnz` nonzeros and
+// `rows` rows, padding included).  Operand indices into the ring are checked
+// once on the host when the layout is built; the kernel clamps them into the
+// shared array, so a damaged layout can give wrong values but never an
+// access outside shared memory.
+template <typename T, int R>
+struct PipeCfg {
+  static constexpr bool d = sizeof(T) == 8;
+  static constexpr int ring = d ? (R == 1 ? 8192 : R == 2 ? 4096 : 2048) : (R == 4 ? 4096 : 8192);
+  static constexpr int far = d ? (R == 1 ? 512 : 256) : 512;
+  static constexpr int nnz = d ? (R == 4 ? 1536 : 2048) : (R == 1 ? 4096 : R == 2 ? 3072 : 2560);
+  static constexpr int rows = d ? 256 : (R == 1 ? 512 : R == 2 ? 384 : 320);
+  // per stage: va[nnz] T | sb[R][rows] T | sd[rows] T | cj[nnz] | ord[rows] | rp[rows+4] | lvb[rows+4] | fc[far]
   static constexpr size_t buf_bytes =
-      sizeof(T) * (size_t)(nnz + 2 * rows) + sizeof(int) * (size_t)(nnz + rows + 2 * (rows + 4));
-  // ring and the two far-operand buffers are one array: operand index -(c+1)
-  static constexpr size_t bytes = sizeof(T) * (size_t)(ring + 2 * far) + 2 * buf_bytes;
-  static_assert(bytes * kCompMinBlocks <= 227 * 1024, "per-subdomain solve exceeds the shared memory of an SM");
-  static_assert(far <= kCompThreads && rows <= kCompThreads, "one gather per thread");
+      sizeof(T) * (size_t)(nnz + (R + 1) * rows) + sizeof(int) * (size_t)(nnz + rows + 2 * (rows + 4) + far);
+  static constexpr size_t ring_bytes = sizeof(T) * R * (size_t)(ring + 3 * far);
+  static constexpr size_t bytes = ring_bytes + kPipeStages * buf_bytes;
+  static_assert(bytes <= 227 * 1024, "pipelined per-subdomain solve exceeds the shared memory of a CTA");
+  static_assert(far <= kPipeThreads && rows <= kPipeThreads, "one gather per thread");
+  static_assert((ring & (ring - 1)) == 0, "ring size must be a power of two");
+  static_assert(nnz % 4 == 0 && rows % 4 == 0 && far % 4 == 0 && buf_bytes % 16 == 0 && ring_bytes % 16 == 0,
+                "every staged array starts on a 16-byte boundary");
 };
 
 // Per-chunk metadata, two int4 per chunk: {row0, rp0, nnz0, lv0} and
 // {pos0, far0, 0, 0}: first slot of the chunk in the row list, the row
 // pointers, the nonzeros and the level boundaries; its first schedule
 // position; its first far operand.  One record past the last chunk closes the
-// ranges.
+// ranges.  Every range starts on a 16-byte boundary and spans a multiple of
+// 16 bytes (padded on the host), so each is one bulk copy.
 struct ChunkMeta {
   int row0, rp0, nnz0, lv0, pos0, far0;
 };
@@ -511,24 +689,62 @@ __device__ __forceinline__ void cp_async_elem(T* dst, const T* src) {
     cp_async4(dst, src);
 }
 
-template <typename T>
-struct CompBuf {
-  T *va, *sb, *sd;
-  int *cj, *ord, *rp, *lvb;
-};
+// mbarrier and bulk-copy (TMA, non-tensor) helpers.  The copies read this
+// GPU's own global memory only.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false (and kErrStage recorded) if the phase did not
+// complete within kMbarWaitCycles SM clocks
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int* err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (clock64() - t0 < kMbarWaitCycles)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicOr(err, kErrStage);
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
 
-template <typename T>
-__device__ __forceinline__ CompBuf<T> comp_buf(unsigned char* base, int which) {
-  using C = CompCfg<T>;
-  unsigned char* b = base + sizeof(T) * (size_t)(C::ring + 2 * C::far) + (size_t)which * C::buf_bytes;
-  CompBuf<T> o;
+template <typename T, int R>
+struct PipeBuf {
+  T *va, *sb, *sd;  // sb: R arrays of `rows`; sd: inverse diagonal (upper) or upper-pass slots (lower, as int)
+  int *cj, *ord, *rp, *lvb, *fc;
+};
+template <typename T, int R, typename C = PipeCfg<T, R>>
+__device__ __forceinline__ PipeBuf<T, R> pipe_buf(unsigned char* base, int stage) {
+  unsigned char* b = base + C::ring_bytes + (size_t)stage * C::buf_bytes;
+  PipeBuf<T, R> o;
   o.va = (T*)b;
   o.sb = o.va + C::nnz;
-  o.sd = o.sb + C::rows;
+  o.sd = o.sb + R * C::rows;
   o.cj = (int*)(o.sd + C::rows);
   o.ord = o.cj + C::nnz;
   o.rp = o.ord + C::rows;
   o.lvb = o.rp + C::rows + 4;
+  o.fc = o.lvb + C::rows + 4;
   return o;
 }
 
@@ -537,279 +753,148 @@ struct CompArrays {
   const int *ord, *rp, *cj, *lvb, *uslot, *far_col;
 };
 
-// all threads: issue the bulk copies of the chunk [m, me) into buffer b
-template <typename T, bool UPPER>
-__device__ __forceinline__ void comp_stage_bulk(const CompBuf<T>& b, const ChunkMeta& m, const ChunkMeta& me,
-                                                const CompArrays& g, const T* __restrict__ va,
-                                                const T* __restrict__ dslot, const T* yslot) {
-  stage16(b.va, va + m.nnz0, (me.nnz0 - m.nnz0) * (int)sizeof(T));
-  stage16(b.cj, g.cj + m.nnz0, (me.nnz0 - m.nnz0) * 4);
-  stage16(b.ord, g.ord + m.row0, (me.row0 - m.row0) * 4);
-  stage16(b.rp, g.rp + m.rp0, (me.rp0 - m.rp0) * 4);
-  stage16(b.lvb, g.lvb + m.lv0, (me.lv0 - m.lv0) * 4);
+// one thread: stage chunk [m, me) into buffer b with bulk copies completing on
+// bar (the byte count is announced first)
+template <typename T, int R, bool UPPER>
+__device__ __forceinline__ void pipe_issue(const PipeBuf<T, R>& b, const ChunkMeta& m, const ChunkMeta& me,
+                                           const CompArrays& g, const T* __restrict__ va, const T* __restrict__ dslot,
+                                           const PtrR<T, R>& yslot, unsigned long long* bar) {
+  const unsigned nz = (unsigned)(me.nnz0 - m.nnz0), nr = (unsigned)(me.row0 - m.row0);
+  const unsigned np = (unsigned)(me.rp0 - m.rp0), nv = (unsigned)(me.lv0 - m.lv0), nf = (unsigned)(me.far0 - m.far0);
+  unsigned total = nz * (sizeof(T) + 4) + nr * 4 + np * 4 + nv * 4 + nf * 4 + nr * (UPPER ? sizeof(T) : 4);
+  if (UPPER) total += R * nr * (unsigned)sizeof(T);
+  mbar_arrive_expect_tx(bar, total);
+  if (nz) {
+    bulk_g2s(b.va, va + m.nnz0, nz * (unsigned)sizeof(T), bar);
+    bulk_g2s(b.cj, g.cj + m.nnz0, nz * 4, bar);
+  }
+  bulk_g2s(b.ord, g.ord + m.row0, nr * 4, bar);
+  bulk_g2s(b.rp, g.rp + m.rp0, np * 4, bar);
+  bulk_g2s(b.lvb, g.lvb + m.lv0, nv * 4, bar);
+  if (nf) bulk_g2s(b.fc, g.far_col + m.far0, nf * 4, bar);
   if (UPPER) {
-    stage16(b.sd, dslot + m.row0, (me.row0 - m.row0) * (int)sizeof(T));
-    stage16(b.sb, yslot + m.row0, (me.row0 - m.row0) * (int)sizeof(T));
+    bulk_g2s(b.sd, dslot + m.row0, nr * (unsigned)sizeof(T), bar);
+#pragma unroll
+    for (int r = 0; r < R; r++) bulk_g2s(b.sb + r * PipeCfg<T, R>::rows, yslot.p[r] + m.row0, nr * (unsigned)sizeof(T), bar);
   } else {
-    stage16(b.sd, g.uslot + m.row0, (me.row0 - m.row0) * 4);  // upper-pass slot of each row (ints in sd)
+    bulk_g2s(b.sd, g.uslot + m.row0, nr * 4, bar);
   }
 }
 
 // One CTA per subdomain solves its rows level by level (the schedule of
-// IluClass::BuildLevels, ilu.cpp:832-1062, restricted to the subdomain): a
-// lower pass y = L^-1 rhs or an upper pass x = D U^-1 y.  Results live in a
-// shared-memory ring indexed by schedule position, so a dependency on the
-// last `ring` positions is a shared-memory read.  An older ("far") operand
-// lies, by construction on the host, before the start of the previous chunk:
-// it was published to global memory before that chunk began, so it is
-// gathered into the far buffer while the previous chunk is being solved and
-// is read from there.  Column indices are encoded as -(index + 1) into the
-// ring-plus-far array.
+// IluClass::BuildLevels, ilu.cpp:832-1062, restricted to the subdomain),
+// for R right-hand sides at once: a lower pass y = L^-1 rhs or an upper pass
+// x = D U^-1 y.  Each staged factor entry is read once and applied to all R
+// vectors.  Results live in a shared-memory ring indexed by schedule
+// position, so a dependency on the last `ring` positions is a shared-memory
+// read (one vector load for the R values).  An older ("far") operand lies,
+// by construction on the host, before the start of the previous chunk: it
+// was published to global memory before that chunk began, so it is gathered
+// into the far buffer while the previous chunk is being solved.  Column
+// indices are encoded as -(index + 1) into the ring-plus-far array.
 //
-// The subdomain's schedule is cut into chunks that fit a staging buffer;
-// there are two buffers.  While the CTA sweeps the levels of chunk k (one
-// barrier per level), the copies of chunk k+1 are in flight: the bulk
-// arrays at once, and, after the first level, the far operands and (lower
-// pass) the right-hand side gathered through the row list.  The chunk
-// metadata is loaded three chunks ahead.  At a chunk boundary the CTA only
-// publishes the chunk's results and waits for its copies.  No CTA waits on
-// another: no tickets, no deadlock.
-template <typename T, int S, bool UPPER>
-__global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_kernel(
-    int n, const int* __restrict__ comp_ch0,  // ncomp+1: chunk range of each subdomain
-    CompArrays g, const T* __restrict__ va, const T* __restrict__ dslot, T* yslot, const T* rhs,
-    const double* __restrict__ rhs_scale, T* y, T* x, int* err, Skip skip) {
-  if (skip.on()) return;
-  using C = CompCfg<T>;
-  constexpr int RF = C::ring + 2 * C::far;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* ring = (T*)smem_raw;  // ring, then far buffer 0, then far buffer 1
-  const int tid = threadIdx.x, lane = tid & 31;
-  const int c0 = comp_ch0[blockIdx.x], c1 = comp_ch0[blockIdx.x + 1];
-  T* out = UPPER ? x : y;  // this pass's result, also the store of far operands
-  const double rs = rhs_scale ? *rhs_scale : 1.0;
-  if (c0 >= c1) return;
-  ChunkMeta m0 = load_meta(g.meta, c0), m1 = load_meta(g.meta, c0 + 1);
-  ChunkMeta m2 = c0 + 2 <= c1 ? load_meta(g.meta, c0 + 2) : m1;
-  {
-    // the first chunk of a subdomain has no far operands
-    const CompBuf<T> b = comp_buf<T>(smem_raw, 0);
-    comp_stage_bulk<T, UPPER>(b, m0, m1, g, va, dslot, yslot);
-    if (!UPPER && tid < m1.row0 - m0.row0) {
-      const int r = __ldg(&g.ord[m0.row0 + tid]);
-      if (r >= 0) cp_async_elem(&b.sb[tid], &rhs[r]);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-  }
-  const int sl = tid & (S - 1), group = tid / S, ngroups = kCompThreads / S;
-  for (int ch = c0; ch < c1; ch++) {
-    const int bi = (ch - c0) & 1;
-    const CompBuf<T> nb = comp_buf<T>(smem_raw, bi ^ 1);
-    int rhs_row = -1, far_col = -1;
-    if (ch + 1 < c1) {
-      comp_stage_bulk<T, UPPER>(nb, m1, m2, g, va, dslot, yslot);
-      if (!UPPER && tid < m2.row0 - m1.row0) rhs_row = __ldg(&g.ord[m1.row0 + tid]);
-      if (tid < m2.far0 - m1.far0) far_col = __ldg(&g.far_col[m1.far0 + tid]);
-    }
-    const ChunkMeta m3 = ch + 3 <= c1 ? load_meta(g.meta, ch + 3) : m2;
-    const CompBuf<T> b = comp_buf<T>(smem_raw, bi);
-    const int pos0 = m0.pos0;
-    const int nl = m1.lv0 - m0.lv0;
-    bool gathered = false;
-    int a = b.lvb[0], e = nl > 1 ? b.lvb[1] : a;
-    for (int lv = 0; lv + 1 < nl; lv++) {
-      if (a >= e) break;  // padding after the last boundary
-      const int e_next = lv + 2 < nl ? b.lvb[lv + 2] : e;
-      for (int i = a + group; i < e; i += ngroups) {
-        const int k1 = b.rp[i], k2 = b.rp[i + 1];
-        // up to kUnroll operands per lane with independent loads, then the rest
-        T acc = 0;
-        int q[kUnroll];
-        T v[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
-          const int k = k1 + sl + u * S;
-          q[u] = k < k2 ? -b.cj[k] - 1 : 0;
-          v[u] = k < k2 ? b.va[k] : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
-          if (k1 + sl + u * S < k2) {  // never read an unwritten ring slot
-            acc += v[u] * ring[min((unsigned)q[u], (unsigned)(RF - 1))];
-          }
-        }
-        for (int k = k1 + sl + kUnroll * S; k < k2; k += S) {
-          const int qq = -b.cj[k] - 1;
-          acc += b.va[k] * ring[min((unsigned)qq, (unsigned)(RF - 1))];
-        }
-        acc = group_reduce(acc, S, lane);
-        if (sl == 0) {
-          // only the writing lane reads the row's right-hand side and inverse diagonal
-          T o;
-          if (UPPER) {
-            o = (b.sb[i] - acc) * b.sd[i];
-          } else {
-            T bb = b.sb[i];
-            if (rhs_scale) bb = (T)((double)bb * rs);
-            o = bb - acc;
-          }
-          ring[(pos0 + i) & (C::ring - 1)] = o;
-        }
-      }
-      __syncthreads();
-      if (!gathered) {
-        // the next chunk's gathers, once the loads of their indices had a level to land
-        gathered = true;
-        if (rhs_row >= 0) cp_async_elem(&nb.sb[tid], &rhs[rhs_row]);
-        if (far_col >= 0) {
-          if ((unsigned)far_col < (unsigned)n)
-            cp_async_elem(&ring[C::ring + (bi ^ 1) * C::far + tid], &out[far_col]);
-          else
-            atomicOr(err, kErrIndex);
-        }
-      }
-      a = e;
-      e = e_next;
-    }
-    if (!gathered) {
-      if (rhs_row >= 0) cp_async_elem(&nb.sb[tid], &rhs[rhs_row]);
-      if (far_col >= 0 && (unsigned)far_col < (unsigned)n)
-        cp_async_elem(&ring[C::ring + (bi ^ 1) * C::far + tid], &out[far_col]);
-    }
-    // publish the chunk's results from the ring: natural order (far operands
-    // and the consumer) and, for the lower pass, the upper pass's slot order
-    for (int i = tid; i < m1.row0 - m0.row0; i += blockDim.x) {
-      const int r = b.ord[i];
-      if (r < 0) continue;
-      const T o = ring[(pos0 + i) & (C::ring - 1)];
-      out[r] = o;
-      if (!UPPER) yslot[((const int*)b.sd)[i]] = o;
-    }
-    if (ch + 1 < c1) {
-      cp_async_wait_all();
-      __syncthreads();
-    }
-    m0 = m1;
-    m1 = m2;
-    m2 = m3;
-  }
-}
-
-// --------------------- per-subdomain triangular solve, several right-hand sides
-// trsv_comp_batch_kernel: trsv_comp_kernel for R right-hand sides at once.
-// The factor's rows, columns and values are staged and read once per chunk
-// and applied to all R vectors; the ring holds R values per schedule
-// position (one vector load per operand).  Shared-memory sizes shrink with R
-// (CompCfgR), so the layout is built for the R it serves.
-template <typename T, int R>
-struct __align__(sizeof(T) * R <= 16 ? sizeof(T) * R : 16) VecR {
-  T v[R];
-};
-template <typename T, int R>
-struct PtrR {
-  T* p[R];
-};
-template <typename T, int R>
-struct CompCfgR {
-  static constexpr bool d = sizeof(T) == 8;
-  static constexpr int ring = R <= 1 ? CompCfg<T>::ring : (d ? (R == 2 ? 4096 : 2048) : (R == 2 ? 8192 : 4096));
-  static constexpr int far = R <= 1 ? CompCfg<T>::far : (d ? (R == 2 ? 512 : 256) : (R == 2 ? 1024 : 512));
-  static constexpr int nnz = R <= 1 ? CompCfg<T>::nnz : (d ? (R == 2 ? 3072 : 2048) : (R == 2 ? 5632 : 4096));
-  static constexpr int rows = R <= 1 ? CompCfg<T>::rows : (d ? (R == 2 ? 768 : 512) : (R == 2 ? 1024 : 768));
-  // per buffer: va[nnz] T | sb[R][rows] T | sd[rows] T | cj[nnz] int | ord[rows] int | rp[rows+4] int | lvb[rows+4] int
-  static constexpr size_t buf_bytes =
-      sizeof(T) * (size_t)(nnz + (R + 1) * rows) + sizeof(int) * (size_t)(nnz + rows + 2 * (rows + 4));
-  static constexpr size_t bytes = sizeof(T) * R * (size_t)(ring + 2 * far) + 2 * buf_bytes;
-  static_assert(bytes <= 227 * 1024, "batched per-subdomain solve exceeds the shared memory of one CTA");
-  static_assert(far <= kCompThreads && rows <= kCompThreads, "one gather per thread");
-};
-
-template <typename T, int R>
-struct CompBufR {
-  T *va, *sb, *sd;  // sb: R arrays of `rows`
-  int *cj, *ord, *rp, *lvb;
-};
-template <typename T, int R, typename C = CompCfgR<T, R>>
-__device__ __forceinline__ CompBufR<T, R> comp_buf_r(unsigned char* base, int which) {
-  unsigned char* b = base + sizeof(T) * R * (size_t)(C::ring + 2 * C::far) + (size_t)which * C::buf_bytes;
-  CompBufR<T, R> o;
-  o.va = (T*)b;
-  o.sb = o.va + C::nnz;
-  o.sd = o.sb + R * C::rows;
-  o.cj = (int*)(o.sd + C::rows);
-  o.ord = o.cj + C::nnz;
-  o.rp = o.ord + C::rows;
-  o.lvb = o.rp + C::rows + 4;
-  return o;
-}
-
-template <typename T, int R, bool UPPER, typename C = CompCfgR<T, R>>
-__device__ __forceinline__ void comp_stage_bulk_r(const CompBufR<T, R>& b, const ChunkMeta& m, const ChunkMeta& me,
-                                                  const CompArrays& g, const T* __restrict__ va,
-                                                  const T* __restrict__ dslot, const PtrR<T, R>& yslot) {
-  stage16(b.va, va + m.nnz0, (me.nnz0 - m.nnz0) * (int)sizeof(T));
-  stage16(b.cj, g.cj + m.nnz0, (me.nnz0 - m.nnz0) * 4);
-  stage16(b.ord, g.ord + m.row0, (me.row0 - m.row0) * 4);
-  stage16(b.rp, g.rp + m.rp0, (me.rp0 - m.rp0) * 4);
-  stage16(b.lvb, g.lvb + m.lv0, (me.lv0 - m.lv0) * 4);
-  if (UPPER) {
-    stage16(b.sd, dslot + m.row0, (me.row0 - m.row0) * (int)sizeof(T));
-#pragma unroll
-    for (int r = 0; r < R; r++) stage16(b.sb + r * C::rows, yslot.p[r] + m.row0, (me.row0 - m.row0) * (int)sizeof(T));
-  } else {
-    stage16(b.sd, g.uslot + m.row0, (me.row0 - m.row0) * 4);
-  }
-}
-
-template <typename T, int S, bool UPPER, int R, typename C = CompCfgR<T, R>>
-__global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_kernel(
+// The subdomain's schedule is cut into chunks.  One thread stages chunk
+// c + kPipeStages - 1 with bulk copies (completing on that stage's mbarrier)
+// as soon as chunk c - 1 is done, so the factor streams in well ahead of the
+// solve; at the start of chunk c the CTA gathers what needs an index (the
+// lower pass's right-hand side through the row list, the far operands) for
+// chunk c + 1.  A chunk's end coincides with the barrier of its last level:
+// a chunk boundary costs no barrier of its own.  Each row's writing lanes
+// publish its result to global memory at once (natural order, and the upper
+// pass's slot order in the lower pass).  No CTA waits on another.
+template <typename T, int S, bool UPPER, int R, typename C = PipeCfg<T, R>>
+__global__ void __launch_bounds__(kPipeThreads, 1) trsv_pipe_kernel(
     int n, const int* __restrict__ comp_ch0, CompArrays g, const T* __restrict__ va, const T* __restrict__ dslot,
     PtrR<T, R> yslot, PtrR<T, R> rhs, PtrR<T, R> y, PtrR<T, R> x, int* err, SkipR<R> skip) {
-  if (skip.on()) return;
+  // a wait of an earlier pass of this solve gave up: the solve reports the
+  // timeout, and the passes after it do no work
+  if (skip.on() || (*(volatile int*)err & (kErrTimeout | kErrStage))) return;
   using V = VecR<T, R>;
-  constexpr int RF = C::ring + 2 * C::far;
+  constexpr int RF = C::ring + 3 * C::far;
+  constexpr int D = kPipeStages;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* ring = (V*)smem_raw;  // ring, then far buffer 0, then far buffer 1
+  __shared__ __align__(8) unsigned long long s_full[D];
+  __shared__ ChunkMeta s_meta[D][2];  // {chunk, next chunk} of the chunk in each stage
+  __shared__ int s_abort;
+  V* ring = (V*)smem_raw;  // ring, then far buffers 0, 1, 2
   const int tid = threadIdx.x, lane = tid & 31;
   const int c0 = comp_ch0[blockIdx.x], c1 = comp_ch0[blockIdx.x + 1];
   const PtrR<T, R> out = UPPER ? x : y;
   if (c0 >= c1) return;
-  ChunkMeta m0 = load_meta(g.meta, c0), m1 = load_meta(g.meta, c0 + 1);
-  ChunkMeta m2 = c0 + 2 <= c1 ? load_meta(g.meta, c0 + 2) : m1;
-  {
-    const CompBufR<T, R> b = comp_buf_r<T, R, C>(smem_raw, 0);
-    comp_stage_bulk_r<T, R, UPPER, C>(b, m0, m1, g, va, dslot, yslot);
-    if (!UPPER && tid < m1.row0 - m0.row0) {
-      const int rr = __ldg(&g.ord[m0.row0 + tid]);
+  // tid 0 keeps the metadata of the next chunk to stage and of the one after
+  ChunkMeta ma{}, mb{};
+  unsigned long long issued = 0, waited = 0;  // per-stage use counts, 16 bits each (tid 0), for the exit path
+  if (tid == 0) {
+    s_abort = 0;
+    for (int s = 0; s < D; s++) mbar_init(&s_full[s], 1);
+    mbar_fence_init();
+    ma = load_meta(g.meta, c0);
+    for (int k = 0; k < D && c0 + k < c1; k++) {
+      mb = load_meta(g.meta, c0 + k + 1);
+      s_meta[k][0] = ma;
+      s_meta[k][1] = mb;
+      pipe_issue<T, R, UPPER>(pipe_buf<T, R>(smem_raw, k), ma, mb, g, va, dslot, yslot, &s_full[k]);
+      issued += 1ull << (16 * k);
+      ma = mb;
+    }
+    mb = c0 + D + 1 <= c1 ? load_meta(g.meta, c0 + D + 1) : ma;
+  }
+  __syncthreads();
+  const int sl = tid & (S - 1), group = tid / S;
+  constexpr int NG = kPipeThreads / S;
+  // What needs an index is gathered two chunks ahead, into chunk j's stage
+  // (the lower pass's right-hand side through the row list) and into far
+  // buffer j % 3 (the far operands, which the host placed before the start
+  // of chunk j - 2, so they are published by then); each chunk's gathers are
+  // one cp.async group.
+  auto gather = [&](int j) {  // j: chunk index within the subdomain
+    const int sj = j % D;
+    if (!mbar_wait(&s_full[sj], (unsigned)((j / D) & 1), err)) {
+      s_abort = 1;  // the staged indices are not there: gather nothing
+      return;
+    }
+    if (tid == 0) waited += 1ull << (16 * sj);
+    const PipeBuf<T, R> nb = pipe_buf<T, R>(smem_raw, sj);
+    const ChunkMeta n0 = s_meta[sj][0], n1 = s_meta[sj][1];
+    if (!UPPER && tid < n1.row0 - n0.row0) {
+      const int rr = nb.ord[tid];
       if (rr >= 0) {
 #pragma unroll
-        for (int r = 0; r < R; r++) cp_async_elem(&b.sb[r * C::rows + tid], &rhs.p[r][rr]);
+        for (int r = 0; r < R; r++) cp_async_elem(&nb.sb[r * C::rows + tid], &rhs.p[r][rr]);
       }
     }
-    cp_async_wait_all();
-    __syncthreads();
-  }
-  const int sl = tid & (S - 1), group = tid / S, ngroups = kCompThreads / S;
-  for (int ch = c0; ch < c1; ch++) {
-    const int bi = (ch - c0) & 1;
-    const CompBufR<T, R> nb = comp_buf_r<T, R, C>(smem_raw, bi ^ 1);
-    int rhs_row = -1, far_col = -1;
-    if (ch + 1 < c1) {
-      comp_stage_bulk_r<T, R, UPPER, C>(nb, m1, m2, g, va, dslot, yslot);
-      if (!UPPER && tid < m2.row0 - m1.row0) rhs_row = __ldg(&g.ord[m1.row0 + tid]);
-      if (tid < m2.far0 - m1.far0) far_col = __ldg(&g.far_col[m1.far0 + tid]);
+    if (tid < n1.far0 - n0.far0) {
+      const int fcol = nb.fc[tid];
+      if ((unsigned)fcol < (unsigned)n) {
+        V* fv = &ring[C::ring + (j % 3) * C::far + tid];
+#pragma unroll
+        for (int r = 0; r < R; r++) cp_async_elem(&fv->v[r], &out.p[r][fcol]);
+      } else if (fcol >= 0) {
+        atomicOr(err, kErrIndex);
+      }
     }
-    const ChunkMeta m3 = ch + 3 <= c1 ? load_meta(g.meta, ch + 3) : m2;
-    const CompBufR<T, R> b = comp_buf_r<T, R, C>(smem_raw, bi);
+  };
+  gather(0);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  if (c0 + 1 < c1) gather(1);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+  __syncthreads();
+  for (int ch = c0; ch < c1; ch++) {
+    if (s_abort) break;
+    const int k = ch - c0;
+    const int st = k % D;
+    const PipeBuf<T, R> b = pipe_buf<T, R>(smem_raw, st);
+    const ChunkMeta m0 = s_meta[st][0], m1 = s_meta[st][1];
+    if (ch + 2 < c1) gather(k + 2);
+    asm volatile("cp.async.commit_group;" ::: "memory");  // (empty near the end: keeps one group per chunk)
     const int pos0 = m0.pos0;
     const int nl = m1.lv0 - m0.lv0;
-    bool gathered = false;
-    int a = b.lvb[0], e = nl > 1 ? b.lvb[1] : a;
+    int a = b.lvb[0];
     for (int lv = 0; lv + 1 < nl; lv++) {
-      if (a >= e) break;
-      const int e_next = lv + 2 < nl ? b.lvb[lv + 2] : e;
-      for (int i = a + group; i < e; i += ngroups) {
+      const int e = b.lvb[lv + 1];
+      if (a >= e) break;  // padding after the last boundary
+      for (int i = a + group; i < e; i += NG) {
         const int k1 = b.rp[i], k2 = b.rp[i + 1];
         T acc[R];
 #pragma unroll
@@ -818,119 +903,100 @@ __global__ void __launch_bounds__(kCompThreads, kCompMinBlocks) trsv_comp_batch_
         T v[kUnroll];
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
-          const int k = k1 + sl + u * S;
-          q[u] = k < k2 ? -b.cj[k] - 1 : 0;
-          v[u] = k < k2 ? b.va[k] : T(0);
+          const int kk = k1 + sl + u * S;
+          q[u] = kk < k2 ? -b.cj[kk] - 1 : 0;
+          v[u] = kk < k2 ? b.va[kk] : T(0);
         }
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
-          if (k1 + sl + u * S < k2) {
+          if (k1 + sl + u * S < k2) {  // never read an unwritten ring slot
             const V w = ring[min((unsigned)q[u], (unsigned)(RF - 1))];
 #pragma unroll
             for (int r = 0; r < R; r++) acc[r] += v[u] * w.v[r];
           }
         }
-        for (int k = k1 + sl + kUnroll * S; k < k2; k += S) {
-          const int qq = -b.cj[k] - 1;
+        for (int kk = k1 + sl + kUnroll * S; kk < k2; kk += S) {
+          const int qq = -b.cj[kk] - 1;
           const V w = ring[min((unsigned)qq, (unsigned)(RF - 1))];
-          const T vv = b.va[k];
+          const T vv = b.va[kk];
 #pragma unroll
           for (int r = 0; r < R; r++) acc[r] += vv * w.v[r];
         }
-        // sum over the group's lanes for every lane value: reduce-scatter
-        // first (each step halves the values a lane carries), then a
-        // butterfly on one value.  Every partial sum adds the same two
-        // operands as group_reduce does, so the results are identical.
+        // sum over the group's lanes for every right-hand side: for R > 1 a
+        // reduce-scatter first (each step halves the values a lane carries),
+        // then a butterfly on one value.  Every partial sum adds the same two
+        // operands as group_reduce does, so the results are identical to the
+        // one-right-hand-side solve's.  Each result is written by one lane:
+        // into the ring and, at once, to global memory.
         const unsigned gmask = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane & ~(S - 1)));
-        if (R == 4 && S >= 4) {
+        auto put = [&](int r, T o) {
+          const T bb = b.sb[r * C::rows + i];
+          const T res = UPPER ? (bb - o) * b.sd[i] : bb - o;
+          ring[(pos0 + i) & (C::ring - 1)].v[r] = res;
+          // pick the lane's pointers by comparison: no dynamic index into a
+          // parameter array (that would go through local memory)
+          T* op = out.p[0];
+          T* ys = yslot.p[0];
+#pragma unroll
+          for (int rr = 1; rr < R; rr++)
+            if (rr == r) {
+              op = out.p[rr];
+              ys = yslot.p[rr];
+            }
+          op[b.ord[i]] = res;
+          if (!UPPER) ys[((const int*)b.sd)[i]] = res;
+        };
+        if constexpr (R == 4 && S >= 4) {
           const bool hb = (sl & (S >> 1)) != 0, qb = (sl & (S >> 2)) != 0;
-          T k0 = hb ? acc[2] : acc[0], k1 = hb ? acc[3] : acc[1];
+          T k0 = hb ? acc[2] : acc[0], kx = hb ? acc[3] : acc[1];
           const T s0 = hb ? acc[0] : acc[2], s1 = hb ? acc[1] : acc[3];
           k0 += __shfl_xor_sync(gmask, s0, S >> 1);
-          k1 += __shfl_xor_sync(gmask, s1, S >> 1);
-          T kk = qb ? k1 : k0;
-          kk += __shfl_xor_sync(gmask, qb ? k0 : k1, S >> 2);
+          kx += __shfl_xor_sync(gmask, s1, S >> 1);
+          T kk = qb ? kx : k0;
+          kk += __shfl_xor_sync(gmask, qb ? k0 : kx, S >> 2);
 #pragma unroll
           for (int off = S >> 3; off > 0; off >>= 1) kk += __shfl_xor_sync(gmask, kk, off);
-          if ((sl & ((S >> 2) - 1)) == 0) {
-            const int r = (hb ? 2 : 0) + (qb ? 1 : 0);
-            const T bb = b.sb[r * C::rows + i];
-            ring[(pos0 + i) & (C::ring - 1)].v[r] = UPPER ? (bb - kk) * b.sd[i] : bb - kk;
-          }
-        } else if (R == 2 && S >= 2) {
+          if ((sl & ((S >> 2) - 1)) == 0) put((hb ? 2 : 0) + (qb ? 1 : 0), kk);
+        } else if constexpr (R == 2 && S >= 2) {
           const bool hb = (sl & (S >> 1)) != 0;
           T kk = hb ? acc[1] : acc[0];
           kk += __shfl_xor_sync(gmask, hb ? acc[0] : acc[1], S >> 1);
 #pragma unroll
           for (int off = S >> 2; off > 0; off >>= 1) kk += __shfl_xor_sync(gmask, kk, off);
-          if ((sl & ((S >> 1) - 1)) == 0) {
-            const int r = hb ? 1 : 0;
-            const T bb = b.sb[r * C::rows + i];
-            ring[(pos0 + i) & (C::ring - 1)].v[r] = UPPER ? (bb - kk) * b.sd[i] : bb - kk;
-          }
+          if ((sl & ((S >> 1) - 1)) == 0) put(hb ? 1 : 0, kk);
         } else {
 #pragma unroll
           for (int r = 0; r < R; r++) acc[r] = group_reduce(acc[r], S, lane);
           if (sl == 0) {
-            V o;
-            const T di_ = UPPER ? b.sd[i] : T(0);
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-              const T bb = b.sb[r * C::rows + i];
-              o.v[r] = UPPER ? (bb - acc[r]) * di_ : bb - acc[r];
-            }
-            ring[(pos0 + i) & (C::ring - 1)] = o;
+            for (int r = 0; r < R; r++) put(r, acc[r]);
           }
         }
       }
+      // the last level of the chunk: the next chunk's gathers (all groups but
+      // the newest) have landed before the barrier
+      if (lv + 2 >= nl || b.lvb[lv + 2] <= e) asm volatile("cp.async.wait_group 1;" ::: "memory");
       __syncthreads();
-      if (!gathered) {
-        gathered = true;
-        if (rhs_row >= 0) {
-#pragma unroll
-          for (int r = 0; r < R; r++) cp_async_elem(&nb.sb[r * C::rows + tid], &rhs.p[r][rhs_row]);
-        }
-        if (far_col >= 0) {
-          if ((unsigned)far_col < (unsigned)n) {
-            V* fv = &ring[C::ring + (bi ^ 1) * C::far + tid];
-#pragma unroll
-            for (int r = 0; r < R; r++) cp_async_elem(&fv->v[r], &out.p[r][far_col]);
-          } else {
-            atomicOr(err, kErrIndex);
-          }
-        }
-      }
       a = e;
-      e = e_next;
     }
-    if (!gathered) {
-      if (rhs_row >= 0) {
-#pragma unroll
-        for (int r = 0; r < R; r++) cp_async_elem(&nb.sb[r * C::rows + tid], &rhs.p[r][rhs_row]);
-      }
-      if (far_col >= 0 && (unsigned)far_col < (unsigned)n) {
-        V* fv = &ring[C::ring + (bi ^ 1) * C::far + tid];
-#pragma unroll
-        for (int r = 0; r < R; r++) cp_async_elem(&fv->v[r], &out.p[r][far_col]);
-      }
+    // chunk done: its stage is free for the chunk kPipeStages ahead
+    if (tid == 0 && ch + D < c1) {
+      s_meta[st][0] = ma;
+      s_meta[st][1] = mb;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      pipe_issue<T, R, UPPER>(b, ma, mb, g, va, dslot, yslot, &s_full[st]);
+      issued += 1ull << (16 * st);
+      ma = mb;
+      if (ch + D + 2 <= c1) mb = load_meta(g.meta, ch + D + 2);
     }
-    for (int i = tid; i < m1.row0 - m0.row0; i += blockDim.x) {
-      const int rr = b.ord[i];
-      if (rr < 0) continue;
-      const V o = ring[(pos0 + i) & (C::ring - 1)];
-#pragma unroll
-      for (int r = 0; r < R; r++) {
-        out.p[r][rr] = o.v[r];
-        if (!UPPER) yslot.p[r][((const int*)b.sd)[i]] = o.v[r];
-      }
+  }
+  if (s_abort && tid == 0) {
+    // a staging wait gave up: let the copies still in flight land (bounded)
+    // before the CTA's shared memory is released
+    for (int s = 0; s < D; s++) {
+      const unsigned is = (unsigned)(issued >> (16 * s)) & 0xffffu, ws = (unsigned)(waited >> (16 * s)) & 0xffffu;
+      for (unsigned u = ws; u < is; u++) mbar_wait(&s_full[s], u & 1u, err);
     }
-    if (ch + 1 < c1) {
-      cp_async_wait_all();
-      __syncthreads();
-    }
-    m0 = m1;
-    m1 = m2;
-    m2 = m3;
   }
 }
 
@@ -1011,6 +1077,8 @@ __device__ inline void fgmres_givens(FgmresDev* st, int j, double t) {
   double gam = sqrt(fabs(hii) * fabs(hii) + fabs(hii1) * fabs(hii1));
   if (fabs(gam) < st->eps) {
     // breakdown: the reference jumps past the solution update (fgmres.hpp:440-443)
+    // and records no residual for this iteration
+    st->hist[j] = 0.0;
     st->breakdown = 1;
     st->i = 0;
     st->cycle_done = 1;
@@ -1023,6 +1091,7 @@ __device__ inline void fgmres_givens(FgmresDev* st, int j, double t) {
   st->rs[j] = st->c[j] * st->rs[j];
   H[j] = st->c[j] * hii + st->s[j] * hii1;
   st->normr = fabs(st->rs[j + 1]);
+  st->hist[j] = st->normr;  // _rel_res_vector[_iter] = normr / normb (fgmres.hpp:450-452)
   const bool conv = st->normr <= st->tolr;
   if (conv) st->converged = 1;
   if (conv || st->i >= st->kdim || st->iter >= st->maxits) {
@@ -1080,6 +1149,7 @@ __device__ inline void ts_epilogue(const TsArgs<TV, TM, TW>& a, const double* su
       if (st->done) break;  // zero right-hand side
       const double normr = sqrt(sums[0]);
       st->normr = normr;
+      st->normr0 = normr;
       if (normr < st->eps) {
         st->done = 1;
         st->cycle_done = 1;

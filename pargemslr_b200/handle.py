@@ -202,6 +202,23 @@ class GemslrHandle:
         _abi.check(_abi.lib().pgx_gemslr_kernel_stats(self._h, which, level, reps, C.byref(ms), C.byref(b)))
         return ms.value, b.value
 
+    def describe(self, slot: int = 0) -> str:
+        """Which kernel and layout every pass and SpMV of a slot uses (pgx_gemslr_describe)."""
+        ln = C.c_int32(0)
+        _abi.check(_abi.lib().pgx_gemslr_describe(self._h, slot, None, 0, C.byref(ln)))
+        buf = C.create_string_buffer(ln.value + 1)
+        _abi.check(_abi.lib().pgx_gemslr_describe(self._h, slot, buf, ln.value + 1, C.byref(ln)))
+        return buf.value.decode()
+
+    def residual_history(self) -> np.ndarray:
+        """Relative Givens residual estimates of the last solve on the handle (FlexGmresClass::GetRelativeResidual):
+        ||r0||/||b|| first, then one per iteration."""
+        cnt = C.c_int32(0)
+        _abi.check(_abi.lib().pgx_gemslr_residual_history(self._h, 0, None, C.byref(cnt)))
+        out = np.zeros(cnt.value)
+        _abi.check(_abi.lib().pgx_gemslr_residual_history(self._h, cnt.value, _abi.ptr(out), C.byref(cnt)))
+        return out
+
     def apply(self, v: np.ndarray) -> np.ndarray:
         """z = M^-1 v (one preconditioner application) on host arrays."""
         v = np.ascontiguousarray(v, np.float64)

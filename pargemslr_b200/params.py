@@ -266,6 +266,17 @@ def workload_params(name: str) -> np.ndarray:
         p[ILU_DROPTOL_C_GLOBAL] = p[ILU_DROPTOL_C_LOCAL] = 1e-3
         p[LR_RANK1_GLOBAL] = p[LR_RANK1_LOCAL] = 16
         p[LR_RANK2_GLOBAL] = p[LR_RANK2_LOCAL] = 16
+    elif name == "serve":
+        # random nonsymmetric sparse systems of the serving workload: 2 levels,
+        # ILUT 1e-2 / 20 per row, rank 8, no inner Schur iteration, FGMRES(40)
+        p[PREPOSS_NLEV_GLOBAL] = 2
+        p[ILU_DROPTOL_B_GLOBAL] = p[ILU_DROPTOL_B_LOCAL] = 1e-2
+        p[ILU_DROPTOL_C_GLOBAL] = p[ILU_DROPTOL_C_LOCAL] = 1e-2
+        p[ILU_ROWNNZ_B_GLOBAL] = p[ILU_ROWNNZ_B_LOCAL] = 20
+        p[ILU_ROWNNZ_C_GLOBAL] = p[ILU_ROWNNZ_C_LOCAL] = 20
+        p[LR_RANK1_GLOBAL] = p[LR_RANK1_LOCAL] = 8
+        p[LR_RANK2_GLOBAL] = p[LR_RANK2_LOCAL] = 8
+        p[SCHUR_ENABLE] = 0
     elif name == "small":
         # small problems for kernel-level checks
         p[PREPOSS_NLEV_GLOBAL] = 3
@@ -277,6 +288,6 @@ def workload_params(name: str) -> np.ndarray:
         p[LR_RANK2_GLOBAL] = p[LR_RANK2_LOCAL] = 4
     else:
         raise ValueError(f"unknown workload {name!r}")
-    p[SOLVER_KDIM] = 50
+    p[SOLVER_KDIM] = 40 if name == "serve" else 50
     p[SOLVER_TOL] = 1e-8
     return p

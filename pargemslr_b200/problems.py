@@ -117,3 +117,28 @@ def random_diag_dominant(n: int, seed: int, nnz_min: int = 7, nnz_max: int = 27,
     allc = np.concatenate([cols, np.arange(n)])
     allv = np.concatenate([vals, diag])
     return _csr_from_rows(n, allr, allc, allv)
+
+
+def random_skewed(n: int, seed: int, heavy_frac: float = 0.02, heavy=(200, 2000), light=(3, 9), factor: float = 1.2):
+    """Random sparse matrix with skewed row lengths: a fraction `heavy_frac` of the rows (at random positions) holds
+    `heavy` = [lo, hi) nonzeros each, the others `light` = [lo, hi); values and diagonal as random_diag_dominant.
+    The long rows carry most of the nonzeros, the case the merge-path SpMV is for."""
+    rng = np.random.default_rng(seed)
+    per_row = rng.integers(light[0] - 1, light[1] - 1, size=n)
+    hv = rng.random(n) < heavy_frac
+    per_row[hv] = rng.integers(heavy[0] - 1, heavy[1] - 1, size=int(hv.sum()))
+    per_row = np.minimum(per_row, n - 1)
+    rows = np.repeat(np.arange(n, dtype=np.int64), per_row)
+    cols = rng.integers(0, n - 1, size=rows.size)
+    cols = cols + (cols >= rows)
+    vals = rng.standard_normal(rows.size)
+    key = rows * n + cols
+    key, inv = np.unique(key, return_inverse=True)
+    vals = np.bincount(inv, weights=vals)
+    rows, cols = key // n, key % n
+    diag = factor * np.bincount(rows, weights=np.abs(vals), minlength=n)
+    diag[diag == 0] = 1.0
+    allr = np.concatenate([rows, np.arange(n)])
+    allc = np.concatenate([cols, np.arange(n)])
+    allv = np.concatenate([vals, diag])
+    return _csr_from_rows(n, allr, allc, allv)

@@ -32,6 +32,10 @@ def test_calls_without_device_fail_cleanly():
     assert L.pgx_gemslr_create(C.byref(h), 4, 7) == _abi.ERROR_INVALID_OPTION
     assert L.pgx_gemslr_solve(None, None, None, 0, None, None) == _abi.ERROR_INVALID_PARAM
     assert b"null" in L.pgx_last_error()
+    assert L.pgx_gemslr_set_wait_limit(None, 5) == _abi.ERROR_INVALID_PARAM
+    st = C.c_int32(0)
+    assert L.pgx_wait_selfcheck(0, C.byref(st), None) == _abi.ERROR_INVALID_PARAM
+    assert L.pgx_wait_selfcheck(5, None, None) == _abi.ERROR_INVALID_PARAM
 
 
 def test_level_schedule_rejects_non_triangular_factor():

@@ -106,3 +106,22 @@ def test_zero_rhs_returns_zero(handles):
     x, r = h.solve(np.zeros(h.n), x0=np.ones(h.n), params=p)
     assert r["iters"] == 0
     assert not np.any(x)
+
+
+@pytest.mark.parametrize("name", ["lap2d_64", "lap3d_32"])
+def test_residual_history_matches_reference(handles, name):
+    """GetRelativeResidual: ||r0||/||b|| then the Givens estimate after each iteration, as the reference records
+    them (its vector is maxits + 1 long and zero past the last iteration).  The FP64 path orthogonalises by CGS2
+    where the reference uses MGS, so the estimates agree to rounding, not bit for bit."""
+    h, ref, p = handles(name, "fp64")
+    b = pgxd.read(ref["problem"])["b"]
+    x, r = h.solve(b, params=p)
+    hist = h.residual_history()
+    href = ref["solution"]["rel_res_hist"]
+    assert hist.size == r["iters"] + 1
+    assert np.all(href[hist.size:] == 0.0)
+    assert hist[0] == pytest.approx(href[0], rel=1e-12)  # ||b - A 0|| / ||b|| = 1
+    np.testing.assert_allclose(hist, href[:hist.size], rtol=1e-6, atol=0)
+    assert hist[-1] == pytest.approx(r["rel_res"], rel=1e-12)
+    _, r0 = h.solve(np.zeros(h.n), params=p)
+    assert list(h.residual_history()) == [0.0]
