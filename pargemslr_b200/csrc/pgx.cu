@@ -327,6 +327,7 @@ struct DTri {
   T* dslot = nullptr;   // upper pass: inverse diagonal in slot order
   int* uslot = nullptr; // lower pass: upper-pass slot of each row, in slot order
   int nslots = 0;       // length of the slot arrays (padded row list)
+  int nslots_up = 0;    // lower pass: length of the yslot vector it fills (the upper layout's nslots)
   long long nnz_total = 0;  // nonzeros of the factor (without padding)
   int *seg_row0 = nullptr, *seg_rp0 = nullptr, *seg_nnz0 = nullptr, *seg_lv0 = nullptr, *seg_nlvb = nullptr,
       *lvb = nullptr;
@@ -938,11 +939,11 @@ struct Engine : EngineBase {
     ca.far_col = T.far_col;
 #define PGX_PIPE(SS)                                                                                             \
   if (upper)                                                                                                     \
-    trsv_pipe_kernel<P, SS, true, R><<<T.ncomp, kPipeThreads, bytes, st>>>(T.n, T.comp_ch0, ca, T.va, T.dslot,    \
-                                                                           yslot, rhs, y, x, err, sk);           \
+    trsv_pipe_kernel<P, SS, true, R><<<T.ncomp, kPipeThreads, bytes, st>>>(                                       \
+        T.n, T.nslots_up, T.comp_ch0, ca, T.va, T.dslot, yslot, rhs, y, x, err, sk);                               \
   else                                                                                                           \
-    trsv_pipe_kernel<P, SS, false, R><<<T.ncomp, kPipeThreads, bytes, st>>>(T.n, T.comp_ch0, ca, T.va, T.dslot,   \
-                                                                            yslot, rhs, y, x, err, sk)
+    trsv_pipe_kernel<P, SS, false, R><<<T.ncomp, kPipeThreads, bytes, st>>>(                                      \
+        T.n, T.nslots_up, T.comp_ch0, ca, T.va, T.dslot, yslot, rhs, y, x, err, sk)
     switch (T.S) {
       case 2: PGX_PIPE(2); break;
       case 4: PGX_PIPE(4); break;
@@ -1019,6 +1020,7 @@ struct Engine : EngineBase {
         rcU = upload_tri_comp(ar, h.U, true, h.dom_ptr, d.U, stream, &h.dinv, &uslot_of_row, nullptr);
         if (rcU == PGX_SUCCESS)
           rcL = upload_tri_comp(ar, h.L, false, h.dom_ptr, d.L, stream, nullptr, nullptr, &uslot_of_row);
+        d.L.nslots_up = d.U.nslots_up = d.U.nslots;
       }
       if (rcL == PGX_SUCCESS && rcU == PGX_SUCCESS) {
         // one CTA per subdomain; y travels from the lower to the upper pass in slot order
@@ -1397,9 +1399,11 @@ struct Engine : EngineBase {
     const int grid = grid_for(M.rows, gpb, 148 * 16);
     const int *rp2 = M2 ? M2->rp : nullptr, *cj2 = M2 ? M2->cj : nullptr;
     const TA* va2 = M2 ? M2->va : nullptr;
-#define PGX_SPMV(SS)                                                                                        \
-  spmv_kernel<TA, TX, TY, TC, SS, true><<<grid, 256, 0, stream>>>(M.rows, M.rp, M.cj, M.va, x, alpha, rp2, cj2, \
-                                                                  va2, x2, alpha2, b, beta, y, xscale, sk)
+    const int xcols2 = M2 ? M2->cols : 0;
+#define PGX_SPMV(SS)                                                                                            \
+  spmv_kernel<TA, TX, TY, TC, SS, true><<<grid, 256, 0, stream>>>(M.rows, M.rp, M.cj, M.va, x, M.cols, alpha, rp2, \
+                                                                  cj2, va2, x2, xcols2, alpha2, b, beta, y, xscale, \
+                                                                  err, sk)
     switch (S) {
       case 2: PGX_SPMV(2); break;
       case 4: PGX_SPMV(4); break;
@@ -2226,6 +2230,7 @@ struct BatchEngine : EngineBase {
         if (rc == PGX_SUCCESS)
           rc = upload_tri_sub<P, CC>(lay->ar, h.L, false, h.dom_ptr, lay->L[l], stream, nullptr, nullptr,
                                      &uslot_of_row);
+        lay->L[l].nslots_up = lay->U[l].nslots_up = lay->U[l].nslots;
         if (rc != PGX_SUCCESS) {
           lay->L[l] = DTri<P>();
           lay->U[l] = DTri<P>();
@@ -3960,12 +3965,12 @@ int pgx_csr_spmv_device_variant(const pgx_csr* Ad, int32_t variant, double alpha
 #define PGX_SPMV1(SS)                                                                                             \
   if (vec)                                                                                                        \
     spmv_kernel<double, double, double, double, SS, true><<<grid, 256>>>(                                         \
-        Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, x, alpha, nullptr, nullptr, nullptr, nullptr, 0.0, b, beta, \
-        y, nullptr, sk);                                                                                          \
+        Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, x, Ad->cols, alpha, nullptr, nullptr, nullptr, nullptr, 0, \
+        0.0, b, beta, y, nullptr, nullptr, sk);                                                                   \
   else                                                                                                            \
     spmv_kernel<double, double, double, double, SS, false><<<grid, 256>>>(                                        \
-        Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, x, alpha, nullptr, nullptr, nullptr, nullptr, 0.0, b, beta, \
-        y, nullptr, sk)
+        Ad->rows, Ad->rowptr, Ad->colidx, Ad->values, x, Ad->cols, alpha, nullptr, nullptr, nullptr, nullptr, 0, \
+        0.0, b, beta, y, nullptr, nullptr, sk)
     switch (S) {
       case 2: PGX_SPMV1(2); break;
       case 4: PGX_SPMV1(4); break;

@@ -108,7 +108,7 @@ constexpr int kSpmvUnroll = 4;
 
 template <typename TA, typename TX, typename TC, int S>
 __device__ __forceinline__ TC row_dot(int k1, int k2, int lane, const int* __restrict__ cj, const TA* __restrict__ va,
-                                      const TX* __restrict__ x) {
+                                      const TX* __restrict__ x, int xcols, bool& bad) {
   int c[kSpmvUnroll];
   TA v[kSpmvUnroll];
 #pragma unroll
@@ -116,6 +116,10 @@ __device__ __forceinline__ TC row_dot(int k1, int k2, int lane, const int* __res
     const int k = k1 + lane + u * S;
     c[u] = k < k2 ? __ldg(&cj[k]) : -1;
     v[u] = k < k2 ? __ldg(&va[k]) : TA(0);
+    if (k < k2 && (unsigned)c[u] >= (unsigned)xcols) {
+      bad = true;  // a column outside x: the entry is skipped
+      c[u] = -1;
+    }
   }
   TX xv[kSpmvUnroll];
 #pragma unroll
@@ -124,7 +128,13 @@ __device__ __forceinline__ TC row_dot(int k1, int k2, int lane, const int* __res
 #pragma unroll
   for (int u = 0; u < kSpmvUnroll; u++)
     if (c[u] >= 0) acc += (TC)v[u] * (TC)xv[u];
-  for (int k = k1 + lane + kSpmvUnroll * S; k < k2; k += S) acc += (TC)__ldg(&va[k]) * (TC)x[__ldg(&cj[k])];
+  for (int k = k1 + lane + kSpmvUnroll * S; k < k2; k += S) {
+    const int cc = __ldg(&cj[k]);
+    if ((unsigned)cc < (unsigned)xcols)
+      acc += (TC)__ldg(&va[k]) * (TC)x[cc];
+    else
+      bad = true;
+  }
   return acc;
 }
 
@@ -155,7 +165,7 @@ __device__ __forceinline__ void load_block4<double>(const double* __restrict__ p
 
 template <typename TA, typename TX, typename TC, int S>
 __device__ __forceinline__ TC row_dot_vec(int k1, int k2, int lane, const int* __restrict__ cj,
-                                          const TA* __restrict__ va, const TX* __restrict__ x) {
+                                          const TA* __restrict__ va, const TX* __restrict__ x, int xcols, bool& bad) {
   TC acc = 0;
   const int b1 = (k2 + 3) >> 2;
   for (int bb = (k1 >> 2) + lane; bb < b1; bb += S) {
@@ -164,12 +174,21 @@ __device__ __forceinline__ TC row_dot_vec(int k1, int k2, int lane, const int* _
     TA v[4];
     load_block4<TA>(va + kb, v);
     const int c[4] = {c4.x, c4.y, c4.z, c4.w};
+    bool in[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      in[u] = kb + u >= k1 && kb + u < k2;
+      if (in[u] && (unsigned)c[u] >= (unsigned)xcols) {
+        bad = true;  // a column outside x: the entry is skipped
+        in[u] = false;
+      }
+    }
     TX xv[4];
 #pragma unroll
-    for (int u = 0; u < 4; u++) xv[u] = (kb + u >= k1 && kb + u < k2) ? x[c[u]] : TX(0);
+    for (int u = 0; u < 4; u++) xv[u] = in[u] ? x[c[u]] : TX(0);
 #pragma unroll
     for (int u = 0; u < 4; u++)
-      if (kb + u >= k1 && kb + u < k2) acc += (TC)v[u] * (TC)xv[u];
+      if (in[u]) acc += (TC)v[u] * (TC)xv[u];
   }
   return acc;
 }
@@ -177,25 +196,26 @@ __device__ __forceinline__ TC row_dot_vec(int k1, int k2, int lane, const int* _
 template <typename TA, typename TX, typename TY, typename TC, int S, bool VEC>
 __global__ void __launch_bounds__(256) spmv_kernel(
     int nrows, const int* __restrict__ rp1, const int* __restrict__ cj1, const TA* __restrict__ va1,
-    const TX* __restrict__ x1, TC alpha, const int* __restrict__ rp2, const int* __restrict__ cj2,
-    const TA* __restrict__ va2, const TX* __restrict__ x2, TC alpha2, const TY* b, TC beta, TY* y,
-    const double* __restrict__ xscale, Skip skip) {
+    const TX* __restrict__ x1, int xcols1, TC alpha, const int* __restrict__ rp2, const int* __restrict__ cj2,
+    const TA* __restrict__ va2, const TX* __restrict__ x2, int xcols2, TC alpha2, const TY* b, TC beta, TY* y,
+    const double* __restrict__ xscale, int* err, Skip skip) {
   if (skip.on()) return;
   const int lane = threadIdx.x & (S - 1);
   const int wlane = threadIdx.x & 31;
   const int groups_per_block = blockDim.x / S;
   const TC xs = xscale ? (TC)(*xscale) : (TC)1;
+  bool bad = false;
   for (int row = blockIdx.x * groups_per_block + threadIdx.x / S; row < nrows;
        row += gridDim.x * groups_per_block) {
     const int k1 = __ldg(&rp1[row]), k2 = __ldg(&rp1[row + 1]);
-    TC acc = VEC ? row_dot_vec<TA, TX, TC, S>(k1, k2, lane, cj1, va1, x1)
-                 : row_dot<TA, TX, TC, S>(k1, k2, lane, cj1, va1, x1);
+    TC acc = VEC ? row_dot_vec<TA, TX, TC, S>(k1, k2, lane, cj1, va1, x1, xcols1, bad)
+                 : row_dot<TA, TX, TC, S>(k1, k2, lane, cj1, va1, x1, xcols1, bad);
     acc = group_reduce(acc, S, wlane);
     TC acc2 = 0;
     if (rp2) {
       const int q1 = __ldg(&rp2[row]), q2 = __ldg(&rp2[row + 1]);
-      acc2 = VEC ? row_dot_vec<TA, TX, TC, S>(q1, q2, lane, cj2, va2, x2)
-                 : row_dot<TA, TX, TC, S>(q1, q2, lane, cj2, va2, x2);
+      acc2 = VEC ? row_dot_vec<TA, TX, TC, S>(q1, q2, lane, cj2, va2, x2, xcols2, bad)
+                 : row_dot<TA, TX, TC, S>(q1, q2, lane, cj2, va2, x2, xcols2, bad);
       acc2 = group_reduce(acc2, S, wlane);
     }
     if (lane == 0) {
@@ -205,6 +225,7 @@ __global__ void __launch_bounds__(256) spmv_kernel(
       y[row] = (TY)v;
     }
   }
+  if (bad && err) atomicOr(err, kErrIndex);
 }
 
 // ---------------------------------------------------- merge-path CSR SpMV
@@ -804,8 +825,9 @@ __device__ __forceinline__ void pipe_issue(const PipeBuf<T, R>& b, const ChunkMe
 // pass's slot order in the lower pass).  No CTA waits on another.
 template <typename T, int S, bool UPPER, int R, typename C = PipeCfg<T, R>>
 __global__ void __launch_bounds__(kPipeThreads, 1) trsv_pipe_kernel(
-    int n, const int* __restrict__ comp_ch0, CompArrays g, const T* __restrict__ va, const T* __restrict__ dslot,
-    PtrR<T, R> yslot, PtrR<T, R> rhs, PtrR<T, R> y, PtrR<T, R> x, int* err, SkipR<R> skip) {
+    int n, int nslots, const int* __restrict__ comp_ch0, CompArrays g, const T* __restrict__ va,
+    const T* __restrict__ dslot, PtrR<T, R> yslot, PtrR<T, R> rhs, PtrR<T, R> y, PtrR<T, R> x, int* err,
+    SkipR<R> skip) {
   // a wait of an earlier pass of this solve gave up: the solve reports the
   // timeout, and the passes after it do no work
   if (skip.on() || (*(volatile int*)err & (kErrTimeout | kErrStage))) return;
@@ -858,9 +880,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) trsv_pipe_kernel(
     const ChunkMeta n0 = s_meta[sj][0], n1 = s_meta[sj][1];
     if (!UPPER && tid < n1.row0 - n0.row0) {
       const int rr = nb.ord[tid];
-      if (rr >= 0) {
+      if ((unsigned)rr < (unsigned)n) {
 #pragma unroll
         for (int r = 0; r < R; r++) cp_async_elem(&nb.sb[r * C::rows + tid], &rhs.p[r][rr]);
+      } else if (rr >= 0) {
+        atomicOr(err, kErrIndex);
       }
     }
     if (tid < n1.far0 - n0.far0) {
@@ -890,12 +914,20 @@ __global__ void __launch_bounds__(kPipeThreads, 1) trsv_pipe_kernel(
     asm volatile("cp.async.commit_group;" ::: "memory");  // (empty near the end: keeps one group per chunk)
     const int pos0 = m0.pos0;
     const int nl = m1.lv0 - m0.lv0;
+    // Every read of this chunk's stage happens before the barrier of its
+    // last level: right after that barrier thread 0 reuses the stage for
+    // the chunk kPipeStages ahead, so the boundary of the next level is read
+    // before each barrier, and the last level ends the loop.
     int a = b.lvb[0];
-    for (int lv = 0; lv + 1 < nl; lv++) {
-      const int e = b.lvb[lv + 1];
-      if (a >= e) break;  // padding after the last boundary
+    int e = nl > 1 ? b.lvb[1] : a;
+    if (a >= e) {  // no level (the host never builds such a chunk): still land the gathers
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+      __syncthreads();
+    }
+    for (int lv = 0; a < e; lv++) {
       for (int i = a + group; i < e; i += NG) {
-        const int k1 = b.rp[i], k2 = b.rp[i + 1];
+        // row pointers stay inside the staged nonzeros
+        const int k1 = max(b.rp[i], 0), k2 = min(b.rp[i + 1], C::nnz);
         T acc[R];
 #pragma unroll
         for (int r = 0; r < R; r++) acc[r] = 0;
@@ -943,8 +975,18 @@ __global__ void __launch_bounds__(kPipeThreads, 1) trsv_pipe_kernel(
               op = out.p[rr];
               ys = yslot.p[rr];
             }
-          op[b.ord[i]] = res;
-          if (!UPPER) ys[((const int*)b.sd)[i]] = res;
+          const int orow = b.ord[i];
+          if ((unsigned)orow < (unsigned)n)
+            op[orow] = res;
+          else
+            atomicOr(err, kErrIndex);
+          if (!UPPER) {
+            const int us = ((const int*)b.sd)[i];
+            if ((unsigned)us < (unsigned)nslots)
+              ys[us] = res;
+            else
+              atomicOr(err, kErrIndex);
+          }
         };
         if constexpr (R == 4 && S >= 4) {
           const bool hb = (sl & (S >> 1)) != 0, qb = (sl & (S >> 2)) != 0;
@@ -973,11 +1015,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) trsv_pipe_kernel(
           }
         }
       }
+      // the next boundary (the padding after the last one repeats it)
+      const int e2 = lv + 2 < nl ? b.lvb[lv + 2] : e;
       // the last level of the chunk: the next chunk's gathers (all groups but
       // the newest) have landed before the barrier
-      if (lv + 2 >= nl || b.lvb[lv + 2] <= e) asm volatile("cp.async.wait_group 1;" ::: "memory");
+      if (e2 <= e) asm volatile("cp.async.wait_group 1;" ::: "memory");
       __syncthreads();
       a = e;
+      e = e2;
     }
     // chunk done: its stage is free for the chunk kPipeStages ahead
     if (tid == 0 && ch + D < c1) {

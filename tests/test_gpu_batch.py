@@ -80,6 +80,28 @@ def test_multilane_slots_equal_single_solves(precision, lanes):
     h.close()
 
 
+def test_many_concurrent_multilane_slots_equal_single_solves():
+    """Fifteen 4-lane slots at once over subdomains of many staged chunks: the
+    per-subdomain passes of different slots share the SMs with every other
+    kernel in flight, and each result still equals its single solve bit for bit
+    (a chunk's staging buffer is reused only after every read of it)."""
+    from pargemslr_b200.handle import GemslrHandle
+    p = P.workload_params("lap3d_128")
+    A, n, B = _system(grid=(48, 48, 48), nrhs=61, seed=31)
+    h = GemslrHandle.from_matrix(A, p, precision="mixed")
+    singles = [h.solve(b, params=p) for b in B]
+    h.set_lanes(4)
+    h.set_slots(16)
+    for _ in range(2):
+        X, res = h.solve_batch(B, params=p)
+        for r, (x1, r1) in enumerate(singles):
+            assert res[r]["status"] == 0, (r, res[r])
+            assert res[r]["iters"] == r1["iters"], (r, res[r]["iters"], r1["iters"])
+            np.testing.assert_array_equal(X[r], x1)
+    h.set_lanes(1)
+    h.close()
+
+
 def test_server_matches_single_solves_in_any_order():
     from pargemslr_b200.handle import GemslrHandle
     p = P.workload_params("lap3d_128")
