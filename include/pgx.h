@@ -59,6 +59,18 @@ extern "C" {
  *   stays FP64. */
 #define PGX_PRECISION_FP64  0
 #define PGX_PRECISION_MIXED 1
+/* Complex systems (the reference's complexd instantiation: FlexGmresClass,
+ * GemslrClass and ParallelGemslrClass over ComplexValueClass<double>,
+ * SRC/utils/complex.hpp; TESTS/parallel/driver_laplacian_gemslrz_par.cpp).
+ * Every value array of such a handle (pgx_csr values, dinv, W, WH, x, b,
+ * X, B) holds n values as 2n doubles {re, im} interleaved, the layout of
+ * ComplexValueClass and of C99 double complex; strides (ldx, ldb) count
+ * values.  PGX_PRECISION_COMPLEX_FP64 keeps everything in complex128;
+ * PGX_PRECISION_COMPLEX_MIXED stores and applies the preconditioner in
+ * complex64 with the outer FGMRES in complex128.  A complex handle is
+ * imported through pgx_gemslr_set_*; pgx_gemslr_setup is real only. */
+#define PGX_PRECISION_COMPLEX_FP64  2
+#define PGX_PRECISION_COMPLEX_MIXED 3
 
 /* ---- memory location of borrowed vectors (reference kMemoryHost/Device) */
 #define PGX_LOCATION_HOST   0

@@ -29,6 +29,8 @@ ERROR_NO_DEVICE = 204
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+PRECISION_COMPLEX_FP64 = 2
+PRECISION_COMPLEX_MIXED = 3
 LOCATION_HOST = 0
 LOCATION_DEVICE = 1
 
@@ -188,6 +190,15 @@ def ptr(a: Optional[np.ndarray]) -> Optional[int]:
     return None if a is None else a.ctypes.data
 
 
+def doubles(a: Optional[np.ndarray]) -> Optional[np.ndarray]:
+    """Values as the C ABI takes them: float64, or a complex array as interleaved {re, im} float64."""
+    if a is None:
+        return None
+    if np.iscomplexobj(a):
+        return np.ascontiguousarray(a, np.complex128).view(np.float64)
+    return np.ascontiguousarray(a, np.float64)
+
+
 def csr_struct(rp: Optional[np.ndarray], cj: Optional[np.ndarray], va: Optional[np.ndarray], rows: int,
                cols: int, keep: list) -> Csr:
     """A pgx_csr view over numpy arrays (kept alive through `keep`)."""
@@ -195,7 +206,7 @@ def csr_struct(rp: Optional[np.ndarray], cj: Optional[np.ndarray], va: Optional[
         return Csr(0, 0, 0, None, None, None)
     rp = np.ascontiguousarray(rp, dtype=np.int32)
     cj = np.ascontiguousarray(cj, dtype=np.int32)
-    va = np.ascontiguousarray(va, dtype=np.float64)
+    va = doubles(va)
     keep.extend([rp, cj, va])
     return Csr(rows, cols, int(cj.size), ptr(rp), ptr(cj) if cj.size else None, ptr(va) if va.size else None)
 

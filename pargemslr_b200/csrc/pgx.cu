@@ -96,6 +96,8 @@ static int guarded(const char* what, F&& body) {
   } while (0)
 
 // ---------------------------------------------------------- host structures
+// A host CSR matrix.  Values are doubles; a complex matrix keeps each value
+// as two doubles {re, im} (va has 2 * nnz entries), as the C ABI passes them.
 struct HostCsr {
   int rows = 0, cols = 0;
   std::vector<int> rp, cj;
@@ -104,7 +106,25 @@ struct HostCsr {
   bool empty() const { return rows == 0; }
 };
 
-static int copy_csr(const pgx_csr* in, HostCsr& out, const char* what) {
+// Value k of a host array of doubles as the device scalar T: a real T takes
+// va[k], a complex T the pair {va[2k], va[2k+1]}.
+template <typename T>
+static inline T hval(const double* va, size_t k) {
+  if constexpr (Sc<T>::complex)
+    return T((typename Sc<T>::real)va[2 * k], (typename Sc<T>::real)va[2 * k + 1]);
+  else
+    return (T)va[k];
+}
+// the first `count` values of a host array as device scalars
+template <typename T>
+static std::vector<T> hvals(const std::vector<double>& va, size_t count) {
+  std::vector<T> out(count);
+  for (size_t k = 0; k < count; k++) out[k] = hval<T>(va.data(), k);
+  return out;
+}
+
+// vw: doubles per value (1 real, 2 complex)
+static int copy_csr(const pgx_csr* in, HostCsr& out, const char* what, int vw = 1) {
   out = HostCsr();
   if (!in || in->rows == 0) return PGX_SUCCESS;
   if (in->rows < 0 || in->cols < 0 || in->nnz < 0 || !in->rowptr)
@@ -116,7 +136,7 @@ static int copy_csr(const pgx_csr* in, HostCsr& out, const char* what) {
   out.cols = in->cols;
   out.rp.assign(in->rowptr, in->rowptr + in->rows + 1);
   out.cj.assign(in->colidx, in->colidx + in->nnz);
-  out.va.assign(in->values, in->values + in->nnz);
+  out.va.assign(in->values, in->values + in->nnz * vw);
   if (out.rp[0] != 0 || out.rp[in->rows] != in->nnz)
     return fail(PGX_ERROR_INVALID_PARAM, "%s: row pointer does not span nnz", what);
   for (int r = 0; r < out.rows; r++)
@@ -304,9 +324,9 @@ static int upload_csr(Arena& ar, const HostCsr& h, DCsr<T>& d, cudaStream_t s) {
   // value 0) for the 128-bit loads of the SpMV
   const size_t padded = (h.cj.size() + 3) / 4 * 4;
   std::vector<int> cj(h.cj);
-  std::vector<double> va(h.va);
+  std::vector<T> va = hvals<T>(h.va, h.cj.size());
   cj.resize(std::max<size_t>(padded, 4), 0);
-  va.resize(std::max<size_t>(padded, 4), 0.0);
+  va.resize(std::max<size_t>(padded, 4), T(0.0));
   PGX_TRY(ar.upload(&d.cj, cj.data(), cj.size(), s));
   PGX_TRY(ar.upload(&d.va, va.data(), va.size(), s));
   return PGX_SUCCESS;
@@ -357,7 +377,7 @@ static int upload_tri(Arena& ar, const HostCsr& h, bool upper, DTri<T>& d, cudaS
   const int G = kWarp / d.S;
   // padded schedule: each level starts on a group boundary
   std::vector<int> ord, rp(1, 0), cj;
-  std::vector<double> va;
+  std::vector<T> va;
   ord.reserve(h.rows + (size_t)d.nlevels * G);
   cj.reserve(h.nnz());
   va.reserve(h.nnz());
@@ -367,7 +387,7 @@ static int upload_tri(Arena& ar, const HostCsr& h, bool upper, DTri<T>& d, cudaS
       ord.push_back(r);
       for (int k = h.rp[r]; k < h.rp[r + 1]; k++) {
         cj.push_back(h.cj[k]);
-        va.push_back(h.va[k]);
+        va.push_back(hval<T>(h.va.data(), k));
       }
       rp.push_back((int)cj.size());
     }
@@ -466,7 +486,7 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
     while (v.size() % 4) v.push_back(fill);
   };
   std::vector<int> ord, rp, cj, lvb, row0(1, 0), rp0(1, 0), nnz0(1, 0), lv0(1, 0), nlvb;
-  std::vector<double> va;
+  std::vector<T> va;
   for (int q = 0; q < d.nseg; q++) {
     const Seg& g = segs[q];
     for (int r : g.rows) ord.push_back(r);
@@ -478,7 +498,7 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
       for (int k = h.rp[r]; k < h.rp[r + 1]; k++) {
         const int j = h.cj[k];
         cj.push_back(seg_of[j] == q ? -(slot_of[j] + 1) : j);
-        va.push_back(h.va[k]);
+        va.push_back(hval<T>(h.va.data(), k));
       }
       acc += h.rp[r + 1] - h.rp[r];
       rp.push_back(acc);
@@ -487,7 +507,7 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
     rp0.push_back((int)rp.size());
     while (cj.size() % 4) {
       cj.push_back(0);
-      va.push_back(0.0);
+      va.push_back(T(0.0));
     }
     nnz0.push_back((int)cj.size());
     const int base = (int)lvb.size();
@@ -585,7 +605,7 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
   for (int r = 0; r < n; r++)
     if (nfar[r] > CC::far) return PGX_ERROR_INVALID_PARAM;
   std::vector<int> ord, rp, cj, lvb, meta, comp_ch0(1, 0), far_col;
-  std::vector<double> va;
+  std::vector<T> va;
   auto push_meta = [&](int pos0) {
     meta.insert(meta.end(), {(int)ord.size(), (int)rp.size(), (int)cj.size(), (int)lvb.size(), pos0,
                              (int)far_col.size(), 0, 0});
@@ -629,7 +649,7 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
             cj.push_back(-(far_base + ((int)far_col.size() - far0) + 1));
             far_col.push_back(j);
           }
-          va.push_back(h.va[k]);
+          va.push_back(hval<T>(h.va.data(), k));
         }
         acc += h.rp[r + 1] - h.rp[r];
         rp.push_back(acc);
@@ -639,7 +659,7 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
       pad4(far_col, -1);
       while (cj.size() % 4) {
         cj.push_back(0);
-        va.push_back(0.0);
+        va.push_back(T(0.0));
       }
       lvb.push_back(0);
       for (size_t q = p + 1; q < e; q++)
@@ -674,12 +694,12 @@ static int upload_tri_sub(Arena& ar, const HostCsr& h, bool upper, const std::ve
   std::vector<int> slot(n, -1);
   for (size_t i = 0; i < ord.size(); i++)
     if (ord[i] >= 0) slot[ord[i]] = (int)i;
-  std::vector<double> dsl;
+  std::vector<T> dsl;
   std::vector<int> usl;
   if (upper) {
-    dsl.assign(ord.size(), 0.0);
+    dsl.assign(ord.size(), T(0.0));
     for (size_t i = 0; i < ord.size(); i++)
-      if (ord[i] >= 0) dsl[i] = (*dinv)[ord[i]];
+      if (ord[i] >= 0) dsl[i] = hval<T>(dinv->data(), ord[i]);
   } else {
     usl.assign(ord.size(), 0);
     for (size_t i = 0; i < ord.size(); i++)
@@ -730,7 +750,7 @@ struct DLevel {
   DCsr<P> E, F;
   P *W = nullptr, *WH = nullptr;
   P *z = nullptr, *xlr = nullptr;
-  double* lrt = nullptr;
+  TsAcc<P>* lrt = nullptr;  // low-rank coefficients W^H x
 };
 
 template <typename T>
@@ -777,6 +797,7 @@ static inline int grid_for(long long work, int per_block, int cap) {
 // ---------------------------------------------------------------- engine
 struct Import {
   int n = 0, precision = 0, nlev = 0;
+  int vw = 1;  // doubles per value: 1 real, 2 complex
   HostCsr A;
   std::vector<int> pperm, qperm, lev_ptr;
   std::vector<HostLevel> levels;
@@ -837,6 +858,12 @@ int make_batch_slot(Engine<P>& own, Import& im, int lanes, std::unique_ptr<Engin
 
 template <typename P>
 struct Engine : EngineBase {
+  // F: the scalar of the outer FGMRES (double, or cf64 when the factors are
+  // complex); SD: its device state.  The inner FGMRES accumulates in the same
+  // type (TsAcc<P> == F for every P).
+  using F = std::conditional_t<Sc<P>::complex, cf64, double>;
+  using SD = FgmresDevT<F>;
+  static constexpr int VW = Sc<P>::complex ? 2 : 1;  // doubles per value at the C ABI
   int n = 0, nlev = 0;
   std::vector<int> lev_ptr;
   cudaStream_t stream = nullptr;
@@ -845,7 +872,7 @@ struct Engine : EngineBase {
   Arena ar, wk, krylov;
   bool owner = true;
   int kdim_alloc = 0;
-  DCsr<double> A;
+  DCsr<F> A;
   int *pperm = nullptr, *qperm = nullptr;
   std::vector<DLevel<P>> lv;
   // level-0 Schur-complement operator C0 x - E0 B0^-1 F0 x and its work space
@@ -855,23 +882,23 @@ struct Engine : EngineBase {
   int inner = 0, inner_maxits = 5;
   double inner_tol = 1e-2;
   P *Vin = nullptr, *Zin = nullptr;
-  FgmresDev* st_in = nullptr;
+  SD* st_in = nullptr;
   // outer FGMRES
-  double* V = nullptr;
+  F* V = nullptr;
   P* Z = nullptr;
-  FgmresDev* st = nullptr;
-  double *bdev = nullptr, *xdev = nullptr, *rdev = nullptr, *scal = nullptr;
+  SD* st = nullptr;
+  F *bdev = nullptr, *xdev = nullptr, *rdev = nullptr, *scal = nullptr;
   P *rt = nullptr, *xt = nullptr;
-  double* partial = nullptr;
+  F* partial = nullptr;
   unsigned int* counter = nullptr;
   // merge-path SpMV carries of this slot (rows and partial sums, one per
   // thread of the largest merge-path matrix); null if no matrix uses it
   int* mcarry_row = nullptr;
-  double* mcarry_val = nullptr;
+  F* mcarry_val = nullptr;
   int* err = nullptr;
   int spin_limit = kSpinLimit;  // polls before a dependency wait gives up (pgx_gemslr_set_wait_limit)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_poll = nullptr;
-  FgmresDev* hs_pin = nullptr;  // pinned copy of the FGMRES state header
+  SD* hs_pin = nullptr;  // pinned copy of the FGMRES state header
   double* r2_pin = nullptr;     // pinned copy of the final residual norm
   double* hist_pin = nullptr;   // pinned copy of one cycle's residual estimates
   // Givens residual estimates of the last solve driven by begin()/poll() or
@@ -971,7 +998,7 @@ struct Engine : EngineBase {
   int64_t device_bytes(int kdim) const override { return (int64_t)ar.bytes + slot_bytes(kdim); }
 
   int64_t slot_bytes(int kdim) const override {
-    return (int64_t)wk.bytes + (int64_t)n * (kdim + 1) * (sizeof(double) + sizeof(P));
+    return (int64_t)wk.bytes + (int64_t)n * (kdim + 1) * (sizeof(F) + sizeof(P));
   }
 
   // ------------------------------------------------------------ commit
@@ -992,10 +1019,10 @@ struct Engine : EngineBase {
     PGX_CUDA(cudaEventCreate(&ev0));
     PGX_CUDA(cudaEventCreate(&ev1));
     PGX_CUDA(cudaEventCreateWithFlags(&ev_poll, cudaEventDisableTiming));
-    PGX_CUDA(cudaMallocHost((void**)&hs_pin, sizeof(FgmresDev)));
+    PGX_CUDA(cudaMallocHost((void**)&hs_pin, sizeof(SD)));
     PGX_CUDA(cudaMallocHost((void**)&r2_pin, sizeof(double)));
     PGX_CUDA(cudaMallocHost((void**)&hist_pin, sizeof(double) * KMAX));
-    memset(hs_pin, 0, sizeof(FgmresDev));
+    memset(hs_pin, 0, sizeof(SD));
     *r2_pin = 0.0;
     return PGX_SUCCESS;
   }
@@ -1035,14 +1062,18 @@ struct Engine : EngineBase {
         PGX_TRY(upload_tri(ar, h.L, false, d.L, stream));
         PGX_TRY(upload_tri(ar, h.U, true, d.U, stream));
       }
-      PGX_TRY(ar.upload(&d.dinv, h.dinv.data(), h.dinv.size(), stream));
+      {
+        const std::vector<P> dv = hvals<P>(h.dinv, (size_t)d.nl);
+        PGX_TRY(ar.upload(&d.dinv, dv.data(), dv.size(), stream));
+      }
       if (l < nlev - 1) {
         PGX_TRY(upload_csr(ar, h.E, d.E, stream));
         PGX_TRY(upload_csr(ar, h.F, d.F, stream));
         d.rank = h.rank;
         if (d.rank > 0) {
-          PGX_TRY(ar.upload(&d.W, h.W.data(), h.W.size(), stream));
-          PGX_TRY(ar.upload(&d.WH, h.WH.data(), h.WH.size(), stream));
+          const std::vector<P> w = hvals<P>(h.W, (size_t)d.m * d.rank), wh = hvals<P>(h.WH, (size_t)d.m * d.rank);
+          PGX_TRY(ar.upload(&d.W, w.data(), w.size(), stream));
+          PGX_TRY(ar.upload(&d.WH, wh.data(), wh.size(), stream));
         }
       }
     }
@@ -1079,12 +1110,12 @@ struct Engine : EngineBase {
       PGX_TRY(wk.zeros(&Vin, (size_t)m0 * (inner_maxits + 1), stream));
       PGX_TRY(wk.zeros(&Zin, (size_t)m0 * (inner_maxits + 1), stream));
       PGX_TRY(wk.zeros(&st_in, 1, stream));
-      FgmresDev h;
+      SD h;
       memset(&h, 0, sizeof(h));
       h.kdim = inner_maxits;
       h.maxits = inner_maxits;
       h.tol = inner_tol;
-      h.eps = std::is_same<P, float>::value ? (double)FLT_EPSILON : DBL_EPSILON;
+      h.eps = std::is_same<typename Sc<P>::real, float>::value ? (double)FLT_EPSILON : DBL_EPSILON;
       *hs_pin = h;
       PGX_CUDA(cudaMemcpyAsync(st_in, hs_pin, sizeof(h), cudaMemcpyHostToDevice, stream));
       PGX_CUDA(cudaStreamSynchronize(stream));
@@ -1199,10 +1230,13 @@ struct Engine : EngineBase {
   int assemble_c(Import& im, int l, DCsr<P>& out) {
     const int base = lev_ptr[l + 1];
     const int m = n - base;
-    std::vector<std::vector<std::pair<int, double>>> rows(m);
+    // (column, value) with the value as {re, im} (im 0 for a real matrix)
+    std::vector<std::vector<std::pair<int, std::pair<double, double>>>> rows(m);
     auto add = [&](const HostCsr& M, int roff, int coff) {
       for (int r = 0; r < M.rows; r++)
-        for (int k = M.rp[r]; k < M.rp[r + 1]; k++) rows[roff + r].push_back({coff + M.cj[k], M.va[k]});
+        for (int k = M.rp[r]; k < M.rp[r + 1]; k++)
+          rows[roff + r].push_back(
+              {coff + M.cj[k], {M.va[(size_t)VW * k], VW == 2 ? M.va[(size_t)VW * k + 1] : 0.0}});
     };
     for (int j = l + 1; j < nlev; j++) {
       const HostLevel& h = im.levels[j];
@@ -1220,7 +1254,8 @@ struct Engine : EngineBase {
       std::sort(rows[r].begin(), rows[r].end());
       for (auto& e : rows[r]) {
         c.cj.push_back(e.first);
-        c.va.push_back(e.second);
+        c.va.push_back(e.second.first);
+        if (VW == 2) c.va.push_back(e.second.second);
       }
       c.rp[r + 1] = (int)c.cj.size();
     }
@@ -1259,6 +1294,15 @@ struct Engine : EngineBase {
   // its times; then H = Q^T G Q, W = Q, WH = Q ((I - H)^-1 - I).
   int build_lowrank(Import& im, int l, int k, int its, unsigned long long seed, std::vector<double>& W,
                     std::vector<double>& WH, int& rank) {
+    if constexpr (Sc<P>::complex) {
+      (void)im, (void)l, (void)k, (void)its, (void)seed, (void)W, (void)WH, (void)rank;
+      return fail(PGX_ERROR_INVALID_OPTION, "the low-rank build of the host setup is real only");
+    } else {
+      return build_lowrank_real(im, l, k, its, seed, W, WH, rank);
+    }
+  }
+  int build_lowrank_real(Import& im, int l, int k, int its, unsigned long long seed, std::vector<double>& W,
+                         std::vector<double>& WH, int& rank) {
     DLevel<P>& d = lv[l];
     const int m = d.m;
     rank = 0;
@@ -1605,7 +1649,7 @@ struct Engine : EngineBase {
   // Gram-Schmidt with one re-orthogonalisation (CGS2, matrixops.cpp:10588-10708),
   // then finish the Hessenberg column with Givens rotations (fgmres.hpp:430-458).
   template <typename TV, typename TW>
-  void arnoldi_step(TV* Vb, long long ld, int j, FgmresDev* s, int nrows, Skip sk) {
+  void arnoldi_step(TV* Vb, long long ld, int j, SD* s, int nrows, Skip sk) {
     TW* w = (TW*)(Vb + (long long)(j + 1) * ld);
     auto a = ts_args<TV, TV, TW>(nrows, sk);
     a.ncols = j + 1;
@@ -1635,9 +1679,9 @@ struct Engine : EngineBase {
   // GemslrClass::Solve (gemslr.cpp:3431-3472): gather by pperm, SolveLevel(0),
   // scatter by qperm (or pperm for symmetric reorderings).
   template <typename TO>
-  void precond(const double* v, const double* v_scale, TO* z, Skip sk) {
-    const int grid = grid_for(n, 256, 148 * 16);
-    gather_kernel<double, P><<<grid, 256, 0, stream>>>(n, pperm, v, v_scale, rt, sk);
+  void precond(const F* v, const double* v_scale, TO* z, Skip sk) {
+    const int grid = grid_for(n, 256 * kPermUnroll, 148 * 16);  // gather / scatter
+    gather_kernel<F, P><<<grid, 256, 0, stream>>>(n, pperm, v, v_scale, rt, sk);
     solve_level(0, xt, rt, sk);
     scatter_kernel<P, TO><<<grid, 256, 0, stream>>>(n, qperm ? qperm : pperm, xt, z, sk);
   }
@@ -1687,11 +1731,11 @@ struct Engine : EngineBase {
         total += ms;
       }
     } else {
-      *bytes = (double)A.nnz * (sizeof(double) + 4.0) + 4.0 * (n + 1) + (double)n * (sizeof(P) + sizeof(double));
+      *bytes = (double)A.nnz * (sizeof(F) + 4.0) + 4.0 * (n + 1) + (double)n * (sizeof(P) + sizeof(F));
       *launches = 1;
       for (int r = 0; r < reps; r++) {
         PGX_CUDA(cudaEventRecord(ev0, stream));
-        spmv<double, P, double, double>(A, Z, 1.0, nullptr, nullptr, 0.0, (const double*)nullptr, 0.0, V,
+        spmv<F, P, F, F>(A, Z, 1.0, nullptr, nullptr, 0.0, (const F*)nullptr, 0.0, V,
                                         nullptr, sk);
         PGX_CUDA(cudaEventRecord(ev1, stream));
         PGX_CUDA(cudaStreamSynchronize(stream));
@@ -1716,47 +1760,49 @@ struct Engine : EngineBase {
     return PGX_SUCCESS;
   }
 
-  int apply(double* z, const double* v, int location) override {
-    const double* vin = v;
-    double* zout = z;
+  int apply(double* z_, const double* v_, int location) override {
+    F* z = (F*)z_;
+    const F* v = (const F*)v_;
+    const F* vin = v;
+    F* zout = z;
     if (location == PGX_LOCATION_HOST) {
-      PGX_CUDA(cudaMemcpyAsync(bdev, v, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaMemcpyAsync(bdev, v, sizeof(F) * n, cudaMemcpyHostToDevice, stream));
       vin = bdev;
       zout = xdev;
     }
     PGX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
-    precond<double>(vin, nullptr, zout, mk_skip());
+    precond<F>(vin, nullptr, zout, mk_skip());
     PGX_CUDA(cudaGetLastError());
     if (location == PGX_LOCATION_HOST)
-      PGX_CUDA(cudaMemcpyAsync(z, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaMemcpyAsync(z, xdev, sizeof(F) * n, cudaMemcpyDeviceToHost, stream));
     return check_err();
   }
 
   // One restart cycle of FlexGmresClass::Solve (fgmres.hpp:379-514): kdim
   // Arnoldi steps, the solution update, the restart residual and the cycle
   // reset.  Steps after convergence see the cycle flag and return at once.
-  void enqueue_cycle(int kdim, double* xd, const double* bd) {
+  void enqueue_cycle(int kdim, F* xd, const F* bd) {
     const long long ld = n;
     Skip sk = mk_skip(&st->done, &st->cycle_done);
     for (int j = 0; j < kdim; j++) {
-      double* vj = V + (long long)j * ld;
+      F* vj = V + (long long)j * ld;
       P* zj = Z + (long long)j * ld;
       precond<P>(vj, &st->sc[j], zj, sk);                                            // z = M^-1 v
-      spmv<double, P, double, double>(A, zj, 1.0, nullptr, nullptr, 0.0, (const double*)nullptr, 0.0,
+      spmv<F, P, F, F>(A, zj, 1.0, nullptr, nullptr, 0.0, (const F*)nullptr, 0.0,
                                       V + (long long)(j + 1) * ld, nullptr, sk);   // w = A z
-      arnoldi_step<double, double>(V, ld, j, st, n, sk);
+      arnoldi_step<F, F>(V, ld, j, st, n, sk);
     }
     {
-      auto u = ts_args<P, P, double>(n, mk_skip());
+      auto u = ts_args<P, P, F>(n, mk_skip());
       u.ncols_dev = &st->i;
       u.M = Z;
       u.ldm = ld;
       u.coef = st->rs;
       u.in = xd;
       u.out = xd;
-      ts<P, P, double, TS_UPDATE>(u);                                                // x += Z y
+      ts<P, P, F, TS_UPDATE>(u);                                                // x += Z y
     }
-    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
+    spmv<F, F, F, F>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
                                          mk_skip(&st->done));                        // restart residual
     fgmres_cycle_reset_kernel<<<1, 1, 0, stream>>>(st, mk_skip());
   }
@@ -1770,15 +1816,17 @@ struct Engine : EngineBase {
   enum { IDLE = 0, RUNNING = 1, FINISHING = 2 };
   int phase = IDLE;
   int s_cyc = 0, s_max_cycles = 0, s_maxits = 0, s_launches = 0, s_location = 0;
-  double* s_xd = nullptr;
-  const double* s_bd = nullptr;
-  double* s_xuser = nullptr;
+  F* s_xd = nullptr;
+  const F* s_bd = nullptr;
+  F* s_xuser = nullptr;
 
-  int begin(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+  int begin(double* x_, const double* b_, int location, int kdim, int maxits, double tol, int atol,
             bool prechecked = false) override {
     if (phase != IDLE) return fail(PGX_ERROR_FUNCTION_CALL, "slot busy");
-    double* xd = nullptr;
-    const double* bd = nullptr;
+    F* x = (F*)x_;
+    const F* b = (const F*)b_;
+    F* xd = nullptr;
+    const F* bd = nullptr;
     PGX_TRY(begin_prologue(x, b, location, kdim, maxits, tol, atol, &xd, &bd, prechecked));
     s_max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
     if (s_max_cycles > 0 && (!cycle_exec || g_kdim != kdim || g_x != xd || g_b != bd)) {
@@ -1819,22 +1867,22 @@ struct Engine : EngineBase {
   // The start of a solve up to the first restart cycle (fgmres.hpp:263-360):
   // inputs to the device, the FGMRES header, ||b||, r0 = b - A x0 and ||r0||.
   // *xd and *bd receive the device vectors the cycles work on.
-  int begin_prologue(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
-                     double** xd_out, const double** bd_out, bool prechecked = false) {
+  int begin_prologue(F* x, const F* b, int location, int kdim, int maxits, double tol, int atol,
+                     F** xd_out, const F** bd_out, bool prechecked = false) {
     if (kdim < 1 || kdim > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", kdim, KMAX);
     if (maxits < 0) return fail(PGX_ERROR_INVALID_PARAM, "maxits %d < 0", maxits);
-    if (location == PGX_LOCATION_HOST && !prechecked && !all_finite(b, n))
+    if (location == PGX_LOCATION_HOST && !prechecked && !all_finite((const double*)b, (long long)n * VW))
       return fail(PGX_ERROR_NOT_FINITE, "b is not finite");
     PGX_TRY(ensure_krylov(kdim));
-    double* xd = x;
-    const double* bd = b;
+    F* xd = x;
+    const F* bd = b;
     if (location == PGX_LOCATION_HOST) {
-      PGX_CUDA(cudaMemcpyAsync(bdev, b, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
-      PGX_CUDA(cudaMemcpyAsync(xdev, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaMemcpyAsync(bdev, b, sizeof(F) * n, cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaMemcpyAsync(xdev, x, sizeof(F) * n, cudaMemcpyHostToDevice, stream));
       xd = xdev;
       bd = bdev;
     }
-    FgmresDev h;
+    SD h;
     memset(&h, 0, sizeof(h));
     h.kdim = kdim;
     h.maxits = maxits;
@@ -1842,27 +1890,27 @@ struct Engine : EngineBase {
     h.absolute = atol;
     h.eps = DBL_EPSILON;
     h.cycle_done = 1;
-    const size_t head = offsetof(FgmresDev, sc);
+    const size_t head = offsetof(SD, sc);
     *hs_pin = h;
     PGX_CUDA(cudaMemcpyAsync(st, hs_pin, head, cudaMemcpyHostToDevice, stream));
     PGX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
     PGX_CUDA(cudaEventRecord(ev0, stream));
     // ||b||, v = b - A x, ||v||  (fgmres.hpp:319-360)
     {
-      auto a = ts_args<double, double, double>(n, mk_skip());
+      auto a = ts_args<F, F, F>(n, mk_skip());
       a.in = bd;
       a.epi = EPI_NORMB;
       a.st = st;
-      ts<double, double, double, TS_NORM_COPY>(a);
+      ts<F, F, F, TS_NORM_COPY>(a);
     }
-    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
+    spmv<F, F, F, F>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
                                          mk_skip(&st->done));
     {
-      auto a = ts_args<double, double, double>(n, mk_skip());
+      auto a = ts_args<F, F, F>(n, mk_skip());
       a.in = V;
       a.epi = EPI_INIT;
       a.st = st;
-      ts<double, double, double, TS_NORM_COPY>(a);
+      ts<F, F, F, TS_NORM_COPY>(a);
     }
     *xd_out = xd;
     *bd_out = bd;
@@ -1875,7 +1923,7 @@ struct Engine : EngineBase {
       PGX_CUDA(cudaGraphLaunch(cycle_exec, stream));
       s_launches += cycle_nodes;
       s_cyc++;
-      PGX_CUDA(cudaMemcpyAsync(hs_pin, st, offsetof(FgmresDev, sc), cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaMemcpyAsync(hs_pin, st, offsetof(SD, sc), cudaMemcpyDeviceToHost, stream));
       PGX_CUDA(cudaMemcpyAsync(hist_pin, st->hist, sizeof(double) * g_kdim, cudaMemcpyDeviceToHost, stream));
       PGX_CUDA(cudaEventRecord(ev_poll, stream));
       return PGX_SUCCESS;
@@ -1889,16 +1937,16 @@ struct Engine : EngineBase {
   // the FP64 true residual ||b - A x|| / ||b|| and the copies of the state
   // header and the residual norm back to the host
   int enqueue_finish() {
-    spmv<double, double, double, double>(A, s_xd, -1.0, nullptr, nullptr, 0.0, s_bd, 1.0, rdev, nullptr, mk_skip());
+    spmv<F, F, F, F>(A, s_xd, -1.0, nullptr, nullptr, 0.0, s_bd, 1.0, rdev, nullptr, mk_skip());
     {
-      auto a = ts_args<double, double, double>(n, mk_skip());
+      auto a = ts_args<F, F, F>(n, mk_skip());
       a.in = rdev;
       a.epi = EPI_STORE;
       a.dst = scal;
-      ts<double, double, double, TS_NORM_COPY>(a);
+      ts<F, F, F, TS_NORM_COPY>(a);
     }
     PGX_CUDA(cudaEventRecord(ev1, stream));
-    PGX_CUDA(cudaMemcpyAsync(hs_pin, st, offsetof(FgmresDev, sc), cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaMemcpyAsync(hs_pin, st, offsetof(SD, sc), cudaMemcpyDeviceToHost, stream));
     PGX_CUDA(cudaMemcpyAsync(r2_pin, scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
     return PGX_SUCCESS;
   }
@@ -1926,7 +1974,7 @@ struct Engine : EngineBase {
       }
     }
     if (phase == RUNNING) {
-      const FgmresDev& hs = *hs_pin;
+      const SD& hs = *hs_pin;
       absorb_history(hs);
       const bool over = hs.done || hs.iter >= s_maxits;
       const int rc = launch_cycle_or_finish(over);
@@ -1944,7 +1992,7 @@ struct Engine : EngineBase {
 
   // the residual estimates of the cycle that just landed (hs: its state
   // header, hist_pin: its per-column estimates)
-  void absorb_history(const FgmresDev& hs) {
+  void absorb_history(const SD& hs) {
     if (history.empty()) history.push_back(hs.normr0);
     const int fresh = std::min(hs.iter - hist_iters, KMAX);
     for (int j = 0; j < fresh; j++) history.push_back(hist_pin[j]);
@@ -1996,17 +2044,17 @@ struct Engine : EngineBase {
   }
 
   int collect_result_body(pgx_result* res) {
-    const FgmresDev hs = *hs_pin;
+    const SD hs = *hs_pin;
     const double r2 = *r2_pin;
     const int rc = check_err();
     float ms = 0.f;
     PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
     if (hs.normb < DBL_EPSILON) {
       // zero right-hand side: x = 0 (fgmres.hpp:321-329)
-      PGX_CUDA(cudaMemsetAsync(s_xd, 0, sizeof(double) * n, stream));
+      PGX_CUDA(cudaMemsetAsync(s_xd, 0, sizeof(F) * n, stream));
     }
     if (s_location == PGX_LOCATION_HOST)
-      PGX_CUDA(cudaMemcpyAsync(s_xuser, xdev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+      PGX_CUDA(cudaMemcpyAsync(s_xuser, xdev, sizeof(F) * n, cudaMemcpyDeviceToHost, stream));
     PGX_CUDA(cudaStreamSynchronize(stream));
     int out = rc;
     if (out == PGX_SUCCESS && !(std::isfinite(hs.normr)))
@@ -2064,40 +2112,40 @@ struct Engine : EngineBase {
     if (kdim < 1 || kdim > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", kdim, KMAX);
     if (maxits < 0) return fail(PGX_ERROR_INVALID_PARAM, "maxits %d < 0", maxits);
     const size_t cols = (size_t)kdim + 1;
-    const size_t vbytes = (sizeof(double) * (size_t)n * cols + 255) & ~(size_t)255;
+    const size_t vbytes = (sizeof(F) * (size_t)n * cols + 255) & ~(size_t)255;
     const size_t zbytes = sizeof(P) * (size_t)n * cols;
     if (vbytes + zbytes > pool_bytes)
       return fail(PGX_ERROR_INVALID_PARAM,
                   "n = %d with kdim = %d needs %zu bytes of Krylov basis; the static pool holds %zu", n, kdim,
                   vbytes + zbytes, pool_bytes);
     if (location == PGX_LOCATION_HOST) {
-      for (int i = 0; i < n; i++)
-        if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%d] is not finite", i);
+      for (long long i = 0; i < (long long)n * VW; i++)
+        if (!std::isfinite(b[i])) return fail(PGX_ERROR_NOT_FINITE, "b[%lld] is not finite", i / VW);
     }
-    double* own_V = V;
+    F* own_V = V;
     P* own_Z = Z;
-    V = (double*)pool;
+    V = (F*)pool;
     Z = (P*)((char*)pool + vbytes);
-    const int rc = run_fixed_basis(x, b, location, kdim, maxits, tol, atol, vbytes, zbytes, res);
+    const int rc = run_fixed_basis((F*)x, (const F*)b, location, kdim, maxits, tol, atol, vbytes, zbytes, res);
     V = own_V;
     Z = own_Z;
     return rc;
   }
 
-  int run_fixed_basis(double* x, const double* b, int location, int kdim, int maxits, double tol, int atol,
+  int run_fixed_basis(F* x, const F* b, int location, int kdim, int maxits, double tol, int atol,
                       size_t vbytes, size_t zbytes, pgx_result* res) {
-    double* xd = x;
-    const double* bd = b;
+    F* xd = x;
+    const F* bd = b;
     if (location == PGX_LOCATION_HOST) {
-      PGX_CUDA(cudaMemcpyAsync(bdev, b, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
-      PGX_CUDA(cudaMemcpyAsync(xdev, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaMemcpyAsync(bdev, b, sizeof(F) * n, cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaMemcpyAsync(xdev, x, sizeof(F) * n, cudaMemcpyHostToDevice, stream));
       xd = xdev;
       bd = bdev;
     }
     // the pool keeps whatever the previous call left in it
     PGX_CUDA(cudaMemsetAsync(V, 0, vbytes, stream));
     PGX_CUDA(cudaMemsetAsync(Z, 0, zbytes, stream));
-    FgmresDev h;
+    SD h;
     memset(&h, 0, sizeof(h));
     h.kdim = kdim;
     h.maxits = maxits;
@@ -2105,26 +2153,26 @@ struct Engine : EngineBase {
     h.absolute = atol;
     h.eps = DBL_EPSILON;
     h.cycle_done = 1;
-    const size_t head = offsetof(FgmresDev, sc);
+    const size_t head = offsetof(SD, sc);
     *hs_pin = h;
     PGX_CUDA(cudaMemcpyAsync(st, hs_pin, head, cudaMemcpyHostToDevice, stream));
     PGX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
     PGX_CUDA(cudaEventRecord(ev0, stream));
     {
-      auto a = ts_args<double, double, double>(n, mk_skip());
+      auto a = ts_args<F, F, F>(n, mk_skip());
       a.in = bd;
       a.epi = EPI_NORMB;
       a.st = st;
-      ts<double, double, double, TS_NORM_COPY>(a);
+      ts<F, F, F, TS_NORM_COPY>(a);
     }
-    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
+    spmv<F, F, F, F>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, V, nullptr,
                                          mk_skip(&st->done));
     {
-      auto a = ts_args<double, double, double>(n, mk_skip());
+      auto a = ts_args<F, F, F>(n, mk_skip());
       a.in = V;
       a.epi = EPI_INIT;
       a.st = st;
-      ts<double, double, double, TS_NORM_COPY>(a);
+      ts<F, F, F, TS_NORM_COPY>(a);
     }
     const int max_cycles = maxits > 0 ? maxits / kdim + 2 : 0;
     history.clear();
@@ -2139,13 +2187,13 @@ struct Engine : EngineBase {
       absorb_history(*hs_pin);
       if (hs_pin->done || hs_pin->iter >= maxits) break;
     }
-    spmv<double, double, double, double>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, rdev, nullptr, mk_skip());
+    spmv<F, F, F, F>(A, xd, -1.0, nullptr, nullptr, 0.0, bd, 1.0, rdev, nullptr, mk_skip());
     {
-      auto a = ts_args<double, double, double>(n, mk_skip());
+      auto a = ts_args<F, F, F>(n, mk_skip());
       a.in = rdev;
       a.epi = EPI_STORE;
       a.dst = scal;
-      ts<double, double, double, TS_NORM_COPY>(a);
+      ts<F, F, F, TS_NORM_COPY>(a);
     }
     PGX_CUDA(cudaEventRecord(ev1, stream));
     PGX_CUDA(cudaMemcpyAsync(hs_pin, st, head, cudaMemcpyDeviceToHost, stream));
@@ -2440,17 +2488,18 @@ struct BatchEngine : EngineBase {
   }
 
   // Engine::enqueue_cycle for every lane, preconditioner applies merged
-  void enqueue_cycle_b(int kdim, const std::array<double*, R>& xd, const std::array<const double*, R>& bd) {
+  using F = typename Engine<P>::F;
+  void enqueue_cycle_b(int kdim, const std::array<F*, R>& xd, const std::array<const F*, R>& bd) {
     const long long ld = n;
     std::array<Skip, R> sk;
     for (int r = 0; r < R; r++) sk[r] = mk_skip(&lane[r]->st->done, &lane[r]->st->cycle_done);
-    const int grid = grid_for(n, 256, 148 * 16);
+    const int grid = grid_for(n, 256 * kPermUnroll, 148 * 16);  // gather / scatter
     for (int j = 0; j < kdim; j++) {
       std::array<P*, R> xt;
       std::array<const P*, R> rt;
       for (int r = 0; r < R; r++) {
         Engine<P>& e = *lane[r];
-        gather_kernel<double, P><<<grid, 256, 0, stream>>>(n, e.pperm, e.V + (long long)j * ld, &e.st->sc[j], e.rt,
+        gather_kernel<F, P><<<grid, 256, 0, stream>>>(n, e.pperm, e.V + (long long)j * ld, &e.st->sc[j], e.rt,
                                                            sk[r]);
         xt[r] = e.xt;
         rt[r] = e.rt;
@@ -2460,22 +2509,22 @@ struct BatchEngine : EngineBase {
         Engine<P>& e = *lane[r];
         P* zj = e.Z + (long long)j * ld;
         scatter_kernel<P, P><<<grid, 256, 0, stream>>>(n, e.qperm ? e.qperm : e.pperm, e.xt, zj, sk[r]);
-        e.template spmv<double, P, double, double>(e.A, zj, 1.0, nullptr, nullptr, 0.0, (const double*)nullptr, 0.0,
+        e.template spmv<F, P, F, F>(e.A, zj, 1.0, nullptr, nullptr, 0.0, (const F*)nullptr, 0.0,
                                                    e.V + (long long)(j + 1) * ld, nullptr, sk[r]);
-        e.template arnoldi_step<double, double>(e.V, ld, j, e.st, n, sk[r]);
+        e.template arnoldi_step<F, F>(e.V, ld, j, e.st, n, sk[r]);
       }
     }
     for (int r = 0; r < R; r++) {
       Engine<P>& e = *lane[r];
-      auto u = Engine<P>::template ts_args<P, P, double>(n, mk_skip());
+      auto u = Engine<P>::template ts_args<P, P, F>(n, mk_skip());
       u.ncols_dev = &e.st->i;
       u.M = e.Z;
       u.ldm = ld;
       u.coef = e.st->rs;
       u.in = xd[r];
       u.out = xd[r];
-      e.template ts<P, P, double, TS_UPDATE>(u);
-      e.template spmv<double, double, double, double>(e.A, xd[r], -1.0, nullptr, nullptr, 0.0, bd[r], 1.0, e.V,
+      e.template ts<P, P, F, TS_UPDATE>(u);
+      e.template spmv<F, F, F, F>(e.A, xd[r], -1.0, nullptr, nullptr, 0.0, bd[r], 1.0, e.V,
                                                       nullptr, mk_skip(&e.st->done));
       fgmres_cycle_reset_kernel<<<1, 1, 0, stream>>>(e.st, mk_skip());
     }
@@ -2485,18 +2534,19 @@ struct BatchEngine : EngineBase {
                  int atol, bool prechecked = false) override {
     if (phase != IDLE) return fail(PGX_ERROR_FUNCTION_CALL, "slot busy");
     if (cnt < 1 || cnt > R) return fail(PGX_ERROR_INVALID_PARAM, "%d right-hand sides for a %d-lane slot", cnt, R);
-    std::array<double*, R> xd;
-    std::array<const double*, R> bd;
+    std::array<F*, R> xd;
+    std::array<const F*, R> bd;
     for (int r = 0; r < R; r++) {
       Engine<P>& e = *lane[r];
       if (r < cnt) {
-        PGX_TRY(e.begin_prologue(x[r], b[r], location, kdim, maxits, tol, atol, &xd[r], &bd[r], prechecked));
+        PGX_TRY(e.begin_prologue((F*)x[r], (const F*)b[r], location, kdim, maxits, tol, atol, &xd[r], &bd[r],
+                                 prechecked));
         e.s_location = location;
-        e.s_xuser = x[r];
+        e.s_xuser = (F*)x[r];
       } else {
         // an idle lane solves b = 0 (finished at once) on its own vectors
-        PGX_CUDA(cudaMemsetAsync(e.bdev, 0, sizeof(double) * n, stream));
-        PGX_CUDA(cudaMemsetAsync(e.xdev, 0, sizeof(double) * n, stream));
+        PGX_CUDA(cudaMemsetAsync(e.bdev, 0, sizeof(F) * n, stream));
+        PGX_CUDA(cudaMemsetAsync(e.xdev, 0, sizeof(F) * n, stream));
         PGX_TRY(e.begin_prologue(e.xdev, e.bdev, PGX_LOCATION_DEVICE, kdim, maxits, tol, atol, &xd[r], &bd[r]));
         e.s_location = PGX_LOCATION_DEVICE;
         e.s_xuser = e.xdev;
@@ -2554,7 +2604,7 @@ struct BatchEngine : EngineBase {
       s_cyc++;
       for (int r = 0; r < R; r++) {
         lane[r]->s_launches += cycle_nodes / R;
-        PGX_CUDA(cudaMemcpyAsync(lane[r]->hs_pin, lane[r]->st, offsetof(FgmresDev, sc), cudaMemcpyDeviceToHost,
+        PGX_CUDA(cudaMemcpyAsync(lane[r]->hs_pin, lane[r]->st, offsetof(typename Engine<P>::SD, sc), cudaMemcpyDeviceToHost,
                                  stream));
       }
       PGX_CUDA(cudaEventRecord(evp, stream));
@@ -2583,7 +2633,7 @@ struct BatchEngine : EngineBase {
     if (phase == RUNNING) {
       bool over = true;
       for (int r = 0; r < R; r++) {
-        const FgmresDev& hs = *lane[r]->hs_pin;
+        const auto& hs = *lane[r]->hs_pin;
         over = over && (hs.done || hs.iter >= s_maxits);
       }
       const int rc = launch_cycle_or_finish(over);
@@ -2790,11 +2840,13 @@ int pgx_gemslr_create(pgx_handle* handle, int32_t n, int32_t precision) {
     if (!handle) return fail(PGX_ERROR_INVALID_PARAM, "null handle pointer");
     *handle = nullptr;
     if (n <= 0) return fail(PGX_ERROR_INVALID_PARAM, "n must be positive");
-    if (precision != PGX_PRECISION_FP64 && precision != PGX_PRECISION_MIXED)
+    if (precision != PGX_PRECISION_FP64 && precision != PGX_PRECISION_MIXED &&
+        precision != PGX_PRECISION_COMPLEX_FP64 && precision != PGX_PRECISION_COMPLEX_MIXED)
       return fail(PGX_ERROR_INVALID_OPTION, "unknown precision %d", precision);
     pgx_gemslr_s* h = new pgx_gemslr_s();
     h->im.n = n;
     h->im.precision = precision;
+    h->im.vw = precision >= PGX_PRECISION_COMPLEX_FP64 ? 2 : 1;
     h->device = g_device;
     *handle = h;
     return PGX_SUCCESS;
@@ -2805,7 +2857,7 @@ int pgx_gemslr_set_matrix(pgx_handle h, const pgx_csr* A) {
   return guarded("pgx_gemslr_set_matrix", [&]() -> int {
     if (!h || !A) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
     if (A->rows != h->im.n || A->cols != h->im.n) return fail(PGX_ERROR_INVALID_PARAM, "A must be n x n");
-    return copy_csr(A, h->im.A, "A");
+    return copy_csr(A, h->im.A, "A", h->im.vw);
   });
 }
 
@@ -2863,26 +2915,27 @@ int pgx_gemslr_set_level(pgx_handle h, int32_t level, const pgx_level* d) {
     HostLevel hl;
     hl.ncomp = d->ncomp;
     if (d->dom_ptr && d->ncomp > 0) hl.dom_ptr.assign(d->dom_ptr, d->dom_ptr + d->ncomp + 1);
-    PGX_TRY(copy_csr(&d->L, hl.L, "L"));
-    PGX_TRY(copy_csr(&d->U, hl.U, "U"));
-    PGX_TRY(copy_csr(&d->B, hl.B, "B"));
+    const int vw = im.vw;
+    PGX_TRY(copy_csr(&d->L, hl.L, "L", vw));
+    PGX_TRY(copy_csr(&d->U, hl.U, "U", vw));
+    PGX_TRY(copy_csr(&d->B, hl.B, "B", vw));
     if (hl.L.rows != nl || hl.L.cols != nl || hl.U.rows != nl || hl.U.cols != nl)
       return fail(PGX_ERROR_INVALID_PARAM, "level %d: L/U must be %d x %d", level, nl, nl);
     if (!d->dinv) return fail(PGX_ERROR_INVALID_PARAM, "level %d: missing dinv", level);
-    hl.dinv.assign(d->dinv, d->dinv + nl);
+    hl.dinv.assign(d->dinv, d->dinv + (size_t)nl * vw);
     if (!hl.B.empty() && (hl.B.rows != nl || hl.B.cols != nl))
       return fail(PGX_ERROR_INVALID_PARAM, "level %d: B must be %d x %d", level, nl, nl);
     if (!last) {
-      PGX_TRY(copy_csr(&d->E, hl.E, "E"));
-      PGX_TRY(copy_csr(&d->F, hl.F, "F"));
+      PGX_TRY(copy_csr(&d->E, hl.E, "E", vw));
+      PGX_TRY(copy_csr(&d->F, hl.F, "F", vw));
       if (hl.E.rows != m || hl.E.cols != nl) return fail(PGX_ERROR_INVALID_PARAM, "level %d: E must be %d x %d", level, m, nl);
       if (hl.F.rows != nl || hl.F.cols != m) return fail(PGX_ERROR_INVALID_PARAM, "level %d: F must be %d x %d", level, nl, m);
       if (d->rank < 0 || d->rank > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "level %d: rank %d outside [0, %d]", level, d->rank, KMAX);
       hl.rank = d->rank;
       if (hl.rank > 0) {
         if (!d->W || !d->WH) return fail(PGX_ERROR_INVALID_PARAM, "level %d: missing W/WH", level);
-        hl.W.assign(d->W, d->W + (size_t)m * hl.rank);
-        hl.WH.assign(d->WH, d->WH + (size_t)m * hl.rank);
+        hl.W.assign(d->W, d->W + (size_t)m * hl.rank * vw);
+        hl.WH.assign(d->WH, d->WH + (size_t)m * hl.rank * vw);
       }
     }
     hl.set = true;
@@ -2915,14 +2968,30 @@ int pgx_gemslr_commit(pgx_handle h) {
   PGX_CUDA(cudaSetDevice(h->device));
   h->extra.clear();
   h->eng.reset();
-  if (im.precision == PGX_PRECISION_MIXED) {
-    auto* e = new Engine<float>();
-    h->eng.reset(e);
-    PGX_TRY(e->commit(im));
-  } else {
-    auto* e = new Engine<double>();
-    h->eng.reset(e);
-    PGX_TRY(e->commit(im));
+  switch (im.precision) {
+    case PGX_PRECISION_MIXED: {
+      auto* e = new Engine<float>();
+      h->eng.reset(e);
+      PGX_TRY(e->commit(im));
+      break;
+    }
+    case PGX_PRECISION_COMPLEX_MIXED: {
+      auto* e = new Engine<cf32>();
+      h->eng.reset(e);
+      PGX_TRY(e->commit(im));
+      break;
+    }
+    case PGX_PRECISION_COMPLEX_FP64: {
+      auto* e = new Engine<cf64>();
+      h->eng.reset(e);
+      PGX_TRY(e->commit(im));
+      break;
+    }
+    default: {
+      auto* e = new Engine<double>();
+      h->eng.reset(e);
+      PGX_TRY(e->commit(im));
+    }
   }
   return PGX_SUCCESS;
 }
@@ -2953,6 +3022,9 @@ int pgx_gemslr_setup(pgx_handle* handle, const pgx_csr* A, const double* params,
     if (!handle || !A || !params) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
     *handle = nullptr;
     if (A->rows != A->cols) return fail(PGX_ERROR_INVALID_PARAM, "A must be square");
+    if (precision == PGX_PRECISION_COMPLEX_FP64 || precision == PGX_PRECISION_COMPLEX_MIXED)
+      return fail(PGX_ERROR_INVALID_OPTION,
+                  "the host setup is real; a complex preconditioner comes in through pgx_gemslr_set_*");
     pgx_handle h = nullptr;
     PGX_TRY(pgx_gemslr_create(&h, A->rows, precision));
     std::unique_ptr<pgx_gemslr_s> guard(h);
@@ -3168,13 +3240,14 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
   read_solver_params(params, kdim, maxits, tol, atol);
   PGX_CUDA(cudaSetDevice(h->device));
   if (results) memset(results, 0, sizeof(pgx_result) * (size_t)nrhs);
+  const int vw = h->im.vw;  // ldx, ldb count values; a complex value is two doubles
   // host columns are checked before any is assigned, so that a bad one does
   // not take the other lanes of its slot down with it
   std::vector<int> order;
   order.reserve((size_t)nrhs);
   int first_bad = -1;
   for (int r = 0; r < nrhs; r++) {
-    const bool ok = location != PGX_LOCATION_HOST || all_finite(B + (size_t)r * ldb, h->im.n);
+    const bool ok = location != PGX_LOCATION_HOST || all_finite(B + (size_t)r * ldb * vw, (long long)h->im.n * vw);
     if (ok) {
       order.push_back(r);
     } else {
@@ -3211,8 +3284,8 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
         double* xs[4];
         const double* bs[4];
         for (int k = 0; k < cnt; k++) {
-          xs[k] = X + (size_t)order[next + k] * ldx;
-          bs[k] = B + (size_t)order[next + k] * ldb;
+          xs[k] = X + (size_t)order[next + k] * ldx * vw;
+          bs[k] = B + (size_t)order[next + k] * ldb * vw;
         }
         const int rc = e->begin_many(cnt, xs, bs, location, kdim, maxits, tol, atol, true);
         progressed = true;
@@ -3267,7 +3340,7 @@ int pgx_server_submit(pgx_server srv, double* x, const double* b, int32_t locati
   if (request_id < 0) return fail(PGX_ERROR_INVALID_PARAM, "request id %lld < 0", (long long)request_id);
   if (location != PGX_LOCATION_HOST && location != PGX_LOCATION_DEVICE)
     return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
-  if (location == PGX_LOCATION_HOST && !all_finite(b, srv->h->im.n))
+  if (location == PGX_LOCATION_HOST && !all_finite(b, (long long)srv->h->im.n * srv->h->im.vw))
     return fail(PGX_ERROR_NOT_FINITE, "b is not finite");
   {
     std::lock_guard<std::mutex> lock(srv->mu);
@@ -3691,7 +3764,8 @@ int pgx_pool_submit(pgx_pool p, int32_t index, double* x, const double* b, int32
     std::lock_guard<std::mutex> lock(p->mu);
     if (index < 0 || index >= (int)p->members.size())
       return fail(PGX_ERROR_INVALID_PARAM, "member %d outside [0, %d)", index, (int)p->members.size());
-    if (location == PGX_LOCATION_HOST && !all_finite(b, p->members[index].h->im.n))
+    if (location == PGX_LOCATION_HOST &&
+        !all_finite(b, (long long)p->members[index].h->im.n * p->members[index].h->im.vw))
       return fail(PGX_ERROR_NOT_FINITE, "b is not finite");
     p->queue.push_back({index, x, b, location, request_id});
   }

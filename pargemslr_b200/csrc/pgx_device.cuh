@@ -11,7 +11,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "pgx_complex.cuh"
+
 namespace pgx {
+
+using ::__shfl_xor_sync;  // the real forms beside the complex overload
 
 constexpr int kWarp = 32;
 constexpr int KMAX = 128;          // largest Krylov dimension a handle accepts
@@ -50,7 +54,12 @@ struct SkipR {
 // ---------------------------------------------------------------- FGMRES
 // Device-resident state of one flexible GMRES solve (FlexGmresClass::Solve,
 // ParGeMSLR SRC/solvers/fgmres.hpp:263-558).  H is column-major (KMAX+1) x KMAX.
-struct FgmresDev {
+// S is the solver's scalar: double, or cf64 for a complex solve (Hessenberg,
+// rotations and right-hand side of the least-squares problem complex; norms,
+// tolerances and the lazy column scales real).  The header up to sc has the
+// same layout for both.
+template <typename S>
+struct FgmresDevT {
   int done;        // solve finished (converged, max iterations or breakdown)
   int cycle_done;  // current restart cycle finished
   int breakdown;   // Givens breakdown: the reference skips the x update
@@ -68,16 +77,39 @@ struct FgmresDev {
   int absolute;
   int pad;
   double sc[KMAX + 1];     // V(:,c) = Vstored(:,c) * sc[c] (lazy normalisation)
-  double hcol[KMAX + 1];   // column of H being built
-  double coefA[KMAX + 1];  // first Gram-Schmidt coefficients
-  double coefB[KMAX + 1];  // re-orthogonalisation coefficients
-  double c[KMAX], s[KMAX], rs[KMAX + 1], y[KMAX];
-  double H[(KMAX + 1) * KMAX];
-  double hist[KMAX];  // Givens estimate after each column of the current cycle (0 at a breakdown)
+  double hist[KMAX];       // Givens estimate after each column of the current cycle (0 at a breakdown)
+  S hcol[KMAX + 1];   // column of H being built
+  S coefA[KMAX + 1];  // first Gram-Schmidt coefficients
+  S coefB[KMAX + 1];  // re-orthogonalisation coefficients
+  S c[KMAX], s[KMAX], rs[KMAX + 1], y[KMAX];
+  S H[(KMAX + 1) * KMAX];
 };
+using FgmresDev = FgmresDevT<double>;
 
 template <typename T>
+__device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
+template <>
+__device__ __forceinline__ cf32 ldg<cf32>(const cf32* p) {
+  const float2 v = __ldg((const float2*)p);
+  return cf32(v.x, v.y);
+}
+template <>
+__device__ __forceinline__ cf64 ldg<cf64>(const cf64* p) {
+  const double2 v = __ldg((const double2*)p);
+  return cf64(v.x, v.y);
+}
+template <typename T>
 __device__ __forceinline__ T ldcg(const T* p) { return __ldcg(p); }
+template <>
+__device__ __forceinline__ cf32 ldcg<cf32>(const cf32* p) {
+  const float2 v = __ldcg((const float2*)p);
+  return cf32(v.x, v.y);
+}
+template <>
+__device__ __forceinline__ cf64 ldcg<cf64>(const cf64* p) {
+  const double2 v = __ldcg((const double2*)p);
+  return cf64(v.x, v.y);
+}
 
 template <typename T>
 __device__ __forceinline__ T group_reduce(T v, int S, int lane) {
@@ -115,7 +147,7 @@ __device__ __forceinline__ TC row_dot(int k1, int k2, int lane, const int* __res
   for (int u = 0; u < kSpmvUnroll; u++) {
     const int k = k1 + lane + u * S;
     c[u] = k < k2 ? __ldg(&cj[k]) : -1;
-    v[u] = k < k2 ? __ldg(&va[k]) : TA(0);
+    v[u] = k < k2 ? ldg(&va[k]) : TA(0);
     if (k < k2 && (unsigned)c[u] >= (unsigned)xcols) {
       bad = true;  // a column outside x: the entry is skipped
       c[u] = -1;
@@ -131,7 +163,7 @@ __device__ __forceinline__ TC row_dot(int k1, int k2, int lane, const int* __res
   for (int k = k1 + lane + kSpmvUnroll * S; k < k2; k += S) {
     const int cc = __ldg(&cj[k]);
     if ((unsigned)cc < (unsigned)xcols)
-      acc += (TC)__ldg(&va[k]) * (TC)x[cc];
+      acc += (TC)ldg(&va[k]) * (TC)x[cc];
     else
       bad = true;
   }
@@ -161,6 +193,23 @@ __device__ __forceinline__ void load_block4<double>(const double* __restrict__ p
   v[1] = a.y;
   v[2] = b.x;
   v[3] = b.y;
+}
+
+template <>
+__device__ __forceinline__ void load_block4<cf32>(const cf32* __restrict__ p, cf32* v) {
+  const float4 a = __ldg((const float4*)p), b = __ldg((const float4*)p + 1);
+  v[0] = cf32(a.x, a.y);
+  v[1] = cf32(a.z, a.w);
+  v[2] = cf32(b.x, b.y);
+  v[3] = cf32(b.z, b.w);
+}
+template <>
+__device__ __forceinline__ void load_block4<cf64>(const cf64* __restrict__ p, cf64* v) {
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const double2 a = __ldg((const double2*)p + u);
+    v[u] = cf64(a.x, a.y);
+  }
 }
 
 template <typename TA, typename TX, typename TC, int S>
@@ -276,7 +325,7 @@ __global__ void __launch_bounds__(256) merge_spmv_kernel(
   int rend = r < nrows ? __ldg(&rp[r + 1]) : nnz;
   while (r < r1 || k < k1) {
     if (r < nrows && k < rend && k < k1) {
-      acc += (TC)__ldg(&va[k]) * (TC)x[__ldg(&cj[k])];
+      acc += (TC)ldg(&va[k]) * (TC)x[__ldg(&cj[k])];
       k++;
     } else {
       // row r ends inside this range: its sum here plus the carries of the
@@ -363,6 +412,49 @@ struct Sentinel<float> {
   }
 };
 
+// Complex values: the sentinel sits in the real part.  A complex64 value is
+// published with one 8-byte store.  A complex128 value spans two 8-byte
+// words: the imaginary part is stored first and the real part after it with
+// release semantics, and a reader loads the real part with acquire semantics
+// before the imaginary part, so a reader that sees a final real part also
+// sees the imaginary part that belongs to it.
+template <>
+struct Sentinel<cf32> {
+  static __device__ __forceinline__ cf32 value() { return cf32(Sentinel<float>::value(), 0.f); }
+  static __device__ __forceinline__ bool is(const cf32& v) { return Sentinel<float>::is(v.x); }
+  static __device__ __forceinline__ cf32 load(const cf32* p) {
+    unsigned long long u;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(u) : "l"(p) : "memory");
+    return cf32(__int_as_float((int)(u & 0xffffffffull)), __int_as_float((int)(u >> 32)));
+  }
+  static __device__ __forceinline__ void store(cf32* p, const cf32& v) {
+    const unsigned long long u =
+        (unsigned long long)(unsigned)__float_as_int(v.x) | ((unsigned long long)(unsigned)__float_as_int(v.y) << 32);
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(u) : "memory");
+  }
+};
+template <>
+struct Sentinel<cf64> {
+  static __device__ __forceinline__ cf64 value() { return cf64(Sentinel<double>::value(), 0.0); }
+  static __device__ __forceinline__ bool is(const cf64& v) { return Sentinel<double>::is(v.x); }
+  static __device__ __forceinline__ cf64 load(const cf64* p) {
+    double re, im;
+    asm volatile("ld.acquire.gpu.global.f64 %0, [%1];" : "=d"(re) : "l"(&p->x) : "memory");
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(im) : "l"(&p->y) : "memory");
+    return cf64(re, im);
+  }
+  static __device__ __forceinline__ void store(cf64* p, const cf64& v) {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(&p->y), "d"(v.y) : "memory");
+    asm volatile("st.release.gpu.global.f64 [%0], %1;" ::"l"(&p->x), "d"(v.x) : "memory");
+  }
+};
+// the segmented solve's operand prefetch: a complex128 operand goes through
+// the acquire/release pair above
+template <typename T>
+__device__ __forceinline__ T ldcg_dep(const T* p) { return ldcg(p); }
+template <>
+__device__ __forceinline__ cf64 ldcg_dep<cf64>(const cf64* p) { return Sentinel<cf64>::load(p); }
+
 template <typename T>
 __global__ void sentinel_fill_kernel(int n, T* p) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = Sentinel<T>::value();
@@ -420,7 +512,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(
           Sentinel<T>::store(&x[r], (yr - acc) * dinv[r]);
         } else {
           T b = rhs[r];
-          if (rhs_scale) b = (T)((double)b * rs);
+          if (rhs_scale) b = to<T>(to<typename Sc<T>::acc>(b) * rs);
           x[r] = Sentinel<T>::value();
           Sentinel<T>::store(&y[r], b - acc);
         }
@@ -455,15 +547,17 @@ constexpr int kSegThreads = 1024;
 constexpr int kSegRows = 1024;
 constexpr int kSegNnzF64 = 8192;    // staged cj + va + gathered operands: 160 KB (FP64)
 constexpr int kSegNnzF32 = 12288;   // 144 KB (FP32)
+constexpr int kSegNnzC128 = 4096;   // 192 KB (complex128)
 
 template <typename T>
 struct SegCfg {
-  static constexpr int nnz = sizeof(T) == 8 ? kSegNnzF64 : kSegNnzF32;
+  static constexpr int nnz = sizeof(T) == 16 ? kSegNnzC128 : sizeof(T) == 8 ? kSegNnzF64 : kSegNnzF32;
   // smem layout: xs[kSegRows] T | sb[kSegRows] T | sd[kSegRows] T | va[nnz] T | ext[nnz] T |
   // cj[nnz] int | ord[kSegRows] int | rp[kSegRows+4] int | lvb[kSegRows+4] int; the host keeps
   // segments within kSegRows-4 rows and nnz-4 nonzeros
   static constexpr size_t bytes =
       sizeof(T) * (size_t)(3 * kSegRows + 2 * nnz) + sizeof(int) * (size_t)(nnz + kSegRows + 2 * (kSegRows + 4));
+  static_assert(bytes <= 227 * 1024, "segmented solve exceeds the shared memory of a CTA");
 };
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
@@ -530,11 +624,11 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
       const int r = __ldg(&ord[r0 + i]);
       if (r < 0) continue;
       if (UPPER) {
-        sb[i] = __ldcg(&y[r]);
-        sd[i] = __ldg(&dinv[r]);
+        sb[i] = ldcg_dep(&y[r]);
+        sd[i] = ldg(&dinv[r]);
       } else {
-        T bb = __ldg(&rhs[r]);
-        if (rhs_scale) bb = (T)((double)bb * rs);
+        T bb = ldg(&rhs[r]);
+        if (rhs_scale) bb = to<T>(to<typename Sc<T>::acc>(bb) * rs);
         sb[i] = bb;
       }
     }
@@ -546,7 +640,7 @@ __global__ void __launch_bounds__(kSegThreads) trsv_seg_kernel(
     // 4/8-byte stores, so a load sees either the sentinel or the final value.
     for (int k = tid; k < z1 - z0; k += blockDim.x) {
       const int c = scj[k];
-      if (c >= 0 && c < n) sext[k] = __ldcg(&dep[c]);
+      if (c >= 0 && c < n) sext[k] = ldcg_dep(&dep[c]);
     }
     // this segment's rows: hand the buffers to the next pass
     for (int i = tid; i < r1 - r0; i += blockDim.x) {
@@ -656,11 +750,15 @@ struct PtrR {
 // access outside shared memory.
 template <typename T, int R>
 struct PipeCfg {
+  // sizes by value width: 4 bytes (FP32), 8 (FP64, complex64), 16 (complex128)
   static constexpr bool d = sizeof(T) == 8;
-  static constexpr int ring = d ? (R == 1 ? 8192 : R == 2 ? 4096 : 2048) : (R == 4 ? 4096 : 8192);
-  static constexpr int far = d ? (R == 1 ? 512 : 256) : 512;
-  static constexpr int nnz = d ? (R == 4 ? 1536 : 2048) : (R == 1 ? 4096 : R == 2 ? 3072 : 2560);
-  static constexpr int rows = d ? 256 : (R == 1 ? 512 : R == 2 ? 384 : 320);
+  static constexpr bool z = sizeof(T) == 16;
+  static constexpr int ring = z ? (R == 1 ? 4096 : R == 2 ? 2048 : 1024)
+                                : d ? (R == 1 ? 8192 : R == 2 ? 4096 : 2048) : (R == 4 ? 4096 : 8192);
+  static constexpr int far = z ? 256 : d ? (R == 1 ? 512 : 256) : 512;
+  static constexpr int nnz = z ? (R == 4 ? 768 : 1024)
+                               : d ? (R == 4 ? 1536 : 2048) : (R == 1 ? 4096 : R == 2 ? 3072 : 2560);
+  static constexpr int rows = z ? (R == 4 ? 128 : 192) : d ? 256 : (R == 1 ? 512 : R == 2 ? 384 : 320);
   // per stage: va[nnz] T | sb[R][rows] T | sd[rows] T | cj[nnz] | ord[rows] | rp[rows+4] | lvb[rows+4] | fc[far]
   static constexpr size_t buf_bytes =
       sizeof(T) * (size_t)(nnz + (R + 1) * rows) + sizeof(int) * (size_t)(nnz + rows + 2 * (rows + 4) + far);
@@ -704,10 +802,14 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) 
 }
 template <typename T>
 __device__ __forceinline__ void cp_async_elem(T* dst, const T* src) {
-  if (sizeof(T) == 8)
+  if (sizeof(T) == 16) {
+    unsigned sd = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(sd), "l"(src) : "memory");
+  } else if (sizeof(T) == 8) {
     cp_async8(dst, src);
-  else
+  } else {
     cp_async4(dst, src);
+  }
 }
 
 // mbarrier and bulk-copy (TMA, non-tensor) helpers.  The copies read this
@@ -1077,8 +1179,15 @@ enum EpiKind {
   EPI_INIT_INNER = 7,  // inner solve from x0 = 0: normb = normr = ||rhs||
 };
 
+// Reductions and coefficients are carried in TsAcc<TW>: double for a real
+// solve, cf64 for a complex one (dots conjugate the basis column,
+// V(:,c)^H w, as the reference's complex VectorDot does).
+template <typename TW>
+using TsAcc = typename Sc<TW>::acc;
+
 template <typename TV, typename TM, typename TW>
 struct TsArgs {
+  using A = TsAcc<TW>;
   int n;
   int ncols;
   const int* ncols_dev;  // if set, the column count is read here (<= KMAX)
@@ -1088,38 +1197,40 @@ struct TsArgs {
   const TM* M;
   long long ldm;
   const double* msc;
-  const double* coef;
+  const A* coef;
   double sign;
   const TW* in;          // null: zero input
   const double* in_scale;
   TW* out;
-  double* partial;       // [KMAX+1][gridDim.x]
+  A* partial;            // [KMAX+1][gridDim.x]
   unsigned int* counter; // zero between launches
   int epi;
-  FgmresDev* st;
-  double* dst;
+  FgmresDevT<A>* st;
+  A* dst;
   int j;
   Skip skip;
 };
 
-__device__ inline void fgmres_givens(FgmresDev* st, int j, double t) {
+template <typename S>
+__device__ inline void fgmres_givens(FgmresDevT<S>* st, int j, double t) {
   // H(:, j) from the Gram-Schmidt coefficients and ||w||
   // (PargemslrMgs sets H(0..k, k) and H(k+1, k), matrixops.cpp:10728-10806)
   const int ldh = KMAX + 1;
-  double* H = st->H + (size_t)j * ldh;
+  S* H = st->H + (size_t)j * ldh;
   for (int c = 0; c <= j; c++) H[c] = st->hcol[c];
-  H[j + 1] = t;
+  H[j + 1] = S(t);
   st->sc[j + 1] = 1.0 / t;
   st->iter += 1;
   st->i = j + 1;
-  // apply the previous rotations, then form the new one (fgmres.hpp:430-458)
+  // apply the previous rotations, then form the new one (fgmres.hpp:430-458;
+  // for complex values the rotation is conj(c), s as in the reference)
   for (int k = 1; k <= j; k++) {
-    double hii = H[k - 1];
-    H[k - 1] = st->c[k - 1] * hii + st->s[k - 1] * H[k];
+    S hii = H[k - 1];
+    H[k - 1] = conj(st->c[k - 1]) * hii + st->s[k - 1] * H[k];
     H[k] = -st->s[k - 1] * hii + st->c[k - 1] * H[k];
   }
-  double hii = H[j], hii1 = H[j + 1];
-  double gam = sqrt(fabs(hii) * fabs(hii) + fabs(hii1) * fabs(hii1));
+  S hii = H[j], hii1 = H[j + 1];
+  double gam = sqrt(cabs(hii) * cabs(hii) + cabs(hii1) * cabs(hii1));
   if (fabs(gam) < st->eps) {
     // breakdown: the reference jumps past the solution update (fgmres.hpp:440-443)
     // and records no residual for this iteration
@@ -1133,9 +1244,9 @@ __device__ inline void fgmres_givens(FgmresDev* st, int j, double t) {
   st->c[j] = hii / gam;
   st->s[j] = hii1 / gam;
   st->rs[j + 1] = -st->s[j] * st->rs[j];
-  st->rs[j] = st->c[j] * st->rs[j];
-  H[j] = st->c[j] * hii + st->s[j] * hii1;
-  st->normr = fabs(st->rs[j + 1]);
+  st->rs[j] = conj(st->c[j]) * st->rs[j];
+  H[j] = conj(st->c[j]) * hii + st->s[j] * hii1;
+  st->normr = cabs(st->rs[j + 1]);
   st->hist[j] = st->normr;  // _rel_res_vector[_iter] = normr / normb (fgmres.hpp:450-452)
   const bool conv = st->normr <= st->tolr;
   if (conv) st->converged = 1;
@@ -1144,41 +1255,42 @@ __device__ inline void fgmres_givens(FgmresDev* st, int j, double t) {
     if (conv || st->iter >= st->maxits) st->done = 1;
     // back substitution H y = rs, in place in rs (fgmres.hpp:471-480)
     const int i = st->i;
-    double* rs = st->rs;
-    rs[i - 1] /= st->H[(size_t)(i - 1) * ldh + (i - 1)];
+    S* rs = st->rs;
+    rs[i - 1] = rs[i - 1] / st->H[(size_t)(i - 1) * ldh + (i - 1)];
     for (int k = i - 2; k >= 0; k--) {
       for (int jj = k + 1; jj < i; jj++) rs[k] -= st->H[(size_t)jj * ldh + k] * rs[jj];
-      rs[k] /= st->H[(size_t)k * ldh + k];
+      rs[k] = rs[k] / st->H[(size_t)k * ldh + k];
     }
   }
 }
 
 template <typename TV, typename TM, typename TW>
-__device__ inline void ts_epilogue(const TsArgs<TV, TM, TW>& a, const double* sums, int ncols) {
-  FgmresDev* st = a.st;
+__device__ inline void ts_epilogue(const TsArgs<TV, TM, TW>& a, const TsAcc<TW>* sums, int ncols) {
+  using A = TsAcc<TW>;
+  FgmresDevT<A>* st = a.st;
   switch (a.epi) {
     case EPI_STORE:
       for (int c = 0; c < ncols; c++) a.dst[c] = sums[c] * (a.vsc ? a.vsc[c] : 1.0);
       break;
     case EPI_CGS_FIRST:
       for (int c = 0; c < ncols; c++) {
-        double h = sums[c] * (a.vsc ? a.vsc[c] : 1.0);
+        A h = sums[c] * (a.vsc ? a.vsc[c] : 1.0);
         st->hcol[c] = h;
         st->coefA[c] = h;
       }
       break;
     case EPI_CGS_SECOND:
       for (int c = 0; c < ncols; c++) {
-        double h = sums[c] * (a.vsc ? a.vsc[c] : 1.0);
+        A h = sums[c] * (a.vsc ? a.vsc[c] : 1.0);
         st->hcol[c] += h;
         st->coefB[c] = h;
       }
       break;
     case EPI_GIVENS:
-      fgmres_givens(st, a.j, sqrt(sums[0]));
+      fgmres_givens(st, a.j, sqrt(re(sums[0])));
       break;
     case EPI_NORMB:
-      st->normb = sqrt(sums[0]);
+      st->normb = sqrt(re(sums[0]));
       if (st->normb < st->eps) {
         st->done = 1;
         st->cycle_done = 1;
@@ -1192,7 +1304,7 @@ __device__ inline void ts_epilogue(const TsArgs<TV, TM, TW>& a, const double* su
       st->converged = 0;
       st->breakdown = 0;
       if (st->done) break;  // zero right-hand side
-      const double normr = sqrt(sums[0]);
+      const double normr = sqrt(re(sums[0]));
       st->normr = normr;
       st->normr0 = normr;
       if (normr < st->eps) {
@@ -1202,13 +1314,13 @@ __device__ inline void ts_epilogue(const TsArgs<TV, TM, TW>& a, const double* su
         break;
       }
       st->tolr = st->absolute ? st->tol : st->tol * st->normb;
-      st->rs[0] = normr;
+      st->rs[0] = A(normr);
       st->sc[0] = 1.0 / normr;
       st->cycle_done = 0;
       break;
     }
     case EPI_INIT_INNER: {
-      const double normb = sqrt(sums[0]);
+      const double normb = sqrt(re(sums[0]));
       st->normb = normb;
       st->normr = normb;
       st->i = 0;
@@ -1223,7 +1335,7 @@ __device__ inline void ts_epilogue(const TsArgs<TV, TM, TW>& a, const double* su
         break;
       }
       st->tolr = st->absolute ? st->tol : st->tol * normb;
-      st->rs[0] = normb;
+      st->rs[0] = A(normb);
       st->sc[0] = 1.0 / normb;
       break;
     }
@@ -1234,9 +1346,10 @@ __device__ inline void ts_epilogue(const TsArgs<TV, TM, TW>& a, const double* su
 
 template <typename TV, typename TM, typename TW, int MODE>
 __global__ void __launch_bounds__(kTsThreads) ts_kernel(TsArgs<TV, TM, TW> a) {
+  using A = TsAcc<TW>;
   if (a.skip.on()) return;
-  __shared__ double scoef[KMAX + 1];
-  __shared__ double sacc[KMAX + 1];
+  __shared__ A scoef[KMAX + 1];
+  __shared__ A sacc[KMAX + 1];
   __shared__ double swarp[kTsThreads / 32];
   __shared__ int s_last;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1248,8 +1361,8 @@ __global__ void __launch_bounds__(kTsThreads) ts_kernel(TsArgs<TV, TM, TW> a) {
   if (MODE == TS_UPDATE && ncols == 0 && a.in == a.out) return;  // nothing to add
   const double in_s = a.in_scale ? *a.in_scale : 1.0;
   for (int c = tid; c <= KMAX; c += kTsThreads) {
-    scoef[c] = (update && c < ncols) ? a.sign * a.coef[c] * (a.msc ? a.msc[c] : 1.0) : 0.0;
-    sacc[c] = 0.0;
+    scoef[c] = (update && c < ncols) ? a.sign * a.coef[c] * (a.msc ? a.msc[c] : 1.0) : A(0.0);
+    sacc[c] = A(0.0);
   }
   if (tid < NW) swarp[tid] = 0.0;
   __syncthreads();
@@ -1257,23 +1370,23 @@ __global__ void __launch_bounds__(kTsThreads) ts_kernel(TsArgs<TV, TM, TW> a) {
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int r0 = tile * kTsThreads;
     const int row = r0 + tid;
-    double wv = 0.0;
+    A wv = A(0.0);
     if (row < a.n) {
-      wv = a.in ? (double)a.in[row] * in_s : 0.0;
+      wv = a.in ? to<A>(a.in[row]) * in_s : A(0.0);
       if (update) {
-        double acc = 0.0;
+        A acc = A(0.0);
         const TM* m = a.M + row;
-        for (int c = 0; c < ncols; c++) acc += (double)m[(long long)c * a.ldm] * scoef[c];
+        for (int c = 0; c < ncols; c++) acc += to<A>(m[(long long)c * a.ldm]) * scoef[c];
         wv += acc;
       }
-      if (MODE != TS_DOT && a.out) a.out[row] = (TW)wv;
+      if (MODE != TS_DOT && a.out) a.out[row] = to<TW>(wv);
     }
     if (MODE == TS_UPDATE_NORM || MODE == TS_NORM_COPY) {
-      double sq = (row < a.n) ? wv * wv : 0.0;
+      double sq = (row < a.n) ? abs2(wv) : 0.0;
       if (MODE == TS_UPDATE_NORM) {
         // the norm of the stored (rounded) vector, as Norm2 of the reference
-        TW stored = (TW)wv;
-        sq = (row < a.n) ? (double)stored * (double)stored : 0.0;
+        TW stored = to<TW>(wv);
+        sq = (row < a.n) ? abs2(to<A>(stored)) : 0.0;
       }
       sq = warp_reduce(sq);
       if (lane == 0) swarp[warp] += sq;  // one writer per slot: deterministic
@@ -1283,11 +1396,10 @@ __global__ void __launch_bounds__(kTsThreads) ts_kernel(TsArgs<TV, TM, TW> a) {
       const int nrows_tile = min(kTsThreads, a.n - r0);
       for (int c = warp; c < ncols; c += NW) {
         const TV* v = a.V + (long long)c * a.ldv + r0;
-        double acc = 0.0;
+        A acc = A(0.0);
         for (int k = lane; k < nrows_tile; k += 32) {
-          double w = (MODE == TS_DOT) ? (a.in ? (double)a.in[r0 + k] * in_s : 0.0)
-                                      : (double)a.out[r0 + k];
-          acc += (double)v[k] * w;
+          A w = (MODE == TS_DOT) ? (a.in ? to<A>(a.in[r0 + k]) * in_s : A(0.0)) : to<A>(a.out[r0 + k]);
+          acc += conj(to<A>(v[k])) * w;
         }
         acc = warp_reduce(acc);
         if (lane == 0) sacc[c] += acc;
@@ -1300,7 +1412,7 @@ __global__ void __launch_bounds__(kTsThreads) ts_kernel(TsArgs<TV, TM, TW> a) {
   if ((MODE == TS_UPDATE_NORM || MODE == TS_NORM_COPY) && tid == 0) {
     double t = 0.0;
     for (int w = 0; w < NW; w++) t += swarp[w];
-    sacc[0] = t;
+    sacc[0] = A(t);
   }
   __syncthreads();
   // block partials -> global, column-major by block
@@ -1315,8 +1427,8 @@ __global__ void __launch_bounds__(kTsThreads) ts_kernel(TsArgs<TV, TM, TW> a) {
   if (!s_last) return;
   __threadfence();
   for (int c = warp; c < nred; c += NW) {
-    double acc = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) acc += __ldcg(&a.partial[(long long)c * gridDim.x + b]);
+    A acc = A(0.0);
+    for (int b = lane; b < (int)gridDim.x; b += 32) acc += ldcg(&a.partial[(long long)c * gridDim.x + b]);
     acc = warp_reduce(acc);
     if (lane == 0) sacc[c] = acc;
   }
@@ -1328,36 +1440,65 @@ __global__ void __launch_bounds__(kTsThreads) ts_kernel(TsArgs<TV, TM, TW> a) {
   }
 }
 
-__global__ void fgmres_cycle_reset_kernel(FgmresDev* st, Skip skip) {
+template <typename S>
+__global__ void fgmres_cycle_reset_kernel(FgmresDevT<S>* st, Skip skip) {
   if (skip.on()) return;
   st->i = 0;
   if (st->done) return;
   st->cycle_done = 0;
-  st->rs[0] = st->normr;
+  st->rs[0] = S(st->normr);
   st->sc[0] = 1.0 / st->normr;
 }
 
 // --------------------------------------------------- permutation + convert
 // out[i] = (TO)(in[perm[i]] * scale)  (IntVectorClass::GatherPerm, int_vector.cpp:668)
+// Each thread handles kPermUnroll entries a block apart: it loads their
+// permutation indices, then the values they name, then stores, so the
+// dependent loads of several entries are in flight together.
+constexpr int kPermUnroll = 4;
 template <typename TI, typename TO>
-__global__ void gather_kernel(int n, const int* __restrict__ perm, const TI* __restrict__ in,
-                              const double* __restrict__ scale, TO* __restrict__ out, Skip skip) {
+__global__ void __launch_bounds__(256) gather_kernel(int n, const int* __restrict__ perm, const TI* __restrict__ in,
+                                                     const double* __restrict__ scale, TO* __restrict__ out,
+                                                     Skip skip) {
   if (skip.on()) return;
   const double s = scale ? *scale : 1.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int p = perm ? perm[i] : i;
-    out[i] = scale ? (TO)((double)in[p] * s) : (TO)in[p];
+  const int stride = gridDim.x * blockDim.x * kPermUnroll;
+  for (int base = blockIdx.x * blockDim.x * kPermUnroll + threadIdx.x; base < n; base += stride) {
+    int p[kPermUnroll];
+#pragma unroll
+    for (int u = 0; u < kPermUnroll; u++) {
+      const int i = base + u * blockDim.x;
+      p[u] = i < n ? (perm ? __ldg(&perm[i]) : i) : -1;
+    }
+    TI v[kPermUnroll];
+#pragma unroll
+    for (int u = 0; u < kPermUnroll; u++) v[u] = p[u] >= 0 ? in[p[u]] : TI(0);
+#pragma unroll
+    for (int u = 0; u < kPermUnroll; u++) {
+      const int i = base + u * blockDim.x;
+      if (i < n) out[i] = scale ? to<TO>(to<typename Sc<TI>::acc>(v[u]) * s) : to<TO>(v[u]);
+    }
   }
 }
 
 // out[perm[i]] = in[i]  (IntVectorClass::ScatterRperm, int_vector.cpp:629)
 template <typename TI, typename TO>
-__global__ void scatter_kernel(int n, const int* __restrict__ perm, const TI* __restrict__ in,
-                               TO* __restrict__ out, Skip skip) {
+__global__ void __launch_bounds__(256) scatter_kernel(int n, const int* __restrict__ perm, const TI* __restrict__ in,
+                                                      TO* __restrict__ out, Skip skip) {
   if (skip.on()) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int p = perm ? perm[i] : i;
-    out[p] = (TO)in[i];
+  const int stride = gridDim.x * blockDim.x * kPermUnroll;
+  for (int base = blockIdx.x * blockDim.x * kPermUnroll + threadIdx.x; base < n; base += stride) {
+    int p[kPermUnroll];
+    TI v[kPermUnroll];
+#pragma unroll
+    for (int u = 0; u < kPermUnroll; u++) {
+      const int i = base + u * blockDim.x;
+      p[u] = i < n ? (perm ? __ldg(&perm[i]) : i) : -1;
+      v[u] = i < n ? in[i] : TI(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kPermUnroll; u++)
+      if (p[u] >= 0) out[p[u]] = to<TO>(v[u]);
   }
 }
 

@@ -24,10 +24,19 @@ def init(device: int = 0) -> None:
         _initialized_device = device
 
 
+def _precision_code(precision: str, cplx: bool) -> int:
+    """The C ABI's precision code: FP64 or mixed, over real or complex values."""
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"unknown precision {precision!r}")
+    if cplx:
+        return _abi.PRECISION_COMPLEX_FP64 if precision == "fp64" else _abi.PRECISION_COMPLEX_MIXED
+    return _abi.PRECISION_FP64 if precision == "fp64" else _abi.PRECISION_MIXED
+
+
 def import_structures(st: GemslrStructures, precision: str = "fp64") -> C.c_void_p:
     """A handle holding the structures, set level by level (pgx_gemslr_create / set_*), not yet committed
     to the device; the caller commits or destroys it."""
-    prec = {"fp64": _abi.PRECISION_FP64, "mixed": _abi.PRECISION_MIXED}[precision]
+    prec = _precision_code(precision, st.complex)
     L = _abi.lib()
     h = C.c_void_p()
     _abi.check(L.pgx_gemslr_create(C.byref(h), st.n, prec))
@@ -45,7 +54,7 @@ def import_structures(st: GemslrStructures, precision: str = "fp64") -> C.c_void
         for l, lv in enumerate(st.levels):
             desc = _abi.Level()
             dom = np.ascontiguousarray(lv.dom_ptr, np.int32)
-            dinv = np.ascontiguousarray(lv.dinv, np.float64)
+            dinv = _abi.doubles(lv.dinv)
             keep.extend([dom, dinv])
             desc.ncomp = lv.ncomp
             desc.dom_ptr = _abi.ptr(dom)
@@ -58,8 +67,8 @@ def import_structures(st: GemslrStructures, precision: str = "fp64") -> C.c_void
                 desc.F = _abi.csr_struct(*lv.F, keep=keep)
             desc.rank = lv.rank
             if lv.rank > 0:
-                W = np.ascontiguousarray(lv.W, np.float64)
-                WH = np.ascontiguousarray(lv.WH, np.float64)
+                W = _abi.doubles(lv.W)
+                WH = _abi.doubles(lv.WH)
                 keep.extend([W, WH])
                 desc.W = _abi.ptr(W)
                 desc.WH = _abi.ptr(WH)
@@ -75,12 +84,16 @@ class GemslrHandle:
     """GeMSLR-preconditioned FGMRES on one GPU, built from post-setup structures.
 
     precision: ``"fp64"`` (the reference's arithmetic) or ``"mixed"`` (FP32
-    preconditioner apply inside FP64 FGMRES).
+    preconditioner apply inside FP64 FGMRES).  Complex structures (the
+    reference's complexd instantiation) give a complex handle: complex128
+    throughout, or a complex64 preconditioner inside complex128 FGMRES; its
+    vectors are complex128 arrays.
     """
 
     def __init__(self, st: GemslrStructures, precision: str = "fp64", device: int = 0):
         init(device)
         self.n = st.n
+        self.complex = st.complex
         self.precision = precision
         self._h = None
         self._h = import_structures(st, precision)
@@ -112,9 +125,14 @@ class GemslrHandle:
         _abi.check(_abi.lib().pgx_gemslr_setup(C.byref(h), C.byref(Ac), _abi.ptr(p), prec))
         self = cls.__new__(cls)
         self.n = n
+        self.complex = False
         self.precision = precision
         self._h = h
         return self
+
+    @property
+    def _dtype(self):
+        return np.complex128 if getattr(self, "complex", False) else np.float64
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -134,8 +152,8 @@ class GemslrHandle:
 
     def solve(self, b: np.ndarray, x0: Optional[np.ndarray] = None, params: Optional[np.ndarray] = None):
         """Host-array solve; returns (x, result dict)."""
-        b = np.ascontiguousarray(b, np.float64)
-        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        b = np.ascontiguousarray(b, self._dtype)
+        x = np.zeros(self.n, self._dtype) if x0 is None else np.array(x0, dtype=self._dtype, copy=True)
         p = None if params is None else np.ascontiguousarray(params, np.float64)
         res = _abi.Result()
         rc = _abi.lib().pgx_gemslr_solve(self._h, _abi.ptr(x), _abi.ptr(b), _abi.LOCATION_HOST, _abi.ptr(p),
@@ -185,8 +203,8 @@ class GemslrHandle:
 
     def solve_batch(self, B: np.ndarray, X0: Optional[np.ndarray] = None, params: Optional[np.ndarray] = None):
         """Host-array batch solve: B is (nrhs, n), one right-hand side per row; returns (X, results)."""
-        B = np.ascontiguousarray(B, np.float64)
-        X = np.zeros_like(B) if X0 is None else np.array(X0, dtype=np.float64, copy=True, order="C")
+        B = np.ascontiguousarray(B, self._dtype)
+        X = np.zeros_like(B) if X0 is None else np.array(X0, dtype=self._dtype, copy=True, order="C")
         res = self.solve_batch_ptr(B.shape[0], _abi.ptr(X), self.n, _abi.ptr(B), self.n, _abi.LOCATION_HOST,
                                    params)
         return X, res
@@ -221,8 +239,8 @@ class GemslrHandle:
 
     def apply(self, v: np.ndarray) -> np.ndarray:
         """z = M^-1 v (one preconditioner application) on host arrays."""
-        v = np.ascontiguousarray(v, np.float64)
-        z = np.zeros(self.n)
+        v = np.ascontiguousarray(v, self._dtype)
+        z = np.zeros(self.n, self._dtype)
         _abi.check(_abi.lib().pgx_gemslr_precond_apply(self._h, _abi.ptr(z), _abi.ptr(v), _abi.LOCATION_HOST))
         return z
 

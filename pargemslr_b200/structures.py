@@ -23,6 +23,12 @@ from . import pgxd
 CsrT = Tuple[np.ndarray, np.ndarray, np.ndarray, int, int]  # rowptr, colidx, values, rows, cols
 
 
+def _values(a: np.ndarray, cplx: bool) -> np.ndarray:
+    """A dumped value array: doubles, or for a complex dump {re, im} pairs as complex128."""
+    a = np.ascontiguousarray(a, np.float64)
+    return a.view(np.complex128) if cplx else a
+
+
 def empty_csr(rows: int, cols: int) -> CsrT:
     return (np.zeros(rows + 1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float64), rows, cols)
 
@@ -37,9 +43,10 @@ def block_diag(blocks: List[CsrT], offsets: List[int], n: int) -> CsrT:
         vas.append(bva)
     rp = np.cumsum(rp)
     cj = np.concatenate(cjs) if cjs else np.zeros(0, np.int64)
-    va = np.concatenate(vas) if vas else np.zeros(0)
+    dt = np.result_type(*[v.dtype for v in vas]) if vas else np.float64
+    va = np.concatenate(vas).astype(dt) if vas else np.zeros(0)
     # blocks are visited in offset order, so rows come out contiguous
-    return (rp.astype(np.int32), cj.astype(np.int32), va.astype(np.float64), n, n)
+    return (rp.astype(np.int32), cj.astype(np.int32), va, n, n)
 
 
 @dataclass
@@ -73,24 +80,30 @@ class GemslrStructures:
     def nlev(self) -> int:
         return len(self.levels)
 
+    @property
+    def complex(self) -> bool:
+        """Complex values (the reference's complexd instantiation)."""
+        return np.iscomplexobj(self.A[2])
+
     def nnz_factors(self) -> int:
         return int(sum(lv.L[1].size + lv.U[1].size for lv in self.levels))
 
 
-def _csr(d: Dict[str, np.ndarray], name: str) -> CsrT:
+def _csr(d: Dict[str, np.ndarray], name: str, cplx: bool = False) -> CsrT:
     shape = d[name + ".shape"]
-    return (d[name + ".i"].astype(np.int32), d[name + ".j"].astype(np.int32), d[name + ".a"].astype(np.float64),
+    return (d[name + ".i"].astype(np.int32), d[name + ".j"].astype(np.int32), _values(d[name + ".a"], cplx),
             int(shape[0]), int(shape[1]))
 
 
 def from_dump(path: str) -> GemslrStructures:
     """Load the structures a reference GemslrClass exported (PGXD container)."""
     d = pgxd.read(path)
+    z = "complex" in d and int(d["complex"][0]) == 1
     n = int(d["n"][0])
     nlev = int(d["nlev"][0])
     lev_ptr = d["lev_ptr"].astype(np.int32)
     qperm = d["qperm"].astype(np.int32) if d["qperm"].size else None
-    st = GemslrStructures(n=n, A=_csr(d, "A"), pperm=d["pperm"].astype(np.int32), qperm=qperm, lev_ptr=lev_ptr,
+    st = GemslrStructures(n=n, A=_csr(d, "A", z), pperm=d["pperm"].astype(np.int32), qperm=qperm, lev_ptr=lev_ptr,
                           inner_enable=int(d["inner.enable"][0]), inner_maxits=int(d["inner.maxits"][0]),
                           inner_tol=float(d["inner.tol"][0]))
     if int(d["solve_option"][0]) != 0:
@@ -107,19 +120,18 @@ def from_dump(path: str) -> GemslrStructures:
             pc = f"{pre}B{c}."
             if d[pc + "rperm"].size or d[pc + "cperm"].size:
                 raise ValueError("ILU factors with an internal permutation are not supported")
-            Ls.append(_csr(d, pc + "L"))
-            Us.append(_csr(d, pc + "U"))
-            Bs.append(_csr(d, pc + "A"))
-            Ds.append(d[pc + "D"])
+            Ls.append(_csr(d, pc + "L", z))
+            Us.append(_csr(d, pc + "U", z))
+            Bs.append(_csr(d, pc + "A", z))
+            Ds.append(_values(d[pc + "D"], z))
         lv = LevelStructures(ncomp=ncomp, dom_ptr=dom.astype(np.int32), L=block_diag(Ls, offs, nl),
-                             U=block_diag(Us, offs, nl), dinv=np.concatenate(Ds).astype(np.float64),
-                             B=block_diag(Bs, offs, nl))
+                             U=block_diag(Us, offs, nl), dinv=np.concatenate(Ds), B=block_diag(Bs, offs, nl))
         if l < nlev - 1:
-            lv.E = _csr(d, pre + "E")
-            lv.F = _csr(d, pre + "F")
+            lv.E = _csr(d, pre + "E", z)
+            lv.F = _csr(d, pre + "F", z)
             lv.rank = int(d[pre + "lrc"][0])
             if lv.rank > 0:
-                lv.W = d[pre + "W"].astype(np.float64)
-                lv.WH = d[pre + "WH"].astype(np.float64)
+                lv.W = _values(d[pre + "W"], z)
+                lv.WH = _values(d[pre + "WH"], z)
         st.levels.append(lv)
     return st

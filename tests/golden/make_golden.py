@@ -3,7 +3,8 @@
     make -C oracle REF=/root/reference/ParGeMSLR && python tests/golden/make_golden.py
 
 Each case runs the reference ParGeMSLR CPU solver (oracle/_ref/pgx_ref_driver,
-one thread) on a small problem and keeps its outputs:
+one thread; oracle/_ref/pgx_ref_driver_z for the complex cases, seeded
+complex-Gaussian right-hand sides) on a small problem and keeps its outputs:
   setup.bin     post-setup GeMSLR structures (permutation, levels, ILU factors,
                 BuildLevels schedules, E, F, W, WH, inner-solve settings)
   problem.bin   the matrix A and right-hand side b = A x_true
@@ -32,8 +33,26 @@ CASES = {
 }
 
 
+# complex cases: (nx ny nz shift_re shift_im alphax alphay alphaz, workload parameters, seed, right-hand sides)
+ZCASES = {
+    "zlap3d_12": ((12, 12, 12, 0.3, 0.05, 0.0, 0.0, 0.0), "zsmall", 11, 2),
+}
+
+
 def main():
-    for name, (lap, wl, seed) in CASES.items():
+    for name, (lap, wl, seed, nrhs) in ZCASES.items():
+        p = P.workload_params(wl)
+        n = lap[0] * lap[1] * lap[2]
+        B = oracle_runs.complex_rhs(n, nrhs, seed)
+        r = oracle_runs.run_complex(lap, p, B, apply_k=2, tag="golden")
+        dst = os.path.join(HERE, name)
+        os.makedirs(dst, exist_ok=True)
+        for f in ("setup.bin", "problem.bin", "apply.bin", "solution.bin", "result.txt"):
+            shutil.copy(os.path.join(r["dir"], f), os.path.join(dst, f))
+        with open(os.path.join(dst, "params.txt"), "w") as f:
+            f.write(f"workload={wl}\nlap={' '.join(str(v) for v in lap)}\nseed={seed}\nnrhs={nrhs}\n")
+        print(name, "iters", r["iters"])
+    for name, (lap, wl, seed) in CASES.items() if "--complex-only" not in sys.argv else ():
         p = P.workload_params(wl)
         n = lap[0] * lap[1] * lap[2]
         r = oracle_runs.run(lap=lap, params=p, xtrue=oracle_runs.x_true(n, seed), apply_k=2, tag="golden")

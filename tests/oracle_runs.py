@@ -94,3 +94,52 @@ def x_true(n: int, seed: int) -> np.ndarray:
     """x_true = 2u - 1, u ~ U[0,1) from a seeded generator (the workloads' solution)."""
     rng = np.random.default_rng(seed)
     return 2.0 * rng.random(n) - 1.0
+
+
+DRIVER_Z = os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver_z")
+
+
+def available_complex() -> bool:
+    return os.path.exists(DRIVER_Z)
+
+
+def complex_rhs(n: int, nrhs: int, seed: int) -> np.ndarray:
+    """nrhs seeded complex-Gaussian right-hand sides (real and imaginary parts ~ N(0,1)), one per row."""
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((nrhs, n)) + 1j * rng.standard_normal((nrhs, n))
+
+
+def run_complex(lap, params: np.ndarray, B: np.ndarray, apply_k: int = 0, threads: int = 1,
+                tag: str = "") -> Dict[str, object]:
+    """Run the reference over complexd (pgx_ref_driver_z) on the complex shifted Laplacian
+    lap = (nx, ny, nz, shift_re, shift_im, ax, ay, az): setup dump, one FGMRES solve per row of B
+    from x0 = 0, and apply_k preconditioner applications.  Cached like run()."""
+    B = np.ascontiguousarray(B, np.complex128)
+    key = hashlib.sha1(repr((lap, params.tobytes(), B.tobytes(), apply_k, threads, tag, _file_digest(DRIVER_Z)))
+                       .encode()).hexdigest()[:16]
+    out = os.path.join(CACHE, "z" + key)
+    done = os.path.join(out, "result.txt")
+    if not os.path.exists(done):
+        os.makedirs(out, exist_ok=True)
+        rf = os.path.join(out, "rhs.bin")
+        pgxd.write(rf, {"B": B.view(np.float64).ravel(), "nrhs": np.array([B.shape[0]], np.int32)})
+        cmd = [DRIVER_Z, "--out", out, "--threads", str(threads), "--lap", *[str(v) for v in lap], "--rhs", rf,
+               "--dump", "--solve"] + param_args(params)
+        if apply_k:
+            cmd += ["--apply", str(apply_k)]
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
+        subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
+    res: Dict[str, object] = {"dir": out, "setup": os.path.join(out, "setup.bin")}
+    with open(done) as f:
+        for line in f:
+            k, v = line.strip().split("=", 1)
+            res[k] = v
+    res["iters"] = [int(t) for t in str(res["iters"]).split(",")]
+    res["true_rel_res"] = [float(t) for t in str(res["true_rel_res"]).split(",")]
+    sol = pgxd.read(os.path.join(out, "solution.bin"))
+    res["x"] = [sol["x%d" % r].view(np.complex128) for r in range(B.shape[0])]
+    if apply_k:
+        ap = pgxd.read(os.path.join(out, "apply.bin"))
+        res["apply_in"] = ap["in"].view(np.complex128).reshape(apply_k, -1)
+        res["apply_out"] = ap["out"].view(np.complex128).reshape(apply_k, -1)
+    return res
