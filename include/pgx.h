@@ -460,6 +460,20 @@ int pgx_csr_spmv_device(const pgx_csr *A_device, double alpha, const double *x, 
 int pgx_csr_spmv_device_variant(const pgx_csr *A_device, int32_t variant, double alpha, const double *x,
                                 double beta, double *y);
 
+/* Block low-rank correction of complex64 vectors on the tensor cores, the
+ * kernel pair a complex mixed-precision slot of 8 or 16 lanes applies at
+ * every level (GemslrClass::SolveApplyLowRankLevel, gemslr.cpp:3681-3722,
+ * followed by the Axpy of gemslr.cpp:3585-3590, for all lanes at once):
+ *   x_q <- x_q + WH (W^H x_q),  q = 0 .. nrhs-1
+ * W and WH are m x r column-major, X holds nrhs vectors ldx values apart;
+ * every array is complex64 ({re, im} floats) in device memory.  nrhs is 8 or
+ * 16 and r at most 64.  The two GEMMs run as tcgen05.mma kind::tf32 with each
+ * FP32 operand split into a high and a low tf32 part (three MMAs per product),
+ * which keeps them to about FP32 accuracy.  This call allocates its scratch
+ * and synchronises the device; the slots keep theirs. */
+int pgx_lowrank_block_apply_c64(int32_t m, int32_t r, int32_t nrhs, const void *W, const void *WH, void *X,
+                                int64_t ldx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,7 +50,7 @@ EXPORTS = (
     "pgx_gemslr_set_wait_limit", "pgx_wait_selfcheck", "pgx_gemslr_residual_history",
     "pgx_csr_spmv_plan", "pgx_csr_spmv_device_variant", "pgx_gemslr_describe",
     "pgx_pool_create", "pgx_pool_add", "pgx_pool_submit", "pgx_pool_step", "pgx_pool_start", "pgx_pool_stop",
-    "pgx_pool_collect", "pgx_pool_stats", "pgx_pool_destroy",
+    "pgx_pool_collect", "pgx_pool_stats", "pgx_pool_destroy", "pgx_lowrank_block_apply_c64",
 )
 
 # every symbol include/pgx_hypre.h declares (the reference's hypre plugin interface)
@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
     L = C.CDLL(LIB_PATH)
     vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
     L.pgx_init.argtypes = [C.c_int]
+    L.pgx_lowrank_block_apply_c64.argtypes = [i32, i32, i32, vp, vp, vp, C.c_int64]
     L.pgx_last_error.restype = C.c_char_p
     L.pgx_gemslr_create.argtypes = [C.POINTER(vp), i32, i32]
     L.pgx_gemslr_set_matrix.argtypes = [vp, C.POINTER(Csr)]

@@ -41,6 +41,7 @@
 #include "../../include/pgx.h"
 #include "pgx_device.cuh"
 #include "pgx_internal.h"
+#include "pgx_umma.cuh"
 #include "pgx_params.h"
 #include "pgx_setup.h"
 
@@ -855,6 +856,7 @@ template <typename P>
 struct Engine;
 template <typename P>
 int make_batch_slot(Engine<P>& own, Import& im, int lanes, std::unique_ptr<EngineBase>& out);
+constexpr int kMaxLanes = 16;  // right-hand sides one slot advances together
 
 template <typename P>
 struct Engine : EngineBase {
@@ -2227,13 +2229,26 @@ struct BatchLayout {
 // solve and its result matches it bit for bit.
 template <typename P, int R>
 struct BatchEngine : EngineBase {
+  // the triangular passes run in groups of G lanes (one merged launch per
+  // group over the G-lane layout, shared with the handle's G-lane slots)
+  static constexpr int G = R > 4 ? 4 : R;
   Engine<P>* owner = nullptr;
-  std::shared_ptr<BatchLayout<P, R>> lay;
+  std::shared_ptr<BatchLayout<P, G>> lay;
   std::unique_ptr<Engine<P>> lane[R];
   cudaStream_t stream = nullptr;
   Arena wk;
   std::vector<std::array<P*, R>> yslot;  // per level, in the R-layout's slot order
   int n = 0, nlev = 0;
+  // Block low-rank correction on the tensor cores: complex64 slots of 8 or
+  // 16 lanes apply W^H X and X + WH Y to all lanes in two tcgen05 GEMMs
+  // (lr_wtx_umma_kernel, lr_update_umma_kernel) instead of one tall-skinny
+  // kernel pair per lane.  Slots of 4 lanes or fewer keep the per-lane kernels,
+  // so their results equal single solves bit for bit.
+  static constexpr bool kTensorLowRank = std::is_same<P, cf32>::value && R >= 8;
+  static constexpr int kLrGrid = 148;  // CTAs of the split-K W^H X
+  cf32* lr_y = nullptr;
+  float* lr_partial = nullptr;
+  unsigned int* lr_counter = nullptr;
   cudaGraphExec_t cycle_exec = nullptr;
   int cycle_nodes = 0, g_kdim = -1;
   std::array<const void*, R> g_x{}, g_b{};
@@ -2247,8 +2262,8 @@ struct BatchEngine : EngineBase {
       if (lane[r]) lane[r]->stream = nullptr;  // lane 0 owns the shared stream
   }
 
-  int setup(Engine<P>& own, Import& im, std::shared_ptr<BatchLayout<P, R>> shared) {
-    PGX_TRY(Engine<P>::template set_pipe_smem<R>());
+  int setup(Engine<P>& own, Import& im, std::shared_ptr<BatchLayout<P, G>> shared) {
+    PGX_TRY(Engine<P>::template set_pipe_smem<G>());
     owner = &own;
     n = own.n;
     nlev = own.nlev;
@@ -2265,14 +2280,14 @@ struct BatchEngine : EngineBase {
     if (shared) {
       lay = shared;
     } else {
-      lay = std::make_shared<BatchLayout<P, R>>();
+      lay = std::make_shared<BatchLayout<P, G>>();
       lay->L.resize(nlev);
       lay->U.resize(nlev);
       for (int l = 0; l < nlev; l++) {
         HostLevel& h = im.levels[l];
         if (h.L.rows == 0 || !own.lv[l].L.comp) continue;
         std::vector<int> uslot_of_row;
-        using CC = PipeCfg<P, R>;
+        using CC = PipeCfg<P, G>;
         int rc = upload_tri_sub<P, CC>(lay->ar, h.U, true, h.dom_ptr, lay->U[l], stream, &h.dinv, &uslot_of_row,
                                        nullptr);
         if (rc == PGX_SUCCESS)
@@ -2295,8 +2310,41 @@ struct BatchEngine : EngineBase {
         yslot[l][r] = nullptr;
         if (lay->U[l].comp) PGX_TRY(wk.zeros(&yslot[l][r], (size_t)lay->U[l].nslots, stream));
       }
+    if constexpr (kTensorLowRank) {
+      PGX_TRY(wk.zeros(&lr_y, (size_t)kUmmaMaxRank * R, stream));
+      PGX_TRY(wk.zeros(&lr_partial, (size_t)kLrGrid * 2 * kUmmaMaxRank * 2 * R, stream));
+      PGX_TRY(wk.zeros(&lr_counter, 1, stream));
+      PGX_CUDA(cudaFuncSetAttribute(lr_update_umma_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)lr_update_smem(kUmmaMaxRank, R)));
+    }
     PGX_CUDA(cudaStreamSynchronize(stream));
     return PGX_SUCCESS;
+  }
+
+  // x'_q = x_q s_q + WH_l (W_l^H (x_q s_q)) for every lane on the tensor cores
+  // (s_q: the lane's scale, or none)
+  void lowrank_block(int l, const std::array<const P*, R>& in, const std::array<P*, R>& out,
+                     const std::array<const double*, R>& scale, const std::array<Skip, R>& sk) {
+    if constexpr (kTensorLowRank) {
+      DLevel<P>& d = lane[0]->lv[l];
+      LrBlock<R> xb;
+      for (int r = 0; r < R; r++) {
+        xb.in[r] = in[r];
+        xb.out[r] = out[r];
+        xb.scale[r] = scale[r];
+      }
+      const int nchunks = (d.m + kUmmaKT - 1) / kUmmaKT;
+      const int grid = std::max(1, std::min(nchunks, kLrGrid));
+      lr_wtx_umma_kernel<R><<<grid, kUmmaThreads, lr_wtx_smem<R>(), stream>>>(
+          d.m, d.rank, d.W, xb, lr_partial, lr_counter, lr_y, lane[0]->err, all(sk));
+      lr_update_umma_kernel<R><<<(d.m + 127) / 128, kUmmaThreads, lr_update_smem(d.rank, R), stream>>>(
+          d.m, d.rank, d.WH, lr_y, xb, lane[0]->err, all(sk));
+    } else {
+      (void)l, (void)in, (void)out, (void)scale, (void)sk;
+    }
+  }
+  bool use_lowrank_block(int l) const {
+    return kTensorLowRank && lane[0]->lv[l].rank > 0 && lane[0]->lv[l].rank <= kUmmaMaxRank;
   }
 
   int lanes() const override { return R; }
@@ -2346,14 +2394,18 @@ struct BatchEngine : EngineBase {
       return;
     }
     if (T.n == 0) return;
-    PtrR<P, R> prhs, py, px, pys;
-    for (int r = 0; r < R; r++) {
-      prhs.p[r] = const_cast<P*>(rhs[r]);
-      py.p[r] = y[r];
-      px.p[r] = x[r];
-      pys.p[r] = yslot[l][r];
+    for (int g0 = 0; g0 < R; g0 += G) {
+      PtrR<P, G> prhs, py, px, pys;
+      SkipR<G> sg;
+      for (int r = 0; r < G; r++) {
+        prhs.p[r] = const_cast<P*>(rhs[g0 + r]);
+        py.p[r] = y[g0 + r];
+        px.p[r] = x[g0 + r];
+        pys.p[r] = yslot[l][g0 + r];
+        sg.s[r] = sk[g0 + r];
+      }
+      Engine<P>::template launch_pipe<G>(T, upper, pys, prhs, py, px, lane[0]->err, sg, stream);
     }
-    Engine<P>::template launch_pipe<R>(T, upper, pys, prhs, py, px, lane[0]->err, all(sk), stream);
   }
 
   void solve_b_b(int l, const std::array<const P*, R>& rhs, const std::array<P*, R>& x,
@@ -2394,8 +2446,18 @@ struct BatchEngine : EngineBase {
     if (l == 0 && lane[0]->inner) {
       inner_solve_b(xl, czl, sk);
     } else {
-      for (int r = 0; r < R; r++)
-        if (lane[r]->lv[l].rank > 0) lane[r]->lowrank_inplace(l, zl[r], sk[r]);
+      if (use_lowrank_block(l)) {
+        std::array<const P*, R> czl2;
+        std::array<const double*, R> none;
+        for (int r = 0; r < R; r++) {
+          czl2[r] = zl[r];
+          none[r] = nullptr;
+        }
+        lowrank_block(l, czl2, zl, none, sk);
+      } else {
+        for (int r = 0; r < R; r++)
+          if (lane[r]->lv[l].rank > 0) lane[r]->lowrank_inplace(l, zl[r], sk[r]);
+      }
       solve_level_b(l + 1, xl, czl, sk);
     }
     for (int r = 0; r < R; r++) {
@@ -2425,13 +2487,20 @@ struct BatchEngine : EngineBase {
       std::array<Skip, R> it;
       std::array<P*, R> zj, xlr, szu, swu;
       std::array<const P*, R> cxlr, cszu;
+      const bool block = use_lowrank_block(0);
+      std::array<const P*, R> vjs;
+      std::array<const double*, R> scs;
       for (int r = 0; r < R; r++) {
         Engine<P>& e = *lane[r];
         DLevel<P>& d0 = e.lv[0];
         it[r] = mk_skip(outer[r].f0, outer[r].f1, &e.st_in->cycle_done);
         P* vj = e.Vin + (long long)j * ld;
         zj[r] = e.Zin + (long long)j * ld;
-        if (d0.rank > 0) {
+        vjs[r] = vj;
+        scs[r] = &e.st_in->sc[j];
+        if (block) {
+          // xlr = v + WH W^H v for all lanes below
+        } else if (d0.rank > 0) {
           auto a = Engine<P>::template ts_args<P, P, P>(m0, it[r]);
           a.ncols = d0.rank;
           a.V = d0.W;
@@ -2442,7 +2511,7 @@ struct BatchEngine : EngineBase {
           a.dst = d0.lrt;
           e.template ts<P, P, P, TS_DOT>(a);
         }
-        {
+        if (!block) {
           auto u = Engine<P>::template ts_args<P, P, P>(m0, it[r]);
           u.ncols = d0.rank;
           u.M = d0.WH;
@@ -2459,6 +2528,7 @@ struct BatchEngine : EngineBase {
         swu[r] = e.s_wu;
         cszu[r] = e.s_zu;
       }
+      if (block) lowrank_block(0, vjs, xlr, scs, it);
       solve_level_b(1, zj, cxlr, it);
       for (int r = 0; r < R; r++) {
         Engine<P>& e = *lane[r];
@@ -2727,9 +2797,10 @@ template <typename P, int R>
 static int make_batch_slot_r(Engine<P>& own, Import& im, std::unique_ptr<EngineBase>& out) {
   auto* e = new BatchEngine<P, R>();
   out.reset(e);
-  auto shared = std::static_pointer_cast<BatchLayout<P, R>>(own.batch_layout[R]);
+  constexpr int G = BatchEngine<P, R>::G;
+  auto shared = std::static_pointer_cast<BatchLayout<P, G>>(own.batch_layout[G]);
   PGX_TRY(e->setup(own, im, shared));
-  if (!shared) own.batch_layout[R] = e->lay;
+  if (!shared) own.batch_layout[G] = e->lay;
   return PGX_SUCCESS;
 }
 
@@ -2746,7 +2817,9 @@ int make_batch_slot(Engine<P>& own, Import& im, int lanes, std::unique_ptr<Engin
   switch (lanes) {
     case 2: return make_batch_slot_r<P, 2>(own, im, out);
     case 4: return make_batch_slot_r<P, 4>(own, im, out);
-    default: return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: one of 1, 2, 4", lanes);
+    case 8: return make_batch_slot_r<P, 8>(own, im, out);
+    case 16: return make_batch_slot_r<P, 16>(own, im, out);
+    default: return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: one of 1, 2, 4, 8, 16", lanes);
   }
 }
 
@@ -2816,6 +2889,40 @@ struct pgx_server_s {
   int worker_rc = 0;
   std::string worker_msg;
 };
+
+// the block low-rank correction for pgx_lowrank_block_apply_c64
+template <int NL>
+static int lowrank_block_apply(int m, int r, const cf32* W, const cf32* WH, cf32* X, int64_t ldx) {
+  Arena tmp;
+  cf32* y = nullptr;
+  float* partial = nullptr;
+  unsigned int* counter = nullptr;
+  int* err = nullptr;
+  const int nchunks = (m + kUmmaKT - 1) / kUmmaKT;
+  const int grid = std::max(1, std::min(nchunks, 148));
+  PGX_TRY(tmp.zeros(&y, (size_t)r * NL, nullptr));
+  PGX_TRY(tmp.zeros(&partial, (size_t)grid * 2 * r * 2 * NL, nullptr));
+  PGX_TRY(tmp.zeros(&counter, 1, nullptr));
+  PGX_TRY(tmp.zeros(&err, 1, nullptr));
+  LrBlock<NL> xb;
+  for (int q = 0; q < NL; q++) {
+    xb.in[q] = X + (size_t)q * ldx;
+    xb.out[q] = X + (size_t)q * ldx;
+    xb.scale[q] = nullptr;
+  }
+  SkipR<NL> sk;
+  for (int q = 0; q < NL; q++) sk.s[q] = mk_skip();
+  PGX_CUDA(cudaFuncSetAttribute(lr_update_umma_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)lr_update_smem(kUmmaMaxRank, NL)));
+  lr_wtx_umma_kernel<NL><<<grid, kUmmaThreads, lr_wtx_smem<NL>()>>>(m, r, W, xb, partial, counter, y, err, sk);
+  lr_update_umma_kernel<NL><<<(m + 127) / 128, kUmmaThreads, lr_update_smem(r, NL)>>>(m, r, WH, y, xb, err, sk);
+  PGX_CUDA(cudaGetLastError());
+  PGX_CUDA(cudaDeviceSynchronize());
+  int h = 0;
+  PGX_CUDA(cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) return fail(PGX_ERROR_TIMEOUT, "tensor-core wait gave up (error word %d)", h);
+  return PGX_SUCCESS;
+}
 
 extern "C" {
 
@@ -3209,7 +3316,8 @@ int pgx_gemslr_set_slots(pgx_handle h, int32_t nslots) {
 int pgx_gemslr_set_lanes(pgx_handle h, int32_t lanes) {
   if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
   if (!h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "handle not committed");
-  if (lanes != 1 && lanes != 2 && lanes != 4) return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: one of 1, 2, 4", lanes);
+  if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16)
+    return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: one of 1, 2, 4, 8, 16", lanes);
   if (h->servers > 0) return fail(PGX_ERROR_FUNCTION_CALL, "lanes cannot change while a server is live");
   if (lanes == h->lanes) return PGX_SUCCESS;
   PGX_CUDA(cudaSetDevice(h->device));
@@ -3266,7 +3374,7 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
       first_msg = g_last_error;
     }
   };
-  std::vector<pgx_result> res(4);
+  std::vector<pgx_result> res(kMaxLanes);
   if (first_bad >= 0) {
     fail(PGX_ERROR_NOT_FINITE, "b(:, %d) is not finite", first_bad);
     note(PGX_ERROR_NOT_FINITE);
@@ -3281,8 +3389,8 @@ int pgx_gemslr_solve_batch(pgx_handle h, int32_t nrhs, double* X, int64_t ldx, c
       EngineBase* e = h->slot(sidx);
       if (busy[sidx].empty() && next < nok) {
         const int cnt = std::min(e->lanes(), nok - next);
-        double* xs[4];
-        const double* bs[4];
+        double* xs[kMaxLanes];
+        const double* bs[kMaxLanes];
         for (int k = 0; k < cnt; k++) {
           xs[k] = X + (size_t)order[next + k] * ldx * vw;
           bs[k] = B + (size_t)order[next + k] * ldb * vw;
@@ -3357,7 +3465,7 @@ static int server_step_locked(pgx_server srv, int32_t* n_active, int32_t* n_queu
   double tol;
   read_solver_params(srv->has_params ? srv->params : nullptr, kdim, maxits, tol, atol);
   int active = 0;
-  pgx_result res[4];
+  pgx_result res[kMaxLanes];
   const int ns = h->nslots();
   // the additional (possibly multi-lane) slots first, the handle's own last
   for (int t = 0; t < ns; t++) {
@@ -3366,8 +3474,8 @@ static int server_step_locked(pgx_server srv, int32_t* n_active, int32_t* n_queu
     std::vector<int64_t>& ids = srv->slot_ids[sidx];
     if (ids.empty() && !srv->queue.empty()) {
       // the oldest waiting requests (one per lane, same memory location) go to the free slot
-      double* xs[4];
-      const double* bs[4];
+      double* xs[kMaxLanes];
+      const double* bs[kMaxLanes];
       const int loc = srv->queue.front().location;
       int cnt = 0;
       while (cnt < e->lanes() && !srv->queue.empty() && srv->queue.front().location == loc) {
@@ -3476,7 +3584,7 @@ int pgx_server_destroy(pgx_server srv) {
   pgx_server_stop(srv);
   cudaSetDevice(srv->h->device);
   // finish the in-flight solves so that no slot is left in the middle of a cycle
-  pgx_result res[4];
+  pgx_result res[kMaxLanes];
   for (int sidx = 0; sidx < srv->h->nslots(); sidx++) {
     if (srv->slot_ids[sidx].empty()) continue;
     bool fin = false;
@@ -4056,6 +4164,20 @@ int pgx_csr_spmv_device_variant(const pgx_csr* Ad, int32_t variant, double alpha
     PGX_CUDA(cudaGetLastError());
     PGX_CUDA(cudaDeviceSynchronize());
     return PGX_SUCCESS;
+  });
+}
+
+int pgx_lowrank_block_apply_c64(int32_t m, int32_t r, int32_t nrhs, const void* W, const void* WH, void* X,
+                                int64_t ldx) {
+  return guarded("pgx_lowrank_block_apply_c64", [&]() -> int {
+    if (!W || !WH || !X) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    if (m < 1 || r < 1 || r > kUmmaMaxRank || ldx < m)
+      return fail(PGX_ERROR_INVALID_PARAM, "m %d, r %d (1..%d), ldx %lld", m, r, kUmmaMaxRank, (long long)ldx);
+    switch (nrhs) {
+      case 8: return lowrank_block_apply<8>(m, r, (const cf32*)W, (const cf32*)WH, (cf32*)X, ldx);
+      case 16: return lowrank_block_apply<16>(m, r, (const cf32*)W, (const cf32*)WH, (cf32*)X, ldx);
+      default: return fail(PGX_ERROR_INVALID_PARAM, "nrhs %d: 8 or 16", nrhs);
+    }
   });
 }
 
