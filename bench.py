@@ -650,6 +650,105 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_complex(args):
+    """The complex workload: a 96^3 7-point Laplacian shifted by -(0.05 + 0.01i) (indefinite), the reference's
+    complexd GemslrClass setup (5 levels, ILUT 1e-3, rank 32), FGMRES(100) to rel-res 1e-8, and 16 seeded
+    complex-Gaussian right-hand sides solved as one block in a 16-lane slot (triangular passes merged four lanes
+    at a time; with the complex64 preconditioner every low-rank correction is one tcgen05 GEMM pair for all 16).
+    The reference solves the first --ref-rhs of them one at a time on all host threads (its setup untimed); the
+    GPU arm reports both preconditioner precisions."""
+    import torch
+    from pargemslr_b200.handle import GemslrHandle
+    from pargemslr_b200.structures import from_dump
+
+    g = args.grid if args.grid != 128 else 96
+    n = g ** 3
+    nrhs = 16
+    p = P.workload_params("zlap3d_96")
+    rng = np.random.default_rng(SEED)
+    Bc = rng.standard_normal((nrhs, n)) + 1j * rng.standard_normal((nrhs, n))
+    threads = os.cpu_count() or 1
+    d = tempfile.mkdtemp(prefix="pgx_zref_")
+    rf = os.path.join(d, "rhs.bin")
+    kref = max(1, min(args.ref_rhs, nrhs))
+    pgxd.write(rf, {"B": np.ascontiguousarray(Bc[:kref]).view(np.float64).ravel(), "nrhs": np.array([kref], np.int32)})
+    drv = os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver_z")
+    if not os.path.exists(drv):
+        raise SystemExit("oracle/_ref/pgx_ref_driver_z not built")
+    cmd = [drv, "--out", d, "--lap", str(g), str(g), str(g), "0.05", "0.01", "0", "0", "0", "--rhs", rf, "--dump",
+           "--solve", "--threads", str(threads)]
+    for i, v in enumerate(p):
+        cmd += ["--param", f"{i}={float(v)!r}"]
+    t0 = time.time()
+    subprocess.run(cmd, check=True, env=dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1"),
+                   stdout=subprocess.DEVNULL)
+    log("complex reference setup and %d solves: %.1f s" % (kref, time.time() - t0))
+    res_ref = dict(line.strip().split("=", 1) for line in open(os.path.join(d, "result.txt")))
+    it_ref = [int(t) for t in res_ref["iters"].split(",")]
+    t_ref = [float(t) for t in res_ref["solve_times"].split(",")]
+    sol = pgxd.read(os.path.join(d, "solution.bin"))
+    x_ref = [sol["x%d" % r].view(np.complex128) for r in range(kref)]
+    st = from_dump(os.path.join(d, "setup.bin"))
+    dev = torch.device("cuda", 0)
+    Bd = torch.from_numpy(np.ascontiguousarray(Bc)).to(dev)
+    ev_a = torch.cuda.Event(enable_timing=True)
+    ev_b = torch.cuda.Event(enable_timing=True)
+    out = {}
+    for precision in ("mixed", "fp64"):
+        h = GemslrHandle(st, precision=precision, device=0)
+        try:
+            h.set_lanes(nrhs)
+            h.set_slots(2)
+            Xd = torch.zeros_like(Bd)
+            Bf = Bd.view(torch.float64)
+            Xf = Xd.view(torch.float64)
+            ms, its, rel = [], [], []
+            for step in range(args.warmup + args.steps):
+                Xd.zero_()
+                torch.cuda.synchronize()
+                ev_a.record()
+                res = h.solve_batch_ptr(nrhs, Xf.data_ptr(), n, Bf.data_ptr(), n, LOCATION_DEVICE, p)
+                ev_b.record()
+                ev_b.synchronize()
+                if step >= args.warmup:
+                    ms.append(ev_a.elapsed_time(ev_b))
+                    its.extend(r["iters"] for r in res)
+                    rel.extend(r["true_rel_res"] for r in res)
+            X = Xd.cpu().numpy()
+            dx = [float(np.linalg.norm(X[r] - x_ref[r]) / np.linalg.norm(x_ref[r])) for r in range(kref)]
+            out[precision] = {"solves_per_s": nrhs * len(ms) / (sum(ms) / 1e3), "ms_per_block": sum(ms) / len(ms),
+                              "iters": [min(its), max(its)], "true_rel_res_max": max(rel),
+                              "x_vs_x_ref": dx, "iters_first": [res[r]["iters"] for r in range(kref)]}
+            log("%s: %.2f solves/s, iterations %s" % (precision, out[precision]["solves_per_s"],
+                                                       out[precision]["iters"]))
+        finally:
+            h.set_lanes(1)
+            h.close()
+    mixed = out["mixed"]
+    ok = all(v <= 1e-6 for v in out["fp64"]["x_vs_x_ref"]) and \
+        all(abs(a - b) <= 1 for a, b in zip(out["fp64"]["iters_first"], it_ref)) and \
+        all(a <= int(np.floor(1.15 * b)) + 1 for a, b in zip(mixed["iters_first"], it_ref))
+    line = {
+        "metric": "solves/s (GeMSLR-FGMRES(100), rel-res 1e-8, complex shifted 3D Laplacian %d^3, 16-RHS block)" % g,
+        "value": mixed["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mixed["ms_per_block"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 preconditioner / c128 FGMRES", "data": "synthetic",
+        "config": {"workload": "complex shifted 3D 7-point Laplacian %d^3 (n=%d), shift 0.05+0.01i, 5 levels, ILUT "
+                               "1e-3, rank 32, inner Schur FGMRES(5), FGMRES(100) to 1e-8 from x0 = 0, 16 seeded "
+                               "complex-Gaussian right-hand sides as one 16-lane block" % (g, n),
+                   "setup": "the reference's complexd GemslrClass::Setup (oracle/_ref/pgx_ref_driver_z), untimed"},
+        "detail": {"mixed": mixed, "fp64": out["fp64"], "mixed_over_fp64": mixed["solves_per_s"] /
+                   out["fp64"]["solves_per_s"],
+                   "reference": {"iters": it_ref, "solve_s": t_ref, "threads": threads,
+                                 "solves_per_s": len(t_ref) / sum(t_ref)},
+                   "parity_ok": bool(ok)},
+        "cpu_baseline": {"value": len(t_ref) / sum(t_ref), "unit": "solves/s", "cores": threads, "kind": "reference",
+                         "sample": "reference complex FGMRES+GemslrClass (oracle/_ref/pgx_ref_driver_z) on %d threads, "
+                                   "the first %d right-hand sides one at a time" % (threads, kref)},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -673,8 +772,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=128,
                     help="cube edge of the Laplacian (128 is the headline workload; smaller grids for profiling)")
-    ap.add_argument("--workload", choices=["laplacian", "serve"], default="laplacian",
-                    help="laplacian: the headline batch benchmark; serve: Poisson arrivals over resident matrices")
+    ap.add_argument("--workload", choices=["laplacian", "serve", "complex"], default="laplacian",
+                    help="laplacian: the headline batch benchmark; serve: Poisson arrivals over resident matrices; "
+                         "complex: 16 right-hand sides of the complex shifted 96^3 Laplacian as one block")
+    ap.add_argument("--ref-rhs", type=int, default=2, help="complex workload: right-hand sides the reference solves")
     ap.add_argument("--serve-matrices", type=int, default=64)
     ap.add_argument("--serve-rows-min", type=int, default=200000)
     ap.add_argument("--serve-rows-max", type=int, default=2000000)
@@ -687,6 +788,8 @@ def main():
         run_reference(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "complex":
+        run_complex(args)
     else:
         run_pgx(args)
 

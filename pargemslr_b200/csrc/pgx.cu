@@ -2245,6 +2245,12 @@ struct BatchEngine : EngineBase {
   // kernel pair per lane.  Slots of 4 lanes or fewer keep the per-lane kernels,
   // so their results equal single solves bit for bit.
   static constexpr bool kTensorLowRank = std::is_same<P, cf32>::value && R >= 8;
+  // groups of lanes beyond the first run their triangular passes on side
+  // streams (fork/join through events; a captured cycle keeps them as
+  // parallel branches), so the R / G merged launches of a pass overlap
+  static constexpr int NSIDE = R / G - 1;
+  cudaStream_t side[NSIDE > 0 ? NSIDE : 1] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[NSIDE > 0 ? NSIDE : 1] = {};
   static constexpr int kLrGrid = 148;  // CTAs of the split-K W^H X
   cf32* lr_y = nullptr;
   float* lr_partial = nullptr;
@@ -2258,6 +2264,11 @@ struct BatchEngine : EngineBase {
   ~BatchEngine() override {
     if (stream) cudaStreamSynchronize(stream);
     if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
+    for (int k = 0; k < NSIDE; k++) {
+      if (side[k]) cudaStreamDestroy(side[k]);
+      if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     for (int r = 1; r < R; r++)
       if (lane[r]) lane[r]->stream = nullptr;  // lane 0 owns the shared stream
   }
@@ -2310,6 +2321,11 @@ struct BatchEngine : EngineBase {
         yslot[l][r] = nullptr;
         if (lay->U[l].comp) PGX_TRY(wk.zeros(&yslot[l][r], (size_t)lay->U[l].nslots, stream));
       }
+    for (int k = 0; k < NSIDE; k++) {
+      PGX_CUDA(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+      PGX_CUDA(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+    }
+    if (NSIDE > 0) PGX_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     if constexpr (kTensorLowRank) {
       PGX_TRY(wk.zeros(&lr_y, (size_t)kUmmaMaxRank * R, stream));
       PGX_TRY(wk.zeros(&lr_partial, (size_t)kLrGrid * 2 * kUmmaMaxRank * 2 * R, stream));
@@ -2333,8 +2349,7 @@ struct BatchEngine : EngineBase {
         xb.out[r] = out[r];
         xb.scale[r] = scale[r];
       }
-      const int nchunks = (d.m + kUmmaKT - 1) / kUmmaKT;
-      const int grid = std::max(1, std::min(nchunks, kLrGrid));
+      const int grid = lr_wtx_grid(d.m);
       lr_wtx_umma_kernel<R><<<grid, kUmmaThreads, lr_wtx_smem<R>(), stream>>>(
           d.m, d.rank, d.W, xb, lr_partial, lr_counter, lr_y, lane[0]->err, all(sk));
       lr_update_umma_kernel<R><<<(d.m + 127) / 128, kUmmaThreads, lr_update_smem(d.rank, R), stream>>>(
@@ -2394,7 +2409,11 @@ struct BatchEngine : EngineBase {
       return;
     }
     if (T.n == 0) return;
+    if (NSIDE > 0) cudaEventRecord(ev_fork, stream);
     for (int g0 = 0; g0 < R; g0 += G) {
+      const int k = g0 / G - 1;  // side stream of this group (-1: the slot's own)
+      cudaStream_t sg_stream = k < 0 ? stream : side[k];
+      if (k >= 0) cudaStreamWaitEvent(sg_stream, ev_fork, 0);
       PtrR<P, G> prhs, py, px, pys;
       SkipR<G> sg;
       for (int r = 0; r < G; r++) {
@@ -2404,8 +2423,10 @@ struct BatchEngine : EngineBase {
         pys.p[r] = yslot[l][g0 + r];
         sg.s[r] = sk[g0 + r];
       }
-      Engine<P>::template launch_pipe<G>(T, upper, pys, prhs, py, px, lane[0]->err, sg, stream);
+      Engine<P>::template launch_pipe<G>(T, upper, pys, prhs, py, px, lane[0]->err, sg, sg_stream);
+      if (k >= 0) cudaEventRecord(ev_join[k], sg_stream);
     }
+    for (int k = 0; k < NSIDE; k++) cudaStreamWaitEvent(stream, ev_join[k], 0);
   }
 
   void solve_b_b(int l, const std::array<const P*, R>& rhs, const std::array<P*, R>& x,
@@ -2898,8 +2919,7 @@ static int lowrank_block_apply(int m, int r, const cf32* W, const cf32* WH, cf32
   float* partial = nullptr;
   unsigned int* counter = nullptr;
   int* err = nullptr;
-  const int nchunks = (m + kUmmaKT - 1) / kUmmaKT;
-  const int grid = std::max(1, std::min(nchunks, 148));
+  const int grid = lr_wtx_grid(m);
   PGX_TRY(tmp.zeros(&y, (size_t)r * NL, nullptr));
   PGX_TRY(tmp.zeros(&partial, (size_t)grid * 2 * r * 2 * NL, nullptr));
   PGX_TRY(tmp.zeros(&counter, 1, nullptr));

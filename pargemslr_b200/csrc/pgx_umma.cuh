@@ -227,18 +227,34 @@ __global__ void __launch_bounds__(kUmmaThreads) lr_wtx_umma_kernel(int m, int r,
   __syncthreads();
   if (!s_last) return;
   __threadfence();
+  // sum of the partial products in CTA order: each thread keeps its entries
+  // (consecutive threads, consecutive entries) in registers, so every step
+  // over the CTAs is one coalesced load per entry, all in flight together
+  constexpr int PER = 2 * kUmmaMaxRank * N / kUmmaThreads;
+  const int ne = 2 * r * N;
+  float acc[PER];
+#pragma unroll
+  for (int u = 0; u < PER; u++) acc[u] = 0.f;
+  for (int g = 0; g < (int)gridDim.x; g++) {
+    const float* pg = partial + (size_t)g * ne;
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      const int e = tid + u * kUmmaThreads;
+      if (e < ne) acc[u] += __ldcg(&pg[e]);
+    }
+  }
+  float* red = (float*)sm;  // the operand buffers are free now
+#pragma unroll
+  for (int u = 0; u < PER; u++) {
+    const int e = tid + u * kUmmaThreads;
+    if (e < ne) red[e] = acc[u];
+  }
+  __syncthreads();
   // Y(c, q) = (D[c, q] + D[r + c, NL + q]) + i (D[c, NL + q] - D[r + c, q])
   for (int e = tid; e < r * NL; e += kUmmaThreads) {
     const int c = e % r, q = e / r;
-    float a = 0.f, b = 0.f, cc = 0.f, dd = 0.f;
-    for (int g = 0; g < (int)gridDim.x; g++) {
-      const float* pg = partial + (size_t)g * 2 * r * N;
-      a += __ldcg(&pg[c * N + q]);
-      b += __ldcg(&pg[(r + c) * N + NL + q]);
-      cc += __ldcg(&pg[c * N + NL + q]);
-      dd += __ldcg(&pg[(r + c) * N + q]);
-    }
-    Y[(size_t)q * r + c] = cf32(a + b, cc - dd);
+    Y[(size_t)q * r + c] =
+        cf32(red[c * N + q] + red[(r + c) * N + NL + q], red[c * N + NL + q] - red[(r + c) * N + q]);
   }
   if (tid == 0) *counter = 0u;
 }
@@ -332,6 +348,13 @@ __global__ void __launch_bounds__(kUmmaThreads) lr_update_umma_kernel(int m, int
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc32(taddr);
+}
+
+// CTAs of the split-K W^H X: at least 8 K chunks each, at most one per SM,
+// so the fixed-order sum of the partial products stays short
+inline int lr_wtx_grid(int m) {
+  const int nchunks = (m + kUmmaKT - 1) / kUmmaKT;
+  return nchunks / 8 < 1 ? 1 : (nchunks / 8 > 148 ? 148 : nchunks / 8);
 }
 
 template <int NL>
