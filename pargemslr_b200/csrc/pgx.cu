@@ -1876,14 +1876,20 @@ struct Engine : EngineBase {
     if (location == PGX_LOCATION_HOST && !prechecked && !all_finite((const double*)b, (long long)n * VW))
       return fail(PGX_ERROR_NOT_FINITE, "b is not finite");
     PGX_TRY(ensure_krylov(kdim));
-    F* xd = x;
-    const F* bd = b;
-    if (location == PGX_LOCATION_HOST) {
-      PGX_CUDA(cudaMemcpyAsync(bdev, b, sizeof(F) * n, cudaMemcpyHostToDevice, stream));
-      PGX_CUDA(cudaMemcpyAsync(xdev, x, sizeof(F) * n, cudaMemcpyHostToDevice, stream));
-      xd = xdev;
-      bd = bdev;
-    }
+    // The solve works on the slot's own b and x (copied in here, x copied
+    // back when it finishes), from host or device memory alike: a captured
+    // restart cycle is keyed by the vectors it reads and writes, so every
+    // request of the slot reuses the same graph whatever its pointers.
+    if (b != bdev)
+      PGX_CUDA(cudaMemcpyAsync(bdev, b, sizeof(F) * n,
+                               location == PGX_LOCATION_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                               stream));
+    if (x != xdev)
+      PGX_CUDA(cudaMemcpyAsync(xdev, x, sizeof(F) * n,
+                               location == PGX_LOCATION_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                               stream));
+    F* xd = xdev;
+    const F* bd = bdev;
     SD h;
     memset(&h, 0, sizeof(h));
     h.kdim = kdim;
@@ -2055,8 +2061,10 @@ struct Engine : EngineBase {
       // zero right-hand side: x = 0 (fgmres.hpp:321-329)
       PGX_CUDA(cudaMemsetAsync(s_xd, 0, sizeof(F) * n, stream));
     }
-    if (s_location == PGX_LOCATION_HOST)
-      PGX_CUDA(cudaMemcpyAsync(s_xuser, xdev, sizeof(F) * n, cudaMemcpyDeviceToHost, stream));
+    if (s_xuser != s_xd)
+      PGX_CUDA(cudaMemcpyAsync(s_xuser, s_xd, sizeof(F) * n,
+                               s_location == PGX_LOCATION_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                               stream));
     PGX_CUDA(cudaStreamSynchronize(stream));
     int out = rc;
     if (out == PGX_SUCCESS && !(std::isfinite(hs.normr)))
