@@ -62,8 +62,10 @@ def metric_name() -> str:
 def workload_config(setup: str) -> dict:
     """The `config` both arms print: the same workload, so their lines compare like for like."""
     n = GRID[0] * GRID[1] * GRID[2]
-    who = ("the reference's GemslrClass::Setup (oracle/_ref) on all host threads, untimed" if setup == "reference"
-           else "this library's host setup (pgx_gemslr_setup), untimed")
+    who = {"reference": "the reference's GemslrClass::Setup (oracle/_ref) on all host threads, untimed",
+           "parallel": "the reference's ParallelGemslrClass::Setup at one rank (oracle/_ref/pgx_ref_driver_par), its "
+                       "per-level permutations composed, untimed"}.get(
+        setup, "this library's host setup (pgx_gemslr_setup), untimed")
     return {"workload": "3D 7-point Laplacian %d^3 (n=%d), 4 levels, ILUT 1e-3/200, rank 16, inner Schur FGMRES(5) "
                         "tol 1e-2, FGMRES(50) to rel-res 1e-8 from x0 = 0, b = A x_true (x_true = 2u-1, seeded)"
                         % (GRID[0], n),
@@ -220,6 +222,35 @@ def reference_run(n_threads: int, solves: int, dump: bool):
     t0 = time.time()
     subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
     return _ref_result(out, time.time() - t0), None
+
+
+def reference_run_parallel_class(n_threads: int):
+    """The reference's ParallelGemslrClass at one rank (oracle/_ref/pgx_ref_driver_par) on the workload with the
+    GeMSLR global preconditioner: its setup (exported with each level's transfer permutation, setup_par.bin), one
+    FGMRES solve of b = A x_true from x0 = 0, b and the solution.  Returns (result, None) or (None, why)."""
+    drv = os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver_par")
+    if not os.path.exists(drv):
+        return None, "oracle/_ref/pgx_ref_driver_par not built"
+    d = tempfile.mkdtemp(prefix="pgx_refpar_")
+    n = GRID[0] * GRID[1] * GRID[2]
+    xf = os.path.join(d, "xtrue.bin")
+    pgxd.write(xf, {"x_true": problems.x_true(n, SEED)})
+    p = P.workload_params(WORKLOAD)
+    p[P.PRECOND_GLOBAL_PRECOND] = 2  # GeMSLR (the parallel drivers' GEMSLR option)
+    cmd = [drv, "--out", d, "--lap", *[str(g) for g in GRID], "0", "0", "0", "0", "--xtrue", xf, "--threads",
+           str(n_threads), "--dump", "--solve"]
+    for i, v in enumerate(p):
+        cmd += ["--param", f"{i}={float(v)!r}"]
+    t0 = time.time()
+    subprocess.run(cmd, check=True, env=dict(os.environ, OMP_NUM_THREADS=str(n_threads), OPENBLAS_NUM_THREADS="1"),
+                   stdout=subprocess.DEVNULL)
+    res = {}
+    with open(os.path.join(d, "result.txt")) as f:
+        for line in f:
+            k, v = line.strip().split("=", 1)
+            res[k] = v
+    return {"dir": d, "times": [float(res["solve_s"])], "iters": int(res["iters"]), "setup_s": float(res["setup_s"]),
+            "true_rel_res": float(res["true_rel_res"]), "wall_s": time.time() - t0, "parallel": True}, None
 
 
 def reference_runs_parallel(procs: int, solves: int):
@@ -396,6 +427,14 @@ def run_pgx(args):
             raise SystemExit("--setup reference: " + ref_why)
         log("reference setup and solve: %.1f s (%d iterations)" % (ref["wall_s"], ref["iters"]))
         st = from_dump(os.path.join(ref["dir"], "setup.bin"))
+        h = GemslrHandle(st, precision=args.precision, device=local)
+    elif args.setup == "parallel":
+        from pargemslr_b200.structures import from_parallel_dump
+        ref, ref_why = reference_run_parallel_class(threads)
+        if ref is None:
+            raise SystemExit("--setup parallel: " + ref_why)
+        log("reference ParallelGemslrClass setup and solve: %.1f s (%d iterations)" % (ref["wall_s"], ref["iters"]))
+        st = from_parallel_dump(os.path.join(ref["dir"], "setup_par.bin"))
         h = GemslrHandle(st, precision=args.precision, device=local)
     else:
         h = GemslrHandle.from_matrix(A, p, precision=args.precision, device=local)
@@ -756,9 +795,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["pgx", "reference"], default="pgx")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--setup", choices=["reference", "own"], default="reference",
+    ap.add_argument("--setup", choices=["reference", "parallel", "own"], default="reference",
                     help="whose setup builds the preconditioner: the reference's GemslrClass::Setup, imported through "
-                         "the C ABI (default), or this library's host setup")
+                         "the C ABI (default); the reference's ParallelGemslrClass::Setup at one rank, its per-level "
+                         "permutations composed; or this library's host setup")
     ap.add_argument("--batch", type=int, default=96, help="right-hand sides solved concurrently per step")
     ap.add_argument("--lanes", type=int, default=4, choices=[1, 2, 4],
                     help="right-hand sides each slot advances in lockstep")

@@ -13,6 +13,7 @@ is the layout the device solve uses (one level = one triangular system).
 """
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Tuple
 
@@ -135,3 +136,99 @@ def from_dump(path: str) -> GemslrStructures:
                 lv.WH = _values(d[pre + "WH"], z)
         st.levels.append(lv)
     return st
+
+
+def _permute_rows(d: Dict[str, np.ndarray], name: str, src: np.ndarray) -> None:
+    """Rows of CSR `name` reordered in place: new row p is old row src[p] (entry order within a row kept)."""
+    rp, cj, va = d[name + ".i"].astype(np.int64), d[name + ".j"], d[name + ".a"]
+    lens = np.diff(rp)[src]
+    nrp = np.zeros(src.size + 1, np.int64)
+    nrp[1:] = np.cumsum(lens)
+    idx = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in src]) if src.size else np.zeros(0, np.int64)
+    d[name + ".i"] = nrp.astype(np.int32)
+    d[name + ".j"] = cj[idx].astype(np.int32)
+    d[name + ".a"] = va[idx]
+
+
+def parallel_to_sequential_dump(d: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+    """The structures a reference ParallelGemslrClass at one rank exported (its per-level transfer
+    permutations included), rewritten as the single-permutation structures of GemslrClass.
+
+    ParallelGemslrClass::SolveLevelGemslr (parallel_gemslr.cpp:5563-5810) permutes level l's vector by that
+    level's transfer before solving it and back after.  Level l + 1 receives the trailing part of level l's
+    frame, so the frames nest: composing the transfers gives one global order (pperm) in which every level's
+    B block keeps its own frame, and each level's E and W (rows) and F (columns), which the reference
+    applies in level l's trailing frame, are re-indexed into the composed order of the levels below.  The
+    entries of a row keep their order, so every SpMV sums as the reference's does.
+    """
+    n = int(d["n"][0])
+    nlev = int(d["nlev"][0])
+    if int(d.get("lrcA", np.zeros(1))[0]) > 0:
+        raise ValueError("a global low-rank correction on A is not supported")
+    if int(d["global_precond"][0]) not in (0, 2):
+        raise ValueError("only the block-Jacobi and GeMSLR global preconditioners are supported")
+    lev_ptr = d["lev_ptr"].astype(np.int64)
+    perms = [d["L%d.perm" % l].astype(np.int64) for l in range(nlev)]
+
+    def composed(start: int, l0: int) -> np.ndarray:
+        # final position (relative to `start`) -> index of the frame whose trailing part begins at `start`,
+        # through the transfers of levels l0 .. nlev-1
+        comp = np.arange(n - start, dtype=np.int64)
+        for j in range(l0, nlev):
+            o = int(lev_ptr[j]) - start
+            comp[o:] = comp[o:][perms[j]]
+        return comp
+
+    out: Dict[str, np.ndarray] = {}
+    for k in ("n", "nlev", "lev_ptr", "solve_option", "inner.enable", "inner.maxits", "inner.tol"):
+        out[k] = d[k]
+    for k in ("A.i", "A.j", "A.a", "A.shape"):
+        out[k] = d[k]
+    out["pperm"] = composed(0, 0).astype(np.int32)
+    out["qperm"] = np.zeros(0, np.int32)
+    for l in range(nlev):
+        pre = "L%d." % l
+        ncomp = int(d[pre + "ncomp"][0])
+        out[pre + "ncomp"] = d[pre + "ncomp"]
+        out[pre + "dom_ptr"] = d[pre + "dom_ptr"]
+        for c in range(ncomp):
+            pc = "%sB%d." % (pre, c)
+            if int(d[pc + "perms"][0]) != 0:
+                raise ValueError("ILU factors with an internal permutation are not supported")
+            for m in ("A", "L", "U"):
+                for suf in (".i", ".j", ".a", ".shape"):
+                    out[pc + m + suf] = d[pc + m + suf]
+            out[pc + "D"] = d[pc + "D"]
+            out[pc + "rperm"] = np.zeros(0, np.int32)
+            out[pc + "cperm"] = np.zeros(0, np.int32)
+        if l < nlev - 1:
+            comp = composed(int(lev_ptr[l + 1]), l + 1)
+            inv = np.empty_like(comp)
+            inv[comp] = np.arange(comp.size)
+            tmp = {}
+            for m in ("E", "F"):
+                for suf in (".i", ".j", ".a", ".shape"):
+                    tmp[pre + m + suf] = d[pre + m + suf].copy()
+            _permute_rows(tmp, pre + "E", comp)
+            tmp[pre + "F.j"] = inv[tmp[pre + "F.j"].astype(np.int64)].astype(np.int32)
+            out.update(tmp)
+            rank = int(d[pre + "lrc"][0])
+            out[pre + "lrc"] = d[pre + "lrc"]
+            if rank > 0:
+                m_l = comp.size
+                for w in ("W", "WH"):
+                    W = d[pre + w].reshape(rank, m_l)  # column-major m_l x rank: one row of this array per column
+                    out[pre + w] = np.ascontiguousarray(W[:, comp]).ravel()
+                    out[pre + w + ".shape"] = d[pre + w + ".shape"]
+    return out
+
+
+def from_parallel_dump(path: str) -> GemslrStructures:
+    """Load the structures a reference ParallelGemslrClass at one rank exported, in GemslrClass form."""
+    seq = parallel_to_sequential_dump(pgxd.read(path))
+    tmp = path + ".seq"
+    pgxd.write(tmp, seq)
+    try:
+        return from_dump(tmp)
+    finally:
+        os.unlink(tmp)

@@ -143,3 +143,45 @@ def run_complex(lap, params: np.ndarray, B: np.ndarray, apply_k: int = 0, thread
         res["apply_in"] = ap["in"].view(np.complex128).reshape(apply_k, -1)
         res["apply_out"] = ap["out"].view(np.complex128).reshape(apply_k, -1)
     return res
+
+
+DRIVER_PAR = os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver_par")
+
+
+def available_parallel() -> bool:
+    return os.path.exists(DRIVER_PAR)
+
+
+def run_parallel(lap, params: np.ndarray, xtrue: np.ndarray, apply_k: int = 0, threads: int = 1,
+                 tag: str = "") -> Dict[str, object]:
+    """Run the reference's ParallelGemslrClass at one rank (pgx_ref_driver_par) on the Laplacian
+    lap = (nx, ny, nz, shift, ax, ay, az) with b = A xtrue: its setup dump (setup_par.bin, with the
+    per-level transfer permutations), one FGMRES solve from x0 = 0 and apply_k preconditioner
+    applications.  Cached like run()."""
+    key = hashlib.sha1(repr((lap, params.tobytes(), np.ascontiguousarray(xtrue, np.float64).tobytes(), apply_k,
+                             threads, tag, _file_digest(DRIVER_PAR))).encode()).hexdigest()[:16]
+    out = os.path.join(CACHE, "p" + key)
+    done = os.path.join(out, "result.txt")
+    if not os.path.exists(done):
+        os.makedirs(out, exist_ok=True)
+        xf = os.path.join(out, "xtrue.bin")
+        pgxd.write(xf, {"x_true": np.ascontiguousarray(xtrue, np.float64)})
+        cmd = [DRIVER_PAR, "--out", out, "--threads", str(threads), "--lap", *[str(v) for v in lap], "--xtrue", xf,
+               "--dump", "--solve"] + param_args(params)
+        if apply_k:
+            cmd += ["--apply", str(apply_k)]
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
+        subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
+    res: Dict[str, object] = {"dir": out, "setup_par": os.path.join(out, "setup_par.bin")}
+    with open(done) as f:
+        for line in f:
+            k, v = line.strip().split("=", 1)
+            res[k] = float(v) if any(c in v for c in ".e") else int(v)
+    res["problem"] = pgxd.read(os.path.join(out, "problem.bin"))
+    res["x"] = pgxd.read(os.path.join(out, "solution.bin"))["x"]
+    if apply_k:
+        ap = pgxd.read(os.path.join(out, "apply.bin"))
+        n = res["x"].size
+        res["apply_in"] = ap["in"].reshape(apply_k, n)
+        res["apply_out"] = ap["out"].reshape(apply_k, n)
+    return res
