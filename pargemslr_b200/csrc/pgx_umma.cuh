@@ -54,6 +54,35 @@ __device__ __forceinline__ void tf32_split(float a, float& hi, float& lo) {
   hi = __int_as_float(__float_as_int(a) & (int)0xFFFFE000);
   lo = a - hi;
 }
+// Stage a rows x KT operand tile: value(row, k) for element e = (row, k) of the
+// tile, split into its hi and lo tiles.  Each thread loads kStageBatch values
+// before it stores any, so their global loads are in flight together.
+constexpr int kStageBatch = 8;
+template <typename F>
+__device__ __forceinline__ void umma_stage(unsigned char* hi_tile, unsigned char* lo_tile, int rows, int KT,
+                                           bool k_fastest, F value) {
+  const int total = rows * KT;
+  for (int base = threadIdx.x; base < total; base += kUmmaThreads * kStageBatch) {
+    float v[kStageBatch];
+#pragma unroll
+    for (int u = 0; u < kStageBatch; u++) {
+      const int e = base + u * kUmmaThreads;
+      v[u] = 0.f;
+      if (e < total) v[u] = k_fastest ? value(e / KT, e % KT) : value(e % rows, e / rows);
+    }
+#pragma unroll
+    for (int u = 0; u < kStageBatch; u++) {
+      const int e = base + u * kUmmaThreads;
+      if (e < total) {
+        const int row = k_fastest ? e / KT : e % rows, k = k_fastest ? e % KT : e / rows;
+        float h, l;
+        tf32_split(v[u], h, l);
+        *(float*)(hi_tile + umma_off(row, k, KT)) = h;
+        *(float*)(lo_tile + umma_off(row, k, KT)) = l;
+      }
+    }
+  }
+}
 
 __device__ __forceinline__ void tmem_alloc32(uint32_t* slot) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(slot)) : "memory");
@@ -148,33 +177,21 @@ __global__ void __launch_bounds__(kUmmaThreads) lr_wtx_umma_kernel(int m, int r,
       phase ^= 1u;
     }
     const int k0 = ch * KT;
-    // A = [Re W, Im W]^T, rows c and r + c; rows 2r..127 zero
-    for (int e = tid; e < 128 * KT; e += kUmmaThreads) {
-      const int k = e % KT, row = e / KT;
-      float v = 0.f;
-      if (row < 2 * r && k0 + k < m) {
-        const cf32 w = W[(size_t)(row % r) * m + k0 + k];
-        v = row < r ? w.x : w.y;
-      }
-      float hi, lo;
-      tf32_split(v, hi, lo);
-      *(float*)(a_hi + umma_off(row, k, KT)) = hi;
-      *(float*)(a_lo + umma_off(row, k, KT)) = lo;
-    }
+    // A = [Re W, Im W]^T, rows c and r + c; rows 2r..127 zero (staged once,
+    // in the first chunk: the loop below only rewrites rows < 2r)
+    umma_stage(a_hi, a_lo, ch == c0 ? 128 : 2 * r, KT, true, [&](int row, int k) -> float {
+      if (row >= 2 * r || k0 + k >= m) return 0.f;
+      const cf32 w = W[(size_t)(row % r) * m + k0 + k];
+      return row < r ? w.x : w.y;
+    });
     // B = [Re X, Im X]^T, rows q and NL + q, scaled by s_q
-    for (int e = tid; e < N * KT; e += kUmmaThreads) {
-      const int k = e % KT, row = e / KT, q = row % NL;
-      float v = 0.f;
-      if (k0 + k < m) {
-        cf32 x = xb.in[q][k0 + k];
-        if (xb.scale[q]) x = x * (float)(*xb.scale[q]);
-        v = row < NL ? x.x : x.y;
-      }
-      float hi, lo;
-      tf32_split(v, hi, lo);
-      *(float*)(b_hi + umma_off(row, k, KT)) = hi;
-      *(float*)(b_lo + umma_off(row, k, KT)) = lo;
-    }
+    umma_stage(b_hi, b_lo, N, KT, true, [&](int row, int k) -> float {
+      if (k0 + k >= m) return 0.f;
+      const int q = row % NL;
+      cf32 x = xb.in[q][k0 + k];
+      if (xb.scale[q]) x = x * (float)(*xb.scale[q]);
+      return row < NL ? x.x : x.y;
+    });
     proxy_fence_smem();
     __syncthreads();
     if (tid == 0) {
@@ -281,35 +298,21 @@ __global__ void __launch_bounds__(kUmmaThreads) lr_update_umma_kernel(int m, int
     mbar_fence_init();
   }
   if (warp == 0) tmem_alloc32(&s_taddr);
-  // A = [Re WH | Im WH] rows i0..i0+127; K padding and rows past m zero
-  for (int e = tid; e < 128 * KT; e += kUmmaThreads) {
-    const int row = e % 128, k = e / 128;
-    float v = 0.f;
-    if (k < 2 * r && i0 + row < m) {
-      const cf32 w = WH[(size_t)(k % r) * m + i0 + row];
-      v = k < r ? w.x : w.y;
-    }
-    float hi, lo;
-    tf32_split(v, hi, lo);
-    *(float*)(a_hi + umma_off(row, k, KT)) = hi;
-    *(float*)(a_lo + umma_off(row, k, KT)) = lo;
-  }
+  // A = [Re WH | Im WH] rows i0..i0+127 (row fastest: coalesced along a
+  // column of WH); K padding and rows past m zero
+  umma_stage(a_hi, a_lo, 128, KT, false, [&](int row, int k) -> float {
+    if (k >= 2 * r || i0 + row >= m) return 0.f;
+    const cf32 w = WH[(size_t)(k % r) * m + i0 + row];
+    return k < r ? w.x : w.y;
+  });
   // B rows q: [Re Y_q, -Im Y_q]; rows NL + q: [Im Y_q, Re Y_q]
-  for (int e = tid; e < N * KT; e += kUmmaThreads) {
-    const int k = e % KT, row = e / KT, q = row % NL;
-    float v = 0.f;
-    if (k < 2 * r) {
-      const cf32 y = Y[(size_t)q * r + (k % r)];
-      if (row < NL)
-        v = k < r ? y.x : -y.y;
-      else
-        v = k < r ? y.y : y.x;
-    }
-    float hi, lo;
-    tf32_split(v, hi, lo);
-    *(float*)(b_hi + umma_off(row, k, KT)) = hi;
-    *(float*)(b_lo + umma_off(row, k, KT)) = lo;
-  }
+  umma_stage(b_hi, b_lo, N, KT, true, [&](int row, int k) -> float {
+    if (k >= 2 * r) return 0.f;
+    const int q = row % NL;
+    const cf32 y = Y[(size_t)q * r + (k % r)];
+    if (row < NL) return k < r ? y.x : -y.y;
+    return k < r ? y.y : y.x;
+  });
   proxy_fence_smem();
   tc_fence_before();
   __syncthreads();
