@@ -609,7 +609,8 @@ def run_serve(args):
     sum), each set up once (untimed) and kept resident; one pool with a device-memory budget of 90% of the free
     memory admits requests by the bytes of their slot (work space and FGMRES(40) Krylov basis).  For every arrival
     rate, --serve-requests requests arrive with exponential gaps, each for a matrix drawn uniformly with a seeded
-    U[-1,1] right-hand side (a few per matrix, reused), solved to rel-res 1e-8.  Latency is arrival to collection on
+    U[-1,1] right-hand side (a few per matrix, reused), solved to rel-res 1e-8.  An untimed burst of --serve-warmup
+    requests first brings the pool to its working set of slots.  Latency is arrival to collection on
     the host clock; throughput is requests finished over the span from the first arrival to the last finish."""
     import torch
     from pargemslr_b200.handle import GemslrHandle
@@ -635,8 +636,26 @@ def run_serve(args):
     B = [[torch.from_numpy(np.random.default_rng(7 * i + k).uniform(-1, 1, h.n)).cuda() for k in range(rhs_per)]
          for i, h in enumerate(hs)]
     pool.start()
-    results = []
     rid = 0
+    # warm-up, untimed: one burst of --serve-warmup requests spread over the members, submitted together, so the
+    # slots (and their captured restart graphs) that the measured rates will use exist before any latency counts
+    if args.serve_warmup > 0:
+        t0 = time.time()
+        pending, warm_x = set(), []
+        for k in range(args.serve_warmup):
+            m = k % len(hs)
+            xs_w = torch.zeros(hs[m].n, dtype=torch.float64, device="cuda")
+            pool.submit_ptr(m, xs_w.data_ptr(), B[m][k % rhs_per].data_ptr(), LOCATION_DEVICE, rid)
+            pending.add(rid)
+            rid += 1
+            warm_x.append(xs_w)
+        while pending:
+            for i, _ in pool.collect():
+                pending.discard(i)
+            time.sleep(0.0005)
+        warm_x.clear()
+        log("warm-up: %d requests, %d slots, %.1f s" % (args.serve_warmup, pool.stats()["slots"], time.time() - t0))
+    results = []
     for rate in args.serve_rates:
         gaps = rng.exponential(1.0 / rate, size=args.serve_requests)
         members = rng.integers(0, len(hs), size=args.serve_requests)
@@ -684,9 +703,177 @@ def run_serve(args):
             "config": {"workload": "%d random nonsymmetric sparse systems, rows log-uniform in [%d, %d], 7-27 "
                                    "nonzeros per row, 2 levels, ILUT 1e-2/20, rank 8, FGMRES(40) to 1e-8"
                                    % (len(hs), lo, hi),
-                       "budget_bytes": budget, "setup_s": round(setup_s, 1), "rows": [int(v) for v in sizes]},
+                       "budget_bytes": budget, "setup_s": round(setup_s, 1), "warmup_requests": args.serve_warmup, "rows": [int(v) for v in sizes]},
             "value": max(r["solves_per_s"] for r in results), "rates": results}
     print(json.dumps(line), flush=True)
+
+
+def run_uneven(args):
+    """Batched uneven systems: --systems upwind convection-diffusion problems -Laplace(u) + beta . grad(u) on n x n
+    grids, n log-uniform in [32, 512] and beta ~ U[0, 50]^2 (seeded), b ~ U[-1, 1]; 2 levels, ILUT 1e-2/20, rank 8,
+    inner Schur FGMRES(5), FGMRES(30) to rel-res 1e-8 from x0 = 0.  Each system is set up once by this library's
+    host setup (untimed) and all of them are packed into one pgx_systems object; a step solves every system with ONE
+    persistent kernel launch under the schedule the autotuner picked.  value: systems per second of device time of
+    that launch (inputs resident); e2e: the same solves from and to host arrays, copies inside the timed region.
+    Compared with each system solved by its own handle (pgx_gemslr_solve, one after another) on a sample, and with
+    the reference CPU solver (its own setup, single-threaded processes, one per host thread) on a sample."""
+    import torch
+    from pargemslr_b200.handle import GemslrHandle
+    from pargemslr_b200.systems import SystemsBatch
+
+    count = args.systems
+    rng = np.random.default_rng(SEED + 4)
+    grid = np.exp(rng.uniform(np.log(32), np.log(512), size=count)).astype(int)
+    beta = rng.uniform(0.0, 50.0, size=(count, 2))
+    p = P.workload_params("convdiff")
+    mats, B, hs = [], [], []
+    t0 = time.time()
+    for k in range(count):
+        g = int(grid[k])
+        A = problems.upwind_convdiff_2d(g, g, float(beta[k, 0]), float(beta[k, 1]))
+        mats.append(A)
+        B.append(rng.uniform(-1.0, 1.0, g * g))
+        hs.append(GemslrHandle.from_matrix(A, p, precision=args.precision))
+        if (k + 1) % 64 == 0:
+            log("set up %d/%d systems (%.1f s)" % (k + 1, count, time.time() - t0))
+    setup_s = time.time() - t0
+    sizes = np.array([g * g for g in grid])
+    sb = SystemsBatch(hs)
+    t0 = time.time()
+    best = sb.tune(B, params=p, stride=args.uneven_tune_stride)
+    table = sb.tune_table()
+    log("autotuner on every %d-th system: %s in %.1f ms (%.1f s for %d candidates)"
+        % (args.uneven_tune_stride, sb.schedule, best, time.time() - t0, len(table)))
+    # device-resident inputs: b and x0 = 0 on the GPU
+    bd = [torch.from_numpy(b).cuda() for b in B]
+    xflat = torch.zeros(int(sizes.sum()), dtype=torch.float64, device="cuda")
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    xptr = [xflat[offs[k]:offs[k + 1]].data_ptr() for k in range(count)]
+    bptr = [b.data_ptr() for b in bd]
+    clocks = ClockSampler(0)
+    R = None
+    for _ in range(args.warmup):
+        xflat.zero_()
+        torch.cuda.synchronize()
+        R = sb.solve_ptrs(xptr, bptr, LOCATION_DEVICE, params=p)
+    ms = []
+    clocks.start()
+    for _ in range(args.steps):
+        xflat.zero_()
+        torch.cuda.synchronize()
+        R = sb.solve_ptrs(xptr, bptr, LOCATION_DEVICE, params=p)
+        ms.append(sb.last_launch_ms())
+    clk = clocks.stop()
+    ms_step = max(ms)
+    iters = np.array([r["iters"] for r in R])
+    trr = np.array([r["true_rel_res"] for r in R])
+    ok = int(np.sum([(r["status"] == 0 and r["true_rel_res"] <= 1e-8) for r in R]))
+    ts, te, ttri = sb.timing()
+    span = te - ts
+    slow = int(np.argmax(span))
+    # end to end from host arrays
+    e2e_s = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        X, Rh = sb.solve(B, params=p)
+        e2e_s.append(time.perf_counter() - t1)
+    e2e = count / max(e2e_s)
+    h2d = int(sizes.sum()) * 8 * 2
+    d2h = int(sizes.sum()) * 8
+    # each system by its own handle, one after another, on a sample spanning the sizes
+    order = np.argsort(sizes)
+    per_handle = None
+    if args.uneven_sample > 0:
+        sample = order[:: max(1, count // args.uneven_sample)]
+        t_one = []
+        it_one = []
+        for k in sample:
+            xs, rs = hs[k].solve(B[k], params=p)
+            t_one.append(rs["solve_ms"] * 1e-3)
+            it_one.append(rs["iters"])
+        scale = float(sizes.sum()) / float(sizes[sample].sum())
+        per_handle = {"systems_per_s": count / (sum(t_one) * scale), "sample": int(len(sample)), "iters": it_one,
+                      "what": "each system by its own handle (pgx_gemslr_solve: per-kernel launches and a graph "
+                              "per restart cycle), one after another; device time summed over every %d-th system by "
+                              "size, scaled by total over sampled unknowns" % max(1, count // args.uneven_sample)}
+    # the reference CPU solver (its own setup) on a sample, one single-threaded process per host thread
+    ref = None
+    drv = os.path.join(ROOT, "oracle", "_ref", "pgx_ref_driver")
+    if os.path.exists(drv) and not args.no_cpu_baseline:
+        from concurrent.futures import ThreadPoolExecutor
+        threads = os.cpu_count() or 1
+        rsample = order[:: max(1, count // args.uneven_ref_sample)]
+
+        def one(k):
+            d = tempfile.mkdtemp(prefix="pgx_uneven_")
+            A = mats[k]
+            f = os.path.join(d, "A.bin")
+            pgxd.write(f, {"A.i": A[0].astype(np.int32), "A.j": A[1].astype(np.int32),
+                           "A.a": A[2].astype(np.float64)})
+            rf = os.path.join(d, "rhs.bin")
+            pgxd.write(rf, {"b": B[k]})
+            cmd = [drv, "--out", d, "--csr", f, "--rhs", rf, "--solve", "--threads", "1"]
+            for i, v in enumerate(p):
+                cmd += ["--param", f"{i}={float(v)!r}"]
+            subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL,
+                           env=dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1"))
+            r = {}
+            with open(os.path.join(d, "result.txt")) as fh:
+                for line in fh:
+                    key, v = line.strip().split("=", 1)
+                    r[key] = v
+            x_ref = pgxd.read(os.path.join(d, "solution.bin"))["x"]
+            return k, float(r["solve_s"]), float(r["setup_s"]), int(r["iters"]), x_ref
+
+        t1 = time.time()
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            outs = list(ex.map(one, rsample))
+        wall = time.time() - t1
+        rscale = float(sizes.sum()) / float(sizes[rsample].sum())
+        solve_sum = sum(o[1] for o in outs)
+        xerr = [float(np.linalg.norm(X[k] - xr) / np.linalg.norm(xr)) for k, _, _, _, xr in outs]
+        ref = {"systems_per_s": count / (solve_sum * rscale / threads), "threads": threads,
+               "sample": int(len(rsample)), "solve_s_sum": solve_sum, "setup_s_sum": sum(o[2] for o in outs),
+               "wall_s": wall, "iters": [o[3] for o in outs], "iters_gpu": [int(iters[k]) for k in rsample],
+               "x_vs_x_ref_max": max(xerr),
+               "what": "reference CPU solver (oracle/_ref) with its own setup, one single-threaded process per host "
+                       "thread, every %d-th system by size; solve time summed over the sample, scaled by total "
+                       "unknowns over sampled unknowns, divided by the threads" % max(1, count // args.uneven_ref_sample)}
+        log("reference sample: %d systems, %.1f s of solves" % (len(rsample), solve_sum))
+    line = {
+        "metric": "systems/s (batched uneven GeMSLR-FGMRES(30), rel-res 1e-8, %d systems in one launch)" % count,
+        "value": count / (ms_step * 1e-3), "unit": "systems/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 preconditioner / f64 FGMRES" if args.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": "%d upwind convection-diffusion systems -Lu + beta.grad u on n x n grids, n "
+                               "log-uniform in [32, 512], beta ~ U[0,50]^2, b ~ U[-1,1], 2 levels, ILUT 1e-2/20, "
+                               "rank 8, inner Schur FGMRES(5), FGMRES(30) to rel-res 1e-8 from x0 = 0" % count,
+                   "unknowns": int(sizes.sum()), "setup": "this library's host setup per system, untimed",
+                   "schedule": {"threads": sb.schedule[0], "ctas_per_sm": sb.schedule[1], "spmv_lanes": sb.schedule[2]},
+                   "l2": "inputs larger than L2 (%.1f GB of packed structures and Krylov bases)"
+                         % (sb.device_bytes() / 1e9)},
+        "e2e": {"value": e2e, "unit": "systems/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": 1,
+        "detail": {"converged": ok, "iters_min": int(iters.min()), "iters_max": int(iters.max()),
+                   "iters_mean": float(iters.mean()), "true_rel_res_max": float(trr.max()),
+                   "setup_s": round(setup_s, 1), "tune_table": table,
+                   "system_ms": {"p50": float(np.percentile(span, 50)), "p99": float(np.percentile(span, 99)),
+                                 "max": float(span.max()), "last_end": float(te.max()),
+                                 "sum": float(span.sum()), "triangular_share": float(ttri.sum() / span.sum()),
+                                 "slowest": {"n": int(sizes[slow]), "iters": int(iters[slow]), "ms": float(span[slow]),
+                                             "triangular_ms": float(ttri[slow])}},
+                   "per_handle": per_handle,
+                   "reference": ref},
+        "clocks": clk,
+    }
+    if ref:
+        line["cpu_baseline"] = {"value": ref["systems_per_s"], "unit": "systems/s", "cores": ref["threads"],
+                                "kind": "reference", "sample": ref["what"]}
+    print(json.dumps(line), flush=True)
+    sb.close()
+    for h in hs:
+        h.close()
 
 
 def run_complex(args):
@@ -812,14 +999,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=128,
                     help="cube edge of the Laplacian (128 is the headline workload; smaller grids for profiling)")
-    ap.add_argument("--workload", choices=["laplacian", "serve", "complex"], default="laplacian",
+    ap.add_argument("--workload", choices=["laplacian", "serve", "complex", "uneven"], default="laplacian",
                     help="laplacian: the headline batch benchmark; serve: Poisson arrivals over resident matrices; "
                          "complex: 16 right-hand sides of the complex shifted 96^3 Laplacian as one block")
     ap.add_argument("--ref-rhs", type=int, default=2, help="complex workload: right-hand sides the reference solves")
+    ap.add_argument("--systems", type=int, default=512, help="uneven workload: number of systems")
+    ap.add_argument("--uneven-sample", type=int, default=32, help="uneven workload: systems solved by their own handle")
+    ap.add_argument("--uneven-ref-sample", type=int, default=32,
+                    help="uneven workload: systems the reference CPU solver solves")
+    ap.add_argument("--uneven-tune-stride", type=int, default=4,
+                    help="uneven workload: the autotuner times every k-th system of the work list")
     ap.add_argument("--serve-matrices", type=int, default=64)
     ap.add_argument("--serve-rows-min", type=int, default=200000)
     ap.add_argument("--serve-rows-max", type=int, default=2000000)
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests per arrival rate")
+    ap.add_argument("--serve-warmup", type=int, default=256, help="untimed burst of requests before the rates")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[50, 200, 500, 1000, 2000])
     args = ap.parse_args()
     global GRID
@@ -830,6 +1024,8 @@ def main():
         run_serve(args)
     elif args.workload == "complex":
         run_complex(args)
+    elif args.workload == "uneven":
+        run_uneven(args)
     else:
         run_pgx(args)
 

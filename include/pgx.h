@@ -346,6 +346,52 @@ int pgx_pool_collect(pgx_pool pool, int32_t max, int64_t *ids, pgx_result *resul
 int pgx_pool_stats(pgx_pool pool, int64_t *bytes_in_use, int64_t *peak_bytes, int32_t *slots);
 int pgx_pool_destroy(pgx_pool pool);
 
+/* ---- many systems in one launch -----------------------------------------
+ * No counterpart in the reference, which solves one system per
+ * FlexGmresClass::Solve call (fgmres.hpp:263-558).  A systems object packs
+ * the preconditioners of `count` committed real handles (each its own
+ * matrix, levels, factors and low-rank bases; sizes may differ) and solves
+ * all of them with ONE persistent kernel launch: each CTA takes the next
+ * system of a work list ordered by estimated cost, largest first, and runs
+ * that system's whole FGMRES(kdim) with its GeMSLR preconditioner (level
+ * recursion, low-rank corrections, the level-0 inner Schur FGMRES) before it
+ * takes the next.  The arithmetic is that of pgx_gemslr_solve with the same
+ * handle and precision; sums are formed in another order, so iterates agree
+ * to rounding, not bit for bit.  The handles stay usable and unchanged; the
+ * object keeps its own copies and may outlive them.
+ *   pgx_systems_solve: x[i] (initial guess in, solution out) and b[i] of
+ *     system i, all on the host or all on the device; params as for
+ *     pgx_gemslr_solve (one set for every system); results[i] receives system
+ *     i's outcome, its solve_ms being the span of that system inside the
+ *     launch and launches 1.
+ *   pgx_systems_tune: the schedule autotuner.  It solves a sample of the
+ *     batch (every stride-th system of the work list; stride 1 is the whole
+ *     batch) once per candidate (threads per CTA 256/512/1024, CTAs per SM,
+ *     SpMV lanes per row 2/4/8) from x0 = 0 into the object's own vectors,
+ *     keeps the fastest and returns its device time; pgx_systems_tune_table
+ *     returns the candidates tried, four doubles each (threads, CTAs per SM,
+ *     lanes, ms).
+ *   pgx_systems_set_schedule / get_schedule: the schedule in use (default 512
+ *     threads, 2 CTAs per SM, 4 lanes).
+ *   pgx_systems_timing: per system, the start and end of its solve in the last
+ *     launch, in ms from the first system's start, and the time it spent in
+ *     its triangular (B-block) solves (device clock; any array may be NULL);
+ *     pgx_systems_last_ms: the device time of the last solve's launch (CUDA
+ *     events around the kernel). */
+typedef struct pgx_systems_s *pgx_systems;
+int pgx_systems_create(pgx_systems *out, const pgx_handle *handles, int32_t count);
+int pgx_systems_solve(pgx_systems systems, double *const *x, const double *const *b, int32_t location,
+                      const double *params, pgx_result *results);
+int pgx_systems_tune(pgx_systems systems, const double *const *b, int32_t location, const double *params,
+                     int32_t stride, double *best_ms);
+int pgx_systems_tune_table(pgx_systems systems, int32_t capacity, double *table, int32_t *rows);
+int pgx_systems_set_schedule(pgx_systems systems, int32_t threads, int32_t ctas_per_sm, int32_t lanes);
+int pgx_systems_get_schedule(pgx_systems systems, int32_t *threads, int32_t *ctas_per_sm, int32_t *lanes);
+int pgx_systems_timing(pgx_systems systems, int32_t capacity, double *start_ms, double *end_ms, double *tri_ms);
+int pgx_systems_last_ms(pgx_systems systems, double *ms);
+int pgx_systems_device_bytes(pgx_systems systems, int64_t *bytes);
+int pgx_systems_destroy(pgx_systems systems);
+
 /* Apply the preconditioner once, z = M^-1 v (GemslrClass::Solve,
  * gemslr.cpp:3431-3472), on host or device vectors. */
 int pgx_gemslr_precond_apply(pgx_handle handle, double *z, const double *v, int32_t location);

@@ -51,6 +51,10 @@ EXPORTS = (
     "pgx_csr_spmv_plan", "pgx_csr_spmv_device_variant", "pgx_gemslr_describe",
     "pgx_pool_create", "pgx_pool_add", "pgx_pool_submit", "pgx_pool_step", "pgx_pool_start", "pgx_pool_stop",
     "pgx_pool_collect", "pgx_pool_stats", "pgx_pool_destroy", "pgx_lowrank_block_apply_c64",
+    "pgx_systems_create", "pgx_systems_solve", "pgx_systems_tune", "pgx_systems_tune_table",
+    "pgx_systems_set_schedule", "pgx_systems_get_schedule", "pgx_systems_timing", "pgx_systems_device_bytes",
+    "pgx_systems_last_ms",
+    "pgx_systems_destroy",
 )
 
 # every symbol include/pgx_hypre.h declares (the reference's hypre plugin interface)
@@ -152,6 +156,16 @@ def lib() -> C.CDLL:
     L.pgx_pool_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32)]
     L.pgx_pool_destroy.argtypes = [vp]
     L.pgx_gemslr_describe.argtypes = [vp, i32, C.c_char_p, i32, C.POINTER(i32)]
+    L.pgx_systems_create.argtypes = [C.POINTER(vp), vp, i32]
+    L.pgx_systems_solve.argtypes = [vp, vp, vp, i32, vp, vp]
+    L.pgx_systems_tune.argtypes = [vp, vp, i32, vp, i32, C.POINTER(dbl)]
+    L.pgx_systems_tune_table.argtypes = [vp, i32, vp, C.POINTER(i32)]
+    L.pgx_systems_set_schedule.argtypes = [vp, i32, i32, i32]
+    L.pgx_systems_get_schedule.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    L.pgx_systems_timing.argtypes = [vp, i32, vp, vp, vp]
+    L.pgx_systems_device_bytes.argtypes = [vp, C.POINTER(i64)]
+    L.pgx_systems_last_ms.argtypes = [vp, C.POINTER(dbl)]
+    L.pgx_systems_destroy.argtypes = [vp]
     L.pgx_csr_spmv_plan.argtypes = [C.POINTER(Csr), C.POINTER(i32), C.POINTER(i32)]
     L.pgx_csr_spmv_device_variant.argtypes = [C.POINTER(Csr), i32, dbl, vp, dbl, vp]
     for name in EXPORTS + HYPRE_EXPORTS:

@@ -19,7 +19,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libpgx.so")
 SOURCES = [os.path.join(CSRC, "pgx.cu"), os.path.join(CSRC, "setup.cpp"), os.path.join(CSRC, "params.cpp"),
            os.path.join(CSRC, "hypre.cpp")]
-HEADERS = [os.path.join(CSRC, "pgx_device.cuh"), os.path.join(CSRC, "pgx_complex.cuh"), os.path.join(CSRC, "pgx_umma.cuh"), os.path.join(CSRC, "pgx_setup.h"), os.path.join(CSRC, "pgx_params.h"),
+HEADERS = [os.path.join(CSRC, "pgx_device.cuh"), os.path.join(CSRC, "pgx_complex.cuh"), os.path.join(CSRC, "pgx_umma.cuh"), os.path.join(CSRC, "pgx_systems.cuh"), os.path.join(CSRC, "pgx_setup.h"), os.path.join(CSRC, "pgx_params.h"),
            os.path.join(CSRC, "pgx_internal.h"), os.path.join(ROOT, "include", "pgx_hypre.h"),
            os.path.join(ROOT, "include", "pgx.h")]
 

@@ -42,6 +42,7 @@
 #include "pgx_device.cuh"
 #include "pgx_internal.h"
 #include "pgx_umma.cuh"
+#include "pgx_systems.cuh"
 #include "pgx_params.h"
 #include "pgx_setup.h"
 
@@ -806,6 +807,44 @@ struct Import {
   double inner_tol = 1e-2;
 };
 
+// The C block below level l, C_l (the operator of GemslrClass::SchurMatVec,
+// gemslr.cpp:3799-3960): the B, E and F blocks of the levels after l,
+// assembled over the trailing n - lev_ptr[l+1] unknowns.
+static HostCsr host_c_block(const Import& im, int l) {
+  const int base = im.lev_ptr[l + 1];
+  const int m = im.n - base;
+  const int vw = im.vw;
+  // (column, value) with the value as {re, im} (im 0 for a real matrix)
+  std::vector<std::vector<std::pair<int, std::pair<double, double>>>> rows(m);
+  auto add = [&](const HostCsr& M, int roff, int coff) {
+    for (int r = 0; r < M.rows; r++)
+      for (int k = M.rp[r]; k < M.rp[r + 1]; k++)
+        rows[roff + r].push_back({coff + M.cj[k], {M.va[(size_t)vw * k], vw == 2 ? M.va[(size_t)vw * k + 1] : 0.0}});
+  };
+  for (int j = l + 1; j < im.nlev; j++) {
+    const HostLevel& h = im.levels[j];
+    const int o = im.lev_ptr[j] - base, o1 = im.lev_ptr[j + 1] - base;
+    add(h.B, o, o);
+    if (j < im.nlev - 1) {
+      add(h.F, o, o1);
+      add(h.E, o1, o);
+    }
+  }
+  HostCsr c;
+  c.rows = c.cols = m;
+  c.rp.assign(m + 1, 0);
+  for (int r = 0; r < m; r++) {
+    std::sort(rows[r].begin(), rows[r].end());
+    for (auto& e : rows[r]) {
+      c.cj.push_back(e.first);
+      c.va.push_back(e.second.first);
+      if (vw == 2) c.va.push_back(e.second.second);
+    }
+    c.rp[r + 1] = (int)c.cj.size();
+  }
+  return c;
+}
+
 struct EngineBase {
   virtual ~EngineBase() {}
   virtual int kernel_stats(int which, int level, int reps, double* avg_ms, double* bytes, int* launches) = 0;
@@ -1229,40 +1268,7 @@ struct Engine : EngineBase {
   // unfactored B_j blocks of levels j > l on the diagonal, E_j / F_j of the
   // non-last levels j > l off the diagonal, in the local numbering of the
   // trailing m_l unknowns.
-  int assemble_c(Import& im, int l, DCsr<P>& out) {
-    const int base = lev_ptr[l + 1];
-    const int m = n - base;
-    // (column, value) with the value as {re, im} (im 0 for a real matrix)
-    std::vector<std::vector<std::pair<int, std::pair<double, double>>>> rows(m);
-    auto add = [&](const HostCsr& M, int roff, int coff) {
-      for (int r = 0; r < M.rows; r++)
-        for (int k = M.rp[r]; k < M.rp[r + 1]; k++)
-          rows[roff + r].push_back(
-              {coff + M.cj[k], {M.va[(size_t)VW * k], VW == 2 ? M.va[(size_t)VW * k + 1] : 0.0}});
-    };
-    for (int j = l + 1; j < nlev; j++) {
-      const HostLevel& h = im.levels[j];
-      const int o = lev_ptr[j] - base, o1 = lev_ptr[j + 1] - base;
-      add(h.B, o, o);
-      if (j < nlev - 1) {
-        add(h.F, o, o1);
-        add(h.E, o1, o);
-      }
-    }
-    HostCsr c;
-    c.rows = c.cols = m;
-    c.rp.assign(m + 1, 0);
-    for (int r = 0; r < m; r++) {
-      std::sort(rows[r].begin(), rows[r].end());
-      for (auto& e : rows[r]) {
-        c.cj.push_back(e.first);
-        c.va.push_back(e.second.first);
-        if (VW == 2) c.va.push_back(e.second.second);
-      }
-      c.rp[r + 1] = (int)c.cj.size();
-    }
-    return upload_csr(ar, c, out, stream);
-  }
+  int assemble_c(Import& im, int l, DCsr<P>& out) { return upload_csr(ar, host_c_block(im, l), out, stream); }
   int assemble_c0(Import& im) { return assemble_c(im, 0, C0); }
 
   // replace the low-rank correction of level l
@@ -2952,6 +2958,503 @@ static int lowrank_block_apply(int m, int r, const cf32* W, const cf32* WH, cf32
   return PGX_SUCCESS;
 }
 
+// ------------------------------------------------- many systems, one launch
+// The systems of several committed handles packed for systems_fgmres_kernel:
+// every structure of every system lives in three arenas (indices, P values,
+// doubles), each array starting on a 64-element boundary, and one SysDesc
+// per system holds its pointers.  The work list orders the systems by an
+// estimate of their cost, largest first, so the CTAs that take the last
+// systems take small ones.
+struct SystemsBase {
+  virtual ~SystemsBase() {}
+  virtual int solve(double* const* x, const double* const* b, int location, int kdim, int maxits, double tol,
+                    int atol, pgx_result* res) = 0;
+  virtual int tune(const double* const* b, int location, int kdim, int maxits, double tol, int atol, int stride,
+                   double* best_ms) = 0;
+  virtual int64_t device_bytes() const = 0;
+  int threads = 512, ctas_per_sm = 2, lanes = 4;
+  double last_ms = 0.0;  // device time of the last solve's launch (CUDA events)
+  std::vector<double> t_start, t_end;  // per system, ms from the launch's first system start
+  std::vector<double> t_tri;           // per system, ms in its triangular (B-block) solves
+  std::vector<std::array<double, 4>> tune_table;  // threads, ctas per SM, lanes, ms
+};
+
+template <typename P>
+struct Systems : SystemsBase {
+  int count = 0, device = 0, nsm = 148;
+  std::vector<int> n_of;             // unknowns per system
+  std::vector<size_t> xoff;          // offsets of each system in the packed b and x
+  size_t ntot = 0;
+  std::vector<SysDesc<P>> desc;      // host copies (device pointers)
+  std::vector<int> order;
+  Arena ar, work;
+  int *d_ints = nullptr, *d_order = nullptr;
+  P* d_p = nullptr;
+  double* d_d = nullptr;
+  SysDesc<P>* d_desc = nullptr;
+  double *d_bpack = nullptr, *d_xpack = nullptr;
+  double *h_bpack = nullptr, *h_xpack = nullptr;  // pinned
+  const double** d_bptr = nullptr;
+  double** d_xptr = nullptr;
+  std::vector<const double*> h_bptr_cur;
+  std::vector<double*> h_xptr_cur;
+  const double** h_bptr = nullptr;  // pinned staging of the pointer tables
+  double** h_xptr = nullptr;
+  unsigned int* d_next = nullptr;
+  SysResult* d_res = nullptr;
+  SysResult* h_res = nullptr;  // pinned
+  FgmresDev *d_st = nullptr, *d_st_in = nullptr;
+  int st_ctas = 0;
+  int work_kdim = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  ~Systems() override {
+    if (stream) cudaStreamSynchronize(stream);
+    if (h_bpack) cudaFreeHost(h_bpack);
+    if (h_xpack) cudaFreeHost(h_xpack);
+    if (h_res) cudaFreeHost(h_res);
+    if (h_bptr) cudaFreeHost(h_bptr);
+    if (h_xptr) cudaFreeHost(h_xptr);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  struct Fix {
+    void* field;
+    int kind;  // 0 ints, 1 P values, 2 doubles
+    size_t off;
+  };
+  std::vector<int> iv;
+  std::vector<P> pv;
+  std::vector<double> dv;
+  std::vector<Fix> fix;
+  static size_t padded(size_t n) { return (n + 63) / 64 * 64; }
+  template <typename T, typename V>
+  static size_t put(std::vector<T>& v, const V* src, size_t n) {
+    const size_t off = v.size();
+    v.resize(off + padded(n), T(0));
+    for (size_t k = 0; k < n; k++) v[off + k] = (T)src[k];
+    return off;
+  }
+  void ints(const int** field, const int* src, size_t n) { fix.push_back({field, 0, put(iv, src, n)}); }
+  void vals(const P** field, const double* src, size_t n) { fix.push_back({field, 1, put(pv, src, n)}); }
+  void dbls(const double** field, const double* src, size_t n) { fix.push_back({field, 2, put(dv, src, n)}); }
+  // a rows x cols block; one given without entries (rows 0) becomes an
+  // all-zero block of the expected shape, so its SpMV still writes y
+  int csr_p(SysCsr<P>& c, const HostCsr& h, int rows, int cols, const char* what) {
+    c.rows = rows;
+    c.cols = cols;
+    if (h.rows == 0) {
+      const std::vector<int> rp(rows + 1, 0);
+      ints(&c.rp, rp.data(), rp.size());
+      return PGX_SUCCESS;
+    }
+    if (h.rows != rows || h.cols != cols)
+      return fail(PGX_ERROR_INVALID_PARAM, "%s is %d x %d, expected %d x %d", what, h.rows, h.cols, rows, cols);
+    ints(&c.rp, h.rp.data(), h.rp.size());
+    ints(&c.cj, h.cj.data(), h.cj.size());
+    vals(&c.va, h.va.data(), h.cj.size());
+    return PGX_SUCCESS;
+  }
+  // rows in level order (IluClass::BuildLevels rule, ilu.cpp:832-1062)
+  int tri(SysTri<P>& t, const HostCsr& h_in, bool upper, const std::vector<double>* dinv, int nl,
+          long long& levels) {
+    t.n = nl;
+    t.nlev = 0;
+    if (nl == 0) return PGX_SUCCESS;
+    HostCsr none;  // a factor given without entries
+    if (h_in.rows == 0) {
+      none.rows = none.cols = nl;
+      none.rp.assign(nl + 1, 0);
+    }
+    const HostCsr& h = h_in.rows == 0 ? none : h_in;
+    if (h.rows != nl) return fail(PGX_ERROR_INVALID_PARAM, "triangular factor has %d rows, level has %d", h.rows, nl);
+    if (upper && (!dinv || (int)dinv->size() < nl))
+      return fail(PGX_ERROR_INVALID_PARAM, "inverse diagonal shorter than the level's %d rows", nl);
+    std::vector<int> lvp, ord;
+    PGX_TRY(build_levels(upper, nl, h.rp.data(), h.cj.data(), lvp, ord));
+    t.nlev = (int)lvp.size() - 1;
+    levels += t.nlev;
+    std::vector<int> rp(nl + 1, 0), cj;
+    std::vector<double> va, di;
+    cj.reserve(h.cj.size());
+    va.reserve(h.cj.size());
+    for (int k = 0; k < nl; k++) {
+      const int r = ord[k];
+      for (int e = h.rp[r]; e < h.rp[r + 1]; e++) {
+        cj.push_back(h.cj[e]);
+        va.push_back(h.va[e]);
+      }
+      rp[k + 1] = (int)cj.size();
+      if (upper) di.push_back((*dinv)[r]);
+    }
+    ints(&t.lvp, lvp.data(), lvp.size());
+    ints(&t.row, ord.data(), ord.size());
+    ints(&t.rp, rp.data(), rp.size());
+    ints(&t.cj, cj.data(), cj.size());
+    vals(&t.va, va.data(), va.size());
+    if (upper) vals(&t.dinv, di.data(), di.size());
+    return PGX_SUCCESS;
+  }
+
+  int create(const std::vector<const Import*>& ims, int dev) {
+    device = dev;
+    count = (int)ims.size();
+    PGX_CUDA(cudaSetDevice(device));
+    PGX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    PGX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    PGX_CUDA(cudaEventCreate(&ev0));
+    PGX_CUDA(cudaEventCreate(&ev1));
+    desc.assign(count, SysDesc<P>());
+    std::memset((void*)desc.data(), 0, sizeof(SysDesc<P>) * count);
+    n_of.resize(count);
+    xoff.resize(count);
+    std::vector<double> cost(count, 0.0);
+    for (int s = 0; s < count; s++) {
+      const Import& im = *ims[s];
+      if (im.vw != 1) return fail(PGX_ERROR_INVALID_OPTION, "system %d: the systems solve is real only", s);
+      if (im.nlev < 1 || im.nlev > kSysMaxLevels)
+        return fail(PGX_ERROR_INVALID_PARAM, "system %d: %d levels (1..%d)", s, im.nlev, kSysMaxLevels);
+      if (im.inner_enable && im.nlev >= 2 && im.inner_maxits > KMAX)
+        return fail(PGX_ERROR_INVALID_PARAM, "system %d: inner maxits above %d", s, KMAX);
+      SysDesc<P>& d = desc[s];
+      const int n = im.n;
+      d.n = n;
+      d.nlev = im.nlev;
+      n_of[s] = n;
+      xoff[s] = ntot;
+      ntot += padded(n);
+      if (im.A.rows != n || im.A.cols != n) return fail(PGX_ERROR_INVALID_PARAM, "system %d: A is not %d x %d", s, n, n);
+      if ((int)im.lev_ptr.size() != im.nlev + 1 || im.lev_ptr[0] != 0 || im.lev_ptr[im.nlev] != n)
+        return fail(PGX_ERROR_INVALID_PARAM, "system %d: level pointer does not span n", s);
+      d.A.rows = im.A.rows;
+      d.A.cols = im.A.cols;
+      ints(&d.A.rp, im.A.rp.data(), im.A.rp.size());
+      ints(&d.A.cj, im.A.cj.data(), im.A.cj.size());
+      dbls(&d.A.va, im.A.va.data(), im.A.cj.size());
+      if ((int)im.pperm.size() != n) return fail(PGX_ERROR_INVALID_PARAM, "system %d: no permutation", s);
+      ints(&d.pperm, im.pperm.data(), n);
+      if (!im.qperm.empty()) ints(&d.qperm, im.qperm.data(), n);
+      long long levels = 0, fnnz = 0;
+      for (int l = 0; l < im.nlev; l++) {
+        const HostLevel& h = im.levels[l];
+        SysLevel<P>& v = d.lev[l];
+        v.nl = im.lev_ptr[l + 1] - im.lev_ptr[l];
+        v.m = n - im.lev_ptr[l + 1];
+        PGX_TRY(tri(v.L, h.L, false, nullptr, v.nl, levels));
+        PGX_TRY(tri(v.U, h.U, true, &h.dinv, v.nl, levels));
+        fnnz += h.L.nnz() + h.U.nnz();
+        if (l < im.nlev - 1) {
+          PGX_TRY(csr_p(v.E, h.E, v.m, v.nl, "E"));
+          PGX_TRY(csr_p(v.F, h.F, v.nl, v.m, "F"));
+          v.rank = h.rank;
+          if (h.rank > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "system %d: rank %d above %d", s, h.rank, KMAX);
+          if (h.rank > 0) {
+            if (h.W.size() < (size_t)v.m * h.rank || h.WH.size() < (size_t)v.m * h.rank)
+              return fail(PGX_ERROR_INVALID_PARAM, "system %d level %d: low-rank bases too short", s, l);
+            vals(&v.W, h.W.data(), (size_t)v.m * h.rank);
+            vals(&v.WH, h.WH.data(), (size_t)v.m * h.rank);
+          }
+        }
+      }
+      d.inner = (im.inner_enable && im.nlev >= 2) ? 1 : 0;
+      d.inner_maxits = im.inner_maxits;
+      d.inner_tol = im.inner_tol;
+      if (d.inner) PGX_TRY(csr_p(d.C0, host_c_block(im, 0), d.lev[0].m, d.lev[0].m, "C0"));
+      const int sweeps = 2 + (d.inner ? 2 * d.inner_maxits : 0);
+      cost[s] = (double)im.A.nnz() + (double)sweeps * ((double)fnnz + 1500.0 * (double)levels);
+    }
+    order.resize(count);
+    for (int s = 0; s < count; s++) order[s] = s;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    PGX_TRY(ar.upload(&d_ints, iv.data(), iv.size(), stream));
+    PGX_TRY(ar.upload(&d_p, pv.data(), pv.size(), stream));
+    PGX_TRY(ar.upload(&d_d, dv.data(), dv.size(), stream));
+    for (const Fix& f : fix) {
+      void* p = f.kind == 0 ? (void*)(d_ints + f.off) : f.kind == 1 ? (void*)(d_p + f.off) : (void*)(d_d + f.off);
+      *(void**)f.field = p;
+    }
+    iv.clear(), iv.shrink_to_fit();
+    pv.clear(), pv.shrink_to_fit();
+    dv.clear(), dv.shrink_to_fit();
+    fix.clear();
+    PGX_TRY(ar.upload(&d_order, order.data(), order.size(), stream));
+    PGX_TRY(ar.zeros(&d_bpack, std::max<size_t>(ntot, 1), stream));
+    PGX_TRY(ar.zeros(&d_xpack, std::max<size_t>(ntot, 1), stream));
+    PGX_TRY(ar.alloc(&d_bptr, count));
+    PGX_TRY(ar.alloc(&d_xptr, count));
+    PGX_TRY(ar.zeros(&d_next, 1, stream));
+    PGX_TRY(ar.zeros(&d_res, count, stream));
+    PGX_TRY(ar.alloc(&d_desc, count));
+    PGX_CUDA(cudaMallocHost(&h_bpack, sizeof(double) * std::max<size_t>(ntot, 1)));
+    PGX_CUDA(cudaMallocHost(&h_xpack, sizeof(double) * std::max<size_t>(ntot, 1)));
+    PGX_CUDA(cudaMallocHost(&h_res, sizeof(SysResult) * count));
+    PGX_CUDA(cudaMallocHost(&h_bptr, sizeof(double*) * count));
+    PGX_CUDA(cudaMallocHost(&h_xptr, sizeof(double*) * count));
+    h_bptr_cur.assign(count, nullptr);
+    h_xptr_cur.assign(count, nullptr);
+    t_start.assign(count, 0.0);
+    t_end.assign(count, 0.0);
+    t_tri.assign(count, 0.0);
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    return PGX_SUCCESS;
+  }
+
+  // work space for FGMRES(kdim): the Krylov bases and the preconditioner's vectors
+  int ensure_work(int kdim) {
+    if (kdim <= work_kdim) return PGX_SUCCESS;
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    work.release();
+    work_kdim = 0;
+    size_t np = 0, nd = 0;
+    for (int s = 0; s < count; s++) {
+      const SysDesc<P>& d = desc[s];
+      const size_t n = d.n, m0 = d.nlev > 1 ? d.lev[0].m : 0, nl0 = d.lev[0].nl;
+      nd += padded(n * (kdim + 1));
+      np += padded(n * kdim) + 2 * padded(n);
+      size_t start = 0;
+      for (int l = 0; l < d.nlev; l++) {
+        np += padded(n - start);
+        start += d.lev[l].nl;
+      }
+      if (d.inner) np += padded(m0 * (d.inner_maxits + 1)) + padded(m0 * d.inner_maxits) + padded(m0) + 2 * padded(nl0);
+    }
+    P* pw = nullptr;
+    double* dw = nullptr;
+    PGX_TRY(work.zeros(&pw, np, stream));
+    PGX_TRY(work.zeros(&dw, nd, stream));
+    size_t op = 0, od = 0;
+    auto takep = [&](size_t k) {
+      P* p = pw + op;
+      op += padded(k);
+      return p;
+    };
+    for (int s = 0; s < count; s++) {
+      SysDesc<P>& d = desc[s];
+      const size_t n = d.n, m0 = d.nlev > 1 ? d.lev[0].m : 0, nl0 = d.lev[0].nl;
+      d.V = dw + od;
+      od += padded(n * (kdim + 1));
+      d.Z = takep(n * kdim);
+      d.rt = takep(n);
+      d.xt = takep(n);
+      size_t start = 0;
+      for (int l = 0; l < d.nlev; l++) {
+        d.lev[l].z = takep(n - start);
+        start += d.lev[l].nl;
+      }
+      if (d.inner) {
+        d.Vin = takep(m0 * (d.inner_maxits + 1));
+        d.Zin = takep(m0 * d.inner_maxits);
+        d.xlr = takep(m0);
+        d.s_zu = takep(nl0);
+        d.s_wu = takep(nl0);
+      }
+    }
+    PGX_CUDA(cudaMemcpyAsync(d_desc, desc.data(), sizeof(SysDesc<P>) * count, cudaMemcpyHostToDevice, stream));
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    work_kdim = kdim;
+    return PGX_SUCCESS;
+  }
+
+  int ensure_states(int ctas) {
+    if (ctas <= st_ctas) return PGX_SUCCESS;
+    PGX_TRY(ar.zeros(&d_st, ctas, stream));
+    PGX_TRY(ar.zeros(&d_st_in, ctas, stream));
+    st_ctas = ctas;
+    return PGX_SUCCESS;
+  }
+
+  int64_t device_bytes() const override { return (int64_t)(ar.bytes + work.bytes); }
+
+  // the pointer tables the kernel reads b and x through
+  int set_pointers(double* const* x, const double* const* b, int location) {
+    bool changed = false;
+    for (int s = 0; s < count; s++) {
+      const double* bp = location == PGX_LOCATION_DEVICE ? b[s] : d_bpack + xoff[s];
+      double* xp = location == PGX_LOCATION_DEVICE ? x[s] : d_xpack + xoff[s];
+      if (bp != h_bptr_cur[s] || xp != h_xptr_cur[s]) changed = true;
+      h_bptr_cur[s] = bp;
+      h_xptr_cur[s] = xp;
+    }
+    if (!changed) return PGX_SUCCESS;
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    std::memcpy(h_bptr, h_bptr_cur.data(), sizeof(double*) * count);
+    std::memcpy(h_xptr, h_xptr_cur.data(), sizeof(double*) * count);
+    PGX_CUDA(cudaMemcpyAsync(d_bptr, h_bptr, sizeof(double*) * count, cudaMemcpyHostToDevice, stream));
+    PGX_CUDA(cudaMemcpyAsync(d_xptr, h_xptr, sizeof(double*) * count, cudaMemcpyHostToDevice, stream));
+    return PGX_SUCCESS;
+  }
+
+  int launch(int kdim, int maxits, double tol, int atol, int th, int cps, int ln, const int* ord = nullptr,
+             int nord = -1) {
+    // CTAs of up to 256 threads use the build with 128 registers per thread
+    void (*kern)(SysArgs<P>) = th <= 256 ? systems_fgmres_kernel<P, 256> : systems_fgmres_kernel<P, kSysMaxThreads>;
+    int occ = 0;
+    PGX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, th, 0));
+    if (occ < 1) return fail(PGX_ERROR_INVALID_PARAM, "%d threads per CTA do not fit an SM", th);
+    cps = std::min(cps, occ);
+    // the rest of the SM's shared memory, split over its CTAs, holds the
+    // triangular solves' vector for every block that fits
+    size_t smem = 0;
+    PGX_CUDA(cudaOccupancyAvailableDynamicSMemPerBlock(&smem, kern, cps, th));
+    smem = smem / 256 * 256;
+    PGX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (!ord) {
+      ord = d_order;
+      nord = count;
+    }
+    const int grid = std::max(1, std::min(nord, nsm * cps));
+    PGX_TRY(ensure_states(grid));
+    SysArgs<P> a;
+    a.sys = d_desc;
+    a.order = ord;
+    a.count = nord;
+    a.b = d_bptr;
+    a.x = d_xptr;
+    a.kdim = kdim;
+    a.maxits = maxits;
+    a.atol = atol;
+    a.tol = tol;
+    a.lanes = ln;
+    a.scap = (int)(smem / sizeof(P));
+    a.next = d_next;
+    a.st = d_st;
+    a.st_in = d_st_in;
+    a.res = d_res;
+    PGX_CUDA(cudaMemsetAsync(d_next, 0, sizeof(unsigned int), stream));
+    PGX_CUDA(cudaEventRecord(ev0, stream));
+    kern<<<grid, th, smem, stream>>>(a);
+    PGX_CUDA(cudaGetLastError());
+    PGX_CUDA(cudaEventRecord(ev1, stream));
+    return PGX_SUCCESS;
+  }
+
+  int check_params(int kdim, int maxits) {
+    if (kdim < 1 || kdim > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "kdim %d outside [1, %d]", kdim, KMAX);
+    if (maxits < 0) return fail(PGX_ERROR_INVALID_PARAM, "maxits %d < 0", maxits);
+    return PGX_SUCCESS;
+  }
+
+  int solve(double* const* x, const double* const* b, int location, int kdim, int maxits, double tol, int atol,
+            pgx_result* res) override {
+    PGX_TRY(check_params(kdim, maxits));
+    PGX_CUDA(cudaSetDevice(device));
+    for (int s = 0; s < count; s++)
+      if (!x[s] || !b[s]) return fail(PGX_ERROR_INVALID_PARAM, "system %d: null x or b", s);
+    if (location == PGX_LOCATION_HOST) {
+      int bad = -1;
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int s = 0; s < count; s++) {
+        if (!all_finite(b[s], n_of[s])) {
+#pragma omp critical
+          bad = s;
+        }
+        std::memcpy(h_bpack + xoff[s], b[s], sizeof(double) * n_of[s]);
+        std::memcpy(h_xpack + xoff[s], x[s], sizeof(double) * n_of[s]);
+      }
+      if (bad >= 0) return fail(PGX_ERROR_NOT_FINITE, "system %d: b is not finite", bad);
+    } else if (location != PGX_LOCATION_DEVICE) {
+      return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+    }
+    PGX_TRY(ensure_work(kdim));
+    PGX_TRY(set_pointers(x, b, location));
+    if (location == PGX_LOCATION_HOST) {
+      PGX_CUDA(cudaMemcpyAsync(d_bpack, h_bpack, sizeof(double) * ntot, cudaMemcpyHostToDevice, stream));
+      PGX_CUDA(cudaMemcpyAsync(d_xpack, h_xpack, sizeof(double) * ntot, cudaMemcpyHostToDevice, stream));
+    }
+    PGX_TRY(launch(kdim, maxits, tol, atol, threads, ctas_per_sm, lanes));
+    PGX_CUDA(cudaMemcpyAsync(h_res, d_res, sizeof(SysResult) * count, cudaMemcpyDeviceToHost, stream));
+    if (location == PGX_LOCATION_HOST)
+      PGX_CUDA(cudaMemcpyAsync(h_xpack, d_xpack, sizeof(double) * ntot, cudaMemcpyDeviceToHost, stream));
+    PGX_CUDA(cudaStreamSynchronize(stream));
+    if (location == PGX_LOCATION_HOST) {
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int s = 0; s < count; s++) std::memcpy(x[s], h_xpack + xoff[s], sizeof(double) * n_of[s]);
+    }
+    float ms = 0.f;
+    PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+    unsigned long long tmin = ~0ull;
+    for (int s = 0; s < count; s++) tmin = std::min(tmin, h_res[s].t0);
+    int out = PGX_SUCCESS;
+    for (int s = 0; s < count; s++) {
+      const SysResult& r = h_res[s];
+      t_start[s] = (double)(r.t0 - tmin) * 1e-6;
+      t_end[s] = (double)(r.t1 - tmin) * 1e-6;
+      t_tri[s] = (double)r.tri_ns * 1e-6;
+      int st = PGX_SUCCESS;
+      if (!std::isfinite(r.normr) || !std::isfinite(r.true_r2)) {
+        st = PGX_ERROR_NOT_FINITE;
+        if (out == PGX_SUCCESS) out = fail(st, "system %d: FGMRES residual is not finite", s);
+      }
+      if (res) {
+        res[s].status = st;
+        res[s].iters = r.iters;
+        res[s].rel_res = r.normb > 0 ? r.normr / r.normb : 0.0;
+        res[s].true_rel_res = r.normb > 0 ? sqrt(r.true_r2) / r.normb : 0.0;
+        res[s].solve_ms = t_end[s] - t_start[s];
+        res[s].launches = 1;
+      }
+    }
+    last_ms = ms;
+    return out;
+  }
+
+  // The schedule autotuner: a sample of the batch (every stride-th system of
+  // the work list, so it spans the sizes) solved once per candidate (threads
+  // per CTA, CTAs per SM, SpMV lanes per row) from x0 = 0 into the library's
+  // own x; the fastest by device time is kept.
+  int tune(const double* const* b, int location, int kdim, int maxits, double tol, int atol, int stride,
+           double* best_ms) override {
+    PGX_TRY(check_params(kdim, maxits));
+    if (stride < 1) return fail(PGX_ERROR_INVALID_PARAM, "stride %d < 1", stride);
+    PGX_CUDA(cudaSetDevice(device));
+    if (location == PGX_LOCATION_HOST) {
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int s = 0; s < count; s++) std::memcpy(h_bpack + xoff[s], b[s], sizeof(double) * n_of[s]);
+      PGX_CUDA(cudaMemcpyAsync(d_bpack, h_bpack, sizeof(double) * ntot, cudaMemcpyHostToDevice, stream));
+    } else if (location == PGX_LOCATION_DEVICE) {
+      for (int s = 0; s < count; s++)
+        PGX_CUDA(cudaMemcpyAsync(d_bpack + xoff[s], b[s], sizeof(double) * n_of[s], cudaMemcpyDeviceToDevice,
+                                 stream));
+    } else {
+      return fail(PGX_ERROR_MEMORY_LOCATION, "unknown location %d", location);
+    }
+    PGX_TRY(ensure_work(kdim));
+    std::vector<double*> xs(count);
+    std::vector<const double*> bs(count);
+    PGX_TRY(set_pointers(xs.data(), bs.data(), PGX_LOCATION_HOST));
+    std::vector<int> sample;
+    for (int w = 0; w < count; w += stride) sample.push_back(order[w]);
+    Arena tmp;
+    int* d_sample = nullptr;
+    PGX_TRY(tmp.upload(&d_sample, sample.data(), sample.size(), stream));
+    static const int cand[][2] = {{256, 2}, {512, 1}, {512, 2}, {1024, 1}};
+    static const int lane_c[] = {2, 4, 8};
+    tune_table.clear();
+    double best = 1e300;
+    int bt = threads, bc = ctas_per_sm, bl = lanes;
+    for (const auto& c : cand) {
+      for (int ln : lane_c) {
+        PGX_CUDA(cudaMemsetAsync(d_xpack, 0, sizeof(double) * ntot, stream));
+        PGX_TRY(launch(kdim, maxits, tol, atol, c[0], c[1], ln, d_sample, (int)sample.size()));
+        PGX_CUDA(cudaStreamSynchronize(stream));
+        float ms = 0.f;
+        PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        tune_table.push_back({(double)c[0], (double)c[1], (double)ln, (double)ms});
+        if (ms < best) {
+          best = ms;
+          bt = c[0], bc = c[1], bl = ln;
+        }
+      }
+    }
+    threads = bt, ctas_per_sm = bc, lanes = bl;
+    if (best_ms) *best_ms = best;
+    return PGX_SUCCESS;
+  }
+};
+
 extern "C" {
 
 int pgx_init(int device) {
@@ -4211,6 +4714,132 @@ int pgx_lowrank_block_apply_c64(int32_t m, int32_t r, int32_t nrhs, const void* 
 
 int pgx_csr_spmv_device(const pgx_csr* Ad, double alpha, const double* x, double beta, double* y) {
   return pgx_csr_spmv_device_variant(Ad, 0, alpha, x, beta, y);
+}
+
+// ------------------------------------------------- many systems, one launch
+struct pgx_systems_s {
+  std::unique_ptr<SystemsBase> impl;
+  int device = 0;
+  int count = 0;
+};
+
+int pgx_systems_create(pgx_systems* out, const pgx_handle* handles, int32_t count) {
+  return guarded("pgx_systems_create", [&]() -> int {
+    if (!out || !handles || count < 1) return fail(PGX_ERROR_INVALID_PARAM, "null argument or count %d", count);
+    *out = nullptr;
+    std::vector<const Import*> ims(count);
+    int precision = -1, device = -1;
+    for (int s = 0; s < count; s++) {
+      pgx_handle h = handles[s];
+      if (!h || !h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "system %d: handle not committed", s);
+      if (s == 0) {
+        precision = h->im.precision;
+        device = h->device;
+      }
+      if (h->im.precision != precision) return fail(PGX_ERROR_INVALID_PARAM, "system %d: precisions differ", s);
+      if (h->device != device) return fail(PGX_ERROR_INVALID_PARAM, "system %d: devices differ", s);
+      ims[s] = &h->im;
+    }
+    if (precision != PGX_PRECISION_MIXED && precision != PGX_PRECISION_FP64)
+      return fail(PGX_ERROR_INVALID_OPTION, "the systems solve is real only (precision %d)", precision);
+    std::unique_ptr<pgx_systems_s> o(new pgx_systems_s());
+    o->device = device;
+    o->count = count;
+    if (precision == PGX_PRECISION_MIXED) {
+      auto* sy = new Systems<float>();
+      o->impl.reset(sy);
+      PGX_TRY(sy->create(ims, device));
+    } else {
+      auto* sy = new Systems<double>();
+      o->impl.reset(sy);
+      PGX_TRY(sy->create(ims, device));
+    }
+    *out = o.release();
+    return PGX_SUCCESS;
+  });
+}
+
+int pgx_systems_solve(pgx_systems s, double* const* x, const double* const* b, int32_t location,
+                      const double* params, pgx_result* results) {
+  return guarded("pgx_systems_solve", [&]() -> int {
+    if (!s || !x || !b) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    int kdim, maxits, atol;
+    double tol;
+    read_solver_params(params, kdim, maxits, tol, atol);
+    return s->impl->solve(x, b, location, kdim, maxits, tol, atol, results);
+  });
+}
+
+int pgx_systems_tune(pgx_systems s, const double* const* b, int32_t location, const double* params, int32_t stride,
+                     double* best_ms) {
+  return guarded("pgx_systems_tune", [&]() -> int {
+    if (!s || !b) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+    int kdim, maxits, atol;
+    double tol;
+    read_solver_params(params, kdim, maxits, tol, atol);
+    return s->impl->tune(b, location, kdim, maxits, tol, atol, stride, best_ms);
+  });
+}
+
+int pgx_systems_tune_table(pgx_systems s, int32_t capacity, double* table, int32_t* rows) {
+  if (!s) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  const auto& t = s->impl->tune_table;
+  if (rows) *rows = (int32_t)t.size();
+  if (table)
+    for (int i = 0; i < (int)t.size() && i < capacity; i++)
+      for (int k = 0; k < 4; k++) table[4 * i + k] = t[i][k];
+  return PGX_SUCCESS;
+}
+
+int pgx_systems_set_schedule(pgx_systems s, int32_t threads, int32_t ctas_per_sm, int32_t lanes) {
+  if (!s) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (threads < 64 || threads > kSysMaxThreads || threads % 32)
+    return fail(PGX_ERROR_INVALID_PARAM, "threads %d: a multiple of 32 in [64, %d]", threads, kSysMaxThreads);
+  if (ctas_per_sm < 1 || ctas_per_sm > 32) return fail(PGX_ERROR_INVALID_PARAM, "ctas_per_sm %d", ctas_per_sm);
+  if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: a power of two up to 32", lanes);
+  s->impl->threads = threads;
+  s->impl->ctas_per_sm = ctas_per_sm;
+  s->impl->lanes = lanes;
+  return PGX_SUCCESS;
+}
+
+int pgx_systems_get_schedule(pgx_systems s, int32_t* threads, int32_t* ctas_per_sm, int32_t* lanes) {
+  if (!s) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  if (threads) *threads = s->impl->threads;
+  if (ctas_per_sm) *ctas_per_sm = s->impl->ctas_per_sm;
+  if (lanes) *lanes = s->impl->lanes;
+  return PGX_SUCCESS;
+}
+
+int pgx_systems_timing(pgx_systems s, int32_t capacity, double* start_ms, double* end_ms, double* tri_ms) {
+  if (!s) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  const int k = std::min<int>(capacity, (int)s->impl->t_start.size());
+  for (int i = 0; i < k; i++) {
+    if (start_ms) start_ms[i] = s->impl->t_start[i];
+    if (end_ms) end_ms[i] = s->impl->t_end[i];
+    if (tri_ms) tri_ms[i] = s->impl->t_tri[i];
+  }
+  return PGX_SUCCESS;
+}
+
+int pgx_systems_last_ms(pgx_systems s, double* ms) {
+  if (!s || !ms) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  *ms = s->impl->last_ms;
+  return PGX_SUCCESS;
+}
+
+int pgx_systems_device_bytes(pgx_systems s, int64_t* bytes) {
+  if (!s || !bytes) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
+  *bytes = s->impl->device_bytes();
+  return PGX_SUCCESS;
+}
+
+int pgx_systems_destroy(pgx_systems s) {
+  if (!s) return PGX_SUCCESS;
+  cudaSetDevice(s->device);
+  delete s;
+  return PGX_SUCCESS;
 }
 
 }  // extern "C"

@@ -1,0 +1,608 @@
+// Many independent systems of uneven sizes solved by ONE persistent kernel
+// launch: every CTA takes the next system of a packed work list (largest
+// first) and runs its whole GeMSLR-preconditioned flexible GMRES on its own,
+// restart cycles, level recursion and the level-0 inner Schur FGMRES
+// included, then takes the next system.  The only synchronisation is
+// __syncthreads inside a CTA, so no CTA ever waits on another.
+//
+// The arithmetic follows the per-system engine (and through it the
+// reference):
+//   FlexGmresClass::Solve, ParGeMSLR SRC/solvers/fgmres.hpp:263-558
+//     (restarted right-preconditioned FGMRES, Givens rotations, the restart
+//     residual b - A x and the Givens estimate carried into the next cycle);
+//   GemslrClass::Solve / SolveLevel, gemslr.cpp:3431-3630 (gather by pperm,
+//     block LU per level, scatter by qperm);
+//   GemslrClass::SolveB, gemslr.cpp:3632-3678 with IluClass::SolveHost,
+//     ilu.cpp:3677-3790 (unit lower L, strict upper U, inverse diagonal);
+//   SolveApplyLowRankLevel, gemslr.cpp:3681-3722 (x += WH (W^T x));
+//   the level-0 inner FlexGmres over GemslrSchurMatrixClass,
+//     gemslr.cpp:294-330 and 1660-1674, with SchurMatVec, gemslr.cpp:3799-3960;
+//   CGS2 orthogonalisation (PargemslrCgs2, matrixops.cpp:10588-10708).
+// Krylov vectors, Givens rotations and the true residual are FP64; the
+// preconditioner (factors, coupling blocks, low-rank bases and its vectors)
+// is stored and accumulated in P (float for the mixed precision, double for
+// FP64), with the low-rank and Gram-Schmidt coefficients reduced in FP64.
+#pragma once
+
+#include "pgx_device.cuh"
+
+namespace pgx {
+
+constexpr int kSysMaxThreads = 1024;
+constexpr int kSysMaxLevels = 8;
+constexpr int kSysDotCols = 8;   // dot products one pass over the rows accumulates
+
+template <typename T>
+struct SysCsr {
+  int rows, cols;
+  const int* rp;
+  const int* cj;
+  const T* va;
+};
+
+// A triangular factor with its rows stored level by level (IluClass level
+// sets, ilu.cpp:832-1062): packed row k is row `row[k]`; levels are the
+// ranges lvp[t]..lvp[t+1] of packed rows.  Upper factors carry the inverse
+// diagonal per packed row.
+template <typename P>
+struct SysTri {
+  int n, nlev;
+  const int* lvp;
+  const int* row;
+  const int* rp;
+  const int* cj;
+  const P* va;
+  const P* dinv;
+};
+
+template <typename P>
+struct SysLevel {
+  int nl, m, rank;  // rows of B_l, rows below it, low-rank columns
+  SysTri<P> L, U;
+  SysCsr<P> E, F;   // E: m x nl, F: nl x m
+  const P* W;       // m x rank, column-major
+  const P* WH;
+  P* z;             // nl + m: (zu | zl)
+};
+
+template <typename P>
+struct SysDesc {
+  int n, nlev;
+  SysCsr<double> A;
+  const int* pperm;
+  const int* qperm;  // null: scatter by pperm
+  SysLevel<P> lev[kSysMaxLevels];
+  SysCsr<P> C0;      // level-0 C block (inner Schur FGMRES)
+  int inner, inner_maxits;
+  double inner_tol;
+  // work space
+  double* V;   // n x (kdim + 1)
+  P* Z;        // n x kdim
+  P* rt;       // n: permuted right-hand side of the preconditioner
+  P* xt;       // n: permuted preconditioner output
+  P* Vin;      // m0 x (inner_maxits + 1)
+  P* Zin;      // m0 x inner_maxits
+  P* xlr;      // m0
+  P* s_zu;     // nl0
+  P* s_wu;     // nl0
+};
+
+struct SysResult {
+  int iters, converged, breakdown, pad;
+  double normb, normr, true_r2;
+  unsigned long long t0, t1;  // %globaltimer at the start and end of the system's solve (ns)
+  unsigned long long tri_ns;  // of which in the triangular (B-block) solves
+  int cta, pad2;
+};
+
+template <typename P>
+struct SysArgs {
+  const SysDesc<P>* sys;
+  const int* order;  // work list
+  int count;
+  const double* const* b;
+  double* const* x;
+  int kdim, maxits, atol;
+  double tol;
+  int lanes;          // SpMV lanes per row (1, 2, 4 or 8)
+  int scap;           // values of the dynamic shared-memory solve buffer
+  unsigned int* next;
+  FgmresDev* st;      // per CTA: outer solve
+  FgmresDev* st_in;   // per CTA: inner solve
+  SysResult* res;
+};
+
+// shared memory of one CTA: reduction partials, coefficient vectors and the
+// products an update applies
+struct SysShared {
+  double red[kSysDotCols * 32];
+  void* sbuf;  // the CTA's triangular-solve buffer (dynamic shared memory)
+  int scap;    // its capacity in values
+  unsigned long long tri_ns;  // time in the B-block solves of the current system (thread 0)
+  double coef[KMAX + kSysDotCols];
+  double coef2[KMAX + kSysDotCols];
+  double prod[KMAX + kSysDotCols];
+  double tmp[kSysDotCols];
+  int sys;
+};
+
+__device__ __forceinline__ unsigned long long sys_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Block sums of NV per-thread values, combined in a fixed order (warp
+// shuffles, then the warps in index order) into out[0..NV).  All threads
+// call it; out is valid for all of them on return.
+template <int NV>
+__device__ __forceinline__ void sys_block_sum(double (&v)[NV], double* red, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int c = 0; c < NV; c++) {
+    double t = v[c];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    v[c] = t;
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int c = 0; c < NV; c++) red[c * 32 + warp] = v[c];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int w = 0; w < nw; w++) s += red[threadIdx.x * 32 + w];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// out[c] = vsc[c] * isc * sum_i V(i, c) in(i), c < ncols (FP64 sums)
+template <typename TV, typename TI>
+__device__ void sys_multidot(int n, int ncols, const TV* V, long long ld, const double* vsc, const TI* in,
+                             double isc, double* red, double* out) {
+  for (int c0 = 0; c0 < ncols; c0 += kSysDotCols) {
+    const int nc = min(kSysDotCols, ncols - c0);
+    double acc[kSysDotCols];
+#pragma unroll
+    for (int c = 0; c < kSysDotCols; c++) acc[c] = 0.0;
+    const TV* Vc = V + (long long)c0 * ld;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const double w = (double)in[i];
+#pragma unroll
+      for (int c = 0; c < kSysDotCols; c++)
+        if (c < nc) acc[c] += (double)Vc[(long long)c * ld + i] * w;
+    }
+    sys_block_sum<kSysDotCols>(acc, red, out + c0);
+    if (threadIdx.x < nc) out[c0 + threadIdx.x] *= (vsc ? vsc[c0 + threadIdx.x] : 1.0) * isc;
+    __syncthreads();
+  }
+}
+
+// out(i) = in(i) * isc + sign * sum_c M(i, c) msc[c] coef[c]  (in may be null:
+// zero); returns the block sum of out(i)^2 when NORM.  coef may live in
+// global or shared memory; the products sign * msc[c] * coef[c] are formed
+// once in shared memory.
+template <bool NORM, typename TM, typename TI, typename TO>
+__device__ double sys_update(int n, int ncols, const TM* M, long long ld, const double* msc, const double* coef,
+                             double sign, const TI* in, double isc, TO* out, SysShared& sh) {
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) sh.prod[c] = sign * (msc ? msc[c] : 1.0) * coef[c];
+  __syncthreads();
+  double nrm[1] = {0.0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double u = in ? (double)in[i] * isc : 0.0;
+    for (int c = 0; c < ncols; c++) u += (double)M[(long long)c * ld + i] * sh.prod[c];
+    const TO o = (TO)u;
+    out[i] = o;
+    if (NORM) nrm[0] += (double)o * (double)o;
+  }
+  if (NORM) {
+    sys_block_sum<1>(nrm, sh.red, sh.tmp);
+    return sh.tmp[0];
+  }
+  __syncthreads();
+  return 0.0;
+}
+
+// y(i) = alpha * sum_k M(i, k) x(k) + beta * yin(i)  (yin may alias y or be
+// null), S lanes per row; every lane runs the same number of row rounds so
+// the shuffles of a group see all of its lanes
+template <typename TA, typename TM, typename TX, typename TY, typename TYI>
+__device__ void sys_spmv(const SysCsr<TM>& M, const TX* x, TA alpha, const TYI* yin, TA beta, TY* y, int S) {
+  const int g = threadIdx.x / S, l = threadIdx.x % S, ng = blockDim.x / S;
+  for (int i0 = 0; i0 < M.rows; i0 += ng) {
+    const int i = i0 + g;
+    TA acc = TA(0);
+    if (i < M.rows) {
+      const int e1 = M.rp[i + 1];
+      for (int e = M.rp[i] + l; e < e1; e += S) acc += (TA)M.va[e] * (TA)x[M.cj[e]];
+    }
+    for (int o = S >> 1; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (l == 0 && i < M.rows) y[i] = (TY)(alpha * acc + (yin ? beta * (TA)yin[i] : TA(0)));
+  }
+  __syncthreads();
+}
+
+// Level-scheduled triangular solve in place (IluClass::SolveHost,
+// ilu.cpp:3677-3790): v holds the right-hand side on entry and the solution
+// on return; lower, unit diagonal: v_r -= L(r,:) v;  upper: v_r = dinv_r
+// (v_r - U(r,:) v).  Rows of one level depend only on rows of earlier
+// levels, so a row reads solved entries and its own right-hand side.  A
+// thread takes kSysRows rows of a level at a time (a block-stride apart) and
+// interleaves their loads, so a wide level costs a few load round trips, not
+// a few per row.  The row data of the thread's first rows of the next level
+// (row index and extent) is fetched before the barrier.  v is in shared
+// memory when the block fits there.
+constexpr int kSysRows = 4;
+template <bool UPPER, typename P>
+__device__ void sys_trsv(const SysTri<P>& T, P* v) {
+  int r[kSysRows], e0[kSysRows], e1[kSysRows];
+  int kbeg = 0, kend = 0;
+  auto fetch = [&](int t) {
+#pragma unroll
+    for (int q = 0; q < kSysRows; q++) r[q] = -1;
+    if (t >= T.nlev) return;
+    kbeg = T.lvp[t];
+    kend = T.lvp[t + 1];
+#pragma unroll
+    for (int q = 0; q < kSysRows; q++) {
+      const int k = kbeg + threadIdx.x + q * blockDim.x;
+      if (k < kend) {
+        r[q] = T.row[k];
+        e0[q] = T.rp[k];
+        e1[q] = T.rp[k + 1];
+      }
+    }
+  };
+  fetch(0);
+  for (int t = 0; t < T.nlev; t++) {
+    for (int kb = kbeg + threadIdx.x;; kb += kSysRows * blockDim.x) {
+      if (kb != kbeg + (int)threadIdx.x) {  // later batches of a wide level
+#pragma unroll
+        for (int q = 0; q < kSysRows; q++) {
+          const int k = kb + q * blockDim.x;
+          r[q] = -1;
+          if (k < kend) {
+            r[q] = T.row[k];
+            e0[q] = T.rp[k];
+            e1[q] = T.rp[k + 1];
+          }
+        }
+      }
+      if (r[0] < 0) break;
+      P s[kSysRows];
+      int len = 0;
+#pragma unroll
+      for (int q = 0; q < kSysRows; q++) {
+        s[q] = r[q] >= 0 ? v[r[q]] : P(0);
+        if (r[q] >= 0) len = max(len, e1[q] - e0[q]);
+      }
+      for (int u = 0; u < len; u++) {
+#pragma unroll
+        for (int q = 0; q < kSysRows; q++) {
+          const int e = e0[q] + u;
+          if (r[q] >= 0 && e < e1[q]) s[q] -= T.va[e] * v[T.cj[e]];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kSysRows; q++)
+        if (r[q] >= 0) v[r[q]] = UPPER ? T.dinv[kb + q * blockDim.x] * s[q] : s[q];
+      if (r[kSysRows - 1] < 0) break;
+    }
+    fetch(t + 1);
+    __syncthreads();
+  }
+}
+
+// x = U^-1 L^-1 rhs of level l (GemslrClass::SolveB): in shared memory when
+// the block's rows fit the CTA's buffer, else in place in x
+template <typename P>
+__device__ void sys_solve_b(const SysDesc<P>& d, int l, const P* rhs, P* x, P* sbuf, int scap,
+                            unsigned long long* tri_ns) {
+  const unsigned long long t0 = threadIdx.x == 0 ? sys_clock() : 0ull;
+  const SysLevel<P>& v = d.lev[l];
+  const int nl = v.nl;
+  P* w = nl <= scap ? sbuf : x;
+  for (int i = threadIdx.x; i < nl; i += blockDim.x) w[i] = rhs[i];
+  __syncthreads();
+  sys_trsv<false>(v.L, w);
+  sys_trsv<true>(v.U, w);
+  if (w != x) {
+    for (int i = threadIdx.x; i < nl; i += blockDim.x) x[i] = w[i];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *tri_ns += sys_clock() - t0;
+}
+
+// x += WH (W^T x) in place (SolveApplyLowRankLevel, gemslr.cpp:3585-3590)
+template <typename P>
+__device__ void sys_lowrank(const SysLevel<P>& v, P* x, SysShared& sh) {
+  sys_multidot(v.m, v.rank, v.W, v.m, (const double*)nullptr, x, 1.0, sh.red, sh.coef);
+  sys_update<false>(v.m, v.rank, v.WH, v.m, (const double*)nullptr, sh.coef, 1.0, x, 1.0, x, sh);
+}
+
+// Orthogonalise column j+1 of the basis against columns 0..j by CGS2, then
+// finish the Hessenberg column with the Givens rotations (one thread).
+template <typename TV>
+__device__ void sys_arnoldi(TV* Vb, long long ld, int j, FgmresDev* st, int nrows, SysShared& sh) {
+  TV* w = Vb + (long long)(j + 1) * ld;
+  sys_multidot(nrows, j + 1, Vb, ld, st->sc, w, 1.0, sh.red, sh.coef);
+  for (int c = threadIdx.x; c <= j; c += blockDim.x) {
+    st->hcol[c] = sh.coef[c];
+    st->coefA[c] = sh.coef[c];
+  }
+  sys_update<false>(nrows, j + 1, Vb, ld, st->sc, sh.coef, -1.0, w, 1.0, w, sh);
+  sys_multidot(nrows, j + 1, Vb, ld, st->sc, w, 1.0, sh.red, sh.coef2);
+  for (int c = threadIdx.x; c <= j; c += blockDim.x) {
+    st->hcol[c] += sh.coef2[c];
+    st->coefB[c] = sh.coef2[c];
+  }
+  const double t2 = sys_update<true>(nrows, j + 1, Vb, ld, st->sc, sh.coef2, -1.0, w, 1.0, w, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) fgmres_givens(st, j, sqrt(t2));
+  __syncthreads();
+}
+
+template <typename P>
+__device__ void sys_inner_solve(const SysDesc<P>& d, P* xl, const P* zl, FgmresDev* st, int S, SysShared& sh);
+
+// GemslrClass::SolveLevel from level l0 down (gemslr.cpp:3474-3630) with the
+// recursion unrolled: the descent keeps each level's right-hand side, the
+// ascent finishes the levels bottom up.  x and rhs hold the trailing
+// n - lev_ptr[l0] unknowns.  With INNER, level 0 runs the inner Schur FGMRES
+// in place of the low-rank correction and the lower levels.
+template <bool INNER, typename P>
+__device__ void sys_solve_from(const SysDesc<P>& d, int l0, P* x, const P* rhs, FgmresDev* st_in, int S,
+                               SysShared& sh) {
+  const P* rh[kSysMaxLevels];
+  P* xs[kSysMaxLevels];
+  int l = l0;
+  const P* r = rhs;
+  P* xv = x;
+  bool stop_inner = false;
+  for (; l < d.nlev - 1; l++) {
+    const SysLevel<P>& v = d.lev[l];
+    rh[l] = r;
+    xs[l] = xv;
+    P* zu = v.z;
+    P* zl = v.z + v.nl;
+    sys_solve_b(d, l, r, zu, (P*)sh.sbuf, sh.scap, &sh.tri_ns);                                         // 1. zu = B^-1 rhs_u
+    sys_spmv<P>(v.E, (const P*)zu, P(-1), r + v.nl, P(1), zl, S);     // 2-3. zl = rhs_l - E zu
+    if (INNER && l == 0 && d.inner) {
+      sys_inner_solve(d, xv + v.nl, zl, st_in, S, sh);                // 4. inner FGMRES
+      stop_inner = true;
+      break;
+    }
+    if (v.rank > 0) sys_lowrank(v, zl, sh);                           // 4. low rank
+    r = zl;
+    xv = xv + v.nl;
+  }
+  int top;
+  if (stop_inner) {
+    top = l;
+  } else {
+    sys_solve_b(d, d.nlev - 1, r, xv, (P*)sh.sbuf, sh.scap, &sh.tri_ns);                                // last level: B^-1 rhs
+    top = d.nlev - 2;
+  }
+  for (int t = top; t >= l0; t--) {
+    const SysLevel<P>& v = d.lev[t];
+    P* zu = v.z;
+    sys_spmv<P>(v.F, (const P*)(xs[t] + v.nl), P(-1), rh[t], P(1), zu, S);  // 5-6. zu = rhs_u - F xl
+    sys_solve_b(d, t, zu, xs[t], (P*)sh.sbuf, sh.scap, &sh.tri_ns);                                           // 7. xu = B^-1 zu
+  }
+}
+
+// Level-0 inner flexible GMRES on S0 = C0 - E0 B0^-1 F0 from x0 = 0, one cycle
+// of inner_maxits steps (gemslr.cpp:1660-1674, 3566-3572); its preconditioner
+// is the low-rank correction followed by the level-1 recursion
+// (GemslrSchurMatrixClass::Solve, gemslr.cpp:294-330).
+template <typename P>
+__device__ void sys_inner_solve(const SysDesc<P>& d, P* xl, const P* zl, FgmresDev* st, int S, SysShared& sh) {
+  const SysLevel<P>& v0 = d.lev[0];
+  const int m0 = v0.m;
+  const long long ld = m0;
+  {
+    double nrm[1] = {0.0};
+    for (int i = threadIdx.x; i < m0; i += blockDim.x) {
+      const P z = zl[i];
+      d.Vin[i] = z;
+      nrm[0] += (double)z * (double)z;
+    }
+    sys_block_sum<1>(nrm, sh.red, sh.tmp);
+    if (threadIdx.x == 0) {
+      const double normb = sqrt(sh.tmp[0]);
+      st->normb = normb;
+      st->normr = normb;
+      st->i = 0;
+      st->iter = 0;
+      st->converged = 0;
+      st->breakdown = 0;
+      st->done = 0;
+      st->cycle_done = 0;
+      if (normb < st->eps) {
+        st->done = 1;
+        st->cycle_done = 1;
+      } else {
+        st->tolr = st->absolute ? st->tol : st->tol * normb;
+        st->rs[0] = normb;
+        st->sc[0] = 1.0 / normb;
+      }
+    }
+    __syncthreads();
+  }
+  for (int j = 0; j < d.inner_maxits; j++) {
+    if (*(volatile int*)&st->cycle_done) break;
+    P* vj = d.Vin + (long long)j * ld;
+    P* zj = d.Zin + (long long)j * ld;
+    P* wj = d.Vin + (long long)(j + 1) * ld;
+    const double scj = st->sc[j];
+    if (v0.rank > 0) sys_multidot(m0, v0.rank, v0.W, ld, (const double*)nullptr, vj, scj, sh.red, sh.coef);
+    sys_update<false>(m0, v0.rank, v0.WH, ld, (const double*)nullptr, sh.coef, 1.0, vj, scj, d.xlr, sh);
+    sys_solve_from<false>(d, 1, zj, (const P*)d.xlr, st, S, sh);
+    // w = S0 z (GemslrClass::SchurMatVec, gemslr.cpp:3799-3960)
+    sys_spmv<P>(v0.F, (const P*)zj, P(1), (const P*)nullptr, P(0), d.s_zu, S);
+    sys_solve_b(d, 0, d.s_zu, d.s_wu, (P*)sh.sbuf, sh.scap, &sh.tri_ns);
+    sys_spmv<P>(d.C0, (const P*)zj, P(1), (const P*)nullptr, P(0), wj, S);
+    sys_spmv<P>(v0.E, (const P*)d.s_wu, P(-1), (const P*)wj, P(1), wj, S);
+    sys_arnoldi(d.Vin, ld, j, st, m0, sh);
+  }
+  const int ni = *(volatile int*)&st->i;
+  sys_update<false>(m0, ni, d.Zin, ld, (const double*)nullptr, st->rs, 1.0, (const P*)nullptr, 1.0, xl, sh);
+}
+
+// GemslrClass::Solve (gemslr.cpp:3431-3472): z = Q^T M^-1 P v with v scaled
+template <typename P>
+__device__ void sys_precond(const SysDesc<P>& d, const double* v, double vsc, P* z, FgmresDev* st_in, int S,
+                            SysShared& sh) {
+  for (int i = threadIdx.x; i < d.n; i += blockDim.x) d.rt[i] = (P)(v[d.pperm[i]] * vsc);
+  __syncthreads();
+  sys_solve_from<true>(d, 0, d.xt, (const P*)d.rt, st_in, S, sh);
+  const int* q = d.qperm ? d.qperm : d.pperm;
+  for (int i = threadIdx.x; i < d.n; i += blockDim.x) z[q[i]] = d.xt[i];
+  __syncthreads();
+}
+
+// MAXT bounds the CTA size the kernel is compiled for: 1024 leaves 64
+// registers per thread; 256, with two CTAs per SM, leaves 128 (the
+// autotuner tries both).
+template <typename P, int MAXT>
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) systems_fgmres_kernel(SysArgs<P> a) {
+  __shared__ SysShared sh;
+  extern __shared__ __align__(16) unsigned char sys_dyn[];
+  if (threadIdx.x == 0) {
+    sh.sbuf = sys_dyn;
+    sh.scap = a.scap;
+  }
+  __syncthreads();
+  FgmresDev* st = a.st + blockIdx.x;
+  FgmresDev* st_in = a.st_in + blockIdx.x;
+  const int S = a.lanes;
+  for (;;) {
+    if (threadIdx.x == 0) sh.sys = (int)atomicAdd(a.next, 1u);
+    __syncthreads();
+    const int w = sh.sys;
+    __syncthreads();
+    if (w >= a.count) return;
+    const int s = a.order[w];
+    const SysDesc<P>& d = a.sys[s];
+    const double* b = a.b[s];
+    double* x = a.x[s];
+    const int n = d.n;
+    const long long ld = n;
+    const unsigned long long t0 = sys_clock();
+    if (threadIdx.x == 0) {
+      sh.tri_ns = 0ull;
+      st->kdim = a.kdim;
+      st->maxits = a.maxits;
+      st->tol = a.tol;
+      st->absolute = a.atol;
+      st->eps = DBL_EPSILON;
+      st->done = 0;
+      st->cycle_done = 1;
+      st->i = 0;
+      st->iter = 0;
+      st->converged = 0;
+      st->breakdown = 0;
+      st->normr = 0.0;
+      st_in->kdim = d.inner_maxits;
+      st_in->maxits = d.inner_maxits;
+      st_in->tol = d.inner_tol;
+      st_in->absolute = 0;
+      st_in->eps = DBL_EPSILON;
+    }
+    // ||b||  (fgmres.hpp:319-329)
+    {
+      double nrm[1] = {0.0};
+      for (int i = threadIdx.x; i < n; i += blockDim.x) nrm[0] += b[i] * b[i];
+      sys_block_sum<1>(nrm, sh.red, sh.tmp);
+      if (threadIdx.x == 0) {
+        st->normb = sqrt(sh.tmp[0]);
+        if (st->normb < st->eps) {
+          st->done = 1;
+          st->cycle_done = 1;
+        }
+      }
+      __syncthreads();
+    }
+    const bool zero_b = *(volatile int*)&st->done;
+    if (!zero_b) {
+      // v = b - A x, ||v|| (fgmres.hpp:331-360)
+      sys_spmv<double>(d.A, (const double*)x, -1.0, b, 1.0, d.V, S);
+      double nrm[1] = {0.0};
+      for (int i = threadIdx.x; i < n; i += blockDim.x) nrm[0] += d.V[i] * d.V[i];
+      sys_block_sum<1>(nrm, sh.red, sh.tmp);
+      if (threadIdx.x == 0) {
+        const double normr = sqrt(sh.tmp[0]);
+        st->normr = normr;
+        st->normr0 = normr;
+        if (normr < st->eps) {
+          st->done = 1;
+          st->cycle_done = 1;
+          st->converged = 1;
+        } else {
+          st->tolr = st->absolute ? st->tol : st->tol * st->normb;
+          st->rs[0] = normr;
+          st->sc[0] = 1.0 / normr;
+          st->cycle_done = 0;
+        }
+      }
+      __syncthreads();
+    }
+    const int max_cycles = a.maxits > 0 ? a.maxits / a.kdim + 2 : 0;
+    for (int cyc = 0; cyc < max_cycles; cyc++) {
+      if (*(volatile int*)&st->done || *(volatile int*)&st->iter >= a.maxits) break;
+      for (int j = 0; j < a.kdim; j++) {
+        if (*(volatile int*)&st->cycle_done) break;
+        P* zj = d.Z + (long long)j * ld;
+        sys_precond(d, d.V + (long long)j * ld, st->sc[j], zj, st_in, S, sh);           // z = M^-1 v
+        sys_spmv<double>(d.A, (const P*)zj, 1.0, (const double*)nullptr, 0.0, d.V + (long long)(j + 1) * ld, S);
+        sys_arnoldi(d.V, ld, j, st, n, sh);
+      }
+      // x += Z y  (fgmres.hpp:471-490)
+      const int ni = *(volatile int*)&st->i;
+      sys_update<false>(n, ni, d.Z, ld, (const double*)nullptr, st->rs, 1.0, (const double*)x, 1.0, x, sh);
+      if (!*(volatile int*)&st->done)
+        sys_spmv<double>(d.A, (const double*)x, -1.0, b, 1.0, d.V, S);                 // restart residual
+      if (threadIdx.x == 0) {
+        st->i = 0;
+        if (!st->done) {
+          st->cycle_done = 0;
+          st->rs[0] = st->normr;
+          st->sc[0] = 1.0 / st->normr;
+        }
+      }
+      __syncthreads();
+    }
+    if (zero_b) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = 0.0;
+      __syncthreads();
+    }
+    // FP64 true residual ||b - A x||
+    sys_spmv<double>(d.A, (const double*)x, -1.0, b, 1.0, d.V, S);
+    {
+      double nrm[1] = {0.0};
+      for (int i = threadIdx.x; i < n; i += blockDim.x) nrm[0] += d.V[i] * d.V[i];
+      sys_block_sum<1>(nrm, sh.red, sh.tmp);
+    }
+    if (threadIdx.x == 0) {
+      SysResult r;
+      r.iters = st->iter;
+      r.converged = st->converged;
+      r.breakdown = st->breakdown;
+      r.pad = 0;
+      r.normb = st->normb;
+      r.normr = st->normr;
+      r.true_r2 = sh.tmp[0];
+      r.t0 = t0;
+      r.t1 = sys_clock();
+      r.tri_ns = sh.tri_ns;
+      r.cta = blockIdx.x;
+      r.pad2 = 0;
+      a.res[s] = r;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace pgx

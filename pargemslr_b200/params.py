@@ -277,6 +277,16 @@ def workload_params(name: str) -> np.ndarray:
         p[LR_RANK1_GLOBAL] = p[LR_RANK1_LOCAL] = 8
         p[LR_RANK2_GLOBAL] = p[LR_RANK2_LOCAL] = 8
         p[SCHUR_ENABLE] = 0
+    elif name == "convdiff":
+        # batched uneven upwind convection-diffusion systems: 2 levels, ILUT
+        # 1e-2 / 20 per row, rank 8, inner Schur FGMRES on, FGMRES(30)
+        p[PREPOSS_NLEV_GLOBAL] = 2
+        p[ILU_DROPTOL_B_GLOBAL] = p[ILU_DROPTOL_B_LOCAL] = 1e-2
+        p[ILU_DROPTOL_C_GLOBAL] = p[ILU_DROPTOL_C_LOCAL] = 1e-2
+        p[ILU_ROWNNZ_B_GLOBAL] = p[ILU_ROWNNZ_B_LOCAL] = 20
+        p[ILU_ROWNNZ_C_GLOBAL] = p[ILU_ROWNNZ_C_LOCAL] = 20
+        p[LR_RANK1_GLOBAL] = p[LR_RANK1_LOCAL] = 8
+        p[LR_RANK2_GLOBAL] = p[LR_RANK2_LOCAL] = 8
     elif name == "zlap3d_96":
         # complex shifted 3D Laplacian 96^3 (shift 0.05 + 0.01i): 5 levels,
         # ILUT 1e-3, rank 32, FGMRES(100)
@@ -303,6 +313,6 @@ def workload_params(name: str) -> np.ndarray:
         p[LR_RANK2_GLOBAL] = p[LR_RANK2_LOCAL] = 4
     else:
         raise ValueError(f"unknown workload {name!r}")
-    p[SOLVER_KDIM] = {"serve": 40, "zlap3d_96": 100, "zsmall": 100}.get(name, 50)
+    p[SOLVER_KDIM] = {"serve": 40, "convdiff": 30, "zlap3d_96": 100, "zsmall": 100}.get(name, 50)
     p[SOLVER_TOL] = 1e-8
     return p

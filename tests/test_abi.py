@@ -36,6 +36,13 @@ def test_calls_without_device_fail_cleanly():
     st = C.c_int32(0)
     assert L.pgx_wait_selfcheck(0, C.byref(st), None) == _abi.ERROR_INVALID_PARAM
     assert L.pgx_wait_selfcheck(5, None, None) == _abi.ERROR_INVALID_PARAM
+    sy = C.c_void_p()
+    assert L.pgx_systems_create(C.byref(sy), None, 0) == _abi.ERROR_INVALID_PARAM
+    hs = (C.c_void_p * 2)(None, None)
+    assert L.pgx_systems_create(C.byref(sy), C.cast(hs, C.c_void_p), 2) == _abi.ERROR_FUNCTION_CALL
+    assert L.pgx_systems_solve(None, None, None, 0, None, None) == _abi.ERROR_INVALID_PARAM
+    assert L.pgx_systems_set_schedule(None, 512, 2, 4) == _abi.ERROR_INVALID_PARAM
+    assert L.pgx_systems_destroy(None) == 0
 
 
 def test_level_schedule_rejects_non_triangular_factor():
