@@ -850,7 +850,8 @@ def run_uneven(args):
                                "log-uniform in [32, 512], beta ~ U[0,50]^2, b ~ U[-1,1], 2 levels, ILUT 1e-2/20, "
                                "rank 8, inner Schur FGMRES(5), FGMRES(30) to rel-res 1e-8 from x0 = 0" % count,
                    "unknowns": int(sizes.sum()), "setup": "this library's host setup per system, untimed",
-                   "schedule": {"threads": sb.schedule[0], "ctas_per_sm": sb.schedule[1], "spmv_lanes": sb.schedule[2]},
+                   "schedule": {"threads": sb.schedule[0], "ctas_per_sm": sb.schedule[1], "spmv_lanes": sb.schedule[2],
+                                "prefetch_levels": sb.schedule[3]},
                    "l2": "inputs larger than L2 (%.1f GB of packed structures and Krylov bases)"
                          % (sb.device_bytes() / 1e9)},
         "e2e": {"value": e2e, "unit": "systems/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

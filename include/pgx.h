@@ -365,14 +365,16 @@ int pgx_pool_destroy(pgx_pool pool);
  *     i's outcome, its solve_ms being the span of that system inside the
  *     launch and launches 1.
  *   pgx_systems_tune: the schedule autotuner.  It solves a sample of the
- *     batch (every stride-th system of the work list; stride 1 is the whole
- *     batch) once per candidate (threads per CTA 256/512/1024, CTAs per SM,
- *     SpMV lanes per row 2/4/8) from x0 = 0 into the object's own vectors,
- *     keeps the fastest and returns its device time; pgx_systems_tune_table
- *     returns the candidates tried, four doubles each (threads, CTAs per SM,
- *     lanes, ms).
- *   pgx_systems_set_schedule / get_schedule: the schedule in use (default 512
- *     threads, 2 CTAs per SM, 4 lanes).
+ *     batch (every stride-th system of the work list past its largest
+ *     sixteenth; stride 1 is the whole batch) from x0 = 0 into the object's
+ *     own vectors, by coordinate descent over the CTA shape (256 threads x 2
+ *     per SM, 512 x 1, 512 x 2, 1024 x 1), then the SpMV lanes per row (2, 4,
+ *     8), then the levels the triangular passes fetch ahead (2, 4); it keeps
+ *     the fastest and returns its device time.  pgx_systems_tune_table returns
+ *     the candidates tried, five doubles each (threads, CTAs per SM, lanes,
+ *     depth, ms).
+ *   pgx_systems_set_schedule / get_schedule: the schedule in use (default 256
+ *     threads, 2 CTAs per SM, 2 lanes, depth 2).
  *   pgx_systems_timing: per system, the start and end of its solve in the last
  *     launch, in ms from the first system's start, and the time it spent in
  *     its triangular (B-block) solves (device clock; any array may be NULL);
@@ -385,8 +387,10 @@ int pgx_systems_solve(pgx_systems systems, double *const *x, const double *const
 int pgx_systems_tune(pgx_systems systems, const double *const *b, int32_t location, const double *params,
                      int32_t stride, double *best_ms);
 int pgx_systems_tune_table(pgx_systems systems, int32_t capacity, double *table, int32_t *rows);
-int pgx_systems_set_schedule(pgx_systems systems, int32_t threads, int32_t ctas_per_sm, int32_t lanes);
-int pgx_systems_get_schedule(pgx_systems systems, int32_t *threads, int32_t *ctas_per_sm, int32_t *lanes);
+int pgx_systems_set_schedule(pgx_systems systems, int32_t threads, int32_t ctas_per_sm, int32_t lanes,
+                             int32_t depth);
+int pgx_systems_get_schedule(pgx_systems systems, int32_t *threads, int32_t *ctas_per_sm, int32_t *lanes,
+                             int32_t *depth);
 int pgx_systems_timing(pgx_systems systems, int32_t capacity, double *start_ms, double *end_ms, double *tri_ms);
 int pgx_systems_last_ms(pgx_systems systems, double *ms);
 int pgx_systems_device_bytes(pgx_systems systems, int64_t *bytes);

@@ -160,8 +160,8 @@ def lib() -> C.CDLL:
     L.pgx_systems_solve.argtypes = [vp, vp, vp, i32, vp, vp]
     L.pgx_systems_tune.argtypes = [vp, vp, i32, vp, i32, C.POINTER(dbl)]
     L.pgx_systems_tune_table.argtypes = [vp, i32, vp, C.POINTER(i32)]
-    L.pgx_systems_set_schedule.argtypes = [vp, i32, i32, i32]
-    L.pgx_systems_get_schedule.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    L.pgx_systems_set_schedule.argtypes = [vp, i32, i32, i32, i32]
+    L.pgx_systems_get_schedule.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
     L.pgx_systems_timing.argtypes = [vp, i32, vp, vp, vp]
     L.pgx_systems_device_bytes.argtypes = [vp, C.POINTER(i64)]
     L.pgx_systems_last_ms.argtypes = [vp, C.POINTER(dbl)]

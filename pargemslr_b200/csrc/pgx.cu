@@ -52,6 +52,21 @@ namespace pgx {
 static thread_local std::string g_last_error;
 static thread_local int g_device = 0;
 
+// streaming multiprocessors of the current device (queried once per device)
+static int num_sms() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 148;
+  if (dev < 64) {
+    const int c = cache[dev].load(std::memory_order_relaxed);
+    if (c > 0) return c;
+  }
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+  if (dev < 64) cache[dev].store(n, std::memory_order_relaxed);
+  return n;
+}
+
 static int fail(int code, const char* fmt, ...) {
   char buf[512];
   va_list ap;
@@ -362,7 +377,7 @@ static int tri_blocks(int ngroups, int nlevels) {
   double avg = nlevels > 0 ? (double)ngroups / nlevels : (double)ngroups;
   long long warps = (long long)std::ceil(8.0 * avg);
   warps = std::max<long long>(warps, 64);
-  warps = std::min<long long>(warps, 148LL * 32);
+  warps = std::min<long long>(warps, (long long)num_sms() * 32);
   warps = std::min<long long>(warps, ((long long)ngroups + wpb - 1) / wpb * wpb);
   return (int)std::max<long long>(1, (warps + wpb - 1) / wpb);
 }
@@ -522,7 +537,7 @@ static int upload_tri_seg(Arena& ar, const HostCsr& h, bool upper, const std::ve
     lv0.push_back((int)lvb.size());
   }
   d.ncomp = (int)cuts.size() - 1;
-  d.nblocks = std::max(1, std::min(d.nseg, 148));
+  d.nblocks = std::max(1, std::min(d.nseg, num_sms()));
   PGX_TRY(ar.upload(&d.ord, ord.data(), ord.size(), s));
   PGX_TRY(ar.upload(&d.rp, rp.data(), rp.size(), s));
   PGX_TRY(ar.upload(&d.cj, cj.data(), cj.size(), s));
@@ -1136,7 +1151,7 @@ struct Engine : EngineBase {
         if (d.U.ticket) PGX_TRY(wk.zeros(&d.U.ticket, 2, stream));
       }
       PGX_TRY(wk.alloc(&d.y, (size_t)d.nl));
-      sentinel_fill_kernel<P><<<grid_for(d.nl, 256, 148 * 8), 256, 0, stream>>>(d.nl, d.y);
+      sentinel_fill_kernel<P><<<grid_for(d.nl, 256, num_sms() * 8), 256, 0, stream>>>(d.nl, d.y);
       PGX_CUDA(cudaGetLastError());
       if (l < nlev - 1) {
         PGX_TRY(wk.zeros(&d.xlr, (size_t)d.m, stream));
@@ -1221,8 +1236,9 @@ struct Engine : EngineBase {
       if (!d.L.seg || !d.U.seg || d.nl < 32768) continue;  // one-CTA-per-subdomain kernels have no grid choice
       const int comps = std::max(d.L.ncomp, 1);
       std::vector<int> cand;
-      for (int f : {2, 4, 8, 16}) cand.push_back(std::min(148, comps * f));
-      cand.push_back(148);
+      const int sms = num_sms();
+      for (int f : {2, 4, 8, 16}) cand.push_back(std::min(sms, comps * f));
+      cand.push_back(sms);
       std::sort(cand.begin(), cand.end());
       cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
       int bestL = d.L.nblocks, bestU = d.U.nblocks;
@@ -1441,14 +1457,14 @@ struct Engine : EngineBase {
       const int nt = merge_threads(M.rows, M.nnz);
       merge_spmv_kernel<TA, TX, TY, TC><<<(nt + 255) / 256, 256, 0, stream>>>(
           M.rows, (int)M.nnz, M.rp, M.cj, M.va, x, alpha, b, beta, y, mcarry_row, (TC*)mcarry_val, sk);
-      merge_spmv_fixup_kernel<TY, TC><<<grid_for(nt, 256, 148 * 8), 256, 0, stream>>>(nt, mcarry_row,
+      merge_spmv_fixup_kernel<TY, TC><<<grid_for(nt, 256, num_sms() * 8), 256, 0, stream>>>(nt, mcarry_row,
                                                                                      (const TC*)mcarry_val, alpha,
                                                                                      y, sk);
       return;
     }
     const int S = M.S;
     const int gpb = 256 / S;
-    const int grid = grid_for(M.rows, gpb, 148 * 16);
+    const int grid = grid_for(M.rows, gpb, num_sms() * 16);
     const int *rp2 = M2 ? M2->rp : nullptr, *cj2 = M2 ? M2->cj : nullptr;
     const TA* va2 = M2 ? M2->va : nullptr;
     const int xcols2 = M2 ? M2->cols : 0;
@@ -1688,7 +1704,7 @@ struct Engine : EngineBase {
   // scatter by qperm (or pperm for symmetric reorderings).
   template <typename TO>
   void precond(const F* v, const double* v_scale, TO* z, Skip sk) {
-    const int grid = grid_for(n, 256 * kPermUnroll, 148 * 16);  // gather / scatter
+    const int grid = grid_for(n, 256 * kPermUnroll, num_sms() * 16);  // gather / scatter
     gather_kernel<F, P><<<grid, 256, 0, stream>>>(n, pperm, v, v_scale, rt, sk);
     solve_level(0, xt, rt, sk);
     scatter_kernel<P, TO><<<grid, 256, 0, stream>>>(n, qperm ? qperm : pperm, xt, z, sk);
@@ -2598,7 +2614,7 @@ struct BatchEngine : EngineBase {
     const long long ld = n;
     std::array<Skip, R> sk;
     for (int r = 0; r < R; r++) sk[r] = mk_skip(&lane[r]->st->done, &lane[r]->st->cycle_done);
-    const int grid = grid_for(n, 256 * kPermUnroll, 148 * 16);  // gather / scatter
+    const int grid = grid_for(n, 256 * kPermUnroll, num_sms() * 16);  // gather / scatter
     for (int j = 0; j < kdim; j++) {
       std::array<P*, R> xt;
       std::array<const P*, R> rt;
@@ -2972,11 +2988,11 @@ struct SystemsBase {
   virtual int tune(const double* const* b, int location, int kdim, int maxits, double tol, int atol, int stride,
                    double* best_ms) = 0;
   virtual int64_t device_bytes() const = 0;
-  int threads = 512, ctas_per_sm = 2, lanes = 4;
+  int threads = 256, ctas_per_sm = 2, lanes = 2, depth = 2;
   double last_ms = 0.0;  // device time of the last solve's launch (CUDA events)
   std::vector<double> t_start, t_end;  // per system, ms from the launch's first system start
   std::vector<double> t_tri;           // per system, ms in its triangular (B-block) solves
-  std::vector<std::array<double, 4>> tune_table;  // threads, ctas per SM, lanes, ms
+  std::vector<std::array<double, 5>> tune_table;  // threads, ctas per SM, lanes, depth, ms
 };
 
 template <typename P>
@@ -3077,23 +3093,33 @@ struct Systems : SystemsBase {
     PGX_TRY(build_levels(upper, nl, h.rp.data(), h.cj.data(), lvp, ord));
     t.nlev = (int)lvp.size() - 1;
     levels += t.nlev;
-    std::vector<int> rp(nl + 1, 0), cj;
+    std::vector<int> pos(nl);
+    for (int k = 0; k < nl; k++) pos[ord[k]] = k;
+    // columns as packed positions; the span is the farthest dependency plus
+    // the widest level
+    std::vector<int> rp(nl + 1, 0), pc;
     std::vector<double> va, di;
-    cj.reserve(h.cj.size());
+    pc.reserve(h.cj.size());
     va.reserve(h.cj.size());
+    int far = 0, wide = 0;
+    for (int lv = 0; lv < t.nlev; lv++) wide = std::max(wide, lvp[lv + 1] - lvp[lv]);
     for (int k = 0; k < nl; k++) {
       const int r = ord[k];
       for (int e = h.rp[r]; e < h.rp[r + 1]; e++) {
-        cj.push_back(h.cj[e]);
+        const int q = pos[h.cj[e]];
+        if (q >= k) return fail(PGX_ERROR_INVALID_PARAM, "triangular factor: row %d reads an unsolved entry", r);
+        far = std::max(far, k - q);
+        pc.push_back(q);
         va.push_back(h.va[e]);
       }
-      rp[k + 1] = (int)cj.size();
+      rp[k + 1] = (int)pc.size();
       if (upper) di.push_back((*dinv)[r]);
     }
+    t.span = far + wide;
     ints(&t.lvp, lvp.data(), lvp.size());
     ints(&t.row, ord.data(), ord.size());
     ints(&t.rp, rp.data(), rp.size());
-    ints(&t.cj, cj.data(), cj.size());
+    ints(&t.pc, pc.data(), pc.size());
     vals(&t.va, va.data(), va.size());
     if (upper) vals(&t.dinv, di.data(), di.size());
     return PGX_SUCCESS;
@@ -3213,7 +3239,7 @@ struct Systems : SystemsBase {
       const SysDesc<P>& d = desc[s];
       const size_t n = d.n, m0 = d.nlev > 1 ? d.lev[0].m : 0, nl0 = d.lev[0].nl;
       nd += padded(n * (kdim + 1));
-      np += padded(n * kdim) + 2 * padded(n);
+      np += padded(n * kdim) + 3 * padded(n);
       size_t start = 0;
       for (int l = 0; l < d.nlev; l++) {
         np += padded(n - start);
@@ -3239,6 +3265,7 @@ struct Systems : SystemsBase {
       d.Z = takep(n * kdim);
       d.rt = takep(n);
       d.xt = takep(n);
+      d.y = takep(n);
       size_t start = 0;
       for (int l = 0; l < d.nlev; l++) {
         d.lev[l].z = takep(n - start);
@@ -3287,7 +3314,7 @@ struct Systems : SystemsBase {
     return PGX_SUCCESS;
   }
 
-  int launch(int kdim, int maxits, double tol, int atol, int th, int cps, int ln, const int* ord = nullptr,
+  int launch(int kdim, int maxits, double tol, int atol, int th, int cps, int ln, int dp, const int* ord = nullptr,
              int nord = -1) {
     // CTAs of up to 256 threads use the build with 128 registers per thread
     void (*kern)(SysArgs<P>) = th <= 256 ? systems_fgmres_kernel<P, 256> : systems_fgmres_kernel<P, kSysMaxThreads>;
@@ -3319,6 +3346,7 @@ struct Systems : SystemsBase {
     a.tol = tol;
     a.lanes = ln;
     a.scap = (int)(smem / sizeof(P));
+    a.depth = dp;
     a.next = d_next;
     a.st = d_st;
     a.st_in = d_st_in;
@@ -3364,7 +3392,7 @@ struct Systems : SystemsBase {
       PGX_CUDA(cudaMemcpyAsync(d_bpack, h_bpack, sizeof(double) * ntot, cudaMemcpyHostToDevice, stream));
       PGX_CUDA(cudaMemcpyAsync(d_xpack, h_xpack, sizeof(double) * ntot, cudaMemcpyHostToDevice, stream));
     }
-    PGX_TRY(launch(kdim, maxits, tol, atol, threads, ctas_per_sm, lanes));
+    PGX_TRY(launch(kdim, maxits, tol, atol, threads, ctas_per_sm, lanes, depth));
     PGX_CUDA(cudaMemcpyAsync(h_res, d_res, sizeof(SysResult) * count, cudaMemcpyDeviceToHost, stream));
     if (location == PGX_LOCATION_HOST)
       PGX_CUDA(cudaMemcpyAsync(h_xpack, d_xpack, sizeof(double) * ntot, cudaMemcpyDeviceToHost, stream));
@@ -3402,7 +3430,7 @@ struct Systems : SystemsBase {
   }
 
   // The schedule autotuner: a sample of the batch (every stride-th system of
-  // the work list, so it spans the sizes) solved once per candidate (threads
+  // the work list past its largest sixteenth) solved once per candidate (threads
   // per CTA, CTAs per SM, SpMV lanes per row) from x0 = 0 into the library's
   // own x; the fastest by device time is kept.
   int tune(const double* const* b, int location, int kdim, int maxits, double tol, int atol, int stride,
@@ -3425,31 +3453,37 @@ struct Systems : SystemsBase {
     std::vector<double*> xs(count);
     std::vector<const double*> bs(count);
     PGX_TRY(set_pointers(xs.data(), bs.data(), PGX_LOCATION_HOST));
+    // the largest sixteenth of the work list is left out of a sample (stride
+    // > 1): every candidate would last as long as its largest system
     std::vector<int> sample;
-    for (int w = 0; w < count; w += stride) sample.push_back(order[w]);
+    for (int w = stride > 1 ? count / 16 : 0; w < count; w += stride) sample.push_back(order[w]);
     Arena tmp;
     int* d_sample = nullptr;
     PGX_TRY(tmp.upload(&d_sample, sample.data(), sample.size(), stream));
-    static const int cand[][2] = {{256, 2}, {512, 1}, {512, 2}, {1024, 1}};
-    static const int lane_c[] = {2, 4, 8};
+    // coordinate descent: the CTA shape first, then the SpMV lanes, then the
+    // levels the triangular passes fetch ahead
     tune_table.clear();
     double best = 1e300;
-    int bt = threads, bc = ctas_per_sm, bl = lanes;
-    for (const auto& c : cand) {
-      for (int ln : lane_c) {
-        PGX_CUDA(cudaMemsetAsync(d_xpack, 0, sizeof(double) * ntot, stream));
-        PGX_TRY(launch(kdim, maxits, tol, atol, c[0], c[1], ln, d_sample, (int)sample.size()));
-        PGX_CUDA(cudaStreamSynchronize(stream));
-        float ms = 0.f;
-        PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-        tune_table.push_back({(double)c[0], (double)c[1], (double)ln, (double)ms});
-        if (ms < best) {
-          best = ms;
-          bt = c[0], bc = c[1], bl = ln;
-        }
+    int bt = 256, bc = 2, bl = 2, bd = 2;
+    auto trial = [&](int th, int cps, int ln, int dp) -> int {
+      PGX_CUDA(cudaMemsetAsync(d_xpack, 0, sizeof(double) * ntot, stream));
+      PGX_TRY(launch(kdim, maxits, tol, atol, th, cps, ln, dp, d_sample, (int)sample.size()));
+      PGX_CUDA(cudaStreamSynchronize(stream));
+      float ms = 0.f;
+      PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+      tune_table.push_back({(double)th, (double)cps, (double)ln, (double)dp, (double)ms});
+      if (ms < best) {
+        best = ms;
+        bt = th, bc = cps, bl = ln, bd = dp;
       }
-    }
-    threads = bt, ctas_per_sm = bc, lanes = bl;
+      return PGX_SUCCESS;
+    };
+    static const int shapes[][2] = {{256, 2}, {512, 1}, {512, 2}, {1024, 1}};
+    for (const auto& c : shapes) PGX_TRY(trial(c[0], c[1], 2, 2));
+    const int st = bt, sc = bc;
+    for (int ln : {4, 8}) PGX_TRY(trial(st, sc, ln, 2));
+    PGX_TRY(trial(st, sc, bl, 4));
+    threads = bt, ctas_per_sm = bc, lanes = bl, depth = bd;
     if (best_ms) *best_ms = best;
     return PGX_SUCCESS;
   }
@@ -4665,13 +4699,13 @@ int pgx_csr_spmv_device_variant(const pgx_csr* Ad, int32_t variant, double alpha
       PGX_TRY(tmp.alloc(&cval, (size_t)nt));
       merge_spmv_kernel<double, double, double, double><<<(nt + 255) / 256, 256>>>(
           Ad->rows, (int)Ad->nnz, Ad->rowptr, Ad->colidx, Ad->values, x, alpha, b, beta, y, crow, cval, sk);
-      merge_spmv_fixup_kernel<double, double><<<grid_for(nt, 256, 148 * 8), 256>>>(nt, crow, cval, alpha, y, sk);
+      merge_spmv_fixup_kernel<double, double><<<grid_for(nt, 256, num_sms() * 8), 256>>>(nt, crow, cval, alpha, y, sk);
       PGX_CUDA(cudaGetLastError());
       PGX_CUDA(cudaDeviceSynchronize());
       return PGX_SUCCESS;
     }
     const int S = p.S;
-    const int grid = grid_for(Ad->rows, 256 / S, 148 * 16);
+    const int grid = grid_for(Ad->rows, 256 / S, num_sms() * 16);
     // caller-owned arrays: 128-bit loads only where both are 16-byte aligned
     // and the nonzeros fill whole 4-entry blocks
     const bool vec = ((uintptr_t)Ad->colidx % 16 == 0) && ((uintptr_t)Ad->values % 16 == 0) && Ad->nnz % 4 == 0;
@@ -4787,28 +4821,31 @@ int pgx_systems_tune_table(pgx_systems s, int32_t capacity, double* table, int32
   if (rows) *rows = (int32_t)t.size();
   if (table)
     for (int i = 0; i < (int)t.size() && i < capacity; i++)
-      for (int k = 0; k < 4; k++) table[4 * i + k] = t[i][k];
+      for (int k = 0; k < 5; k++) table[5 * i + k] = t[i][k];
   return PGX_SUCCESS;
 }
 
-int pgx_systems_set_schedule(pgx_systems s, int32_t threads, int32_t ctas_per_sm, int32_t lanes) {
+int pgx_systems_set_schedule(pgx_systems s, int32_t threads, int32_t ctas_per_sm, int32_t lanes, int32_t depth) {
   if (!s) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   if (threads < 64 || threads > kSysMaxThreads || threads % 32)
     return fail(PGX_ERROR_INVALID_PARAM, "threads %d: a multiple of 32 in [64, %d]", threads, kSysMaxThreads);
   if (ctas_per_sm < 1 || ctas_per_sm > 32) return fail(PGX_ERROR_INVALID_PARAM, "ctas_per_sm %d", ctas_per_sm);
   if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
     return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: a power of two up to 32", lanes);
+  if (depth != 2 && depth != 4) return fail(PGX_ERROR_INVALID_PARAM, "depth %d: 2 or 4", depth);
   s->impl->threads = threads;
   s->impl->ctas_per_sm = ctas_per_sm;
   s->impl->lanes = lanes;
+  s->impl->depth = depth;
   return PGX_SUCCESS;
 }
 
-int pgx_systems_get_schedule(pgx_systems s, int32_t* threads, int32_t* ctas_per_sm, int32_t* lanes) {
+int pgx_systems_get_schedule(pgx_systems s, int32_t* threads, int32_t* ctas_per_sm, int32_t* lanes, int32_t* depth) {
   if (!s) return fail(PGX_ERROR_INVALID_PARAM, "null argument");
   if (threads) *threads = s->impl->threads;
   if (ctas_per_sm) *ctas_per_sm = s->impl->ctas_per_sm;
   if (lanes) *lanes = s->impl->lanes;
+  if (depth) *depth = s->impl->depth;
   return PGX_SUCCESS;
 }
 

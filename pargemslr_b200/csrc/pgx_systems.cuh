@@ -42,15 +42,18 @@ struct SysCsr {
 
 // A triangular factor with its rows stored level by level (IluClass level
 // sets, ilu.cpp:832-1062): packed row k is row `row[k]`; levels are the
-// ranges lvp[t]..lvp[t+1] of packed rows.  Upper factors carry the inverse
-// diagonal per packed row.
+// ranges lvp[t]..lvp[t+1] of packed rows.  Column entries hold PACKED
+// positions (pc[e] = position of column cj[e] in this order), so the solve
+// keeps solved values in packed order; `span` is the farthest dependency
+// (k - pc[e]) plus the widest level, the ring a pass needs.  Upper factors
+// carry the inverse diagonal per packed row.
 template <typename P>
 struct SysTri {
-  int n, nlev;
+  int n, nlev, span;
   const int* lvp;
   const int* row;
   const int* rp;
-  const int* cj;
+  const int* pc;
   const P* va;
   const P* dinv;
 };
@@ -80,6 +83,7 @@ struct SysDesc {
   P* Z;        // n x kdim
   P* rt;       // n: permuted right-hand side of the preconditioner
   P* xt;       // n: permuted preconditioner output
+  P* y;        // n: packed scratch of the triangular passes whose span exceeds the shared ring
   P* Vin;      // m0 x (inner_maxits + 1)
   P* Zin;      // m0 x inner_maxits
   P* xlr;      // m0
@@ -106,6 +110,7 @@ struct SysArgs {
   double tol;
   int lanes;          // SpMV lanes per row (1, 2, 4 or 8)
   int scap;           // values of the dynamic shared-memory solve buffer
+  int depth;          // levels the triangular passes fetch ahead (2 or 4)
   unsigned int* next;
   FgmresDev* st;      // per CTA: outer solve
   FgmresDev* st_in;   // per CTA: inner solve
@@ -118,6 +123,7 @@ struct SysShared {
   double red[kSysDotCols * 32];
   void* sbuf;  // the CTA's triangular-solve buffer (dynamic shared memory)
   int scap;    // its capacity in values
+  int depth;   // levels the triangular passes fetch ahead (2 or 4)
   unsigned long long tri_ns;  // time in the B-block solves of the current system (thread 0)
   double coef[KMAX + kSysDotCols];
   double coef2[KMAX + kSysDotCols];
@@ -224,93 +230,101 @@ __device__ void sys_spmv(const SysCsr<TM>& M, const TX* x, TA alpha, const TYI* 
   __syncthreads();
 }
 
-// Level-scheduled triangular solve in place (IluClass::SolveHost,
-// ilu.cpp:3677-3790): v holds the right-hand side on entry and the solution
-// on return; lower, unit diagonal: v_r -= L(r,:) v;  upper: v_r = dinv_r
-// (v_r - U(r,:) v).  Rows of one level depend only on rows of earlier
-// levels, so a row reads solved entries and its own right-hand side.  A
-// thread takes kSysRows rows of a level at a time (a block-stride apart) and
-// interleaves their loads, so a wide level costs a few load round trips, not
-// a few per row.  The row data of the thread's first rows of the next level
-// (row index and extent) is fetched before the barrier.  v is in shared
-// memory when the block fits there.
-constexpr int kSysRows = 4;
+// Level-scheduled triangular solve (IluClass::SolveHost, ilu.cpp:3677-3790):
+// lower, unit diagonal: x_r = rhs_r - L(r,:) x;  upper: x_r = dinv_r (rhs_r -
+// U(r,:) x).  Rows of one level depend only on rows of earlier levels.
+// Solved values are kept in packed (level) order in `buf`, at position
+// p & mask: a shared-memory ring when the factor's span fits it (a value is
+// overwritten only after every row that reads it is done), else a global
+// vector of the factor's length (mask all ones).  Each solved value is also
+// written to out[row], off the dependency chain.  A thread's first row of
+// each level is fetched DEPTH levels ahead in registers (row index,
+// right-hand side, extent, the first kSysPrefetch entries, the inverse
+// diagonal): those loads do not depend on solved values, so after a barrier
+// only the ring reads remain on the chain.  DEPTH (2 or 4) is a schedule
+// choice: deeper hides more of the global-load latency behind short levels,
+// at the price of registers.  rhs must not change during the pass; it may be
+// `out` itself (the upper pass reads the lower pass's result there, each row
+// only for itself).
+constexpr int kSysPrefetch = 4;
+template <typename P>
+struct SysRowPF {
+  int row, e0, e1;
+  P rhs, dg;
+  int pc[kSysPrefetch];
+  P va[kSysPrefetch];
+};
 template <bool UPPER, typename P>
-__device__ void sys_trsv(const SysTri<P>& T, P* v) {
-  int r[kSysRows], e0[kSysRows], e1[kSysRows];
-  int kbeg = 0, kend = 0;
-  auto fetch = [&](int t) {
+__device__ __forceinline__ void sys_fetch_row(const SysTri<P>& T, const P* rhs, int t, SysRowPF<P>& f) {
+  f.row = -1;
+  if (t >= T.nlev) return;
+  const int k = T.lvp[t] + threadIdx.x;
+  if (k >= T.lvp[t + 1]) return;
+  f.row = T.row[k];
+  f.e0 = T.rp[k];
+  f.e1 = T.rp[k + 1];
+  f.rhs = rhs[f.row];
+  f.dg = UPPER ? T.dinv[k] : P(1);
 #pragma unroll
-    for (int q = 0; q < kSysRows; q++) r[q] = -1;
-    if (t >= T.nlev) return;
-    kbeg = T.lvp[t];
-    kend = T.lvp[t + 1];
+  for (int u = 0; u < kSysPrefetch; u++) {
+    f.pc[u] = f.e0 + u < f.e1 ? T.pc[f.e0 + u] : 0;
+    f.va[u] = f.e0 + u < f.e1 ? T.va[f.e0 + u] : P(0);
+  }
+}
+template <bool UPPER, int DEPTH, typename P>
+__device__ __noinline__ void sys_trsv(const SysTri<P>& T, const P* rhs, P* out, P* buf, unsigned mask) {
+  SysRowPF<P> pf[DEPTH];
 #pragma unroll
-    for (int q = 0; q < kSysRows; q++) {
-      const int k = kbeg + threadIdx.x + q * blockDim.x;
-      if (k < kend) {
-        r[q] = T.row[k];
-        e0[q] = T.rp[k];
-        e1[q] = T.rp[k + 1];
-      }
-    }
-  };
-  fetch(0);
+  for (int d = 0; d < DEPTH; d++) sys_fetch_row<UPPER>(T, rhs, d, pf[d]);
   for (int t = 0; t < T.nlev; t++) {
-    for (int kb = kbeg + threadIdx.x;; kb += kSysRows * blockDim.x) {
-      if (kb != kbeg + (int)threadIdx.x) {  // later batches of a wide level
+    const SysRowPF<P>& a = pf[0];
+    if (a.row >= 0) {
+      const int k = T.lvp[t] + threadIdx.x;
+      P s = a.rhs;
 #pragma unroll
-        for (int q = 0; q < kSysRows; q++) {
-          const int k = kb + q * blockDim.x;
-          r[q] = -1;
-          if (k < kend) {
-            r[q] = T.row[k];
-            e0[q] = T.rp[k];
-            e1[q] = T.rp[k + 1];
-          }
-        }
+      for (int u = 0; u < kSysPrefetch; u++)
+        if (a.e0 + u < a.e1) s -= a.va[u] * buf[(unsigned)a.pc[u] & mask];
+      for (int e = a.e0 + kSysPrefetch; e < a.e1; e++) s -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
+      const P x = a.dg * s;
+      buf[(unsigned)k & mask] = x;
+      out[a.row] = x;
+      // rows past the first blockDim of a wide level
+      const int kend = T.lvp[t + 1];
+      for (int kk = k + blockDim.x; kk < kend; kk += blockDim.x) {
+        const int r = T.row[kk];
+        P q = rhs[r];
+        const int f1 = T.rp[kk + 1];
+        for (int e = T.rp[kk]; e < f1; e++) q -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
+        const P y = UPPER ? T.dinv[kk] * q : q;
+        buf[(unsigned)kk & mask] = y;
+        out[r] = y;
       }
-      if (r[0] < 0) break;
-      P s[kSysRows];
-      int len = 0;
-#pragma unroll
-      for (int q = 0; q < kSysRows; q++) {
-        s[q] = r[q] >= 0 ? v[r[q]] : P(0);
-        if (r[q] >= 0) len = max(len, e1[q] - e0[q]);
-      }
-      for (int u = 0; u < len; u++) {
-#pragma unroll
-        for (int q = 0; q < kSysRows; q++) {
-          const int e = e0[q] + u;
-          if (r[q] >= 0 && e < e1[q]) s[q] -= T.va[e] * v[T.cj[e]];
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < kSysRows; q++)
-        if (r[q] >= 0) v[r[q]] = UPPER ? T.dinv[kb + q * blockDim.x] * s[q] : s[q];
-      if (r[kSysRows - 1] < 0) break;
     }
-    fetch(t + 1);
+#pragma unroll
+    for (int d = 0; d + 1 < DEPTH; d++) pf[d] = pf[d + 1];
+    sys_fetch_row<UPPER>(T, rhs, t + DEPTH, pf[DEPTH - 1]);
     __syncthreads();
   }
 }
 
-// x = U^-1 L^-1 rhs of level l (GemslrClass::SolveB): in shared memory when
-// the block's rows fit the CTA's buffer, else in place in x
+// x = U^-1 L^-1 rhs of level l (GemslrClass::SolveB): the lower pass
+// writes its result into x, the upper pass reads it there row by row and
+// overwrites it; each pass keeps its solved values in the CTA's shared ring
+// when the factor's span fits (ring = the largest power of two within the
+// shared buffer), else in the system's packed scratch vector
 template <typename P>
-__device__ void sys_solve_b(const SysDesc<P>& d, int l, const P* rhs, P* x, P* sbuf, int scap,
+__device__ void sys_solve_b(const SysDesc<P>& d, int l, const P* rhs, P* x, P* sbuf, int scap, int depth,
                             unsigned long long* tri_ns) {
   const unsigned long long t0 = threadIdx.x == 0 ? sys_clock() : 0ull;
   const SysLevel<P>& v = d.lev[l];
-  const int nl = v.nl;
-  P* w = nl <= scap ? sbuf : x;
-  for (int i = threadIdx.x; i < nl; i += blockDim.x) w[i] = rhs[i];
-  __syncthreads();
-  sys_trsv<false>(v.L, w);
-  sys_trsv<true>(v.U, w);
-  if (w != x) {
-    for (int i = threadIdx.x; i < nl; i += blockDim.x) x[i] = w[i];
-    __syncthreads();
+  const unsigned ring = scap > 0 ? 1u << (31 - __clz(scap)) : 0u;
+  const bool lr = v.L.span < (int)ring, ur = v.U.span < (int)ring;
+  if (depth == 4) {
+    sys_trsv<false, 4>(v.L, rhs, x, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<true, 4>(v.U, (const P*)x, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
+  } else {
+    sys_trsv<false, 2>(v.L, rhs, x, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<true, 2>(v.U, (const P*)x, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
   }
   if (threadIdx.x == 0) *tri_ns += sys_clock() - t0;
 }
@@ -367,7 +381,7 @@ __device__ void sys_solve_from(const SysDesc<P>& d, int l0, P* x, const P* rhs, 
     xs[l] = xv;
     P* zu = v.z;
     P* zl = v.z + v.nl;
-    sys_solve_b(d, l, r, zu, (P*)sh.sbuf, sh.scap, &sh.tri_ns);                                         // 1. zu = B^-1 rhs_u
+    sys_solve_b(d, l, r, zu, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // 1. zu = B^-1 rhs_u
     sys_spmv<P>(v.E, (const P*)zu, P(-1), r + v.nl, P(1), zl, S);     // 2-3. zl = rhs_l - E zu
     if (INNER && l == 0 && d.inner) {
       sys_inner_solve(d, xv + v.nl, zl, st_in, S, sh);                // 4. inner FGMRES
@@ -382,14 +396,14 @@ __device__ void sys_solve_from(const SysDesc<P>& d, int l0, P* x, const P* rhs, 
   if (stop_inner) {
     top = l;
   } else {
-    sys_solve_b(d, d.nlev - 1, r, xv, (P*)sh.sbuf, sh.scap, &sh.tri_ns);                                // last level: B^-1 rhs
+    sys_solve_b(d, d.nlev - 1, r, xv, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // last level
     top = d.nlev - 2;
   }
   for (int t = top; t >= l0; t--) {
     const SysLevel<P>& v = d.lev[t];
     P* zu = v.z;
     sys_spmv<P>(v.F, (const P*)(xs[t] + v.nl), P(-1), rh[t], P(1), zu, S);  // 5-6. zu = rhs_u - F xl
-    sys_solve_b(d, t, zu, xs[t], (P*)sh.sbuf, sh.scap, &sh.tri_ns);                                           // 7. xu = B^-1 zu
+    sys_solve_b(d, t, zu, xs[t], (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // 7. xu = B^-1 zu
   }
 }
 
@@ -442,7 +456,7 @@ __device__ void sys_inner_solve(const SysDesc<P>& d, P* xl, const P* zl, FgmresD
     sys_solve_from<false>(d, 1, zj, (const P*)d.xlr, st, S, sh);
     // w = S0 z (GemslrClass::SchurMatVec, gemslr.cpp:3799-3960)
     sys_spmv<P>(v0.F, (const P*)zj, P(1), (const P*)nullptr, P(0), d.s_zu, S);
-    sys_solve_b(d, 0, d.s_zu, d.s_wu, (P*)sh.sbuf, sh.scap, &sh.tri_ns);
+    sys_solve_b(d, 0, d.s_zu, d.s_wu, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);
     sys_spmv<P>(d.C0, (const P*)zj, P(1), (const P*)nullptr, P(0), wj, S);
     sys_spmv<P>(v0.E, (const P*)d.s_wu, P(-1), (const P*)wj, P(1), wj, S);
     sys_arnoldi(d.Vin, ld, j, st, m0, sh);
@@ -473,6 +487,7 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) systems_fgmres_kern
   if (threadIdx.x == 0) {
     sh.sbuf = sys_dyn;
     sh.scap = a.scap;
+    sh.depth = a.depth;
   }
   __syncthreads();
   FgmresDev* st = a.st + blockIdx.x;

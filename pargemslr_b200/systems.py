@@ -73,21 +73,24 @@ class SystemsBatch:
                                                _abi.ptr(prm), int(stride), C.byref(best)))
         return best.value
 
-    def tune_table(self) -> List[Tuple[int, int, int, float]]:
+    def tune_table(self) -> List[Tuple[int, int, int, int, float]]:
+        """The candidates the last tune tried: (threads, CTAs per SM, SpMV lanes, prefetch depth, ms)."""
         rows = C.c_int32(0)
         _abi.check(_abi.lib().pgx_systems_tune_table(self._p, 0, None, C.byref(rows)))
-        t = np.zeros(4 * max(rows.value, 1))
+        t = np.zeros(5 * max(rows.value, 1))
         _abi.check(_abi.lib().pgx_systems_tune_table(self._p, rows.value, _abi.ptr(t), C.byref(rows)))
-        return [(int(t[4 * i]), int(t[4 * i + 1]), int(t[4 * i + 2]), float(t[4 * i + 3])) for i in range(rows.value)]
+        return [(int(t[5 * i]), int(t[5 * i + 1]), int(t[5 * i + 2]), int(t[5 * i + 3]), float(t[5 * i + 4]))
+                for i in range(rows.value)]
 
     @property
-    def schedule(self) -> Tuple[int, int, int]:
-        a, b, c = C.c_int32(0), C.c_int32(0), C.c_int32(0)
-        _abi.check(_abi.lib().pgx_systems_get_schedule(self._p, C.byref(a), C.byref(b), C.byref(c)))
-        return a.value, b.value, c.value
+    def schedule(self) -> Tuple[int, int, int, int]:
+        """(threads per CTA, CTAs per SM, SpMV lanes per row, levels the triangular passes fetch ahead)."""
+        a, b, c, d = C.c_int32(0), C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        _abi.check(_abi.lib().pgx_systems_get_schedule(self._p, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return a.value, b.value, c.value, d.value
 
-    def set_schedule(self, threads: int, ctas_per_sm: int, lanes: int) -> None:
-        _abi.check(_abi.lib().pgx_systems_set_schedule(self._p, threads, ctas_per_sm, lanes))
+    def set_schedule(self, threads: int, ctas_per_sm: int, lanes: int, depth: int = 2) -> None:
+        _abi.check(_abi.lib().pgx_systems_set_schedule(self._p, threads, ctas_per_sm, lanes, depth))
 
     def timing(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
         """Per system: start and end of its solve in the last launch (ms from the first start), and its time in

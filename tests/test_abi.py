@@ -41,7 +41,7 @@ def test_calls_without_device_fail_cleanly():
     hs = (C.c_void_p * 2)(None, None)
     assert L.pgx_systems_create(C.byref(sy), C.cast(hs, C.c_void_p), 2) == _abi.ERROR_FUNCTION_CALL
     assert L.pgx_systems_solve(None, None, None, 0, None, None) == _abi.ERROR_INVALID_PARAM
-    assert L.pgx_systems_set_schedule(None, 512, 2, 4) == _abi.ERROR_INVALID_PARAM
+    assert L.pgx_systems_set_schedule(None, 512, 2, 4, 2) == _abi.ERROR_INVALID_PARAM
     assert L.pgx_systems_destroy(None) == 0
 
 

@@ -74,7 +74,7 @@ def test_schedules_and_autotuner_agree():
     sb = SystemsBatch([h for _, _, h in systems])
     B = [b for _, b, _ in systems]
     base, _ = sb.solve(B, params=p)
-    for sched in [(256, 4, 2), (1024, 1, 8), (512, 2, 1)]:
+    for sched in [(256, 4, 2, 2), (1024, 1, 8, 4), (512, 2, 1, 2), (256, 2, 4, 4)]:
         sb.set_schedule(*sched)
         assert sb.schedule == sched
         X, R = sb.solve(B, params=p)
@@ -83,10 +83,10 @@ def test_schedules_and_autotuner_agree():
             assert np.linalg.norm(X[k] - base[k]) <= 1e-6 * np.linalg.norm(base[k])
     best = sb.tune(B, params=p)
     table = sb.tune_table()
-    assert len(table) == 12 and best > 0
-    assert min(t[3] for t in table) == pytest.approx(best)
+    assert len(table) == 7 and best > 0
+    assert min(t[4] for t in table) == pytest.approx(best)
     chosen = sb.schedule
-    assert any(t[:3] == chosen and t[3] == pytest.approx(best) for t in table)
+    assert any(t[:4] == chosen and t[4] == pytest.approx(best) for t in table)
     X, R = sb.solve(B, params=p)
     _check_against_singles(systems, X, R, p)
     sb.close()
