@@ -369,7 +369,7 @@ int pgx_pool_destroy(pgx_pool pool);
  *     sixteenth; stride 1 is the whole batch) from x0 = 0 into the object's
  *     own vectors, by coordinate descent over the CTA shape (256 threads x 2
  *     per SM, 512 x 1, 512 x 2, 1024 x 1), then the SpMV lanes per row (2, 4,
- *     8), then the levels the triangular passes fetch ahead (2, 4); it keeps
+ *     8), then the levels the triangular passes fetch ahead (2, 3); it keeps
  *     the fastest and returns its device time.  pgx_systems_tune_table returns
  *     the candidates tried, five doubles each (threads, CTAs per SM, lanes,
  *     depth, ms).

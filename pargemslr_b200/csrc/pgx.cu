@@ -3075,8 +3075,10 @@ struct Systems : SystemsBase {
     return PGX_SUCCESS;
   }
   // rows in level order (IluClass::BuildLevels rule, ilu.cpp:832-1062)
+  // dst_map: where the solved value of each row goes (null: the row itself);
+  // pos_out receives each row's packed position
   int tri(SysTri<P>& t, const HostCsr& h_in, bool upper, const std::vector<double>* dinv, int nl,
-          long long& levels) {
+          long long& levels, const std::vector<int>* dst_map, std::vector<int>* pos_out) {
     t.n = nl;
     t.nlev = 0;
     if (nl == 0) return PGX_SUCCESS;
@@ -3116,12 +3118,26 @@ struct Systems : SystemsBase {
       if (upper) di.push_back((*dinv)[r]);
     }
     t.span = far + wide;
+    // fixed-size heads of every packed row and the destination of its value
+    std::vector<int> hpc((size_t)nl * kSysHead, 0), dst(nl);
+    std::vector<double> hva((size_t)nl * kSysHead, 0.0);
+    for (int k = 0; k < nl; k++) {
+      for (int e = rp[k], u = 0; e < rp[k + 1] && u < kSysHead; e++, u++) {
+        hpc[(size_t)k * kSysHead + u] = pc[e];
+        hva[(size_t)k * kSysHead + u] = va[e];
+      }
+      dst[k] = dst_map ? (*dst_map)[ord[k]] : ord[k];
+    }
     ints(&t.lvp, lvp.data(), lvp.size());
     ints(&t.row, ord.data(), ord.size());
     ints(&t.rp, rp.data(), rp.size());
     ints(&t.pc, pc.data(), pc.size());
     vals(&t.va, va.data(), va.size());
+    ints(&t.hpc, hpc.data(), hpc.size());
+    vals(&t.hva, hva.data(), hva.size());
+    ints(&t.dst, dst.data(), dst.size());
     if (upper) vals(&t.dinv, di.data(), di.size());
+    if (pos_out) pos_out->swap(pos);
     return PGX_SUCCESS;
   }
 
@@ -3169,8 +3185,14 @@ struct Systems : SystemsBase {
         SysLevel<P>& v = d.lev[l];
         v.nl = im.lev_ptr[l + 1] - im.lev_ptr[l];
         v.m = n - im.lev_ptr[l + 1];
-        PGX_TRY(tri(v.L, h.L, false, nullptr, v.nl, levels));
-        PGX_TRY(tri(v.U, h.U, true, &h.dinv, v.nl, levels));
+        // the upper factor's order first: the lower pass writes its result there
+        std::vector<int> pos_u;
+        PGX_TRY(tri(v.U, h.U, true, &h.dinv, v.nl, levels, nullptr, &pos_u));
+        if (v.nl > 0 && (int)pos_u.size() != v.nl) {
+          pos_u.resize(v.nl);
+          for (int r = 0; r < v.nl; r++) pos_u[r] = r;
+        }
+        PGX_TRY(tri(v.L, h.L, false, nullptr, v.nl, levels, &pos_u, nullptr));
         fnnz += h.L.nnz() + h.U.nnz();
         if (l < im.nlev - 1) {
           PGX_TRY(csr_p(v.E, h.E, v.m, v.nl, "E"));
@@ -3239,7 +3261,7 @@ struct Systems : SystemsBase {
       const SysDesc<P>& d = desc[s];
       const size_t n = d.n, m0 = d.nlev > 1 ? d.lev[0].m : 0, nl0 = d.lev[0].nl;
       nd += padded(n * (kdim + 1));
-      np += padded(n * kdim) + 3 * padded(n);
+      np += padded(n * kdim) + 5 * padded(n);
       size_t start = 0;
       for (int l = 0; l < d.nlev; l++) {
         np += padded(n - start);
@@ -3266,6 +3288,8 @@ struct Systems : SystemsBase {
       d.rt = takep(n);
       d.xt = takep(n);
       d.y = takep(n);
+      d.yr = takep(n);
+      d.yu = takep(n);
       size_t start = 0;
       for (int l = 0; l < d.nlev; l++) {
         d.lev[l].z = takep(n - start);
@@ -3482,7 +3506,7 @@ struct Systems : SystemsBase {
     for (const auto& c : shapes) PGX_TRY(trial(c[0], c[1], 2, 2));
     const int st = bt, sc = bc;
     for (int ln : {4, 8}) PGX_TRY(trial(st, sc, ln, 2));
-    PGX_TRY(trial(st, sc, bl, 4));
+    PGX_TRY(trial(st, sc, bl, 3));
     threads = bt, ctas_per_sm = bc, lanes = bl, depth = bd;
     if (best_ms) *best_ms = best;
     return PGX_SUCCESS;
@@ -4832,7 +4856,7 @@ int pgx_systems_set_schedule(pgx_systems s, int32_t threads, int32_t ctas_per_sm
   if (ctas_per_sm < 1 || ctas_per_sm > 32) return fail(PGX_ERROR_INVALID_PARAM, "ctas_per_sm %d", ctas_per_sm);
   if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
     return fail(PGX_ERROR_INVALID_PARAM, "lanes %d: a power of two up to 32", lanes);
-  if (depth != 2 && depth != 4) return fail(PGX_ERROR_INVALID_PARAM, "depth %d: 2 or 4", depth);
+  if (depth != 2 && depth != 3) return fail(PGX_ERROR_INVALID_PARAM, "depth %d: 2 or 3", depth);
   s->impl->threads = threads;
   s->impl->ctas_per_sm = ctas_per_sm;
   s->impl->lanes = lanes;

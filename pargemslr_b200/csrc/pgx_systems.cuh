@@ -45,8 +45,14 @@ struct SysCsr {
 // ranges lvp[t]..lvp[t+1] of packed rows.  Column entries hold PACKED
 // positions (pc[e] = position of column cj[e] in this order), so the solve
 // keeps solved values in packed order; `span` is the farthest dependency
-// (k - pc[e]) plus the widest level, the ring a pass needs.  Upper factors
-// carry the inverse diagonal per packed row.
+// (k - pc[e]) plus the widest level, the ring a pass needs.  The first
+// kSysHead entries of every packed row are repeated in fixed-size heads
+// (hpc, hva: kSysHead per row, zero-padded) so a row's data is addressed by
+// its position alone; dst[k] is where the solved value of packed row k goes:
+// the upper factor's packed position of that row (lower factor), or the row
+// itself (upper factor).  Upper factors carry the inverse diagonal per
+// packed row.
+constexpr int kSysHead = 8;
 template <typename P>
 struct SysTri {
   int n, nlev, span;
@@ -55,6 +61,9 @@ struct SysTri {
   const int* rp;
   const int* pc;
   const P* va;
+  const int* hpc;
+  const P* hva;
+  const int* dst;
   const P* dinv;
 };
 
@@ -84,6 +93,8 @@ struct SysDesc {
   P* rt;       // n: permuted right-hand side of the preconditioner
   P* xt;       // n: permuted preconditioner output
   P* y;        // n: packed scratch of the triangular passes whose span exceeds the shared ring
+  P* yr;       // n: the lower pass's right-hand side in its packed order
+  P* yu;       // n: the lower pass's result in the upper factor's packed order
   P* Vin;      // m0 x (inner_maxits + 1)
   P* Zin;      // m0 x inner_maxits
   P* xlr;      // m0
@@ -110,7 +121,7 @@ struct SysArgs {
   double tol;
   int lanes;          // SpMV lanes per row (1, 2, 4 or 8)
   int scap;           // values of the dynamic shared-memory solve buffer
-  int depth;          // levels the triangular passes fetch ahead (2 or 4)
+  int depth;          // levels the triangular passes fetch ahead (2 or 3)
   unsigned int* next;
   FgmresDev* st;      // per CTA: outer solve
   FgmresDev* st_in;   // per CTA: inner solve
@@ -123,7 +134,7 @@ struct SysShared {
   double red[kSysDotCols * 32];
   void* sbuf;  // the CTA's triangular-solve buffer (dynamic shared memory)
   int scap;    // its capacity in values
-  int depth;   // levels the triangular passes fetch ahead (2 or 4)
+  int depth;   // levels the triangular passes fetch ahead (2 or 3)
   unsigned long long tri_ns;  // time in the B-block solves of the current system (thread 0)
   double coef[KMAX + kSysDotCols];
   double coef2[KMAX + kSysDotCols];
@@ -231,87 +242,95 @@ __device__ void sys_spmv(const SysCsr<TM>& M, const TX* x, TA alpha, const TYI* 
 }
 
 // Level-scheduled triangular solve (IluClass::SolveHost, ilu.cpp:3677-3790):
-// lower, unit diagonal: x_r = rhs_r - L(r,:) x;  upper: x_r = dinv_r (rhs_r -
-// U(r,:) x).  Rows of one level depend only on rows of earlier levels.
-// Solved values are kept in packed (level) order in `buf`, at position
-// p & mask: a shared-memory ring when the factor's span fits it (a value is
-// overwritten only after every row that reads it is done), else a global
-// vector of the factor's length (mask all ones).  Each solved value is also
-// written to out[row], off the dependency chain.  A thread's first row of
-// each level is fetched DEPTH levels ahead in registers (row index,
-// right-hand side, extent, the first kSysPrefetch entries, the inverse
-// diagonal): those loads do not depend on solved values, so after a barrier
-// only the ring reads remain on the chain.  DEPTH (2 or 4) is a schedule
-// choice: deeper hides more of the global-load latency behind short levels,
-// at the price of registers.  rhs must not change during the pass; it may be
-// `out` itself (the upper pass reads the lower pass's result there, each row
-// only for itself).
-constexpr int kSysPrefetch = 4;
+// lower, unit diagonal: x_k = rhs_k - L(k,:) x;  upper: x_k = dinv_k (rhs_k -
+// U(k,:) x), all in the factor's packed (level) order.  Rows of one level
+// depend only on rows of earlier levels.  Solved values are kept in `buf`
+// at position k & mask: a shared-memory ring when the factor's span fits it
+// (a value is overwritten only after every row that reads it is done), else
+// a global vector of the factor's length (mask all ones); each is also
+// stored to out[dst[k]], off the dependency chain.
+//
+// A thread's first row of each level is fetched DEPTH levels ahead into
+// registers: its right-hand side (already in packed order), destination,
+// extent, head entries and inverse diagonal.  Every one of those loads is
+// addressed by the row's packed position alone, and the level pointers that
+// give the positions are loaded two levels before they are used, so no load
+// waits on another and none stands before a barrier: after a barrier only
+// the ring reads (shared memory) remain on the chain.  DEPTH (2 or 3) is a
+// schedule choice.
 template <typename P>
 struct SysRowPF {
-  int row, e0, e1;
+  int dst, e0, e1;
   P rhs, dg;
-  int pc[kSysPrefetch];
-  P va[kSysPrefetch];
+  int pc[kSysHead];
+  P va[kSysHead];
 };
 template <bool UPPER, typename P>
-__device__ __forceinline__ void sys_fetch_row(const SysTri<P>& T, const P* rhs, int t, SysRowPF<P>& f) {
-  f.row = -1;
-  if (t >= T.nlev) return;
-  const int k = T.lvp[t] + threadIdx.x;
-  if (k >= T.lvp[t + 1]) return;
-  f.row = T.row[k];
+__device__ __forceinline__ void sys_fetch_row(const SysTri<P>& T, const P* rhs, int k, int kend, SysRowPF<P>& f) {
+  f.dst = -1;
+  if (k >= kend) return;
+  f.dst = T.dst[k];
   f.e0 = T.rp[k];
   f.e1 = T.rp[k + 1];
-  f.rhs = rhs[f.row];
+  f.rhs = rhs[k];
   f.dg = UPPER ? T.dinv[k] : P(1);
+  const int4* hp = reinterpret_cast<const int4*>(T.hpc + (size_t)k * kSysHead);
 #pragma unroll
-  for (int u = 0; u < kSysPrefetch; u++) {
-    f.pc[u] = f.e0 + u < f.e1 ? T.pc[f.e0 + u] : 0;
-    f.va[u] = f.e0 + u < f.e1 ? T.va[f.e0 + u] : P(0);
+  for (int u = 0; u < kSysHead / 4; u++) {
+    const int4 q = hp[u];
+    f.pc[4 * u] = q.x, f.pc[4 * u + 1] = q.y, f.pc[4 * u + 2] = q.z, f.pc[4 * u + 3] = q.w;
   }
+#pragma unroll
+  for (int u = 0; u < kSysHead; u++) f.va[u] = T.hva[(size_t)k * kSysHead + u];
 }
 template <bool UPPER, int DEPTH, typename P>
 __device__ __noinline__ void sys_trsv(const SysTri<P>& T, const P* rhs, P* out, P* buf, unsigned mask) {
+  if (T.nlev == 0) return;
+  // lq[j] = lvp[t + j], j = 0 .. DEPTH + 2 (entries past nlev read as n)
+  int lq[DEPTH + 3];
+#pragma unroll
+  for (int j = 0; j < DEPTH + 3; j++) lq[j] = j <= T.nlev ? T.lvp[j] : T.n;
   SysRowPF<P> pf[DEPTH];
 #pragma unroll
-  for (int d = 0; d < DEPTH; d++) sys_fetch_row<UPPER>(T, rhs, d, pf[d]);
+  for (int d = 0; d < DEPTH; d++) sys_fetch_row<UPPER>(T, rhs, lq[d] + threadIdx.x, lq[d + 1], pf[d]);
   for (int t = 0; t < T.nlev; t++) {
     const SysRowPF<P>& a = pf[0];
-    if (a.row >= 0) {
-      const int k = T.lvp[t] + threadIdx.x;
+    if (a.dst >= 0) {
+      const int k = lq[0] + threadIdx.x;
       P s = a.rhs;
 #pragma unroll
-      for (int u = 0; u < kSysPrefetch; u++)
+      for (int u = 0; u < kSysHead; u++)
         if (a.e0 + u < a.e1) s -= a.va[u] * buf[(unsigned)a.pc[u] & mask];
-      for (int e = a.e0 + kSysPrefetch; e < a.e1; e++) s -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
+      for (int e = a.e0 + kSysHead; e < a.e1; e++) s -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
       const P x = a.dg * s;
       buf[(unsigned)k & mask] = x;
-      out[a.row] = x;
+      out[a.dst] = x;
       // rows past the first blockDim of a wide level
-      const int kend = T.lvp[t + 1];
-      for (int kk = k + blockDim.x; kk < kend; kk += blockDim.x) {
-        const int r = T.row[kk];
-        P q = rhs[r];
+      for (int kk = k + blockDim.x; kk < lq[1]; kk += blockDim.x) {
+        P q = rhs[kk];
         const int f1 = T.rp[kk + 1];
         for (int e = T.rp[kk]; e < f1; e++) q -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
         const P y = UPPER ? T.dinv[kk] * q : q;
         buf[(unsigned)kk & mask] = y;
-        out[r] = y;
+        out[T.dst[kk]] = y;
       }
     }
 #pragma unroll
     for (int d = 0; d + 1 < DEPTH; d++) pf[d] = pf[d + 1];
-    sys_fetch_row<UPPER>(T, rhs, t + DEPTH, pf[DEPTH - 1]);
+    sys_fetch_row<UPPER>(T, rhs, lq[DEPTH] + threadIdx.x, lq[DEPTH + 1], pf[DEPTH - 1]);  // level t + DEPTH
+#pragma unroll
+    for (int j = 0; j + 1 < DEPTH + 3; j++) lq[j] = lq[j + 1];
+    lq[DEPTH + 2] = t + DEPTH + 3 <= T.nlev ? T.lvp[t + DEPTH + 3] : T.n;
     __syncthreads();
   }
 }
 
-// x = U^-1 L^-1 rhs of level l (GemslrClass::SolveB): the lower pass
-// writes its result into x, the upper pass reads it there row by row and
-// overwrites it; each pass keeps its solved values in the CTA's shared ring
-// when the factor's span fits (ring = the largest power of two within the
-// shared buffer), else in the system's packed scratch vector
+// x = U^-1 L^-1 rhs of level l (GemslrClass::SolveB): rhs is gathered into
+// the lower factor's packed order, the lower pass writes its result in the
+// upper factor's packed order and the upper pass writes x in row order.
+// Each pass keeps its solved values in the CTA's shared ring when the
+// factor's span fits (ring = the largest power of two within the shared
+// buffer), else in the system's packed scratch vector.
 template <typename P>
 __device__ void sys_solve_b(const SysDesc<P>& d, int l, const P* rhs, P* x, P* sbuf, int scap, int depth,
                             unsigned long long* tri_ns) {
@@ -319,12 +338,25 @@ __device__ void sys_solve_b(const SysDesc<P>& d, int l, const P* rhs, P* x, P* s
   const SysLevel<P>& v = d.lev[l];
   const unsigned ring = scap > 0 ? 1u << (31 - __clz(scap)) : 0u;
   const bool lr = v.L.span < (int)ring, ur = v.U.span < (int)ring;
-  if (depth == 4) {
-    sys_trsv<false, 4>(v.L, rhs, x, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
-    sys_trsv<true, 4>(v.U, (const P*)x, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
+  constexpr int G = 4;  // gathers in flight per thread
+  for (int k0 = threadIdx.x; k0 < v.nl; k0 += G * blockDim.x) {
+    int r[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) r[g] = k0 + g * (int)blockDim.x < v.nl ? v.L.row[k0 + g * blockDim.x] : -1;
+    P q[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) q[g] = r[g] >= 0 ? rhs[r[g]] : P(0);
+#pragma unroll
+    for (int g = 0; g < G; g++)
+      if (r[g] >= 0) d.yr[k0 + g * blockDim.x] = q[g];
+  }
+  __syncthreads();
+  if (depth == 3) {
+    sys_trsv<false, 3>(v.L, (const P*)d.yr, d.yu, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<true, 3>(v.U, (const P*)d.yu, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
   } else {
-    sys_trsv<false, 2>(v.L, rhs, x, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
-    sys_trsv<true, 2>(v.U, (const P*)x, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<false, 2>(v.L, (const P*)d.yr, d.yu, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<true, 2>(v.U, (const P*)d.yu, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
   }
   if (threadIdx.x == 0) *tri_ns += sys_clock() - t0;
 }

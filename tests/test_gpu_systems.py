@@ -74,7 +74,7 @@ def test_schedules_and_autotuner_agree():
     sb = SystemsBatch([h for _, _, h in systems])
     B = [b for _, b, _ in systems]
     base, _ = sb.solve(B, params=p)
-    for sched in [(256, 4, 2, 2), (1024, 1, 8, 4), (512, 2, 1, 2), (256, 2, 4, 4)]:
+    for sched in [(256, 4, 2, 2), (1024, 1, 8, 3), (512, 2, 1, 2), (256, 2, 4, 3)]:
         sb.set_schedule(*sched)
         assert sb.schedule == sched
         X, R = sb.solve(B, params=p)
