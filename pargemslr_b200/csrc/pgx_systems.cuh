@@ -253,22 +253,28 @@ __device__ void sys_spmv(const SysCsr<TM>& M, const TX* x, TA alpha, const TYI* 
 // A thread's first row of each level is fetched DEPTH levels ahead into
 // registers: its right-hand side (already in packed order), destination,
 // extent, head entries and inverse diagonal.  Every one of those loads is
-// addressed by the row's packed position alone, and the level pointers that
-// give the positions are loaded two levels before they are used, so no load
-// waits on another and none stands before a barrier: after a barrier only
-// the ring reads (shared memory) remain on the chain.  DEPTH (2 or 3) is a
-// schedule choice.
+// addressed by the row's packed position alone.  The registers rotate by
+// slot, not by copy: slot d holds level t + d, is consumed there and
+// refilled in place for level t + d + DEPTH (a register copy of a value
+// still in flight would wait for it), and the level pointers each refill
+// needs were loaded into the slot DEPTH levels before.  So no load is
+// waited on before it has had DEPTH levels to arrive, and after a barrier
+// only the ring reads (shared memory) remain on the chain.  DEPTH (2 or 3)
+// is a schedule choice.
 template <typename P>
 struct SysRowPF {
-  int dst, e0, e1;
+  int k, kend, dst, e0, e1;
   P rhs, dg;
   int pc[kSysHead];
   P va[kSysHead];
 };
 template <bool UPPER, typename P>
-__device__ __forceinline__ void sys_fetch_row(const SysTri<P>& T, const P* rhs, int k, int kend, SysRowPF<P>& f) {
+__device__ __forceinline__ void sys_fetch_row(const SysTri<P>& T, const P* rhs, int lv0, int lv1, SysRowPF<P>& f) {
+  f.k = lv0 + threadIdx.x;
+  f.kend = lv1;
   f.dst = -1;
-  if (k >= kend) return;
+  const int k = f.k;
+  if (k >= lv1) return;
   f.dst = T.dst[k];
   f.e0 = T.rp[k];
   f.e1 = T.rp[k + 1];
@@ -283,45 +289,57 @@ __device__ __forceinline__ void sys_fetch_row(const SysTri<P>& T, const P* rhs, 
 #pragma unroll
   for (int u = 0; u < kSysHead; u++) f.va[u] = T.hva[(size_t)k * kSysHead + u];
 }
-template <bool UPPER, int DEPTH, typename P>
+// level pointer j, or n past the last level
+template <typename P>
+__device__ __forceinline__ int sys_lvp(const SysTri<P>& T, int j) {
+  return j <= T.nlev ? T.lvp[j] : T.n;
+}
+template <bool UPPER, typename P>
+__device__ __forceinline__ void sys_row_solve(const SysTri<P>& T, const SysRowPF<P>& a, const P* rhs, P* out, P* buf,
+                                              unsigned mask) {
+  if (a.dst < 0) return;
+  P s = a.rhs;
+#pragma unroll
+  for (int u = 0; u < kSysHead; u++)
+    if (a.e0 + u < a.e1) s -= a.va[u] * buf[(unsigned)a.pc[u] & mask];
+  for (int e = a.e0 + kSysHead; e < a.e1; e++) s -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
+  const P x = a.dg * s;
+  buf[(unsigned)a.k & mask] = x;
+  out[a.dst] = x;
+  // rows past the first blockDim of a wide level
+  for (int kk = a.k + blockDim.x; kk < a.kend; kk += blockDim.x) {
+    P q = rhs[kk];
+    const int f1 = T.rp[kk + 1];
+    for (int e = T.rp[kk]; e < f1; e++) q -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
+    const P y = UPPER ? T.dinv[kk] * q : q;
+    buf[(unsigned)kk & mask] = y;
+    out[T.dst[kk]] = y;
+  }
+}
+// MAXT: the CTA-size bound of the calling kernel; each build gets its own
+// copy, compiled with that build's register budget
+template <bool UPPER, int DEPTH, int MAXT, typename P>
 __device__ __noinline__ void sys_trsv(const SysTri<P>& T, const P* rhs, P* out, P* buf, unsigned mask) {
   if (T.nlev == 0) return;
-  // lq[j] = lvp[t + j], j = 0 .. DEPTH + 2 (entries past nlev read as n)
-  int lq[DEPTH + 3];
-#pragma unroll
-  for (int j = 0; j < DEPTH + 3; j++) lq[j] = j <= T.nlev ? T.lvp[j] : T.n;
   SysRowPF<P> pf[DEPTH];
+  int la[DEPTH], lb[DEPTH];  // slot d: level pointers of the level its next refill fetches
 #pragma unroll
-  for (int d = 0; d < DEPTH; d++) sys_fetch_row<UPPER>(T, rhs, lq[d] + threadIdx.x, lq[d + 1], pf[d]);
-  for (int t = 0; t < T.nlev; t++) {
-    const SysRowPF<P>& a = pf[0];
-    if (a.dst >= 0) {
-      const int k = lq[0] + threadIdx.x;
-      P s = a.rhs;
+  for (int d = 0; d < DEPTH; d++) {
+    sys_fetch_row<UPPER>(T, rhs, sys_lvp(T, d), sys_lvp(T, d + 1), pf[d]);
+    la[d] = sys_lvp(T, d + DEPTH);
+    lb[d] = sys_lvp(T, d + DEPTH + 1);
+  }
+  for (int t = 0; t < T.nlev; t += DEPTH) {
 #pragma unroll
-      for (int u = 0; u < kSysHead; u++)
-        if (a.e0 + u < a.e1) s -= a.va[u] * buf[(unsigned)a.pc[u] & mask];
-      for (int e = a.e0 + kSysHead; e < a.e1; e++) s -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
-      const P x = a.dg * s;
-      buf[(unsigned)k & mask] = x;
-      out[a.dst] = x;
-      // rows past the first blockDim of a wide level
-      for (int kk = k + blockDim.x; kk < lq[1]; kk += blockDim.x) {
-        P q = rhs[kk];
-        const int f1 = T.rp[kk + 1];
-        for (int e = T.rp[kk]; e < f1; e++) q -= T.va[e] * buf[(unsigned)T.pc[e] & mask];
-        const P y = UPPER ? T.dinv[kk] * q : q;
-        buf[(unsigned)kk & mask] = y;
-        out[T.dst[kk]] = y;
+    for (int d = 0; d < DEPTH; d++) {
+      if (t + d < T.nlev) {
+        sys_row_solve<UPPER>(T, pf[d], rhs, out, buf, mask);
+        sys_fetch_row<UPPER>(T, rhs, la[d], lb[d], pf[d]);  // level t + d + DEPTH
+        la[d] = sys_lvp(T, t + d + 2 * DEPTH);
+        lb[d] = sys_lvp(T, t + d + 2 * DEPTH + 1);
+        __syncthreads();
       }
     }
-#pragma unroll
-    for (int d = 0; d + 1 < DEPTH; d++) pf[d] = pf[d + 1];
-    sys_fetch_row<UPPER>(T, rhs, lq[DEPTH] + threadIdx.x, lq[DEPTH + 1], pf[DEPTH - 1]);  // level t + DEPTH
-#pragma unroll
-    for (int j = 0; j + 1 < DEPTH + 3; j++) lq[j] = lq[j + 1];
-    lq[DEPTH + 2] = t + DEPTH + 3 <= T.nlev ? T.lvp[t + DEPTH + 3] : T.n;
-    __syncthreads();
   }
 }
 
@@ -331,7 +349,7 @@ __device__ __noinline__ void sys_trsv(const SysTri<P>& T, const P* rhs, P* out, 
 // Each pass keeps its solved values in the CTA's shared ring when the
 // factor's span fits (ring = the largest power of two within the shared
 // buffer), else in the system's packed scratch vector.
-template <typename P>
+template <int MAXT, typename P>
 __device__ void sys_solve_b(const SysDesc<P>& d, int l, const P* rhs, P* x, P* sbuf, int scap, int depth,
                             unsigned long long* tri_ns) {
   const unsigned long long t0 = threadIdx.x == 0 ? sys_clock() : 0ull;
@@ -352,11 +370,11 @@ __device__ void sys_solve_b(const SysDesc<P>& d, int l, const P* rhs, P* x, P* s
   }
   __syncthreads();
   if (depth == 3) {
-    sys_trsv<false, 3>(v.L, (const P*)d.yr, d.yu, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
-    sys_trsv<true, 3>(v.U, (const P*)d.yu, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<false, 3, MAXT>(v.L, (const P*)d.yr, d.yu, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<true, 3, MAXT>(v.U, (const P*)d.yu, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
   } else {
-    sys_trsv<false, 2>(v.L, (const P*)d.yr, d.yu, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
-    sys_trsv<true, 2>(v.U, (const P*)d.yu, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<false, 2, MAXT>(v.L, (const P*)d.yr, d.yu, lr ? sbuf : d.y, lr ? ring - 1 : 0xFFFFFFFFu);
+    sys_trsv<true, 2, MAXT>(v.U, (const P*)d.yu, x, ur ? sbuf : d.y, ur ? ring - 1 : 0xFFFFFFFFu);
   }
   if (threadIdx.x == 0) *tri_ns += sys_clock() - t0;
 }
@@ -390,7 +408,7 @@ __device__ void sys_arnoldi(TV* Vb, long long ld, int j, FgmresDev* st, int nrow
   __syncthreads();
 }
 
-template <typename P>
+template <int MAXT, typename P>
 __device__ void sys_inner_solve(const SysDesc<P>& d, P* xl, const P* zl, FgmresDev* st, int S, SysShared& sh);
 
 // GemslrClass::SolveLevel from level l0 down (gemslr.cpp:3474-3630) with the
@@ -398,7 +416,7 @@ __device__ void sys_inner_solve(const SysDesc<P>& d, P* xl, const P* zl, FgmresD
 // ascent finishes the levels bottom up.  x and rhs hold the trailing
 // n - lev_ptr[l0] unknowns.  With INNER, level 0 runs the inner Schur FGMRES
 // in place of the low-rank correction and the lower levels.
-template <bool INNER, typename P>
+template <bool INNER, int MAXT, typename P>
 __device__ void sys_solve_from(const SysDesc<P>& d, int l0, P* x, const P* rhs, FgmresDev* st_in, int S,
                                SysShared& sh) {
   const P* rh[kSysMaxLevels];
@@ -413,10 +431,10 @@ __device__ void sys_solve_from(const SysDesc<P>& d, int l0, P* x, const P* rhs, 
     xs[l] = xv;
     P* zu = v.z;
     P* zl = v.z + v.nl;
-    sys_solve_b(d, l, r, zu, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // 1. zu = B^-1 rhs_u
+    sys_solve_b<MAXT>(d, l, r, zu, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // 1. zu = B^-1 rhs_u
     sys_spmv<P>(v.E, (const P*)zu, P(-1), r + v.nl, P(1), zl, S);     // 2-3. zl = rhs_l - E zu
     if (INNER && l == 0 && d.inner) {
-      sys_inner_solve(d, xv + v.nl, zl, st_in, S, sh);                // 4. inner FGMRES
+      sys_inner_solve<MAXT>(d, xv + v.nl, zl, st_in, S, sh);                // 4. inner FGMRES
       stop_inner = true;
       break;
     }
@@ -428,14 +446,14 @@ __device__ void sys_solve_from(const SysDesc<P>& d, int l0, P* x, const P* rhs, 
   if (stop_inner) {
     top = l;
   } else {
-    sys_solve_b(d, d.nlev - 1, r, xv, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // last level
+    sys_solve_b<MAXT>(d, d.nlev - 1, r, xv, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // last level
     top = d.nlev - 2;
   }
   for (int t = top; t >= l0; t--) {
     const SysLevel<P>& v = d.lev[t];
     P* zu = v.z;
     sys_spmv<P>(v.F, (const P*)(xs[t] + v.nl), P(-1), rh[t], P(1), zu, S);  // 5-6. zu = rhs_u - F xl
-    sys_solve_b(d, t, zu, xs[t], (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // 7. xu = B^-1 zu
+    sys_solve_b<MAXT>(d, t, zu, xs[t], (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // 7. xu = B^-1 zu
   }
 }
 
@@ -443,7 +461,7 @@ __device__ void sys_solve_from(const SysDesc<P>& d, int l0, P* x, const P* rhs, 
 // of inner_maxits steps (gemslr.cpp:1660-1674, 3566-3572); its preconditioner
 // is the low-rank correction followed by the level-1 recursion
 // (GemslrSchurMatrixClass::Solve, gemslr.cpp:294-330).
-template <typename P>
+template <int MAXT, typename P>
 __device__ void sys_inner_solve(const SysDesc<P>& d, P* xl, const P* zl, FgmresDev* st, int S, SysShared& sh) {
   const SysLevel<P>& v0 = d.lev[0];
   const int m0 = v0.m;
@@ -485,10 +503,10 @@ __device__ void sys_inner_solve(const SysDesc<P>& d, P* xl, const P* zl, FgmresD
     const double scj = st->sc[j];
     if (v0.rank > 0) sys_multidot(m0, v0.rank, v0.W, ld, (const double*)nullptr, vj, scj, sh.red, sh.coef);
     sys_update<false>(m0, v0.rank, v0.WH, ld, (const double*)nullptr, sh.coef, 1.0, vj, scj, d.xlr, sh);
-    sys_solve_from<false>(d, 1, zj, (const P*)d.xlr, st, S, sh);
+    sys_solve_from<false, MAXT>(d, 1, zj, (const P*)d.xlr, st, S, sh);
     // w = S0 z (GemslrClass::SchurMatVec, gemslr.cpp:3799-3960)
     sys_spmv<P>(v0.F, (const P*)zj, P(1), (const P*)nullptr, P(0), d.s_zu, S);
-    sys_solve_b(d, 0, d.s_zu, d.s_wu, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);
+    sys_solve_b<MAXT>(d, 0, d.s_zu, d.s_wu, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);
     sys_spmv<P>(d.C0, (const P*)zj, P(1), (const P*)nullptr, P(0), wj, S);
     sys_spmv<P>(v0.E, (const P*)d.s_wu, P(-1), (const P*)wj, P(1), wj, S);
     sys_arnoldi(d.Vin, ld, j, st, m0, sh);
@@ -498,12 +516,12 @@ __device__ void sys_inner_solve(const SysDesc<P>& d, P* xl, const P* zl, FgmresD
 }
 
 // GemslrClass::Solve (gemslr.cpp:3431-3472): z = Q^T M^-1 P v with v scaled
-template <typename P>
+template <int MAXT, typename P>
 __device__ void sys_precond(const SysDesc<P>& d, const double* v, double vsc, P* z, FgmresDev* st_in, int S,
                             SysShared& sh) {
   for (int i = threadIdx.x; i < d.n; i += blockDim.x) d.rt[i] = (P)(v[d.pperm[i]] * vsc);
   __syncthreads();
-  sys_solve_from<true>(d, 0, d.xt, (const P*)d.rt, st_in, S, sh);
+  sys_solve_from<true, MAXT>(d, 0, d.xt, (const P*)d.rt, st_in, S, sh);
   const int* q = d.qperm ? d.qperm : d.pperm;
   for (int i = threadIdx.x; i < d.n; i += blockDim.x) z[q[i]] = d.xt[i];
   __syncthreads();
@@ -602,7 +620,7 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) systems_fgmres_kern
       for (int j = 0; j < a.kdim; j++) {
         if (*(volatile int*)&st->cycle_done) break;
         P* zj = d.Z + (long long)j * ld;
-        sys_precond(d, d.V + (long long)j * ld, st->sc[j], zj, st_in, S, sh);           // z = M^-1 v
+        sys_precond<MAXT>(d, d.V + (long long)j * ld, st->sc[j], zj, st_in, S, sh);           // z = M^-1 v
         sys_spmv<double>(d.A, (const P*)zj, 1.0, (const double*)nullptr, 0.0, d.V + (long long)(j + 1) * ld, S);
         sys_arnoldi(d.V, ld, j, st, n, sh);
       }
