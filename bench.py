@@ -723,7 +723,7 @@ def run_uneven(args):
 
     count = args.systems
     rng = np.random.default_rng(SEED + 4)
-    grid = np.exp(rng.uniform(np.log(32), np.log(512), size=count)).astype(int)
+    grid = np.exp(rng.uniform(np.log(32), np.log(args.uneven_nmax), size=count)).astype(int)
     beta = rng.uniform(0.0, 50.0, size=(count, 2))
     p = P.workload_params("convdiff")
     mats, B, hs = [], [], []
@@ -847,8 +847,9 @@ def run_uneven(args):
         "vs_baseline": None, "dtype": "f32 preconditioner / f64 FGMRES" if args.precision == "mixed" else "f64",
         "data": "synthetic",
         "config": {"workload": "%d upwind convection-diffusion systems -Lu + beta.grad u on n x n grids, n "
-                               "log-uniform in [32, 512], beta ~ U[0,50]^2, b ~ U[-1,1], 2 levels, ILUT 1e-2/20, "
-                               "rank 8, inner Schur FGMRES(5), FGMRES(30) to rel-res 1e-8 from x0 = 0" % count,
+                               "log-uniform in [32, %d], beta ~ U[0,50]^2, b ~ U[-1,1], 2 levels, ILUT 1e-2/20, "
+                               "rank 8, inner Schur FGMRES(5), FGMRES(30) to rel-res 1e-8 from x0 = 0"
+                               % (count, args.uneven_nmax),
                    "unknowns": int(sizes.sum()), "setup": "this library's host setup per system, untimed",
                    "schedule": {"threads": sb.schedule[0], "ctas_per_sm": sb.schedule[1], "spmv_lanes": sb.schedule[2],
                                 "prefetch_levels": sb.schedule[3]},
@@ -1008,6 +1009,8 @@ def main():
     ap.add_argument("--uneven-sample", type=int, default=32, help="uneven workload: systems solved by their own handle")
     ap.add_argument("--uneven-ref-sample", type=int, default=32,
                     help="uneven workload: systems the reference CPU solver solves")
+    ap.add_argument("--uneven-nmax", type=int, default=512,
+                    help="uneven workload: largest grid edge (512 is the workload; smaller for profiling)")
     ap.add_argument("--uneven-tune-stride", type=int, default=4,
                     help="uneven workload: the autotuner times every k-th system of the work list")
     ap.add_argument("--serve-matrices", type=int, default=64)
