@@ -163,6 +163,14 @@ int pgx_gemslr_set_perm(pgx_handle handle, const int32_t *pperm, const int32_t *
 int pgx_gemslr_set_levels(pgx_handle handle, int32_t nlev, const int32_t *lev_ptr);
 int pgx_gemslr_set_level(pgx_handle handle, int32_t level, const pgx_level *desc);
 int pgx_gemslr_set_inner(pgx_handle handle, int32_t enable, int32_t maxits, double tol);
+/* The solve option of GemslrClass (PARGEMSLR_IO_ADVANCED_GLOBAL_SOLVE,
+ * params[141]; GemslrSolveOptionEnum, gemslr.hpp:120-128), set before commit:
+ * 0 the additive LU solve (default), 1 the U solve, in which every level of
+ * the solve phase skips its block-L part and starts from z = rhs
+ * (GemslrClass::SolveLevel, gemslr.cpp:3527-3532).  The multiplicative
+ * solves (2, 3) are refused with PGX_ERROR_INVALID_OPTION.  pgx_gemslr_setup
+ * reads the option from its params. */
+int pgx_gemslr_set_solve_option(pgx_handle handle, int32_t option);
 int pgx_gemslr_commit(pgx_handle handle);
 int pgx_gemslr_destroy(pgx_handle handle);
 

@@ -238,6 +238,9 @@ class GemslrOracle:
         self.inner = int(d["inner.enable"][0]) != 0
         self.inner_maxits = int(d["inner.maxits"][0])
         self.inner_tol = float(d["inner.tol"][0])
+        # solve option 1, the U solve (gemslr.cpp:3527-3532): in the solve phase a
+        # level skips its block-L part and starts from z = rhs
+        self.usolve = "solve_option" in d and int(d["solve_option"][0]) == 1
         self.lv: List[dict] = []
         for l in range(self.nlev):
             pre = f"L{l}."
@@ -301,9 +304,12 @@ class GemslrOracle:
         rhsu, rhsl = rhs[:nl], rhs[nl:]
         xu, xl = x[:nl], x[nl:]
         zu, zl = lv["z"][:nl], lv["z"][nl:]
-        self.solve_b(zu, rhsu, level)
-        lv["E"].matvec(-1.0, zu, 0.0, zl)
-        axpy(1.0, rhsl, zl)
+        if self.usolve:
+            zl[:] = rhsl
+        else:
+            self.solve_b(zu, rhsu, level)
+            lv["E"].matvec(-1.0, zu, 0.0, zl)
+            axpy(1.0, rhsl, zl)
         if self.inner and level == 0:
             xl[:] = 0.0
             fgmres(self.schur_matvec, self.schur_solve, xl, zl, self.inner_maxits, self.inner_maxits, self.inner_tol)

@@ -53,7 +53,7 @@ EXPORTS = (
     "pgx_pool_collect", "pgx_pool_stats", "pgx_pool_destroy", "pgx_lowrank_block_apply_c64",
     "pgx_systems_create", "pgx_systems_solve", "pgx_systems_tune", "pgx_systems_tune_table",
     "pgx_systems_set_schedule", "pgx_systems_get_schedule", "pgx_systems_timing", "pgx_systems_device_bytes",
-    "pgx_systems_last_ms",
+    "pgx_systems_last_ms", "pgx_gemslr_set_solve_option",
     "pgx_systems_destroy",
 )
 
@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
     L.pgx_gemslr_set_levels.argtypes = [vp, i32, vp]
     L.pgx_gemslr_set_level.argtypes = [vp, i32, C.POINTER(Level)]
     L.pgx_gemslr_set_inner.argtypes = [vp, i32, i32, dbl]
+    L.pgx_gemslr_set_solve_option.argtypes = [vp, i32]
     L.pgx_gemslr_commit.argtypes = [vp]
     L.pgx_gemslr_destroy.argtypes = [vp]
     L.pgx_gemslr_device_bytes.argtypes = [vp, i32, C.POINTER(i64)]

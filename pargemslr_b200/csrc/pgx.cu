@@ -820,6 +820,9 @@ struct Import {
   std::vector<HostLevel> levels;
   int inner_enable = 0, inner_maxits = 5;
   double inner_tol = 1e-2;
+  // the solve option of GemslrClass (PARGEMSLR_IO_ADVANCED_GLOBAL_SOLVE,
+  // gemslr.hpp:120-128): 0 the additive LU solve, 1 the U solve
+  int solve_option = 0;
 };
 
 // The C block below level l, C_l (the operator of GemslrClass::SchurMatVec,
@@ -936,6 +939,10 @@ struct Engine : EngineBase {
   P *s_zu = nullptr, *s_wu = nullptr;
   // inner FGMRES on level 0
   int inner = 0, inner_maxits = 5;
+  // U solve (GemslrClass::SolveLevel, gemslr.cpp:3527-3532): in the solve
+  // phase a level skips its block-L part, z = rhs; the setup phase (the
+  // low-rank build) always runs the LU sequence
+  int usolve = 0;
   double inner_tol = 1e-2;
   P *Vin = nullptr, *Zin = nullptr;
   SD* st_in = nullptr;
@@ -1134,6 +1141,7 @@ struct Engine : EngineBase {
       }
     }
     inner = (im.inner_enable && nlev >= 2) ? 1 : 0;
+    usolve = im.solve_option == 1 ? 1 : 0;
     inner_maxits = im.inner_maxits;
     inner_tol = im.inner_tol;
     if (inner) PGX_TRY(assemble_c0(im));
@@ -1215,6 +1223,7 @@ struct Engine : EngineBase {
     lv = s.lv;  // factor pointers are shared, work pointers are replaced by alloc_work
     C0 = s.C0;
     inner = s.inner;
+    usolve = s.usolve;
     inner_maxits = s.inner_maxits;
     inner_tol = s.inner_tol;
     use_seg = s.use_seg;
@@ -1595,8 +1604,13 @@ struct Engine : EngineBase {
     P* zu = d.z;
     P* zl = d.z + d.nl;
     P* xl = x + d.nl;
-    solve_b(l, rhs, nullptr, zu, sk);                                              // 1. zu = B^-1 rhs_u
-    spmv<P, P, P, P>(d.E, zu, (P)-1, nullptr, nullptr, (P)0, rhs + d.nl, (P)1, zl, nullptr, sk);  // 2-3.
+    if (usolve) {                                                                  // U solve: zl = rhs_l
+      gather_kernel<P, P><<<grid_for(d.m, 256 * kPermUnroll, num_sms() * 16), 256, 0, stream>>>(
+          d.m, nullptr, rhs + d.nl, nullptr, zl, sk);
+    } else {
+      solve_b(l, rhs, nullptr, zu, sk);                                            // 1. zu = B^-1 rhs_u
+      spmv<P, P, P, P>(d.E, zu, (P)-1, nullptr, nullptr, (P)0, rhs + d.nl, (P)1, zl, nullptr, sk);  // 2-3.
+    }
     if (l == 0 && inner) {
       inner_solve(xl, zl, sk);                                                     // 4. inner FGMRES
     } else {
@@ -1776,7 +1790,11 @@ struct Engine : EngineBase {
   int build_lowrank_level(Import& im, int l, int k, int its, unsigned long long seed) override {
     std::vector<double> W, WH;
     int rank = 0;
-    PGX_TRY(build_lowrank(im, l, k, its, seed, W, WH, rank));
+    const int us = usolve;
+    usolve = 0;  // the setup phase runs the LU sequence
+    const int rc = build_lowrank(im, l, k, its, seed, W, WH, rank);
+    usolve = us;
+    PGX_TRY(rc);
     PGX_TRY(set_lowrank(l, W, WH, rank));
     im.levels[l].rank = rank;
     im.levels[l].W.swap(W);
@@ -2488,11 +2506,19 @@ struct BatchEngine : EngineBase {
       czu[r] = zu[r];
       czl[r] = zl[r];
     }
-    solve_b_b(l, rhs, zu, sk);
-    for (int r = 0; r < R; r++) {
-      DLevel<P>& d = lane[r]->lv[l];
-      lane[r]->template spmv<P, P, P, P>(d.E, zu[r], (P)-1, nullptr, nullptr, (P)0, rhs[r] + nl, (P)1, zl[r], nullptr,
-                                         sk[r]);
+    if (lane[0]->usolve) {  // U solve: zl = rhs_l
+      for (int r = 0; r < R; r++) {
+        const int m = lane[r]->lv[l].m;
+        gather_kernel<P, P><<<grid_for(m, 256 * kPermUnroll, num_sms() * 16), 256, 0, stream>>>(
+            m, nullptr, rhs[r] + nl, nullptr, zl[r], sk[r]);
+      }
+    } else {
+      solve_b_b(l, rhs, zu, sk);
+      for (int r = 0; r < R; r++) {
+        DLevel<P>& d = lane[r]->lv[l];
+        lane[r]->template spmv<P, P, P, P>(d.E, zu[r], (P)-1, nullptr, nullptr, (P)0, rhs[r] + nl, (P)1, zl[r],
+                                           nullptr, sk[r]);
+      }
     }
     if (l == 0 && lane[0]->inner) {
       inner_solve_b(xl, czl, sk);
@@ -3208,6 +3234,7 @@ struct Systems : SystemsBase {
         }
       }
       d.inner = (im.inner_enable && im.nlev >= 2) ? 1 : 0;
+      d.usolve = im.solve_option == 1 ? 1 : 0;
       d.inner_maxits = im.inner_maxits;
       d.inner_tol = im.inner_tol;
       if (d.inner) PGX_TRY(csr_p(d.C0, host_c_block(im, 0), d.lev[0].m, d.lev[0].m, "C0"));
@@ -3649,6 +3676,16 @@ int pgx_gemslr_set_inner(pgx_handle h, int32_t enable, int32_t maxits, double to
   return PGX_SUCCESS;
 }
 
+int pgx_gemslr_set_solve_option(pgx_handle h, int32_t option) {
+  if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
+  if (h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "solve option set after commit");
+  if (option != 0 && option != 1)
+    return fail(PGX_ERROR_INVALID_OPTION, "solve option %d: 0 (LU) or 1 (U); the multiplicative solves are not built",
+                option);
+  h->im.solve_option = option;
+  return PGX_SUCCESS;
+}
+
 int pgx_gemslr_commit(pgx_handle h) {
   if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
   Import& im = h->im;
@@ -3736,6 +3773,9 @@ int pgx_gemslr_setup(pgx_handle* handle, const pgx_csr* A, const double* params,
     const double rfac1 = params[78] > 0 ? params[78] : 1.0, rfac2 = params[79] > 0 ? params[79] : 1.0;
     const int lr_its = std::max(1, (int)params[90]);
     im.inner_enable = params[130] != 0.0;
+    im.solve_option = (int)params[141];
+    if (im.solve_option != 0 && im.solve_option != 1)
+      return fail(PGX_ERROR_INVALID_OPTION, "solve option %d: the multiplicative solves are not built", im.solve_option);
     im.inner_tol = params[131];
     im.inner_maxits = std::max(1, (int)params[132]);
     if (im.inner_maxits > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "inner maxits above %d", KMAX);

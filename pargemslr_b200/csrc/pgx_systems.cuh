@@ -87,6 +87,7 @@ struct SysDesc {
   SysCsr<P> C0;      // level-0 C block (inner Schur FGMRES)
   int inner, inner_maxits;
   double inner_tol;
+  int usolve;        // the U solve: a level's block-L part is skipped, z = rhs (gemslr.cpp:3527-3532)
   // work space
   double* V;   // n x (kdim + 1)
   P* Z;        // n x kdim
@@ -431,8 +432,13 @@ __device__ void sys_solve_from(const SysDesc<P>& d, int l0, P* x, const P* rhs, 
     xs[l] = xv;
     P* zu = v.z;
     P* zl = v.z + v.nl;
-    sys_solve_b<MAXT>(d, l, r, zu, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // 1. zu = B^-1 rhs_u
-    sys_spmv<P>(v.E, (const P*)zu, P(-1), r + v.nl, P(1), zl, S);     // 2-3. zl = rhs_l - E zu
+    if (d.usolve) {                                                   // U solve: zl = rhs_l
+      for (int i = threadIdx.x; i < v.m; i += blockDim.x) zl[i] = r[v.nl + i];
+      __syncthreads();
+    } else {
+      sys_solve_b<MAXT>(d, l, r, zu, (P*)sh.sbuf, sh.scap, sh.depth, &sh.tri_ns);  // 1. zu = B^-1 rhs_u
+      sys_spmv<P>(v.E, (const P*)zu, P(-1), r + v.nl, P(1), zl, S);   // 2-3. zl = rhs_l - E zu
+    }
     if (INNER && l == 0 && d.inner) {
       sys_inner_solve<MAXT>(d, xv + v.nl, zl, st_in, S, sh);                // 4. inner FGMRES
       stop_inner = true;

@@ -74,6 +74,8 @@ def import_structures(st: GemslrStructures, precision: str = "fp64") -> C.c_void
                 desc.WH = _abi.ptr(WH)
             _abi.check(L.pgx_gemslr_set_level(h, l, C.byref(desc)))
         _abi.check(L.pgx_gemslr_set_inner(h, st.inner_enable, st.inner_maxits, st.inner_tol))
+        if st.solve_option:
+            _abi.check(L.pgx_gemslr_set_solve_option(h, st.solve_option))
     except Exception:
         L.pgx_gemslr_destroy(h)
         raise

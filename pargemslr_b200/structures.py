@@ -76,6 +76,7 @@ class GemslrStructures:
     inner_enable: int = 1
     inner_maxits: int = 5
     inner_tol: float = 1e-2
+    solve_option: int = 0  # GemslrClass solve option: 0 LU, 1 U (gemslr.hpp:120-128)
 
     @property
     def nlev(self) -> int:
@@ -106,9 +107,11 @@ def from_dump(path: str) -> GemslrStructures:
     qperm = d["qperm"].astype(np.int32) if d["qperm"].size else None
     st = GemslrStructures(n=n, A=_csr(d, "A", z), pperm=d["pperm"].astype(np.int32), qperm=qperm, lev_ptr=lev_ptr,
                           inner_enable=int(d["inner.enable"][0]), inner_maxits=int(d["inner.maxits"][0]),
-                          inner_tol=float(d["inner.tol"][0]))
-    if int(d["solve_option"][0]) != 0:
-        raise ValueError("only the LU global solve option (the reference default) is supported")
+                          inner_tol=float(d["inner.tol"][0]),
+                          solve_option=int(d["solve_option"][0]) if "solve_option" in d else 0)
+    if st.solve_option not in (0, 1):
+        raise ValueError("solve option %d: the LU (0) and U (1) solves are built, the multiplicative ones are not"
+                         % st.solve_option)
     for l in range(nlev):
         pre = f"L{l}."
         ncomp = int(d[pre + "ncomp"][0])

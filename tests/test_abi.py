@@ -43,6 +43,7 @@ def test_calls_without_device_fail_cleanly():
     assert L.pgx_systems_solve(None, None, None, 0, None, None) == _abi.ERROR_INVALID_PARAM
     assert L.pgx_systems_set_schedule(None, 512, 2, 4, 2) == _abi.ERROR_INVALID_PARAM
     assert L.pgx_systems_destroy(None) == 0
+    assert L.pgx_gemslr_set_solve_option(None, 1) == _abi.ERROR_INVALID_PARAM
 
 
 def test_level_schedule_rejects_non_triangular_factor():

@@ -165,3 +165,29 @@ def test_residual_history_is_a_running_product_of_givens_sines(case):
         hist.append(prod / r["normb"])
     np.testing.assert_array_equal(np.array(hist), np.array(r["hist"]))
     assert same(np.array(hist), sol["rel_res_hist"], case, rtol=1e-12)
+
+
+@pytest.mark.parametrize("lap,workload", [((64, 64, 1, 0.0, 0.0, 0.0, 0.0), "lap2d_256"),
+                                          ((32, 32, 32, 0.0, 0.0, 0.0, 0.0), "lap3d_128")])
+def test_oracle_usolve_matches_reference(lap, workload):
+    """The U solve option (params[141] = 1, gemslr.cpp:3527-3532) against the reference run with it: the
+    preconditioner applications bit for bit up to 1e-13 and the FGMRES solve with the same iteration count."""
+    from tests import oracle_runs
+    if not oracle_runs.available():
+        pytest.skip("reference solver not built here")
+    p = P.workload_params(workload)
+    p[P.ADVANCED_GLOBAL_SOLVE] = 1
+    n = lap[0] * lap[1] * lap[2]
+    ref = oracle_runs.run(lap=lap, params=p, xtrue=oracle_runs.x_true(n, seed=7), apply_k=2)
+    g = O.GemslrOracle(pgxd.read(ref["setup"]))
+    assert g.usolve
+    ap = ref["apply"]
+    for k in range(int(ap["k"][0])):
+        z = g.solve(ap["in"][k * n:(k + 1) * n])
+        z_ref = ap["out"][k * n:(k + 1) * n]
+        assert np.linalg.norm(z - z_ref) <= 1e-13 * np.linalg.norm(z_ref)
+    b = pgxd.read(ref["problem"])["b"]
+    x, r = g.fgmres_solve(b, int(p[P.SOLVER_KDIM]), int(p[P.SOLVER_MAXITS]), float(p[P.SOLVER_TOL]))
+    assert r["iters"] == int(ref["iters"])
+    x_ref = ref["solution"]["x"]
+    assert np.linalg.norm(x - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
