@@ -17,7 +17,8 @@
 //   SolveApplyLowRankLevel, gemslr.cpp:3681-3722 (x += WH (W^T x));
 //   the level-0 inner FlexGmres over GemslrSchurMatrixClass,
 //     gemslr.cpp:294-330 and 1660-1674, with SchurMatVec, gemslr.cpp:3799-3960;
-//   CGS2 orthogonalisation (PargemslrCgs2, matrixops.cpp:10588-10708).
+//   CGS2 orthogonalisation (PargemslrCgs2, matrixops.cpp:10588-10708);
+//   the U solve option (gemslr.cpp:3527-3532: a level skips its block-L part).
 // Krylov vectors, Givens rotations and the true residual are FP64; the
 // preconditioner (factors, coupling blocks, low-rank bases and its vectors)
 // is stored and accumulated in P (float for the mixed precision, double for
