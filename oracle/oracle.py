@@ -241,6 +241,10 @@ class GemslrOracle:
         # solve option 1, the U solve (gemslr.cpp:3527-3532): in the solve phase a
         # level skips its block-L part and starts from z = rhs
         self.usolve = "solve_option" in d and int(d["solve_option"][0]) == 1
+        # solve option 2, the multiplicative solve of ParallelGemslrClass
+        # (SolveLevelGemslrMul, parallel_gemslr.cpp:5816-6050), with the inner
+        # iteration on the RAP operator (RAPMatVec, parallel_gemslr.cpp:7194)
+        self.mul = "solve_option" in d and int(d["solve_option"][0]) == 2
         self.lv: List[dict] = []
         for l in range(self.nlev):
             pre = f"L{l}."
@@ -276,7 +280,10 @@ class GemslrOracle:
         """z = M^-1 rhs (GemslrClass::Solve)."""
         rhs_t = np.ascontiguousarray(rhs[self.pperm])       # GatherPerm
         x_t = np.zeros(self.n)
-        self.solve_level(x_t, rhs_t, 0)
+        if self.mul:
+            self.solve_level_mul(x_t, rhs_t, 0)
+        else:
+            self.solve_level(x_t, rhs_t, 0)
         out = np.empty(self.n)
         out[self.qperm if self.qperm is not None else self.pperm] = x_t  # ScatterRperm
         return out
@@ -321,6 +328,96 @@ class GemslrOracle:
         lv["F"].matvec(-1.0, xl, 0.0, zu)
         axpy(1.0, rhsu, zu)
         self.solve_b(xu, zu, level)
+
+    def b_matvec(self, level: int, alpha: float, x: np.ndarray, beta: float, y: np.ndarray) -> None:
+        """y = alpha B_l x + beta y over the level's subdomain blocks (BMatVec)."""
+        lv = self.lv[level]
+        start = int(self.lev_ptr[level])
+        for c in range(lv["ncomp"]):
+            a, b = int(lv["dom"][c]) - start, int(lv["dom"][c + 1]) - start
+            yc = np.ascontiguousarray(y[a:b])
+            lv["B"][c].matvec(alpha, np.ascontiguousarray(x[a:b]), beta, yc)
+            y[a:b] = yc
+
+    def solve_level_mul(self, x: np.ndarray, rhs: np.ndarray, level: int) -> None:
+        """ParallelGemslrClass::SolveLevelGemslrMul (parallel_gemslr.cpp:5816-6050): the smoothing
+        x_u = B^-1 b_u, the residual r = b - A [x_u; 0], its restriction r_l - E B^-1 r_u, the Schur solve
+        (inner FGMRES on RAP at level 0, else low rank and the next level) and x = x + [-B^-1 F; I] x_l."""
+        if level == self.nlev - 1:
+            self.solve_b(x, rhs, level)
+            return
+        lv = self.lv[level]
+        nl = int(self.lev_ptr[level + 1] - self.lev_ptr[level])
+        rhsu, rhsl = rhs[:nl], rhs[nl:]
+        xu, xl = x[:nl], x[nl:]
+        y = np.zeros(x.size)
+        z = np.zeros(x.size)
+        yu, zu, zl = y[:nl], z[:nl], z[nl:]
+        self.solve_b(xu, rhsu, level)                      # 1. x_u = B^-1 b_u
+        zu[:] = rhsu                                       # 2. z = b - A [x_u; 0]
+        self.b_matvec(level, -1.0, xu, 1.0, zu)
+        zl[:] = rhsl
+        lv["E"].matvec(-1.0, xu, 1.0, zl)
+        self.solve_b(yu, zu, level)                        # 3. z_l -= E B^-1 z_u
+        lv["E"].matvec(-1.0, yu, 1.0, zl)
+        if self.inner and level == 0:                      # 4. Schur solve
+            xl[:] = 0.0
+            fgmres(self.rap_matvec, self.schur_solve, xl, zl, self.inner_maxits, self.inner_maxits, self.inner_tol)
+        else:
+            if lv["lrc"] > 0:
+                self.lowrank(lv["xlr"], zl, level)
+                axpy(1.0, lv["xlr"], zl)
+            self.solve_level_mul(xl, zl, level + 1)
+        lv["F"].matvec(-1.0, xl, 0.0, yu)                  # 5. x_u += -B^-1 F x_l
+        self.solve_b(zu, yu, level)
+        axpy(1.0, zu, xu)
+
+    def rap_matvec(self, alpha: float, x: np.ndarray, beta: float, y: np.ndarray) -> None:
+        """y = alpha R A P x + beta y at level 0 (RAPMatVec, parallel_gemslr.cpp:7194): P x = [-B^-1 F x; x],
+        A P x through B, F, E and C, R = [-E B^-1, I]."""
+        level = 0
+        lv = self.lv[level]
+        nl = int(self.lev_ptr[level + 1] - self.lev_ptr[level])
+        vu = np.zeros(nl)
+        wu = np.zeros(nl)
+        vl = np.array(x, copy=True)
+        lv["F"].matvec(-1.0, x, 0.0, wu)
+        self.solve_b(vu, wu, level)
+        self.b_matvec(level, 1.0, vu, 0.0, wu)
+        lv["F"].matvec(1.0, vl, 1.0, wu)
+        wl = np.zeros(x.size)
+        lv["E"].matvec(1.0, vu, 0.0, wl)
+        wl += self.c_matvec(vl)
+        self.solve_b(vu, wu, level)
+        lv["E"].matvec(-alpha, vu, beta, y)
+        axpy(alpha, wl, y)
+
+    def c_matvec(self, x: np.ndarray) -> np.ndarray:
+        """C_0 x: the blocks of the levels below level 0 (CMatVec)."""
+        level = 0
+        n_start = int(self.lev_ptr[level])
+        nl = int(self.lev_ptr[level + 1] - self.lev_ptr[level])
+        w = np.zeros(self.n - n_start)
+        for j in range(level + 1, self.nlev):
+            lj = self.lv[j]
+            sj = int(self.lev_ptr[j])
+            ej = int(self.lev_ptr[j + 1])
+            for c in range(lj["ncomp"]):
+                a, b = int(lj["dom"][c]), int(lj["dom"][c + 1])
+                xi = x[a - n_start - nl:b - n_start - nl]
+                zi = np.ascontiguousarray(w[a - n_start:b - n_start])
+                lj["B"][c].matvec(1.0, np.ascontiguousarray(xi), 1.0, zi)
+                w[a - n_start:b - n_start] = zi
+            if j == self.nlev - 1:
+                break
+            nli = ej - sj
+            ziu = np.ascontiguousarray(w[sj - n_start:sj - n_start + nli])
+            lj["F"].matvec(1.0, np.ascontiguousarray(x[ej - n_start - nl:]), 1.0, ziu)
+            w[sj - n_start:sj - n_start + nli] = ziu
+            zil = np.ascontiguousarray(w[ej - n_start:])
+            lj["E"].matvec(1.0, np.ascontiguousarray(x[sj - n_start - nl:sj - n_start - nl + nli]), 1.0, zil)
+            w[ej - n_start:] = zil
+        return w[nl:]
 
     def schur_solve(self, x: np.ndarray, rhs: np.ndarray) -> None:
         lv = self.lv[0]

@@ -73,3 +73,31 @@ def test_parallel_dump_refusals():
     bad["global_precond"] = np.array([1], np.int32)
     with pytest.raises(ValueError, match="global preconditioners"):
         parallel_to_sequential_dump(bad)
+
+
+@pytest.mark.parametrize("lap,workload", [((16, 16, 16, 0.0, 0.0, 0.0, 0.0), "lap3d_128"),
+                                          ((48, 48, 1, 0.0, 0.3, -0.2, 0.0), "lap2d_256")])
+@pytest.mark.parametrize("option,schur", [(1, 1), (2, 0), (2, 1)])
+def test_solve_options_match_reference(lap, workload, option, schur):
+    """The U solve (option 1, parallel_gemslr.cpp:5682) and the multiplicative solve (option 2,
+    SolveLevelGemslrMul, :5816-6050; with the inner iteration on the RAP operator, RAPMatVec, :7194) of the
+    reference's ParallelGemslrClass, restated by the oracle on the composed structures: the preconditioner
+    applications to 1e-15 and the FGMRES solve with the same iteration count."""
+    if not oracle_runs.available_parallel():
+        pytest.skip("oracle/_ref/pgx_ref_driver_par is not built here")
+    p = P.workload_params(workload)
+    p[P.PRECOND_GLOBAL_PRECOND] = 2
+    p[P.ADVANCED_GLOBAL_SOLVE] = option
+    p[P.SCHUR_ENABLE] = schur
+    n = lap[0] * lap[1] * lap[2]
+    ref = oracle_runs.run_parallel(lap, p, oracle_runs.x_true(n, 7), apply_k=2)
+    seq = parallel_to_sequential_dump(pgxd.read(ref["setup_par"]))
+    g = O.GemslrOracle(seq)
+    assert g.usolve == (option == 1) and g.mul == (option == 2)
+    for k in range(2):
+        z = g.solve(ref["apply_in"][k])
+        assert np.linalg.norm(z - ref["apply_out"][k]) <= 1e-15 * np.linalg.norm(ref["apply_out"][k]) * 10
+    x, r = g.fgmres_solve(ref["problem"]["b"], int(p[P.SOLVER_KDIM]), int(p[P.SOLVER_MAXITS]),
+                          float(p[P.SOLVER_TOL]))
+    assert r["iters"] == int(ref["iters"])
+    assert np.linalg.norm(x - ref["x"]) <= 1e-13 * np.linalg.norm(ref["x"])
