@@ -163,13 +163,19 @@ int pgx_gemslr_set_perm(pgx_handle handle, const int32_t *pperm, const int32_t *
 int pgx_gemslr_set_levels(pgx_handle handle, int32_t nlev, const int32_t *lev_ptr);
 int pgx_gemslr_set_level(pgx_handle handle, int32_t level, const pgx_level *desc);
 int pgx_gemslr_set_inner(pgx_handle handle, int32_t enable, int32_t maxits, double tol);
-/* The solve option of GemslrClass (PARGEMSLR_IO_ADVANCED_GLOBAL_SOLVE,
- * params[141]; GemslrSolveOptionEnum, gemslr.hpp:120-128), set before commit:
- * 0 the additive LU solve (default), 1 the U solve, in which every level of
- * the solve phase skips its block-L part and starts from z = rhs
- * (GemslrClass::SolveLevel, gemslr.cpp:3527-3532).  The multiplicative
- * solves (2, 3) are refused with PGX_ERROR_INVALID_OPTION.  pgx_gemslr_setup
- * reads the option from its params. */
+/* The solve option (PARGEMSLR_IO_ADVANCED_GLOBAL_SOLVE, params[141];
+ * GemslrSolveOptionEnum, gemslr.hpp:120-128), set before commit:
+ *   0 the additive LU solve (default);
+ *   1 the U solve: every level of the solve phase skips its block-L part and
+ *     starts from z = rhs (GemslrClass::SolveLevel, gemslr.cpp:3527-3532);
+ *   2 the multiplicative solve of ParallelGemslrClass (SolveLevelGemslrMul,
+ *     parallel_gemslr.cpp:5816-6050) with the level-0 inner FGMRES on the RAP
+ *     operator (RAPMatVec, :7194); it needs every level's B blocks
+ *     (pgx_level.B), the reference's setup run with the same option, and runs
+ *     one right-hand side per slot (no multi-lane slots, no systems solve).
+ * GemslrClass itself solves options 2 and 3 as 0; option 3 (the modified-ILU
+ * multiplicative solve) is refused with PGX_ERROR_INVALID_OPTION.
+ * pgx_gemslr_setup reads options 0 and 1 from its params. */
 int pgx_gemslr_set_solve_option(pgx_handle handle, int32_t option);
 int pgx_gemslr_commit(pgx_handle handle);
 int pgx_gemslr_destroy(pgx_handle handle);

@@ -765,6 +765,8 @@ struct DLevel {
   P* y = nullptr;  // lower-pass result, holds the sentinel between solves
   P* yslot = nullptr;  // lower-pass result in the upper pass's slot order (per-subdomain kernels)
   DCsr<P> E, F;
+  DCsr<P> B;            // the level's unfactored blocks (multiplicative solve only)
+  P* wmul = nullptr;    // nl: work vector of the multiplicative solve
   P *W = nullptr, *WH = nullptr;
   P *z = nullptr, *xlr = nullptr;
   TsAcc<P>* lrt = nullptr;  // low-rank coefficients W^H x
@@ -943,6 +945,11 @@ struct Engine : EngineBase {
   // phase a level skips its block-L part, z = rhs; the setup phase (the
   // low-rank build) always runs the LU sequence
   int usolve = 0;
+  // multiplicative solve of ParallelGemslrClass (SolveLevelGemslrMul,
+  // parallel_gemslr.cpp:5816-6050), its inner iteration on the RAP operator
+  // (RAPMatVec, :7194); the inner preconditioner stays the additive level
+  // solve (ParallelGemslrSchurMatrixClass::Solve, :370-410)
+  int mul = 0;
   double inner_tol = 1e-2;
   P *Vin = nullptr, *Zin = nullptr;
   SD* st_in = nullptr;
@@ -1132,6 +1139,11 @@ struct Engine : EngineBase {
       if (l < nlev - 1) {
         PGX_TRY(upload_csr(ar, h.E, d.E, stream));
         PGX_TRY(upload_csr(ar, h.F, d.F, stream));
+        if (im.solve_option == 2) {
+          if (h.B.rows != d.nl)
+            return fail(PGX_ERROR_INVALID_PARAM, "the multiplicative solve needs the B blocks of level %d", l);
+          PGX_TRY(upload_csr(ar, h.B, d.B, stream));
+        }
         d.rank = h.rank;
         if (d.rank > 0) {
           const std::vector<P> w = hvals<P>(h.W, (size_t)d.m * d.rank), wh = hvals<P>(h.WH, (size_t)d.m * d.rank);
@@ -1142,6 +1154,7 @@ struct Engine : EngineBase {
     }
     inner = (im.inner_enable && nlev >= 2) ? 1 : 0;
     usolve = im.solve_option == 1 ? 1 : 0;
+    mul = im.solve_option == 2 ? 1 : 0;
     inner_maxits = im.inner_maxits;
     inner_tol = im.inner_tol;
     if (inner) PGX_TRY(assemble_c0(im));
@@ -1166,6 +1179,7 @@ struct Engine : EngineBase {
         PGX_TRY(wk.zeros(&d.lrt, (size_t)KMAX + 1, stream));
       }
       PGX_TRY(wk.zeros(&d.z, (size_t)(n - d.start), stream));
+      if (mul && l < nlev - 1) PGX_TRY(wk.zeros(&d.wmul, (size_t)d.nl, stream));
     }
     if (inner) {
       const int m0 = lv[0].m;
@@ -1224,6 +1238,7 @@ struct Engine : EngineBase {
     C0 = s.C0;
     inner = s.inner;
     usolve = s.usolve;
+    mul = s.mul;
     inner_maxits = s.inner_maxits;
     inner_tol = s.inner_tol;
     use_seg = s.use_seg;
@@ -1621,6 +1636,36 @@ struct Engine : EngineBase {
     solve_b(l, zu, nullptr, x, sk);                                                // 7. xu = B^-1 zu
   }
 
+  // ParallelGemslrClass::SolveLevelGemslrMul (parallel_gemslr.cpp:5816-6050):
+  // the smoothing x_u = B^-1 b_u, the residual z = b - A [x_u; 0], its
+  // restriction z_l - E B^-1 z_u, the Schur solve (the inner FGMRES on RAP at
+  // level 0, else the low rank and the next level) and x_u += -B^-1 F x_l.
+  void solve_level_mul(int l, P* x, const P* rhs, Skip sk) {
+    DLevel<P>& d = lv[l];
+    if (l == nlev - 1) {
+      solve_b(l, rhs, nullptr, x, sk);
+      return;
+    }
+    P* xu = x;
+    P* xl = x + d.nl;
+    P* zu = d.z;
+    P* zl = d.z + d.nl;
+    P* yu = d.wmul;
+    solve_b(l, rhs, nullptr, xu, sk);                                                        // 1.
+    spmv<P, P, P, P>(d.B, xu, (P)-1, nullptr, nullptr, (P)0, rhs, (P)1, zu, nullptr, sk);      // 2. z_u
+    solve_b(l, zu, nullptr, yu, sk);                                                          // 3.
+    spmv<P, P, P, P>(d.E, xu, (P)-1, &d.E, yu, (P)-1, rhs + d.nl, (P)1, zl, nullptr, sk);    // 2-3. z_l
+    if (l == 0 && inner) {
+      inner_solve(xl, zl, sk);                                                                // 4.
+    } else {
+      if (d.rank > 0) lowrank_inplace(l, zl, sk);
+      solve_level_mul(l + 1, xl, zl, sk);
+    }
+    spmv<P, P, P, P>(d.F, xl, (P)-1, nullptr, nullptr, (P)0, (const P*)nullptr, (P)0, yu, nullptr, sk);  // 5.
+    solve_b(l, yu, nullptr, zu, sk);
+    axpy_kernel<P><<<grid_for(d.nl, 256, num_sms() * 16), 256, 0, stream>>>(d.nl, zu, xu, sk);
+  }
+
   // Level-0 inner flexible GMRES on the Schur complement S0 = C0 - E0 B0^-1 F0,
   // from x0 = 0, one cycle of inner_maxits steps (gemslr.cpp:1660-1674, 3566-3572).
   void inner_solve(P* xl, const P* zl, Skip outer) {
@@ -1665,10 +1710,21 @@ struct Engine : EngineBase {
         ts<P, P, P, TS_UPDATE>(u);
       }
       solve_level(1, zj, d0.xlr, it);
-      // w = S0 z  (GemslrClass::SchurMatVec, gemslr.cpp:3799-3960)
-      spmv<P, P, P, P>(d0.F, zj, (P)1, nullptr, nullptr, (P)0, (const P*)nullptr, (P)0, s_zu, nullptr, it);
-      solve_b(0, s_zu, nullptr, s_wu, it);
-      spmv<P, P, P, P>(C0, zj, (P)1, &d0.E, s_wu, (P)-1, (const P*)nullptr, (P)0, wj, nullptr, it);
+      if (mul) {
+        // w = R A P z (RAPMatVec, parallel_gemslr.cpp:7194): P z = [-B^-1 F z; z],
+        // A P z through B, F, E and C0, R = [-E B^-1, I]; xlr holds the lower part
+        spmv<P, P, P, P>(d0.F, zj, (P)-1, nullptr, nullptr, (P)0, (const P*)nullptr, (P)0, s_zu, nullptr, it);
+        solve_b(0, s_zu, nullptr, s_wu, it);
+        spmv<P, P, P, P>(d0.B, s_wu, (P)1, &d0.F, zj, (P)1, (const P*)nullptr, (P)0, s_zu, nullptr, it);
+        spmv<P, P, P, P>(d0.E, s_wu, (P)1, &C0, zj, (P)1, (const P*)nullptr, (P)0, d0.xlr, nullptr, it);
+        solve_b(0, s_zu, nullptr, s_wu, it);
+        spmv<P, P, P, P>(d0.E, s_wu, (P)-1, nullptr, nullptr, (P)0, (const P*)d0.xlr, (P)1, wj, nullptr, it);
+      } else {
+        // w = S0 z  (GemslrClass::SchurMatVec, gemslr.cpp:3799-3960)
+        spmv<P, P, P, P>(d0.F, zj, (P)1, nullptr, nullptr, (P)0, (const P*)nullptr, (P)0, s_zu, nullptr, it);
+        solve_b(0, s_zu, nullptr, s_wu, it);
+        spmv<P, P, P, P>(C0, zj, (P)1, &d0.E, s_wu, (P)-1, (const P*)nullptr, (P)0, wj, nullptr, it);
+      }
       arnoldi_step<P, P>(Vin, ld, j, st_in, m0, it);
     }
     {
@@ -1720,7 +1776,10 @@ struct Engine : EngineBase {
   void precond(const F* v, const double* v_scale, TO* z, Skip sk) {
     const int grid = grid_for(n, 256 * kPermUnroll, num_sms() * 16);  // gather / scatter
     gather_kernel<F, P><<<grid, 256, 0, stream>>>(n, pperm, v, v_scale, rt, sk);
-    solve_level(0, xt, rt, sk);
+    if (mul)
+      solve_level_mul(0, xt, rt, sk);
+    else
+      solve_level(0, xt, rt, sk);
     scatter_kernel<P, TO><<<grid, 256, 0, stream>>>(n, qperm ? qperm : pperm, xt, z, sk);
   }
 
@@ -1790,10 +1849,12 @@ struct Engine : EngineBase {
   int build_lowrank_level(Import& im, int l, int k, int its, unsigned long long seed) override {
     std::vector<double> W, WH;
     int rank = 0;
-    const int us = usolve;
+    const int us = usolve, mu = mul;
     usolve = 0;  // the setup phase runs the LU sequence
+    mul = 0;
     const int rc = build_lowrank(im, l, k, its, seed, W, WH, rank);
     usolve = us;
+    mul = mu;
     PGX_TRY(rc);
     PGX_TRY(set_lowrank(l, W, WH, rank));
     im.levels[l].rank = rank;
@@ -2891,6 +2952,8 @@ int64_t Engine<P>::layout_bytes() const {
 
 template <typename P>
 int make_batch_slot(Engine<P>& own, Import& im, int lanes, std::unique_ptr<EngineBase>& out) {
+  if (im.solve_option == 2)
+    return fail(PGX_ERROR_INVALID_OPTION, "the multiplicative solve runs one right-hand side per slot");
   switch (lanes) {
     case 2: return make_batch_slot_r<P, 2>(own, im, out);
     case 4: return make_batch_slot_r<P, 4>(own, im, out);
@@ -3183,6 +3246,8 @@ struct Systems : SystemsBase {
     for (int s = 0; s < count; s++) {
       const Import& im = *ims[s];
       if (im.vw != 1) return fail(PGX_ERROR_INVALID_OPTION, "system %d: the systems solve is real only", s);
+      if (im.solve_option == 2)
+        return fail(PGX_ERROR_INVALID_OPTION, "system %d: the systems solve runs the LU and U solves only", s);
       if (im.nlev < 1 || im.nlev > kSysMaxLevels)
         return fail(PGX_ERROR_INVALID_PARAM, "system %d: %d levels (1..%d)", s, im.nlev, kSysMaxLevels);
       if (im.inner_enable && im.nlev >= 2 && im.inner_maxits > KMAX)
@@ -3679,9 +3744,8 @@ int pgx_gemslr_set_inner(pgx_handle h, int32_t enable, int32_t maxits, double to
 int pgx_gemslr_set_solve_option(pgx_handle h, int32_t option) {
   if (!h) return fail(PGX_ERROR_INVALID_PARAM, "null handle");
   if (h->eng) return fail(PGX_ERROR_FUNCTION_CALL, "solve option set after commit");
-  if (option != 0 && option != 1)
-    return fail(PGX_ERROR_INVALID_OPTION, "solve option %d: 0 (LU) or 1 (U); the multiplicative solves are not built",
-                option);
+  if (option < 0 || option > 2)
+    return fail(PGX_ERROR_INVALID_OPTION, "solve option %d: 0 (LU), 1 (U) or 2 (multiplicative)", option);
   h->im.solve_option = option;
   return PGX_SUCCESS;
 }
@@ -3775,7 +3839,9 @@ int pgx_gemslr_setup(pgx_handle* handle, const pgx_csr* A, const double* params,
     im.inner_enable = params[130] != 0.0;
     im.solve_option = (int)params[141];
     if (im.solve_option != 0 && im.solve_option != 1)
-      return fail(PGX_ERROR_INVALID_OPTION, "solve option %d: the multiplicative solves are not built", im.solve_option);
+      return fail(PGX_ERROR_INVALID_OPTION,
+                  "solve option %d: this library's setup builds the LU and U solves only (the multiplicative solve "
+                  "needs the reference's setup)", im.solve_option);
     im.inner_tol = params[131];
     im.inner_maxits = std::max(1, (int)params[132]);
     if (im.inner_maxits > KMAX) return fail(PGX_ERROR_INVALID_PARAM, "inner maxits above %d", KMAX);

@@ -1481,6 +1481,13 @@ __global__ void __launch_bounds__(256) gather_kernel(int n, const int* __restric
   }
 }
 
+// y += x  (the solution update of the multiplicative level solve)
+template <typename T>
+__global__ void __launch_bounds__(256) axpy_kernel(int n, const T* __restrict__ x, T* __restrict__ y, Skip skip) {
+  if (skip.on()) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += x[i];
+}
+
 // out[perm[i]] = in[i]  (IntVectorClass::ScatterRperm, int_vector.cpp:629)
 template <typename TI, typename TO>
 __global__ void __launch_bounds__(256) scatter_kernel(int n, const int* __restrict__ perm, const TI* __restrict__ in,

@@ -109,8 +109,11 @@ def from_dump(path: str) -> GemslrStructures:
                           inner_enable=int(d["inner.enable"][0]), inner_maxits=int(d["inner.maxits"][0]),
                           inner_tol=float(d["inner.tol"][0]),
                           solve_option=int(d["solve_option"][0]) if "solve_option" in d else 0)
-    if st.solve_option not in (0, 1):
-        raise ValueError("solve option %d: the LU (0) and U (1) solves are built, the multiplicative ones are not"
+    if "solve_class" not in d and st.solve_option in (2, 3):
+        # GemslrClass checks only the U option (gemslr.cpp:3527): it solves 2 and 3 with the LU sequence
+        st.solve_option = 0
+    if st.solve_option not in (0, 1, 2):
+        raise ValueError("solve option %d: the LU (0), U (1) and multiplicative (2) solves are built"
                          % st.solve_option)
     for l in range(nlev):
         pre = f"L{l}."
@@ -187,6 +190,7 @@ def parallel_to_sequential_dump(d: Dict[str, np.ndarray]) -> Dict[str, np.ndarra
         out[k] = d[k]
     for k in ("A.i", "A.j", "A.a", "A.shape"):
         out[k] = d[k]
+    out["solve_class"] = np.array([1], np.int32)  # ParallelGemslrClass: option 2 is its multiplicative solve
     out["pperm"] = composed(0, 0).astype(np.int32)
     out["qperm"] = np.zeros(0, np.int32)
     for l in range(nlev):
