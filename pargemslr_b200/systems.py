@@ -19,6 +19,24 @@ from . import _abi
 from .handle import GemslrHandle, _result
 
 
+def shard_systems(costs: Sequence[float], world: int) -> List[List[int]]:
+    """Split systems over `world` GPUs so that their estimated costs balance: largest first, each to the GPU whose
+    total is smallest so far (ties to the lower rank).  The split depends only on the costs, so every rank computes
+    the same one and no exchange is needed; independent systems never talk to each other."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda k: (-float(costs[k]), k))
+    load = [0.0] * world
+    out: List[List[int]] = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda j: (load[j], j))
+        out[r].append(k)
+        load[r] += float(costs[k])
+    for part in out:
+        part.sort()
+    return out
+
+
 class SystemsBatch:
     def __init__(self, handles: Sequence[GemslrHandle]):
         if not handles:
