@@ -101,3 +101,27 @@ def test_solve_options_match_reference(lap, workload, option, schur):
                           float(p[P.SOLVER_TOL]))
     assert r["iters"] == int(ref["iters"])
     assert np.linalg.norm(x - ref["x"]) <= 1e-13 * np.linalg.norm(ref["x"])
+
+
+def test_solve_option_mapping_at_import(tmp_path):
+    """GemslrClass checks only the U option (gemslr.cpp:3527), so a sequential setup run with option 2 or 3 solves
+    with the LU sequence and imports as option 0; ParallelGemslrClass's option 2 is its multiplicative solve and
+    imports as 2; the modified-ILU multiplicative option 3 is refused."""
+    from pargemslr_b200.structures import from_dump
+    if not (oracle_runs.available() and oracle_runs.available_parallel()):
+        pytest.skip("reference solvers not built here")
+    lap = (16, 16, 16, 0.0, 0.0, 0.0, 0.0)
+    p = P.workload_params("lap3d_128")
+    p[P.ADVANCED_GLOBAL_SOLVE] = 2
+    seq = oracle_runs.run(lap=lap, params=p, xtrue=oracle_runs.x_true(16 ** 3, 7), solve=False)
+    assert int(pgxd.read(seq["setup"])["solve_option"][0]) == 2
+    assert from_dump(seq["setup"]).solve_option == 0
+    p[P.PRECOND_GLOBAL_PRECOND] = 2
+    par = oracle_runs.run_parallel(lap, p, oracle_runs.x_true(16 ** 3, 7))
+    assert from_parallel_dump(par["setup_par"]).solve_option == 2
+    d = pgxd.read(par["setup_par"])
+    d["solve_option"] = np.array([3], np.int32)
+    f = str(tmp_path / "opt3.bin")
+    pgxd.write(f, d)
+    with pytest.raises(ValueError, match="solve option 3"):
+        from_parallel_dump(f)
